@@ -1,0 +1,376 @@
+"""Benchmark of the point -> sparse-volume step on B200.
+
+Workload (the dynamic SPH-like configuration): 4,194,304 points on a jittered
+lattice filling a 256x128x256-voxel block, velocity ~ N(0,1), Configure
+(3,3,3,3,3) (8^3 bricks, apron 1), channels density + 3 x velocity.  One step:
+advect p += 0.1 v -> RebuildTopology(N, 2.0) -> UpdateAtlas -> cubic B-spline
+scatter (r = 2) of mass and momentum -> UpdateApron -> cubic gather of the 3
+velocity channels back to the points.
+
+`python bench.py [--gpus N --steps K --warmup W]` prints one JSON line.
+`--impl reference` times the CPU restatement of the reference's path on the
+host cores instead (the reference's host library does not build here).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gvdb-voxels_b200"))
+
+METRIC = "points/s rebuild+scatter+gather at <=1e-5 err, % HBM peak; adjoint & batched vs plain"
+WORKLOAD = "dynamic SPH-like step: 4,194,304-pt jittered lattice, cubic B-spline r=2, density+3 vel channels"
+N_POINTS = 4_194_304
+SITES = (256, 64, 256)
+DT = 0.1
+RADIUS = 2.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--incremental", action="store_true", help="reference state machine instead of full rebuilds")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+class Pipeline:
+    """The benchmark step over libgvdb2 (through the VolumeGVDB mirror)."""
+
+    def __init__(self, device, pos_host, vel_host, full_rebuild=True):
+        import torch
+        import gvdb2
+        self.torch = torch
+        self.gvdb2 = gvdb2
+        self.dev = f"cuda:{device}"
+        self.n = pos_host.shape[0]
+        self.pos0 = torch.from_numpy(pos_host).to(self.dev)
+        self.vel = torch.from_numpy(vel_host).to(self.dev)
+        self.pos = self.pos0.clone()
+        self.out = torch.empty((self.n, 3), dtype=torch.float32, device=self.dev)
+        self.full = full_rebuild
+        v = gvdb2.VolumeGVDB(device)
+        v.Configure(3, 3, 3, 3, 3)
+        for c in range(4):
+            v.AddChannel(c, gvdb2.T_FLOAT, 1)
+        v.SetPoints(self.pos)
+        self.v = v
+        self.attrs = [None, (self.vel, 0), (self.vel, 1), (self.vel, 2)]
+
+    def reset(self):
+        self.pos.copy_(self.pos0)
+
+    def step(self, events=None):
+        v, n, K = self.v, self.n, self.gvdb2.KERNEL_CUBIC2
+        rec = (lambda name: events.append((name, self._ev()))) if events is not None else (lambda name: None)
+        rec("start")
+        self.pos.add_(self.vel, alpha=DT)  # advect (the simulation's own update)
+        rec("advect")
+        if self.full:
+            v.RequestFullRebuild(True)
+        v.RebuildTopology(n, RADIUS)
+        v.UpdateAtlas()
+        rec("topology")
+        if events is not None:  # bin first so the scatter interval is the scatter kernel alone
+            v.GatherKernel(K, n, [1, 2, 3], out=self.out)
+            rec("binning")
+        v.ScatterKernel(K, n, [0, 1, 2, 3], weight=1.0, attrs=self.attrs)
+        rec("scatter")
+        v.UpdateApron(-1, 0.0)
+        rec("apron")
+        v.GatherKernel(K, n, [1, 2, 3], out=self.out)
+        rec("gather")
+
+    def _ev(self):
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record()
+        return e
+
+    def geometry(self):
+        inf = self.v.info()
+        U = sum(int(inf.pool_count[l]) for l in range(5))
+        CL = sum(int(inf.pool_count[l]) * 8 * int(inf.res[l]) ** 3 for l in range(1, 5))
+        return {"B": int(inf.atlas_slots), "U": U, "CL": CL, "T": int(inf.tile_res) ** 3, "R3": int(inf.res[0]) ** 3}
+
+
+# ----------------------------------------------------------------------------
+# CPU restatement (oracle) timing: the reference arm and the cpu_baseline leg
+# ----------------------------------------------------------------------------
+def _oracle_step(args):
+    """One step of the workload on the CPU oracle over a sample of points."""
+    pos, vel = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    t0 = time.perf_counter()
+    o = oracle.Oracle()
+    o.configure(3, 3, 3, 3, 3)
+    for c in range(4):
+        o.add_channel(c, 1)
+    p = (pos + np.float32(DT) * vel).astype(np.float32)
+    st = o.rebuild_topology(p, RADIUS)
+    if st != 0:
+        raise RuntimeError(f"oracle rebuild failed: {st}")
+    o.update_atlas()
+    o.scatter_kernel(oracle.KERNEL_CUBIC2, p, [0, 1, 2, 3], attrs=[None, vel[:, 0], vel[:, 1], vel[:, 2]])
+    for c in range(4):
+        o.update_apron(c, 0.0)
+    o.gather_kernel(oracle.KERNEL_CUBIC2, p, [1, 2, 3])
+    o.close()
+    return time.perf_counter() - t0
+
+
+def _sample(pos, vel, n, part=0):
+    """A contiguous run of lattice rows (a spatial sub-block of the dam)."""
+    start = (part * n) % max(1, len(pos) - n)
+    return pos[start:start + n].copy(), vel[start:start + n].copy()
+
+
+def cpu_baseline(pos, vel, n=N_POINTS):
+    dt = _oracle_step(_sample(pos, vel, n))
+    return {"value": n / dt, "unit": "points/s", "cores": 1, "kind": "port",
+            "sample": f"one full step over {n} lattice points, single-threaded C restatement",
+            "seconds": round(dt, 3)}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    import gvdb2.workloads as wl
+    pos, vel = wl.dam_block(sites=SITES)
+    cores = os.cpu_count() or 1
+    per = 262_144
+    samples = [_sample(pos, vel, per, k) for k in range(cores)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for _ in range(a.warmup):
+            pool.map(_oracle_step, samples)
+        times = []
+        for _ in range(a.steps):
+            t0 = time.perf_counter()
+            pool.map(_oracle_step, samples)
+            times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = per * cores * a.steps / total
+    line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * total / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample_points_per_step": per * cores},
+            "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": "port",
+                             "sample": f"{cores} processes x {per} contiguous lattice points per step"},
+            "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------
+def count_launches(pipe):
+    """Kernels of libgvdb2 in one step (names in the gvdb2 namespace)."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        pipe.step()
+        torch.cuda.synchronize()
+    ours = 0
+    for e in prof.events():
+        if e.device_type == torch.autograd.DeviceType.CUDA and "gvdb2" in e.name:
+            ours += 1
+    return ours
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import gvdb2.workloads as wl
+    from gvdb2 import metrics
+
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    pos, vel = wl.dam_block(sites=SITES)
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(pos, vel)
+
+    pipe = Pipeline(local, pos, vel, full_rebuild=not a.incremental)
+    n = pipe.n
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(max(3, a.warmup)):
+        pipe.step()
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        pipe.step()
+    e1.record()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = n * a.steps * ws / (ms / 1e3)
+
+    # per-stage intervals (CUDA events on the launching stream), averaged
+    geo = pipe.geometry()
+    stage_ms = {}
+    reps = 3
+    for _ in range(reps):
+        ev = []
+        pipe.step(events=ev)
+        torch.cuda.synchronize()
+        for (n0, a0), (n1, a1) in zip(ev[:-1], ev[1:]):
+            stage_ms[n1] = stage_ms.get(n1, 0.0) + a0.elapsed_time(a1) / reps
+    sb = metrics.stage_bytes(N=n, B=geo["B"], U=geo["U"], C=4, Cw=4, G=3, T=geo["T"], R3=geo["R3"], CL=geo["CL"])
+    launches_per_stage = {"scatter": 1, "gather": 1, "apron": 4}
+    peak, peak_kind = peaks()
+    stages = {}
+    for k in ("topology", "binning", "scatter", "apron", "gather"):
+        gbs = sb[k] / (stage_ms[k] / 1e3) / 1e9 if stage_ms.get(k) else None
+        stages[k] = {"ms": round(stage_ms.get(k, 0.0), 4), "alg_bytes": sb[k], "GBps": gbs}
+    dom = max(("scatter", "gather", "apron"), key=lambda k: stage_ms.get(k, 0.0))
+    per_launch_ms = stage_ms[dom] / launches_per_stage[dom]
+    achieved = sb[dom] / launches_per_stage[dom] / (per_launch_ms / 1e3) / 1e9
+    kernel_name = {"scatter": "k_scatter_tile<cubic,float>", "gather": "k_gather_tile<cubic,fwd>",
+                   "apron": "k_apron"}[dom]
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": TRAFFIC.get(dom), "kernel": kernel_name, "peak_source": peak_kind}
+
+    # end to end through the public API: pinned host inputs in, gathered velocities out
+    pipe.reset()
+    hpos = torch.from_numpy(pos).pin_memory()
+    hvel = torch.from_numpy(vel).pin_memory()
+    hout = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    for _ in range(2):
+        pipe.pos.copy_(hpos, non_blocking=True)
+        pipe.vel.copy_(hvel, non_blocking=True)
+        pipe.step()
+        hout.copy_(pipe.out, non_blocking=True)
+    barrier()
+    e0.record()
+    for _ in range(a.steps):
+        pipe.pos.copy_(hpos, non_blocking=True)
+        pipe.vel.copy_(hvel, non_blocking=True)
+        pipe.step()
+        hout.copy_(pipe.out, non_blocking=True)
+    e1.record()
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    e2e = {"value": n * a.steps * ws / (ms_e2e / 1e3), "unit": "points/s", "h2d_bytes_per_step": 24 * n,
+           "d2h_bytes_per_step": 12 * n}
+    launches = count_launches(pipe) * a.steps
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
+                "warmup": max(3, a.warmup), "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "points_per_gpu": n, "bricks": geo["B"], "nodes": geo["U"],
+                           "rebuild": "incremental state machine" if a.incremental else "full rebuild every step",
+                           "l2": "inputs larger than L2 (positions+velocities 100 MB, atlas "
+                                 f"{4 * 4 * geo['B'] * geo['T'] / 1e6:.0f} MB per step)",
+                           "parallelism": f"replicas x{ws}"},
+                "roofline": roofline, "stages": stages, "clocks": clk, "e2e": e2e, "gpu_launches": launches,
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    del pipe
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+# DRAM bytes per launch from ncu captures (profiles/*.md); None until captured.
+TRAFFIC = {}
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

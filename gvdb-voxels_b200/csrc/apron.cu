@@ -1,0 +1,97 @@
+// apron.cu -- apron updates.
+//
+//   UpdateApron (V:4411-4457, O:72-126): every apron voxel (faces, edges
+//     and corners) takes the value of the interior voxel of the leaf that
+//     contains its world position (centre = corner + 0.5, N:145-153), or
+//     boundval when no leaf does.  The reference resolves each voxel by a
+//     root-to-leaf traversal; here the owning brick is one of the 26
+//     neighbours recorded per slot when the atlas was assigned, so the
+//     kernel is a pure gather: one CTA per brick, one 4-byte read and one
+//     4-byte write per apron voxel.
+//   UpdateApronFaces (V:4461-4496, O:27-61): faces only, using the 6-entry
+//     neighbour table of UpdateNeighbors (V:2527-2556).  A missing
+//     neighbour is -1 here; the reference stores 0xFFFF and then fails to
+//     recognise it (O:51).
+#include "dev_common.cuh"
+
+namespace gvdb2 {
+
+namespace {
+
+__global__ void __launch_bounds__(256) k_apron(float *chan, const int32_t *nbr27, int res, int apron, int tile,
+                                               int64_t tvox, float boundval) {
+    const int64_t slot = blockIdx.x;
+    float *self = chan + slot * tvox;
+    const int32_t *nb27 = nbr27 + slot * 27;
+    for (int t = threadIdx.x; t < tvox; t += blockDim.x) {
+        int x = t % tile, y = (t / tile) % tile, z = t / (tile * tile);
+        int lx = x - apron, ly = y - apron, lz = z - apron;
+        int dx = floor_div(lx, res), dy = floor_div(ly, res), dz = floor_div(lz, res);
+        if ((dx | dy | dz) == 0) continue; // interior voxel
+        int32_t nb = nb27[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
+        float val = boundval;
+        if (nb >= 0)
+            val = chan[(int64_t)nb * tvox +
+                       ((int64_t)(lz - dz * res + apron) * tile + (ly - dy * res + apron)) * tile + (lx - dx * res + apron)];
+        self[t] = val;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_apron_faces(float *chan, const int32_t *slot_leaf, const int32_t *leaf_slot,
+                                                     const int32_t *nbr6, int res, int apron, int tile, int64_t tvox) {
+    const int64_t slot = blockIdx.x;
+    const int32_t leaf = slot_leaf[slot];
+    for (int t = threadIdx.x; t < 3 * res * res; t += blockDim.x) {
+        int side = t / (res * res), r = t - side * res * res;
+        int su = r % res, sv = r / res;
+        int32_t nl = nbr6[(int64_t)leaf * 6 + side];
+        if (nl < 0) continue;
+        int32_t ns = leaf_slot[nl];
+        if (ns < 0) continue;
+        int vox[3];
+        if (side == 0) { vox[0] = 0; vox[1] = su; vox[2] = sv; }
+        else if (side == 1) { vox[0] = su; vox[1] = 0; vox[2] = sv; }
+        else { vox[0] = su; vox[1] = sv; vox[2] = 0; }
+        int inc[3] = {side == 0, side == 1, side == 2};
+        auto idx = [&](int x, int y, int z) { return ((int64_t)(z + apron) * tile + (y + apron)) * tile + (x + apron); };
+        int vn[3] = {vox[0] + inc[0] * (res - 1), vox[1] + inc[1] * (res - 1), vox[2] + inc[2] * (res - 1)};
+        float v1 = chan[slot * tvox + idx(vox[0], vox[1], vox[2])];
+        float v2 = chan[(int64_t)ns * tvox + idx(vn[0], vn[1], vn[2])];
+        chan[(int64_t)ns * tvox + idx(vn[0] + inc[0], vn[1] + inc[1], vn[2] + inc[2])] = v1;
+        chan[slot * tvox + idx(vox[0] - inc[0], vox[1] - inc[1], vox[2] - inc[2])] = v2;
+    }
+}
+
+} // namespace
+
+gvdb2_status update_apron(Volume *v, int chan, float boundval) {
+    if (v->apron == 0) return GVDB2_OK; // V:4421
+    if (!v->atlas_valid) return fail(v, GVDB2_ERR_STATE, "UpdateAtlas must follow the topology rebuild");
+    for (int c = 0; c < kMaxChan; c++) {
+        if (chan >= 0 && c != chan) continue;
+        if (!v->has_chan[c]) {
+            if (chan >= 0) return fail(v, GVDB2_ERR_ARG, "bad channel");
+            continue;
+        }
+        if (v->atlas_last == 0) continue;
+        k_apron<<<(unsigned)v->atlas_last, 256, 0, v->stream>>>(v->atlas[c].as<float>(), v->nbr27.as<int32_t>(), v->res(0),
+                                                                v->apron, v->tile_res(), v->tile_vox(), boundval);
+        GV_CUDA(v, cudaGetLastError());
+    }
+    return GVDB2_OK;
+}
+
+gvdb2_status update_apron_faces(Volume *v, int chan) {
+    if (v->apron == 0) return GVDB2_OK;
+    if (chan < 0 || chan >= kMaxChan || !v->has_chan[chan]) return fail(v, GVDB2_ERR_ARG, "bad channel");
+    if (!v->atlas_valid) return fail(v, GVDB2_ERR_STATE, "UpdateAtlas must follow the topology rebuild");
+    if (!v->nbr6_valid) return fail(v, GVDB2_ERR_STATE, "UpdateNeighbors must precede UpdateApronFaces");
+    if (v->atlas_last == 0) return GVDB2_OK;
+    k_apron_faces<<<(unsigned)v->atlas_last, 256, 0, v->stream>>>(v->atlas[chan].as<float>(), v->slot_leaf.as<int32_t>(),
+                                                                  v->leaf_slot.as<int32_t>(), v->nbr6.as<int32_t>(),
+                                                                  v->res(0), v->apron, v->tile_res(), v->tile_vox());
+    GV_CUDA(v, cudaGetLastError());
+    return GVDB2_OK;
+}
+
+} // namespace gvdb2

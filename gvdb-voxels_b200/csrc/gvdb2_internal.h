@@ -1,0 +1,253 @@
+// gvdb2_internal.h -- host-side state and shared declarations of the
+// B200-native point -> sparse-volume pipeline (libgvdb2).
+//
+// Layout contracts kept from the reference (paths relative to gvdb-voxels):
+//   Node        : 64 bytes, source/gvdb_library/src/gvdb_node.h:27-40
+//   child lists : 8*res^3 bytes per interior node of pool group 1 (V:2424-2426)
+//   pool refs   : grp | lev<<8 | ndx<<16 (gvdb_allocator.h:59-62)
+//   brick keys  : lev<<48 | x<<32 | y<<16 | z (P:352-382)
+// The atlas departs from the reference's CUarray: per channel a linear run
+// of (res+2*apron)^3-float tiles, one per atlas slot, z-major.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "gvdb2.h"
+
+namespace gvdb2 {
+
+constexpr int kMaxLev = 10;      // MAXLEV, gvdb_volume_gvdb.h:40
+constexpr int kMaxChan = 32;     // MAX_CHANNEL, N:22
+constexpr int kMaxSplatChan = 8; // channels one kernel splat call may touch
+constexpr uint64_t kUndefL = 0xFFFFFFFFull;
+constexpr uint64_t kUndef64 = 0xFFFFFFFFFFFFFFFFull;
+constexpr uint64_t kEmptyKey = 0xFFFFFFFFFFFFFFFFull;
+constexpr float kNoHit = 1.0e10f; // NOHIT, gvdb_types.h:52
+
+struct __align__(16) Node {
+    uint8_t mLev, mFlags, mPriority, pad;
+    int32_t mPos[3];
+    int32_t mValue[3];
+    float mVRange[3];
+    uint64_t mParent;
+    uint64_t mChildList;
+    uint64_t mMask;
+};
+static_assert(sizeof(Node) == 64, "Node must keep the reference's 64-byte layout");
+
+struct AtlasNode {
+    int32_t mPos[3];
+    int32_t mLeafID;
+};
+static_assert(sizeof(AtlasNode) == 16, "AtlasNode is 16 bytes");
+
+struct PointsView {
+    const char *base;
+    int64_t count;
+    int32_t stride;
+    int32_t offset;
+};
+
+// Open-addressed hash set / map of 64-bit brick keys (linear probing).
+struct HashTable {
+    uint64_t *keys;   // kEmptyKey = free
+    int32_t *vals;    // optional payload (map)
+    uint32_t mask;    // capacity - 1 (power of two)
+    int32_t *count;   // device counter of inserted keys
+};
+
+// Device-resident status word set by kernels (never trap).
+enum DevStatusBits : int32_t {
+    kDevHashFull = 1,
+    kDevCapacity = 2,
+    kDevBadIndex = 4,
+};
+
+// Growable device buffer, stream-ordered (cudaMallocAsync / cudaFreeAsync
+// on the stream that last grew it).  Non-copyable; frees itself.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    cudaError_t ensure(size_t need, cudaStream_t s, bool preserve = false);
+    void release();
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+struct Volume {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int deterministic = 0;
+
+    // configuration (Configure, V:2364-2434)
+    int nlev = 0;
+    int logdim[kMaxLev] = {0};
+    int default_axiscnt[3] = {16, 16, 1}; // SetChannelDefault(16,16,1), V:2348
+
+    // channels / atlas
+    bool has_chan[kMaxChan] = {false};
+    int apron = 0;
+    int subdim[3] = {0, 0, 0};
+    int64_t atlas_cap = 0;    // bricks the atlas holds
+    int64_t atlas_last = 0;   // slots in use (lastEle)
+    DevBuf atlas[kMaxChan];   // float tiles
+    DevBuf amap;              // AtlasNode per atlas brick
+    DevBuf slot_leaf;         // int32 per slot: leaf pool index
+    DevBuf leaf_slot;         // int32 per pool leaf: slot or -1
+    DevBuf nbr27;             // int32 per slot x 27: neighbour slots
+    DevBuf nbr6;              // int32 per pool leaf x 6 (UpdateNeighbors)
+    bool nbr6_valid = false;
+    bool atlas_valid = false; // slots assigned for the current topology
+
+    // points (SetPoints, V:4900-4908)
+    PointsView pos{}, vel{}, clr{};
+
+    // topology state (host mirrors of device pools)
+    bool rebuild_topo = true; // V:2355
+    int cur_depth = -1;       // V:2356
+    int depth = 0;
+    int root_pos[3] = {0, 0, 0};
+    float posmin[3] = {0, 0, 0}, posmax[3] = {0, 0, 0};
+    int64_t pool_cnt[kMaxLev] = {0};
+    int64_t used_leaves = 0;
+    DevBuf pool[kMaxLev];     // Node arrays
+    DevBuf clist[kMaxLev];    // uint64 child lists (lev >= 1)
+    uint64_t topo_version = 0;
+
+    // leaf lookup: level-0 key -> leaf pool index (linked leaves only)
+    DevBuf leafmap_keys, leafmap_vals;
+    uint32_t leafmap_mask = 0;
+    // per-level maps of linked interior nodes (incremental rebuild)
+    DevBuf levmap_keys[kMaxLev], levmap_vals[kMaxLev];
+    uint32_t levmap_mask[kMaxLev] = {0};
+
+    // scratch for the rebuild
+    DevBuf hs_keys[2];        // hash sets (base, box)
+    uint32_t hs_mask = 0;
+    DevBuf lev_keys[kMaxLev][2]; // sorted unique keys per level: [0]=base [1]=extra (or new)
+    int64_t lev_count[kMaxLev][2] = {{0}};
+    DevBuf tmp_a, tmp_b, tmp_c, scratch;
+    DevBuf dev_small;         // small device words: counters, status, bbox
+    void *host_small = nullptr; // pinned mirror of dev_small
+
+    // InsertPoints results
+    DevBuf pnode, poff, gcnt, goff, psorted;
+    int64_t pnode_n = 0;
+
+    // kernel-splat binning
+    DevBuf pbin, prank, bin_cnt, bin_off, perm;
+    struct BinKey {
+        bool valid = false;
+        int kernel = 0;
+        int64_t n = 0;
+        PointsView pos{};
+        float trans[3] = {0, 0, 0};
+        uint64_t topo = 0;
+    } bin_key;
+
+    // subcells (InsertPointsSubcell)
+    DevBuf sc_map, sc_flag, sc_cnt, sc_off, sc_nid, sc_pos, sc_pnt;
+    int sc_size = 0, sc_dim = 0, sc_per_brick = 0;
+    int64_t num_sc = 0, sc_len = 0;
+
+    // ---- helpers ----
+    int res(int lev) const { return lev < 0 ? 1 : (1 << logdim[lev]); }
+    int64_t res3(int lev) const {
+        int64_t r = res(lev);
+        return r * r * r;
+    }
+    int64_t range(int lev) const {
+        if (lev < 0) return 1;
+        int64_t r = res(0);
+        for (int l = 1; l <= lev; l++) r *= res(l);
+        return r;
+    }
+    int tile_res() const { return res(0) + 2 * apron; }
+    int64_t tile_vox() const {
+        int64_t t = tile_res();
+        return t * t * t;
+    }
+    int top_level() const {
+        int tlev = 1; // PrepareVDB, V:3952-3965
+        for (int n = nlev - 1; n >= 0; n--)
+            if (pool_cnt[n] == 1) tlev = n;
+        return tlev;
+    }
+    bool any_channel() const {
+        for (int c = 0; c < kMaxChan; c++)
+            if (has_chan[c]) return true;
+        return false;
+    }
+    Node *pool_ptr(int lev) const { return pool[lev].as<Node>(); }
+};
+
+// status helpers
+gvdb2_status fail(Volume *v, gvdb2_status st, const std::string &msg);
+gvdb2_status cuda_fail(Volume *v, cudaError_t e, const char *what);
+
+#define GV_CUDA(v, call)                                         \
+    do {                                                         \
+        cudaError_t e__ = (call);                                \
+        if (e__ != cudaSuccess) return ::gvdb2::cuda_fail((v), e__, #call); \
+    } while (0)
+#define GV_TRY(expr)                          \
+    do {                                      \
+        gvdb2_status s__ = (expr);            \
+        if (s__ != GVDB2_OK) return s__;      \
+    } while (0)
+
+// ---- primitives.cu ----
+// exclusive scan of n uint32 -> out[0..n], out[n] = total
+gvdb2_status exclusive_scan_u32(Volume *v, const uint32_t *in, uint32_t *out, int64_t n);
+// stable LSD radix sort of n uint64 keys (optionally with int32 values) over
+// bits [lo_bit, hi_bit); the sorted result is written back to keys/vals.
+gvdb2_status radix_sort_u64(Volume *v, uint64_t *keys, int32_t *vals, int64_t n, int lo_bit, int hi_bit);
+
+// ---- topology.cu ----
+gvdb2_status rebuild_topology(Volume *v, int n, float radius, const float orig[3], bool accumulate, int min_depth);
+gvdb2_status update_atlas(Volume *v);
+gvdb2_status update_neighbors(Volume *v);
+gvdb2_status clear_channel(Volume *v, int chan);
+gvdb2_status sync_counts(Volume *v);
+
+// ---- points.cu ----
+gvdb2_status insert_points(Volume *v, int n, const float trans[3], int prefix);
+gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]);
+gvdb2_status insert_points_subcell(Volume *v, int sc, int n, float radius, const float trans[3], int *len);
+
+// ---- splat.cu ----
+gvdb2_status scatter_density_ref(Volume *v, int n, float radius, float amp, const float trans[3], int expand);
+gvdb2_status gather_voxels(Volume *v, int sc, float radius, int chan, int accum, bool levelset);
+gvdb2_status scatter_kernel(Volume *v, int kernel, int n, const float trans[3], gvdb2_points_view weight,
+                            float weight_const, const gvdb2_points_view *attrs, const int *chans, int nch);
+gvdb2_status gather_kernel(Volume *v, int kernel, int n, const float trans[3], const int *chans, int nch, float *out,
+                           int64_t out_stride);
+gvdb2_status scatter_kernel_backward(Volume *v, int kernel, int n, const float trans[3], gvdb2_points_view weight,
+                                     float weight_const, const gvdb2_points_view *attrs, int nch,
+                                     const int *grad_chans, float *grad_pos, float *grad_weight, float *grad_attr);
+gvdb2_status gather_kernel_backward(Volume *v, int kernel, int n, const float trans[3], const int *chans, int nch,
+                                    const float *grad_out, const int *grad_chans, float *grad_pos);
+
+// ---- apron.cu ----
+gvdb2_status update_apron(Volume *v, int chan, float boundval);
+gvdb2_status update_apron_faces(Volume *v, int chan);
+
+inline PointsView to_view(gvdb2_points_view w) {
+    PointsView p;
+    p.base = reinterpret_cast<const char *>(w.base);
+    p.count = w.count;
+    p.stride = w.stride_bytes;
+    p.offset = w.offset_bytes;
+    return p;
+}
+
+} // namespace gvdb2

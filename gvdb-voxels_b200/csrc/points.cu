@@ -1,0 +1,331 @@
+// points.cu -- point insertion and binning.
+//
+//   InsertPoints (V:5219-5267, P:19-36, P:59-72): per point the leaf it
+//     falls in (pnode), its slot inside that leaf (poff) and per-leaf
+//     counts (gcnt); with `prefix`, a counting sort of positions by leaf.
+//   Kernel-splat binning (no reference counterpart): a warp-aggregated
+//     counting sort of points by (atlas slot, region) where the 27 regions
+//     say which neighbouring bricks a point's stencil reaches; the splat
+//     kernels read a brick's own points plus the matching regions of its
+//     neighbours.
+//   InsertPointsSubcell (V:4971-5092, P:109-118, P:218-315, P:677-694).
+#include <algorithm>
+
+#include "dev_common.cuh"
+
+namespace gvdb2 {
+
+namespace {
+
+// gvdbInsertPoints (P:19-36): NOHIT positions and points outside every
+// leaf get pnode = ID_UNDEFL; others take an atomic slot in their leaf.
+__global__ void k_insert_points(PointsView pos, int64_t n, float3 trans, LeafLookup L, int32_t *pnode, int32_t *poff,
+                                int32_t *gcnt) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 p = load_f3(pos, i);
+    if (p.z == kNoHit) {
+        pnode[i] = (int32_t)kUndefL;
+        return;
+    }
+    int32_t leaf = leaf_at(L, p.x + trans.x, p.y + trans.y, p.z + trans.z);
+    if (leaf < 0) {
+        pnode[i] = (int32_t)kUndefL;
+        return;
+    }
+    pnode[i] = leaf;
+    poff[i] = atomicAdd(&gcnt[leaf], 1);
+}
+
+// gvdbSortPoints (P:59-72)
+__global__ void k_sort_points(PointsView pos, int64_t n, float3 trans, const int32_t *pnode, const int32_t *poff,
+                              int64_t nleaves, const uint32_t *goff, float *out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int32_t nid = pnode[i];
+    if (nid < 0 || nid >= nleaves) return;
+    int64_t k = (int64_t)goff[nid] + poff[i];
+    float3 p = load_f3(pos, i);
+    out[3 * k + 0] = p.x + trans.x;
+    out[3 * k + 1] = p.y + trans.y;
+    out[3 * k + 2] = p.z + trans.z;
+}
+
+template <int KERNEL>
+__global__ void k_bin_count(PointsView pos, int64_t n, float3 trans, LeafLookup L, const int32_t *leaf_slot, int res0,
+                            uint32_t *cnt, int32_t *pbin, int32_t *prank) {
+    using T = Taps<KERNEL>;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t bin = -1;
+    if (i < n) {
+        float3 p = load_f3(pos, i);
+        if (p.z != kNoHit) {
+            float w[3] = {p.x + trans.x, p.y + trans.y, p.z + trans.z};
+            int32_t leaf = leaf_at(L, w[0], w[1], w[2]);
+            int32_t slot = leaf >= 0 ? leaf_slot[leaf] : -1;
+            if (slot >= 0) {
+                int code = 0, mul = 1;
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    int bo = ((int)w[a] >> L.g.log2r0) * res0;
+                    int first = (int)floorf(w[a] - 0.5f) - T::LO - bo;
+                    int last = first + T::N - 1;
+                    int c = first < 0 ? 0 : (last >= res0 ? 2 : 1);
+                    code += c * mul;
+                    mul *= 3;
+                }
+                bin = slot * 27 + code;
+            }
+        }
+    }
+    unsigned act = __ballot_sync(0xffffffffu, bin >= 0);
+    if (bin >= 0) {
+        uint32_t r = warp_agg_inc(cnt, (uint32_t)bin, act);
+        pbin[i] = bin;
+        prank[i] = (int32_t)r;
+    } else if (i < n) {
+        pbin[i] = -1;
+    }
+}
+
+__global__ void k_bin_fill(const int32_t *pbin, const int32_t *prank, int64_t n, const uint32_t *off, int32_t *perm) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int32_t b = pbin[i];
+    if (b >= 0) perm[off[b] + prank[i]] = (int32_t)i;
+}
+
+// gvdbSetFlagSubcell (P:109-118)
+__global__ void k_sc_flag(const Node *leaves, int64_t n, uint32_t *flag) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    flag[i] = leaves[i].mParent == kUndef64 ? 0u : 1u;
+}
+
+struct ScArgs {
+    PointsView pos;
+    int64_t n;
+    float3 trans;
+    float radius;
+    int sc, scdim, scpb;
+    int64_t num_sc;
+    LeafLookup L;
+    const Node *leaves;
+    int64_t nleaves;
+    const uint32_t *mapping;
+};
+
+// gvdbCountSubcell (P:275-315, pass 0) / gvdbInsertSubcell (P:218-273,
+// pass 1).  The count pass tests the sign after adding trans, the insert
+// pass before, as in the reference; an insert never writes past the
+// counted capacity of its subcell.
+template <int PASS>
+__global__ void k_sc_visit(ScArgs A, uint32_t *cnt, const uint32_t *cap, const uint32_t *off, float *pnt,
+                           int32_t *status) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    float3 p = load_f3(A.pos, i);
+    if (p.z == kNoHit) return;
+    float w[3];
+    if (PASS == 0) {
+        w[0] = p.x + A.trans.x;
+        w[1] = p.y + A.trans.y;
+        w[2] = p.z + A.trans.z;
+        if (w[0] < 0 || w[1] < 0 || w[2] < 0) return;
+    } else {
+        if (p.x < 0 || p.y < 0 || p.z < 0) return;
+        w[0] = p.x + A.trans.x;
+        w[1] = p.y + A.trans.y;
+        w[2] = p.z + A.trans.z;
+    }
+    int mn[3], mx[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        mn[a] = ((int)(w[a] - A.radius) / A.sc) * A.sc;
+        mx[a] = ((int)(w[a] + 1 + A.radius) / A.sc) * A.sc;
+    }
+    for (int sx = mn[0]; sx <= mx[0]; sx += A.sc)
+        for (int sy = mn[1]; sy <= mx[1]; sy += A.sc)
+            for (int sz = mn[2]; sz <= mx[2]; sz += A.sc) {
+                if (sx < 0 || sy < 0 || sz < 0) continue;
+                int32_t leaf = leaf_at_brick(A.L, sx >> A.L.g.log2r0, sy >> A.L.g.log2r0, sz >> A.L.g.log2r0);
+                if (leaf < 0 || leaf >= A.nleaves) continue;
+                const Node &nd = A.leaves[leaf];
+                int lx = (sx - nd.mPos[0]) / A.sc, ly = (sy - nd.mPos[1]) / A.sc, lz = (sz - nd.mPos[2]) / A.sc;
+                int64_t idx = (int64_t)A.mapping[leaf] * A.scpb + ((int64_t)lz * A.scdim + ly) * A.scdim + lx;
+                if (idx < 0 || idx >= A.num_sc) continue;
+                if (PASS == 0) {
+                    atomicAdd(&cnt[idx], 1u);
+                } else {
+                    uint32_t o = atomicAdd(&cnt[idx], 1u);
+                    if (o >= cap[idx]) {
+                        atomicOr(status, kDevCapacity);
+                        continue;
+                    }
+                    int64_t at = (int64_t)off[idx] + o;
+                    pnt[3 * at + 0] = w[0];
+                    pnt[3 * at + 1] = w[1];
+                    pnt[3 * at + 2] = w[2];
+                }
+            }
+}
+
+// gvdbCalcSubcellPos (P:677-694)
+__global__ void k_sc_pos(const Node *leaves, int64_t n, const uint32_t *mapping, int sc, int scdim, int scpb,
+                         int64_t num_sc, int32_t *sc_nid, int32_t *sc_pos) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Node &nd = leaves[i];
+    if (nd.mParent == kUndef64) return;
+    for (int s = 0; s < scpb; s++) {
+        int64_t idx = (int64_t)mapping[i] * scpb + s;
+        if (idx >= num_sc) continue;
+        sc_pos[3 * idx + 0] = nd.mPos[0] + s % scdim * sc;
+        sc_pos[3 * idx + 1] = nd.mPos[1] + (s / scdim) % scdim * sc;
+        sc_pos[3 * idx + 2] = nd.mPos[2] + (s / scdim / scdim) % scdim * sc;
+        sc_nid[idx] = (int32_t)i;
+    }
+}
+
+} // namespace
+
+gvdb2_status insert_points(Volume *v, int n, const float trans[3], int prefix) {
+    if (v->pool_cnt[0] == 0) return fail(v, GVDB2_ERR_STATE, "no topology");
+    if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count))) return fail(v, GVDB2_ERR_ARG, "bad point count");
+    cudaStream_t s = v->stream;
+    int64_t nl = v->pool_cnt[0];
+    GV_CUDA(v, v->pnode.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
+    GV_CUDA(v, v->poff.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
+    GV_CUDA(v, v->gcnt.ensure(sizeof(int32_t) * (size_t)nl, s));
+    GV_CUDA(v, cudaMemsetAsync(v->gcnt.p, 0, sizeof(int32_t) * (size_t)nl, s));
+    GV_CUDA(v, cudaMemsetAsync(v->poff.p, 0, sizeof(int32_t) * (size_t)std::max(n, 1), s));
+    float3 t = make_float3(trans[0], trans[1], trans[2]);
+    LeafLookup L = make_lookup(v);
+    if (n > 0)
+        k_insert_points<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t, L, v->pnode.as<int32_t>(),
+                                                                    v->poff.as<int32_t>(), v->gcnt.as<int32_t>());
+    GV_CUDA(v, cudaGetLastError());
+    v->pnode_n = n;
+    if (prefix) {
+        GV_CUDA(v, v->goff.ensure(sizeof(uint32_t) * (size_t)(nl + 1), s));
+        GV_TRY(exclusive_scan_u32(v, v->gcnt.as<uint32_t>(), v->goff.as<uint32_t>(), nl));
+        GV_CUDA(v, v->psorted.ensure(sizeof(float) * 3 * (size_t)std::max(n, 1), s));
+        if (n > 0)
+            k_sort_points<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t, v->pnode.as<int32_t>(),
+                                                                      v->poff.as<int32_t>(), nl, v->goff.as<uint32_t>(),
+                                                                      v->psorted.as<float>());
+        GV_CUDA(v, cudaGetLastError());
+    }
+    return GVDB2_OK;
+}
+
+gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
+    Volume::BinKey &k = v->bin_key;
+    if (k.valid && k.kernel == kernel && k.n == n && k.topo == v->topo_version && k.pos.base == v->pos.base &&
+        k.pos.stride == v->pos.stride && k.pos.offset == v->pos.offset && k.trans[0] == trans[0] &&
+        k.trans[1] == trans[1] && k.trans[2] == trans[2])
+        return GVDB2_OK;
+    if (!v->atlas_valid) return fail(v, GVDB2_ERR_STATE, "UpdateAtlas must follow the topology rebuild");
+    if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count))) return fail(v, GVDB2_ERR_ARG, "bad point count");
+    cudaStream_t s = v->stream;
+    int64_t nbins = 27 * v->atlas_last;
+    GV_CUDA(v, v->pbin.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
+    GV_CUDA(v, v->prank.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
+    GV_CUDA(v, v->perm.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
+    GV_CUDA(v, v->bin_cnt.ensure(sizeof(uint32_t) * (size_t)(nbins + 1), s));
+    GV_CUDA(v, v->bin_off.ensure(sizeof(uint32_t) * (size_t)(nbins + 1), s));
+    GV_CUDA(v, cudaMemsetAsync(v->bin_cnt.p, 0, sizeof(uint32_t) * (size_t)(nbins + 1), s));
+    float3 t = make_float3(trans[0], trans[1], trans[2]);
+    LeafLookup L = make_lookup(v);
+    if (n > 0) {
+        int g = grid_for(n, 256, 1ll << 31);
+        if (kernel == GVDB2_KERNEL_TENT1)
+            k_bin_count<GVDB2_KERNEL_TENT1><<<g, 256, 0, s>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(), v->res(0),
+                                                              v->bin_cnt.as<uint32_t>(), v->pbin.as<int32_t>(),
+                                                              v->prank.as<int32_t>());
+        else
+            k_bin_count<GVDB2_KERNEL_CUBIC2><<<g, 256, 0, s>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(), v->res(0),
+                                                               v->bin_cnt.as<uint32_t>(), v->pbin.as<int32_t>(),
+                                                               v->prank.as<int32_t>());
+        GV_CUDA(v, cudaGetLastError());
+    }
+    GV_TRY(exclusive_scan_u32(v, v->bin_cnt.as<uint32_t>(), v->bin_off.as<uint32_t>(), nbins));
+    if (n > 0) {
+        k_bin_fill<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pbin.as<int32_t>(), v->prank.as<int32_t>(), n,
+                                                               v->bin_off.as<uint32_t>(), v->perm.as<int32_t>());
+        GV_CUDA(v, cudaGetLastError());
+    }
+    k.valid = true;
+    k.kernel = kernel;
+    k.n = n;
+    k.topo = v->topo_version;
+    k.pos = v->pos;
+    for (int a = 0; a < 3; a++) k.trans[a] = trans[a];
+    return GVDB2_OK;
+}
+
+gvdb2_status insert_points_subcell(Volume *v, int sc, int n, float radius, const float trans[3], int *len) {
+    int res0 = v->res(0);
+    if (sc <= 0 || res0 % sc) return fail(v, GVDB2_ERR_ARG, "subcell size must divide the brick resolution");
+    if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count))) return fail(v, GVDB2_ERR_ARG, "bad point count");
+    int64_t num_brick = v->used_leaves;
+    if (num_brick == 0) return fail(v, GVDB2_ERR_STATE, "InsertPointsSubcell yet no bricks exist");
+    cudaStream_t s = v->stream;
+    int scdim = res0 / sc, scpb = scdim * scdim * scdim;
+    int64_t num_sc = (int64_t)scpb * num_brick, nmap = v->pool_cnt[0];
+    v->sc_size = sc;
+    v->sc_dim = scdim;
+    v->sc_per_brick = scpb;
+    v->num_sc = num_sc;
+    GV_CUDA(v, v->sc_flag.ensure(sizeof(uint32_t) * (size_t)(nmap + 1), s));
+    GV_CUDA(v, v->sc_map.ensure(sizeof(uint32_t) * (size_t)(nmap + 1), s));
+    GV_CUDA(v, v->sc_cnt.ensure(sizeof(uint32_t) * (size_t)(2 * num_sc + 2), s));
+    GV_CUDA(v, v->sc_off.ensure(sizeof(uint32_t) * (size_t)(num_sc + 1), s));
+    GV_CUDA(v, v->sc_nid.ensure(sizeof(int32_t) * (size_t)num_sc, s));
+    GV_CUDA(v, v->sc_pos.ensure(sizeof(int32_t) * 3 * (size_t)num_sc, s));
+    GV_CUDA(v, cudaMemsetAsync(v->sc_nid.p, 0, sizeof(int32_t) * (size_t)num_sc, s));
+    GV_CUDA(v, cudaMemsetAsync(v->sc_pos.p, 0, sizeof(int32_t) * 3 * (size_t)num_sc, s));
+    k_sc_flag<<<grid_for(nmap, 256, 1ll << 31), 256, 0, s>>>(v->pool_ptr(0), nmap, v->sc_flag.as<uint32_t>());
+    GV_TRY(exclusive_scan_u32(v, v->sc_flag.as<uint32_t>(), v->sc_map.as<uint32_t>(), nmap));
+    uint32_t *cnt = v->sc_cnt.as<uint32_t>(), *cap = cnt + num_sc + 1;
+    GV_CUDA(v, cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (size_t)(num_sc + 1), s));
+    ScArgs A;
+    A.pos = v->pos;
+    A.n = n;
+    A.trans = make_float3(trans[0], trans[1], trans[2]);
+    A.radius = radius;
+    A.sc = sc;
+    A.scdim = scdim;
+    A.scpb = scpb;
+    A.num_sc = num_sc;
+    A.L = make_lookup(v);
+    A.leaves = v->pool_ptr(0);
+    A.nleaves = nmap;
+    A.mapping = v->sc_map.as<uint32_t>();
+    int32_t *status = nullptr;
+    GV_CUDA(v, cudaMallocAsync((void **)&status, sizeof(int32_t), s));
+    GV_CUDA(v, cudaMemsetAsync(status, 0, sizeof(int32_t), s));
+    if (n > 0) k_sc_visit<0><<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(A, cnt, nullptr, nullptr, nullptr, status);
+    GV_TRY(exclusive_scan_u32(v, cnt, v->sc_off.as<uint32_t>(), num_sc));
+    uint32_t total = 0;
+    GV_CUDA(v, cudaMemcpyAsync(&total, v->sc_off.as<uint32_t>() + num_sc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GV_CUDA(v, cudaStreamSynchronize(s));
+    v->sc_len = total;
+    if (len) *len = (int)total;
+    if (total > 0) {
+        GV_CUDA(v, v->sc_pnt.ensure(sizeof(float) * 3 * (size_t)total, s));
+        GV_CUDA(v, cudaMemcpyAsync(cap, cnt, sizeof(uint32_t) * (size_t)num_sc, cudaMemcpyDeviceToDevice, s));
+        GV_CUDA(v, cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (size_t)num_sc, s));
+        if (n > 0)
+            k_sc_visit<1><<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(A, cnt, cap, v->sc_off.as<uint32_t>(),
+                                                                     v->sc_pnt.as<float>(), status);
+    }
+    k_sc_pos<<<grid_for(nmap, 256, 1ll << 31), 256, 0, s>>>(v->pool_ptr(0), nmap, v->sc_map.as<uint32_t>(), sc, scdim,
+                                                            scpb, num_sc, v->sc_nid.as<int32_t>(),
+                                                            v->sc_pos.as<int32_t>());
+    GV_CUDA(v, cudaGetLastError());
+    cudaFreeAsync(status, s);
+    return GVDB2_OK;
+}
+
+} // namespace gvdb2

@@ -1,0 +1,813 @@
+// topology.cu -- dynamic topology rebuild and atlas assignment on device.
+//
+// Reference behaviour restated (paths relative to gvdb-voxels):
+//   RebuildTopology state machine     V:1181-1218
+//   GetBoundingBox / DetermineDepth   V:5404-5467, V:821-837, V:2915-2931
+//   full rebuild (ActivateBricksGPU)  V:1229-1413, P:352-382, V:843-873
+//   extra bricks (radius >= 1)        V:931-1016, P:467-512
+//   incremental (ActivateIncre...)    V:1020-1156, P:420-465, N:401-467
+//   node set-up / links               V:2512-2524, N:470-505
+//   UpdateAtlas                       V:2630-2704, A:692-715
+//
+// The reference sorts N*depth 64-bit keys with Thrust and then allocates
+// nodes in a host loop.  Here every point inserts its level-0 brick (and,
+// for radius >= 1, the bricks of its activation box) into device hash
+// sets; only the unique bricks are sorted, parent levels are derived from
+// them, and node pools, child lists and links are written by kernels in
+// the reference's exact pool order: per level, sorted base keys, then
+// sorted extra keys.  Keys are packed as x<<2b | y<<b | z with b bits per
+// axis, which orders them exactly like the reference's (lev,x,y,z) keys.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "dev_common.cuh"
+
+namespace gvdb2 {
+
+namespace {
+
+struct SmallWords { // layout of Volume::dev_small
+    int32_t bbox[6];
+    int32_t count[8];
+    int32_t status;
+    int32_t pad[17];
+};
+static_assert(sizeof(SmallWords) == 128, "small word block");
+
+__device__ __forceinline__ int32_t f2ord(float f) {
+    int32_t i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+inline float ord2f(int32_t o) {
+    int32_t i = o >= 0 ? o : o ^ 0x7FFFFFFF;
+    float f;
+    std::memcpy(&f, &i, 4);
+    return f;
+}
+
+// GetBoundingBox (V:5404-5467): min/max of pos + trans over all points.
+__global__ void k_bbox(PointsView pos, int64_t n, float3 t, int32_t *bbox) {
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float3 p = load_f3(pos, i);
+        float w[3] = {p.x + t.x, p.y + t.y, p.z + t.z};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            mn[a] = fminf(mn[a], w[a]);
+            mx[a] = fmaxf(mx[a], w[a]);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+            mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+        }
+    }
+    __shared__ float smn[3][32], smx[3][32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0)
+        for (int a = 0; a < 3; a++) {
+            smn[a][warp] = mn[a];
+            smx[a][warp] = mx[a];
+        }
+    __syncthreads();
+    if (warp == 0) {
+        for (int a = 0; a < 3; a++) {
+            float x = lane < nw ? smn[a][lane] : INFINITY;
+            float y = lane < nw ? smx[a][lane] : -INFINITY;
+            for (int o = 16; o > 0; o >>= 1) {
+                x = fminf(x, __shfl_xor_sync(0xffffffffu, x, o));
+                y = fmaxf(y, __shfl_xor_sync(0xffffffffu, y, o));
+            }
+            if (lane == 0) {
+                atomicMin(&bbox[a], f2ord(x));
+                atomicMax(&bbox[3 + a], f2ord(y));
+            }
+        }
+    }
+}
+
+
+// Per point: its level-0 brick into the base set; for radius >= 1 every
+// level-0 brick of the activation box [int(w)-r, int(w)+k*r] (P:481-482 /
+// P:433-434) into the box set.  Box bricks outside the root node are
+// skipped (the reference reads past its child list there).
+__global__ void k_mark_keys(PointsView pos, int64_t n, float3 orig, float radius, float kmax, int do_box, KeyGeom g,
+                            uint64_t *hs_base, uint64_t *hs_box, uint32_t mask, int32_t *counts, int32_t *status) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < n;
+    float w[3] = {0, 0, 0};
+    if (valid) {
+        float3 p = load_f3(pos, i);
+        w[0] = p.x + orig.x;
+        w[1] = p.y + orig.y;
+        w[2] = p.z + orig.z;
+        if (w[0] < 0 || w[1] < 0 || w[2] < 0) valid = false;
+    }
+    unsigned act = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    int bx = (int)w[0] >> g.log2r0, by = (int)w[1] >> g.log2r0, bz = (int)w[2] >> g.log2r0;
+    bool inside = bx >= g.lo[0] && bx < g.lo[0] + g.span && by >= g.lo[1] && by < g.lo[1] + g.span &&
+                  bz >= g.lo[2] && bz < g.lo[2] + g.span;
+    uint64_t key = inside ? pack_key(bx, by, bz, g.b) : kEmptyKey;
+    // warp de-duplication: one insert per distinct key
+    unsigned peers = __match_any_sync(act, key);
+    if (inside && (int)(threadIdx.x & 31) == __ffs(peers) - 1) {
+        int r = hs_insert(hs_base, mask, key);
+        if (r > 0) atomicAdd(&counts[0], 1);
+        if (r < 0) atomicOr(status, kDevHashFull);
+    }
+    if (!do_box) return;
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+        int iw = (int)w[a];
+        int bmin = (int)((float)iw - radius);
+        int bmax = (int)((float)iw + kmax * radius);
+        int l = (bmin < 0 ? 0 : bmin) >> g.log2r0;
+        int h = bmax >> g.log2r0;
+        l = max(l, g.lo[a]);
+        h = min(h, g.lo[a] + g.span - 1);
+        lo[a] = l;
+        hi[a] = h;
+    }
+    for (int x = lo[0]; x <= hi[0]; x++)
+        for (int y = lo[1]; y <= hi[1]; y++)
+            for (int z = lo[2]; z <= hi[2]; z++) {
+                uint64_t k = pack_key(x, y, z, g.b);
+                int r = hs_insert(hs_box, mask, k);
+                if (r > 0) atomicAdd(&counts[1], 1);
+                if (r < 0) atomicOr(status, kDevHashFull);
+            }
+}
+
+__global__ void k_compact_set(const uint64_t *hs, uint32_t cap, uint64_t *out, int32_t *count) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t k = hs[i];
+        bool has = k != kEmptyKey;
+        unsigned m = __ballot_sync(__activemask(), has);
+        if (has) {
+            int leader = __ffs(m) - 1;
+            int base = 0;
+            if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(count, __popc(m));
+            base = __shfl_sync(m, base, leader);
+            out[base + __popc(m & lanemask_lt())] = k;
+        }
+    }
+}
+
+// keys -> parent keys one level up (shift s bits per axis)
+__global__ void k_parentize(const uint64_t *in, int64_t n, int b, int s, uint64_t *out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    unpack_key(in[i], b, x, y, z);
+    out[i] = pack_key(x >> s, y >> s, z >> s, b);
+}
+
+// flags[i] = 1 if keys[i] starts a run (sorted input)
+__global__ void k_run_heads(const uint64_t *keys, int64_t n, uint32_t *flags) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    flags[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+
+__device__ __forceinline__ int64_t bsearch_key(const uint64_t *a, int64_t n, uint64_t k) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (a[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && a[lo] == k) ? lo : -1;
+}
+
+// flags[i] = 1 if keys[i] is not in the sorted set `ref`
+__global__ void k_not_in(const uint64_t *keys, int64_t n, const uint64_t *ref, int64_t nref, uint32_t *flags) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    flags[i] = bsearch_key(ref, nref, keys[i]) < 0 ? 1u : 0u;
+}
+
+__global__ void k_compact_flagged(const uint64_t *in, int64_t n, const uint32_t *flags, const uint32_t *scan,
+                                  uint64_t *out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (flags[i]) out[scan[i]] = in[i];
+}
+
+// The root node (V:1290-1300): level `depth`, flags 1, child list Elem(1,depth,0).
+__global__ void k_root(Node *root, int depth, int3 rootpos) {
+    Node nd;
+    memset(&nd, 0, sizeof(nd));
+    nd.mLev = (uint8_t)depth;
+    nd.mFlags = 1;
+    nd.mPos[0] = rootpos.x;
+    nd.mPos[1] = rootpos.y;
+    nd.mPos[2] = rootpos.z;
+    nd.mValue[0] = nd.mValue[1] = nd.mValue[2] = -1;
+    nd.mParent = kUndefL;
+    nd.mChildList = elem(1, depth, 0);
+    *root = nd;
+}
+
+struct LevelBuild {
+    const uint64_t *base; int64_t nbase;  // sorted base keys at this level
+    const uint64_t *extra; int64_t nextra;
+    const uint64_t *pbase; int64_t npbase; // parent level
+    const uint64_t *pextra; int64_t npextra;
+    Node *nodes;
+    uint64_t *pclist;      // parent level child lists
+    int lev, depth, b;
+    int64_t range;         // node extent at this level (voxels)
+    int shift;             // log2 res(lev+1)
+    int pres;              // res(lev+1)
+    int64_t pres3;
+    int root_lo[3];        // root corner in units of this level's range (for lev == depth-1)
+    uint64_t *leaf_keys; int32_t *leaf_vals; uint32_t leaf_mask; // level 0 only
+    int32_t *status;
+};
+
+// SetupNode (V:2512-2524) for every node of one level, then the link of
+// gvdbLinkBricks (N:470-505): mParent = Elem(0,lev+1,pid) and the parent's
+// child slot (z*res+y)*res+x = Elem(0,lev,i).  Parents are found by key in
+// the parent level's sorted arrays, which is the node getParent reaches.
+__global__ void k_build_link(LevelBuild L) {
+    int64_t n = L.nbase + L.nextra;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t key = i < L.nbase ? L.base[i] : L.extra[i - L.nbase];
+    int x, y, z;
+    unpack_key(key, L.b, x, y, z);
+    Node nd;
+    memset(&nd, 0, sizeof(nd));
+    nd.mLev = (uint8_t)L.lev;
+    nd.mFlags = 1;
+    nd.mPos[0] = (int32_t)(x * L.range);
+    nd.mPos[1] = (int32_t)(y * L.range);
+    nd.mPos[2] = (int32_t)(z * L.range);
+    nd.mValue[0] = nd.mValue[1] = nd.mValue[2] = -1;
+    nd.mParent = kUndefL;
+    nd.mChildList = L.lev > 0 ? elem(1, L.lev, (uint64_t)i) : kUndefL;
+    int ox, oy, oz; // parent corner in units of this level's range
+    int64_t pid;
+    if (L.lev == L.depth - 1) {
+        pid = 0;
+        ox = L.root_lo[0];
+        oy = L.root_lo[1];
+        oz = L.root_lo[2];
+    } else {
+        int px = x >> L.shift, py = y >> L.shift, pz = z >> L.shift;
+        uint64_t pk = pack_key(px, py, pz, L.b);
+        pid = bsearch_key(L.pbase, L.npbase, pk);
+        if (pid < 0) {
+            pid = bsearch_key(L.pextra, L.npextra, pk);
+            if (pid >= 0) pid += L.npbase;
+        }
+        ox = px << L.shift;
+        oy = py << L.shift;
+        oz = pz << L.shift;
+    }
+    int lx = x - ox, ly = y - oy, lz = z - oz;
+    if (pid >= 0 && lx >= 0 && lx < L.pres && ly >= 0 && ly < L.pres && lz >= 0 && lz < L.pres) {
+        nd.mParent = elem(0, L.lev + 1, (uint64_t)pid);
+        int64_t bit = ((int64_t)lz * L.pres + ly) * L.pres + lx;
+        L.pclist[pid * L.pres3 + bit] = elem(0, L.lev, (uint64_t)i);
+        if (L.lev == 0 && hm_insert(L.leaf_keys, L.leaf_vals, L.leaf_mask, key, (int32_t)i) < 0)
+            atomicOr(L.status, kDevHashFull);
+    } else {
+        atomicOr(L.status, kDevBadIndex);
+    }
+    L.nodes[i] = nd;
+}
+
+// ---- UpdateAtlas --------------------------------------------------------
+__global__ void k_leaf_flags(const Node *leaves, int64_t n, uint32_t *flags) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    flags[i] = leaves[i].mFlags ? 1u : 0u;
+}
+
+// AtlasAlloc + getAtlasPos (A:692-715) and AssignMapping (V:2681-2689).
+__global__ void k_atlas_assign(Node *leaves, int64_t n, const uint32_t *flags, const uint32_t *slot, int sx, int sy,
+                               int tile, int apron, AtlasNode *amap, int32_t *slot_leaf, int32_t *leaf_slot) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!flags[i]) {
+        leaf_slot[i] = -1; // stale leaf keeps its old mValue, as in the reference
+        return;
+    }
+    int64_t s = slot[i];
+    int64_t a2 = (int64_t)sx * sy;
+    int bz = (int)(s / a2);
+    int64_t r = s - (int64_t)bz * a2;
+    int by = (int)(r / sx);
+    int bx = (int)(r - (int64_t)by * sx);
+    Node &nd = leaves[i];
+    nd.mValue[0] = bx * tile + apron;
+    nd.mValue[1] = by * tile + apron;
+    nd.mValue[2] = bz * tile + apron;
+    AtlasNode an;
+    an.mPos[0] = nd.mPos[0];
+    an.mPos[1] = nd.mPos[1];
+    an.mPos[2] = nd.mPos[2];
+    an.mLeafID = (int32_t)i;
+    amap[s] = an;
+    slot_leaf[s] = (int32_t)i;
+    leaf_slot[i] = (int32_t)s;
+}
+
+// 27-neighbour slot table of every active slot (offset k = (dz+1)*9 + (dy+1)*3 + (dx+1)).
+__global__ void k_nbr27(const Node *leaves, const int32_t *slot_leaf, int64_t nslots, const int32_t *leaf_slot,
+                        const uint64_t *lk, const int32_t *lv, uint32_t lmask, KeyGeom g, int32_t *nbr) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nslots * 27) return;
+    int64_t s = t / 27;
+    int k = (int)(t - s * 27);
+    int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
+    const Node &nd = leaves[slot_leaf[s]];
+    int bx = (nd.mPos[0] >> g.log2r0) + dx, by = (nd.mPos[1] >> g.log2r0) + dy, bz = (nd.mPos[2] >> g.log2r0) + dz;
+    int32_t out = -1;
+    if (bx >= g.lo[0] && bx < g.lo[0] + g.span && by >= g.lo[1] && by < g.lo[1] + g.span && bz >= g.lo[2] &&
+        bz < g.lo[2] + g.span) {
+        int32_t leaf = hm_lookup(lk, lv, lmask, pack_key(bx, by, bz, g.b));
+        if (leaf >= 0) out = leaf_slot[leaf];
+    }
+    nbr[t] = out;
+}
+
+// UpdateNeighbors (V:2527-2556): 6 face neighbours per pool leaf
+// (-x,-y,-z,+x,+y,+z), -1 when missing.
+__global__ void k_nbr6(const Node *leaves, int64_t n, const uint64_t *lk, const int32_t *lv, uint32_t lmask, KeyGeom g,
+                       int32_t *nbr) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * 6) return;
+    int64_t i = t / 6;
+    int k = (int)(t - i * 6);
+    const int dir[6][3] = {{-1, 0, 0}, {0, -1, 0}, {0, 0, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    const Node &nd = leaves[i];
+    int bx = (nd.mPos[0] >> g.log2r0) + dir[k][0], by = (nd.mPos[1] >> g.log2r0) + dir[k][1],
+        bz = (nd.mPos[2] >> g.log2r0) + dir[k][2];
+    int32_t out = -1;
+    if (bx >= g.lo[0] && bx < g.lo[0] + g.span && by >= g.lo[1] && by < g.lo[1] + g.span && bz >= g.lo[2] &&
+        bz < g.lo[2] + g.span)
+        out = hm_lookup(lk, lv, lmask, pack_key(bx, by, bz, g.b));
+    nbr[t] = out;
+}
+
+inline uint32_t next_pow2(uint64_t x) {
+    uint64_t p = 1;
+    while (p < x) p <<= 1;
+    return (uint32_t)std::min<uint64_t>(p, 1ull << 31);
+}
+
+SmallWords *host_words(Volume *v) { return reinterpret_cast<SmallWords *>(v->host_small); }
+SmallWords *dev_words(Volume *v) { return v->dev_small.as<SmallWords>(); }
+
+gvdb2_status read_words(Volume *v) {
+    GV_CUDA(v, cudaMemcpyAsync(v->host_small, v->dev_small.p, sizeof(SmallWords), cudaMemcpyDeviceToHost, v->stream));
+    GV_CUDA(v, cudaStreamSynchronize(v->stream));
+    return GVDB2_OK;
+}
+
+
+// sort + unique of a device key array in place; returns the unique count
+gvdb2_status sort_unique(Volume *v, uint64_t *keys, int64_t n, int bits, int64_t *out_n) {
+    if (n == 0) {
+        *out_n = 0;
+        return GVDB2_OK;
+    }
+    GV_TRY(radix_sort_u64(v, keys, nullptr, n, 0, bits));
+    uint32_t *flags = nullptr, *scan = nullptr;
+    uint64_t *tmp = nullptr;
+    cudaStream_t s = v->stream;
+    GV_CUDA(v, cudaMallocAsync((void **)&flags, sizeof(uint32_t) * (size_t)(2 * n + 1), s));
+    GV_CUDA(v, cudaMallocAsync((void **)&tmp, sizeof(uint64_t) * (size_t)n, s));
+    scan = flags + n;
+    k_run_heads<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(keys, n, flags);
+    gvdb2_status st = exclusive_scan_u32(v, flags, scan, n);
+    if (st == GVDB2_OK) {
+        k_compact_flagged<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(keys, n, flags, scan, tmp);
+        uint32_t un = 0;
+        cudaError_t e = cudaMemcpyAsync(&un, scan + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(keys, tmp, sizeof(uint64_t) * un, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) st = cuda_fail(v, e, "sort_unique");
+        *out_n = un;
+    }
+    cudaFreeAsync(flags, s);
+    cudaFreeAsync(tmp, s);
+    return st;
+}
+
+// out = keys \ ref (both sorted); stable
+gvdb2_status set_difference(Volume *v, const uint64_t *keys, int64_t n, const uint64_t *ref, int64_t nref,
+                            uint64_t *out, int64_t *out_n) {
+    if (n == 0) {
+        *out_n = 0;
+        return GVDB2_OK;
+    }
+    cudaStream_t s = v->stream;
+    uint32_t *flags = nullptr;
+    GV_CUDA(v, cudaMallocAsync((void **)&flags, sizeof(uint32_t) * (size_t)(2 * n + 1), s));
+    uint32_t *scan = flags + n;
+    k_not_in<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(keys, n, ref, nref, flags);
+    gvdb2_status st = exclusive_scan_u32(v, flags, scan, n);
+    if (st == GVDB2_OK) {
+        k_compact_flagged<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(keys, n, flags, scan, out);
+        uint32_t un = 0;
+        cudaError_t e = cudaMemcpyAsync(&un, scan + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_fail(v, e, "set_difference");
+        *out_n = un;
+    }
+    cudaFreeAsync(flags, s);
+    return st;
+}
+
+gvdb2_status clear_pools(Volume *v) { // Clear (V:2487-2503)
+    for (int l = 0; l < kMaxLev; l++) v->pool_cnt[l] = 0;
+    v->used_leaves = 0;
+    v->atlas_last = 0;
+    v->atlas_valid = false;
+    v->rebuild_topo = true;
+    return GVDB2_OK;
+}
+
+gvdb2_status ensure_pool(Volume *v, int lev, int64_t cnt) {
+    GV_CUDA(v, v->pool[lev].ensure(sizeof(Node) * (size_t)std::max<int64_t>(cnt, 1), v->stream));
+    if (lev > 0) GV_CUDA(v, v->clist[lev].ensure(sizeof(uint64_t) * (size_t)(std::max<int64_t>(cnt, 1) * v->res3(lev)), v->stream));
+    return GVDB2_OK;
+}
+
+// ActivateBricksGPU (+ ActivateExtraBricksGPU when radius >= 1).
+gvdb2_status full_rebuild(Volume *v, int n, float radius, const float orig[3]) {
+    cudaStream_t s = v->stream;
+    const int depth = v->depth;
+    KeyGeom g = key_geom(v);
+    if (g.span > 65536) return fail(v, GVDB2_ERR_UNSUPPORTED, "root spans more than 65536 bricks per axis");
+    const int kbits = 3 * g.b;
+    const bool do_box = radius >= 1.0f;
+
+    // size the hash sets from the bounding box (and the last rebuild)
+    int64_t est = 1;
+    for (int a = 0; a < 3; a++) est *= (int64_t)((v->posmax[a] - v->posmin[a]) / (float)v->range(0)) + 3;
+    est = std::min<int64_t>(est, (int64_t)n * (do_box ? 8 : 1) + 64);
+    est = std::max<int64_t>(est, v->lev_count[0][0] + v->lev_count[0][1]);
+    uint32_t cap = next_pow2((uint64_t)std::max<int64_t>(2 * est, 1 << 16));
+
+    int64_t nb = 0, nx = 0;
+    for (int attempt = 0; attempt < 4; attempt++) {
+        GV_CUDA(v, v->hs_keys[0].ensure(sizeof(uint64_t) * cap, s));
+        GV_CUDA(v, v->hs_keys[1].ensure(sizeof(uint64_t) * cap, s));
+        GV_CUDA(v, cudaMemsetAsync(v->hs_keys[0].p, 0xFF, sizeof(uint64_t) * cap, s));
+        if (do_box) GV_CUDA(v, cudaMemsetAsync(v->hs_keys[1].p, 0xFF, sizeof(uint64_t) * cap, s));
+        GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count, 0, sizeof(int32_t) * 8 + sizeof(int32_t), s));
+        if (n > 0)
+            k_mark_keys<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(
+                v->pos, n, make_float3(orig[0], orig[1], orig[2]), radius, 2.0f, do_box ? 1 : 0, g,
+                v->hs_keys[0].as<uint64_t>(), v->hs_keys[1].as<uint64_t>(), cap - 1, dev_words(v)->count,
+                &dev_words(v)->status);
+        GV_CUDA(v, cudaGetLastError());
+        GV_TRY(read_words(v));
+        nb = host_words(v)->count[0];
+        nx = host_words(v)->count[1];
+        bool full = (host_words(v)->status & kDevHashFull) || 2 * std::max(nb, nx) > (int64_t)cap;
+        if (!full) break;
+        if (attempt == 3) return fail(v, GVDB2_ERR_CAPACITY, "brick hash set overflow");
+        cap = next_pow2((uint64_t)cap * 4);
+    }
+    v->hs_mask = cap - 1;
+
+    // per-level sorted unique key arrays: base B[l] and box X[l]
+    for (int l = 0; l < depth; l++) {
+        GV_CUDA(v, v->lev_keys[l][0].ensure(sizeof(uint64_t) * (size_t)std::max<int64_t>(nb, 1), s));
+        GV_CUDA(v, v->lev_keys[l][1].ensure(sizeof(uint64_t) * (size_t)std::max<int64_t>(do_box ? nx : 1, 1), s));
+    }
+    GV_CUDA(v, v->tmp_a.ensure(sizeof(uint64_t) * (size_t)std::max<int64_t>(nx, 1), s));
+    GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count + 2, 0, sizeof(int32_t) * 2, s));
+    k_compact_set<<<grid_for(cap, 256, 4096), 256, 0, s>>>(v->hs_keys[0].as<uint64_t>(), cap,
+                                                           v->lev_keys[0][0].as<uint64_t>(), dev_words(v)->count + 2);
+    if (do_box)
+        k_compact_set<<<grid_for(cap, 256, 4096), 256, 0, s>>>(v->hs_keys[1].as<uint64_t>(), cap,
+                                                               v->tmp_a.as<uint64_t>(), dev_words(v)->count + 3);
+    GV_CUDA(v, cudaGetLastError());
+    int64_t nB[kMaxLev] = {0}, nX[kMaxLev] = {0}, nE[kMaxLev] = {0};
+    GV_TRY(radix_sort_u64(v, v->lev_keys[0][0].as<uint64_t>(), nullptr, nb, 0, kbits));
+    nB[0] = nb;
+    uint64_t *xkeys[kMaxLev] = {nullptr};
+    DevBuf xbuf[kMaxLev];
+    if (do_box) {
+        GV_TRY(radix_sort_u64(v, v->tmp_a.as<uint64_t>(), nullptr, nx, 0, kbits));
+        nX[0] = nx;
+        xkeys[0] = v->tmp_a.as<uint64_t>();
+    }
+    for (int l = 1; l < depth; l++) {
+        int sh = v->logdim[l];
+        uint64_t *dst = v->lev_keys[l][0].as<uint64_t>();
+        if (nB[l - 1] > 0)
+            k_parentize<<<grid_for(nB[l - 1], 256, 1ll << 31), 256, 0, s>>>(v->lev_keys[l - 1][0].as<uint64_t>(),
+                                                                           nB[l - 1], g.b, sh, dst);
+        GV_TRY(sort_unique(v, dst, nB[l - 1], kbits, &nB[l]));
+        // parents of the previous level's keys; b stays fixed for all levels
+        (void)g;
+        if (do_box) {
+            cudaError_t e = xbuf[l].ensure(sizeof(uint64_t) * (size_t)std::max<int64_t>(nX[l - 1], 1), s);
+            if (e != cudaSuccess) {
+                for (int q = 0; q < kMaxLev; q++) xbuf[q].release();
+                return cuda_fail(v, e, "box keys");
+            }
+            xkeys[l] = xbuf[l].as<uint64_t>();
+            if (nX[l - 1] > 0)
+                k_parentize<<<grid_for(nX[l - 1], 256, 1ll << 31), 256, 0, s>>>(xkeys[l - 1], nX[l - 1], g.b, sh,
+                                                                               xkeys[l]);
+            gvdb2_status st = sort_unique(v, xkeys[l], nX[l - 1], kbits, &nX[l]);
+            if (st) {
+                for (int q = 0; q < kMaxLev; q++) xbuf[q].release();
+                return st;
+            }
+        }
+    }
+    // extra keys E[l] = X[l] \ B[l], sorted (ActivateExtraBricksGPU's
+    // "not present after the base link" test)
+    for (int l = 0; l < depth; l++) {
+        nE[l] = 0;
+        if (!do_box) continue;
+        cudaError_t e = v->lev_keys[l][1].ensure(sizeof(uint64_t) * (size_t)std::max<int64_t>(nX[l], 1), s);
+        if (e != cudaSuccess) return cuda_fail(v, e, "extra keys");
+        gvdb2_status st = set_difference(v, xkeys[l], nX[l], v->lev_keys[l][0].as<uint64_t>(), nB[l],
+                                         v->lev_keys[l][1].as<uint64_t>(), &nE[l]);
+        if (st) {
+            for (int q = 0; q < kMaxLev; q++) xbuf[q].release();
+            return st;
+        }
+    }
+    for (int q = 0; q < kMaxLev; q++) xbuf[q].release();
+
+    // pools: level l < depth holds [B[l], E[l]]; the root sits at `depth`
+    for (int l = 0; l < kMaxLev; l++) v->pool_cnt[l] = 0;
+    for (int l = 0; l < depth; l++) v->pool_cnt[l] = nB[l] + nE[l];
+    v->pool_cnt[depth] = 1;
+    for (int l = 0; l <= depth; l++) {
+        GV_TRY(ensure_pool(v, l, v->pool_cnt[l]));
+        v->lev_count[l][0] = nB[l];
+        v->lev_count[l][1] = nE[l];
+        if (l > 0)
+            GV_CUDA(v, cudaMemsetAsync(v->clist[l].p, 0xFF, sizeof(uint64_t) * (size_t)(v->pool_cnt[l] * v->res3(l)), s));
+    }
+    k_root<<<1, 1, 0, s>>>(v->pool_ptr(depth), depth, make_int3(v->root_pos[0], v->root_pos[1], v->root_pos[2]));
+
+    // leaf map: level-0 key -> pool index
+    uint32_t lcap = next_pow2((uint64_t)std::max<int64_t>(2 * v->pool_cnt[0], 1 << 12));
+    GV_CUDA(v, v->leafmap_keys.ensure(sizeof(uint64_t) * lcap, s));
+    GV_CUDA(v, v->leafmap_vals.ensure(sizeof(int32_t) * lcap, s));
+    GV_CUDA(v, cudaMemsetAsync(v->leafmap_keys.p, 0xFF, sizeof(uint64_t) * lcap, s));
+    v->leafmap_mask = lcap - 1;
+    GV_CUDA(v, cudaMemsetAsync(&dev_words(v)->status, 0, sizeof(int32_t), s));
+
+    for (int l = 0; l < depth; l++) {
+        LevelBuild L;
+        L.base = v->lev_keys[l][0].as<uint64_t>();
+        L.nbase = nB[l];
+        L.extra = v->lev_keys[l][1].as<uint64_t>();
+        L.nextra = nE[l];
+        L.pbase = l + 1 < depth ? v->lev_keys[l + 1][0].as<uint64_t>() : nullptr;
+        L.npbase = l + 1 < depth ? nB[l + 1] : 0;
+        L.pextra = l + 1 < depth ? v->lev_keys[l + 1][1].as<uint64_t>() : nullptr;
+        L.npextra = l + 1 < depth ? nE[l + 1] : 0;
+        L.nodes = v->pool_ptr(l);
+        L.pclist = v->clist[l + 1].as<uint64_t>();
+        L.lev = l;
+        L.depth = depth;
+        L.b = g.b;
+        L.range = v->range(l);
+        L.shift = v->logdim[l + 1];
+        L.pres = v->res(l + 1);
+        L.pres3 = v->res3(l + 1);
+        for (int a = 0; a < 3; a++) L.root_lo[a] = (int)(v->root_pos[a] / v->range(l));
+        L.leaf_keys = v->leafmap_keys.as<uint64_t>();
+        L.leaf_vals = v->leafmap_vals.as<int32_t>();
+        L.leaf_mask = v->leafmap_mask;
+        L.status = &dev_words(v)->status;
+        int64_t cnt = nB[l] + nE[l];
+        if (cnt > 0) k_build_link<<<grid_for(cnt, 256, 1ll << 31), 256, 0, s>>>(L);
+        GV_CUDA(v, cudaGetLastError());
+    }
+    GV_TRY(read_words(v));
+    if (host_words(v)->status & kDevHashFull) return fail(v, GVDB2_ERR_CAPACITY, "leaf map overflow");
+    if (host_words(v)->status & kDevBadIndex) return fail(v, GVDB2_ERR_STATE, "node without parent in full rebuild");
+    v->used_leaves = v->pool_cnt[0];
+    return GVDB2_OK;
+}
+
+// DetermineDepth (V:821-837) with GetCoveringNode (V:2915-2931).
+int determine_depth(const Volume *v, int rootpos[3]) {
+    for (int lev = 0; lev < kMaxLev; lev++) {
+        int a[3], b[3];
+        if (lev == kMaxLev - 1) {
+            a[0] = a[1] = a[2] = b[0] = b[1] = b[2] = 0;
+        } else {
+            int64_t range = v->range(std::min(lev, v->nlev - 1));
+            for (int k = 0; k < 3; k++) {
+                int pa = (int)v->posmin[k], pb = (int)v->posmax[k];
+                a[k] = (int)(pa / range * range);
+                b[k] = (int)(pb / range * range);
+            }
+        }
+        if (a[0] == b[0] && a[1] == b[1] && a[2] == b[2]) {
+            rootpos[0] = a[0];
+            rootpos[1] = a[1];
+            rootpos[2] = a[2];
+            return lev;
+        }
+    }
+    return -1;
+}
+
+} // namespace
+
+KeyGeom key_geom(const Volume *v) {
+    KeyGeom g;
+    g.log2r0 = v->logdim[0];
+    int64_t span = v->range(v->depth) / v->range(0);
+    g.span = (int)span;
+    int64_t hi = span + std::max(v->root_pos[0], std::max(v->root_pos[1], v->root_pos[2])) / v->range(0);
+    int b = 1;
+    while ((1ll << b) < hi) b++;
+    g.b = b;
+    for (int a = 0; a < 3; a++) g.lo[a] = (int)(v->root_pos[a] / v->range(0));
+    return g;
+}
+
+gvdb2_status incremental_rebuild(Volume *v, int n, float radius, const float orig[3], bool accum);
+
+gvdb2_status sync_counts(Volume *v) {
+    GV_CUDA(v, cudaStreamSynchronize(v->stream));
+    return GVDB2_OK;
+}
+
+gvdb2_status rebuild_topology(Volume *v, int n, float radius, const float orig[3], bool accumulate, int min_depth) {
+    if (v->nlev == 0) return fail(v, GVDB2_ERR_STATE, "Configure not called");
+    if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count)))
+        return fail(v, GVDB2_ERR_ARG, "point count exceeds the position view");
+    cudaStream_t s = v->stream;
+    if (!v->dev_small.p) {
+        GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), s));
+        GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
+    }
+    // GetBoundingBox
+    int32_t init[6];
+    for (int a = 0; a < 3; a++) {
+        init[a] = 0x7F800000;            // ord(+inf)
+        init[3 + a] = (int32_t)0x807FFFFF; // ord(-inf)
+    }
+    GV_CUDA(v, cudaMemcpyAsync(dev_words(v)->bbox, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    if (n > 0)
+        k_bbox<<<std::min(grid_for(n, 256), 8 * kSmCount), 256, 0, s>>>(v->pos, n, make_float3(orig[0], orig[1], orig[2]),
+                                                                        dev_words(v)->bbox);
+    GV_CUDA(v, cudaGetLastError());
+    GV_TRY(read_words(v));
+    for (int a = 0; a < 3; a++) {
+        float lo = ord2f(host_words(v)->bbox[a]) - 1.0f, hi = ord2f(host_words(v)->bbox[3 + a]) + 2.0f;
+        v->posmin[a] = 0 > lo ? 0 : lo;
+        v->posmax[a] = 0 > hi ? 0 : hi;
+        if (!std::isfinite(v->posmin[a]) || !std::isfinite(v->posmax[a]) || v->posmax[a] > 2.0e9f)
+            return fail(v, GVDB2_ERR_DEPTH, "point extents exceed 5 levels");
+    }
+    int rootpos[3];
+    int depth = determine_depth(v, rootpos);
+    if (accumulate && depth < min_depth) depth = min_depth;
+    if (depth == 0) return fail(v, GVDB2_ERR_DEPTH, "points extents smaller than 1 brick");
+    if (depth > 5 || depth < 0 || depth >= v->nlev) return fail(v, GVDB2_ERR_DEPTH, "point extents exceed 5 levels");
+
+    v->bin_key.valid = false;
+    v->nbr6_valid = false;
+    v->topo_version++;
+    if (accumulate && !v->rebuild_topo) { // AccumulateTopology (V:1158-1178)
+        v->depth = depth;
+        return incremental_rebuild(v, n, radius, orig, true);
+    }
+    if (v->rebuild_topo) {
+        clear_pools(v);
+    } else if (depth != v->cur_depth) {
+        clear_pools(v);
+        v->rebuild_topo = true;
+        v->cur_depth = depth;
+    }
+    v->depth = depth;
+    if (v->rebuild_topo) {
+        for (int a = 0; a < 3; a++) v->root_pos[a] = rootpos[a];
+        gvdb2_status st = full_rebuild(v, n, radius, orig);
+        v->rebuild_topo = false;
+        v->atlas_valid = false;
+        return st;
+    }
+    return incremental_rebuild(v, n, radius, orig, false);
+}
+
+gvdb2_status incremental_rebuild(Volume *v, int n, float radius, const float orig[3], bool accum) {
+    (void)n;
+    (void)radius;
+    (void)orig;
+    (void)accum;
+    return fail(v, GVDB2_ERR_UNSUPPORTED, "incremental rebuild not built yet");
+}
+
+// Atlas growth along Z with content preserved by slot (AtlasResize, A:622-650).
+static gvdb2_status atlas_resize(Volume *v, int64_t bricks) {
+    int64_t layer = (int64_t)v->subdim[0] * v->subdim[1];
+    int nz = (int)std::ceil((float)bricks / (float)layer);
+    if (nz < 1) nz = 1;
+    if (nz == v->subdim[2] && v->atlas_cap > 0) return GVDB2_OK;
+    int64_t ncap = layer * nz;
+    size_t tv = (size_t)v->tile_vox();
+    for (int c = 0; c < kMaxChan; c++) {
+        if (!v->has_chan[c]) continue;
+        size_t old = (size_t)v->atlas_cap * tv * sizeof(float);
+        GV_CUDA(v, v->atlas[c].ensure((size_t)ncap * tv * sizeof(float), v->stream, true));
+        size_t now = (size_t)ncap * tv * sizeof(float);
+        if (now > old) GV_CUDA(v, cudaMemsetAsync(v->atlas[c].as<char>() + old, 0, now - old, v->stream));
+    }
+    v->subdim[2] = nz;
+    v->atlas_cap = ncap;
+    return GVDB2_OK;
+}
+
+gvdb2_status alloc_channel_storage(Volume *v, int chan) {
+    size_t bytes = (size_t)v->atlas_cap * (size_t)v->tile_vox() * sizeof(float);
+    GV_CUDA(v, v->atlas[chan].ensure(bytes, v->stream));
+    GV_CUDA(v, cudaMemsetAsync(v->atlas[chan].p, 0, bytes, v->stream));
+    return GVDB2_OK;
+}
+
+gvdb2_status update_atlas(Volume *v) {
+    if (!v->any_channel()) return fail(v, GVDB2_ERR_STATE, "no atlas channel");
+    cudaStream_t s = v->stream;
+    int64_t total = v->pool_cnt[0];
+    v->atlas_last = 0;
+    uint32_t *flags = nullptr;
+    GV_CUDA(v, cudaMallocAsync((void **)&flags, sizeof(uint32_t) * (size_t)(2 * total + 2), s));
+    uint32_t *scan = flags + total + 1;
+    if (total > 0) k_leaf_flags<<<grid_for(total, 256, 1ll << 31), 256, 0, s>>>(v->pool_ptr(0), total, flags);
+    gvdb2_status st = exclusive_scan_u32(v, flags, scan, total);
+    uint32_t nflag = 0;
+    if (st == GVDB2_OK) {
+        cudaError_t e = cudaMemcpyAsync(&nflag, scan + total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_fail(v, e, "update_atlas count");
+    }
+    if (st == GVDB2_OK && (v->used_leaves > v->atlas_cap || (int64_t)nflag > v->atlas_cap))
+        st = atlas_resize(v, std::max<int64_t>(v->used_leaves, nflag));
+    if (st == GVDB2_OK) {
+        cudaError_t e = v->amap.ensure(sizeof(AtlasNode) * (size_t)v->atlas_cap, s);
+        if (e == cudaSuccess) e = v->slot_leaf.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(v->atlas_cap, 1), s);
+        if (e == cudaSuccess) e = v->leaf_slot.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(total, 1), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(v->amap.p, 0xFF, sizeof(AtlasNode) * (size_t)v->atlas_cap, s);
+        if (e != cudaSuccess) st = cuda_fail(v, e, "update_atlas alloc");
+    }
+    if (st == GVDB2_OK && total > 0) {
+        k_atlas_assign<<<grid_for(total, 256, 1ll << 31), 256, 0, s>>>(
+            v->pool_ptr(0), total, flags, scan, v->subdim[0], v->subdim[1], v->tile_res(), v->apron,
+            v->amap.as<AtlasNode>(), v->slot_leaf.as<int32_t>(), v->leaf_slot.as<int32_t>());
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(v, e, "k_atlas_assign");
+    }
+    cudaFreeAsync(flags, s);
+    if (st != GVDB2_OK) return st;
+    v->atlas_last = nflag;
+    // 27-neighbour slot table for the splat/apron kernels
+    GV_CUDA(v, v->nbr27.ensure(sizeof(int32_t) * 27 * (size_t)std::max<int64_t>(nflag, 1), s));
+    if (nflag > 0) {
+        KeyGeom g = key_geom(v);
+        k_nbr27<<<grid_for(27 * (int64_t)nflag, 256, 1ll << 31), 256, 0, s>>>(
+            v->pool_ptr(0), v->slot_leaf.as<int32_t>(), nflag, v->leaf_slot.as<int32_t>(), v->leafmap_keys.as<uint64_t>(),
+            v->leafmap_vals.as<int32_t>(), v->leafmap_mask, g, v->nbr27.as<int32_t>());
+        GV_CUDA(v, cudaGetLastError());
+    }
+    v->atlas_valid = true;
+    v->bin_key.valid = false;
+    return GVDB2_OK;
+}
+
+gvdb2_status update_neighbors(Volume *v) {
+    int64_t n = v->pool_cnt[0];
+    if (n == 0) return fail(v, GVDB2_ERR_STATE, "no topology");
+    GV_CUDA(v, v->nbr6.ensure(sizeof(int32_t) * 6 * (size_t)n, v->stream));
+    KeyGeom g = key_geom(v);
+    k_nbr6<<<grid_for(6 * n, 256, 1ll << 31), 256, 0, v->stream>>>(v->pool_ptr(0), n, v->leafmap_keys.as<uint64_t>(),
+                                                                    v->leafmap_vals.as<int32_t>(), v->leafmap_mask, g,
+                                                                    v->nbr6.as<int32_t>());
+    GV_CUDA(v, cudaGetLastError());
+    v->nbr6_valid = true;
+    return GVDB2_OK;
+}
+
+gvdb2_status clear_channel(Volume *v, int chan) {
+    if (chan < 0 || chan >= kMaxChan || !v->has_chan[chan]) return fail(v, GVDB2_ERR_ARG, "bad channel");
+    GV_CUDA(v, cudaMemsetAsync(v->atlas[chan].p, 0, (size_t)v->atlas_cap * v->tile_vox() * sizeof(float), v->stream));
+    return GVDB2_OK;
+}
+
+
+} // namespace gvdb2

@@ -1,0 +1,167 @@
+/*
+ * gvdb2.h -- C-ABI of the B200-native point -> sparse-volume pipeline.
+ *
+ * Each entry point replaces the nvdb::VolumeGVDB method (or kernel launch
+ * sequence) cited beside it; paths are relative to the gvdb-voxels project:
+ *   V  = source/gvdb_library/src/gvdb_volume_gvdb.cpp
+ *   VH = source/gvdb_library/src/gvdb_volume_gvdb.h
+ *
+ * Conventions
+ *  - Every call returns a gvdb2_status; nothing exits, traps or prints.
+ *    gvdb2_last_error() gives a message for the last failure of a volume.
+ *  - Point views and gather outputs are DEVICE pointers (the reference's
+ *    SetDataGPU contract, V:4872-4880): element i of a view lives at
+ *    base + i*stride_bytes + offset_bytes.  Views are non-owning.
+ *  - All work is issued on the volume's stream (gvdb2_set_stream); calls
+ *    that return a host value (counts, lengths) synchronise that stream.
+ *  - The atlas is linear device memory: per channel, one contiguous tile of
+ *    (res+2*apron)^3 floats per atlas slot, z-major (x fastest).  Node
+ *    pools keep the 64-byte nvdb::Node layout and 8*res^3-byte child lists.
+ */
+#ifndef GVDB2_H
+#define GVDB2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define GVDB2_API __declspec(dllexport)
+#else
+#define GVDB2_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int gvdb2_status;
+#define GVDB2_OK 0
+#define GVDB2_ERR_ARG 1          /* invalid argument */
+#define GVDB2_ERR_DEPTH 2        /* point extents smaller than one brick or deeper than 5 levels (V:1187-1194) */
+#define GVDB2_ERR_STATE 3        /* call order violated (e.g. gather before topology) */
+#define GVDB2_ERR_UNSUPPORTED 4  /* configuration outside what this build implements */
+#define GVDB2_ERR_NOMEM 5        /* device allocation failed */
+#define GVDB2_ERR_CUDA 6         /* a CUDA runtime call failed */
+#define GVDB2_ERR_CAPACITY 7     /* a device-side capacity check fired; nothing was written out of bounds */
+#define GVDB2_ERR_NOT_AVAILABLE 8 /* CUDA device or kernel image not available */
+
+#define GVDB2_T_FLOAT 3          /* channel type T_FLOAT (gvdb_types.h) */
+
+#define GVDB2_KERNEL_TENT1 1     /* trilinear tent, radius 1 voxel, voxel centres at i+0.5 */
+#define GVDB2_KERNEL_CUBIC2 2    /* cubic B-spline, radius 2 voxels */
+
+#define GVDB2_OPT_DETERMINISTIC 1 /* 1: kernel splats accumulate in 64-bit fixed point (bit-reproducible) */
+
+typedef struct gvdb2_volume gvdb2_volume;
+
+typedef struct gvdb2_points_view {
+    const void *base;     /* device pointer (NULL = absent) */
+    int64_t count;
+    int32_t stride_bytes; /* DataPtr::stride */
+    int32_t offset_bytes; /* DataPtr::subdim.x */
+} gvdb2_points_view;
+
+typedef struct gvdb2_info {
+    int32_t depth;            /* root level (DetermineDepth, V:821-837) */
+    int32_t top_level;        /* VDBInfo::top_lev (V:3952-3965) */
+    int32_t num_levels;       /* configured levels (5) */
+    int32_t apron;
+    int64_t pool_count[10];   /* getNumTotalNodes per level */
+    int64_t used_leaves;      /* getNumUsedNodes(0) */
+    int64_t atlas_slots;      /* atlas lastEle (active bricks) */
+    int64_t atlas_capacity;   /* bricks the atlas holds */
+    int32_t atlas_subdim[3];  /* atlas brick counts per axis */
+    int32_t res[10];          /* getRes per level */
+    int64_t range[10];        /* getRange per level */
+    float posmin[3];          /* mPosMin after GetBoundingBox (V:5450-5460) */
+    float posmax[3];
+    int32_t root_pos[3];
+    int32_t tile_res;         /* res0 + 2*apron */
+} gvdb2_info;
+
+/* ---- lifetime (SetCudaDevice VH:325 / V:240-334, Initialize VH:326 / V:2320-2361) ---- */
+GVDB2_API gvdb2_status gvdb2_create(gvdb2_volume **out, int device);
+GVDB2_API gvdb2_status gvdb2_destroy(gvdb2_volume *v);
+GVDB2_API const char *gvdb2_last_error(const gvdb2_volume *v);
+GVDB2_API gvdb2_status gvdb2_set_stream(gvdb2_volume *v, void *cuda_stream);
+GVDB2_API gvdb2_status gvdb2_synchronize(gvdb2_volume *v);
+GVDB2_API gvdb2_status gvdb2_set_option(gvdb2_volume *v, int option, int value);
+
+/* ---- configuration ---- */
+GVDB2_API gvdb2_status gvdb2_configure(gvdb2_volume *v, int q4, int q3, int q2, int q1, int q0);   /* Configure, VH:387 / V:2364-2377 */
+GVDB2_API gvdb2_status gvdb2_set_channel_default(gvdb2_volume *v, int cx, int cy, int cz);       /* SetChannelDefault, VH:390 */
+GVDB2_API gvdb2_status gvdb2_add_channel(gvdb2_volume *v, int chan, int dtype, int apron);       /* AddChannel, VH:392 / V:2437-2453 */
+
+/* ---- points (SetPoints VH:541 / V:4900-4908) ---- */
+GVDB2_API gvdb2_status gvdb2_set_points(gvdb2_volume *v, gvdb2_points_view pos, gvdb2_points_view vel, gvdb2_points_view clr);
+
+/* ---- topology ---- */
+GVDB2_API gvdb2_status gvdb2_request_full_rebuild(gvdb2_volume *v, int flag);                     /* RequestFullRebuild, VH:432 */
+GVDB2_API gvdb2_status gvdb2_rebuild_topology(gvdb2_volume *v, int n, float radius, const float orig[3]);  /* RebuildTopology, V:1181-1218 */
+GVDB2_API gvdb2_status gvdb2_accumulate_topology(gvdb2_volume *v, int n, float radius, const float orig[3], int min_depth); /* AccumulateTopology, V:1158-1178 */
+GVDB2_API gvdb2_status gvdb2_finish_topology(gvdb2_volume *v, int commit, int bounds);            /* FinishTopology, V:1579-1593 */
+GVDB2_API gvdb2_status gvdb2_update_atlas(gvdb2_volume *v);                                       /* UpdateAtlas, V:2630-2704 */
+GVDB2_API gvdb2_status gvdb2_clear_channel(gvdb2_volume *v, int chan);                            /* ClearChannel, V:1596-1603 */
+GVDB2_API gvdb2_status gvdb2_update_neighbors(gvdb2_volume *v);                                   /* UpdateNeighbors, V:2527-2556 */
+
+/* ---- point insertion ---- */
+GVDB2_API gvdb2_status gvdb2_insert_points(gvdb2_volume *v, int n, const float trans[3], int prefix);          /* InsertPoints, V:5219-5267 */
+GVDB2_API gvdb2_status gvdb2_insert_points_subcell(gvdb2_volume *v, int subcell, int n, float radius,
+                                         const float trans[3], int *len);                    /* InsertPointsSubcell, V:4971-5092 */
+
+/* ---- reference-mode splat / gathers / apron ---- */
+GVDB2_API gvdb2_status gvdb2_scatter_density(gvdb2_volume *v, int n, float radius, float amp, const float trans[3],
+                                   int expand, int avg_color);                               /* ScatterDensity, V:5624-5660 */
+GVDB2_API gvdb2_status gvdb2_gather_density(gvdb2_volume *v, int subcell, int n, float radius, const float trans[3],
+                                  int *len, int chan_density, int chan_clr, int accum);       /* GatherDensity, V:5318-5344 */
+GVDB2_API gvdb2_status gvdb2_gather_level_set(gvdb2_volume *v, int subcell, int n, float radius, const float trans[3],
+                                    int *len, int chan_levelset, int chan_clr, int accum);    /* GatherLevelSet, V:5348-5373 */
+GVDB2_API gvdb2_status gvdb2_scatter_reduce_level_set(gvdb2_volume *v, int subcell, int n, float radius,
+                                            const float trans[3], int *len, int chan_levelset,
+                                            int chan_clr, int accum); /* same operation as GatherLevelSet, V:5348-5373 */
+GVDB2_API gvdb2_status gvdb2_update_apron(gvdb2_volume *v, int chan, float boundval);             /* UpdateApron, V:4411-4457 (chan<0: all) */
+GVDB2_API gvdb2_status gvdb2_update_apron_faces(gvdb2_volume *v, int chan);                       /* UpdateApronFaces, V:4461-4496 */
+
+/* ---- kernel splats (no reference counterpart: the reference has no tent /
+ * cubic scatter, no grid->point gather and no adjoints) ---- */
+/* channel chans[c] := sum_p weight_p * attr_c(p) * W(v + 0.5 - x_p) on the
+ * interior voxels of every active brick; weight.base == NULL uses
+ * weight_const; attrs[c].base == NULL means attr 1.  Aprons are left for
+ * gvdb2_update_apron. */
+GVDB2_API gvdb2_status gvdb2_scatter_kernel(gvdb2_volume *v, int kernel, int n, const float trans[3],
+                                  gvdb2_points_view weight, float weight_const,
+                                  const gvdb2_points_view *attrs, const int *chans, int nch);
+/* out[p*out_stride + c] := sum_v G_chans[c][v] * W(v + 0.5 - x_p) (0 for
+ * points outside every active brick); out is a device float pointer. */
+GVDB2_API gvdb2_status gvdb2_gather_kernel(gvdb2_volume *v, int kernel, int n, const float trans[3], const int *chans,
+                                 int nch, float *out, int64_t out_stride);
+/* Adjoint of gvdb2_scatter_kernel (ScatterDensityBackward): given dL/dG in
+ * channels grad_chans, writes per point grad_pos[3], grad_weight and
+ * grad_attr[nch] (device float pointers, row-major; any may be NULL). */
+GVDB2_API gvdb2_status gvdb2_scatter_kernel_backward(gvdb2_volume *v, int kernel, int n, const float trans[3],
+                                           gvdb2_points_view weight, float weight_const,
+                                           const gvdb2_points_view *attrs, int nch, const int *grad_chans,
+                                           float *grad_pos, float *grad_weight, float *grad_attr);
+/* Adjoint of gvdb2_gather_kernel (GatherDensityBackward): given dL/dout
+ * (device, grad_out[p*nch + c]), sets channels grad_chans := dL/dG on the
+ * interiors of active bricks (when grad_chans != NULL) and grad_pos[p*3+k]. */
+GVDB2_API gvdb2_status gvdb2_gather_kernel_backward(gvdb2_volume *v, int kernel, int n, const float trans[3],
+                                          const int *chans, int nch, const float *grad_out,
+                                          const int *grad_chans, float *grad_pos);
+
+/* ---- inspection (host copies; synchronise the stream) ---- */
+GVDB2_API gvdb2_status gvdb2_get_info(gvdb2_volume *v, gvdb2_info *out);
+GVDB2_API gvdb2_status gvdb2_copy_nodes(gvdb2_volume *v, int lev, void *host, int64_t max_nodes);            /* getNode / pool 0 (64-byte nodes) */
+GVDB2_API gvdb2_status gvdb2_copy_childlists(gvdb2_volume *v, int lev, uint64_t *host, int64_t max_entries); /* pool 1 child lists */
+GVDB2_API gvdb2_status gvdb2_copy_atlas(gvdb2_volume *v, int chan, float *host, int64_t max_floats);        /* used slots' tiles */
+GVDB2_API gvdb2_status gvdb2_copy_atlas_map(gvdb2_volume *v, void *host, int64_t max_entries);              /* 16-byte {int3 pos; int leaf} */
+GVDB2_API gvdb2_status gvdb2_copy_neighbors(gvdb2_volume *v, int32_t *host, int64_t max_entries);           /* 6 per pool leaf (-x,-y,-z,+x,+y,+z) */
+GVDB2_API gvdb2_status gvdb2_copy_point_nodes(gvdb2_volume *v, int32_t *pnode, int32_t *poff, int64_t n,
+                                    int32_t *gcnt, int64_t ngcnt);                                /* InsertPoints results */
+GVDB2_API gvdb2_status gvdb2_copy_subcells(gvdb2_volume *v, int32_t *cnt, int32_t *nid, int32_t *pos3, int64_t max_subcells);
+GVDB2_API gvdb2_status gvdb2_atlas_device_ptr(gvdb2_volume *v, int chan, float **dev_ptr);                 /* device view of a channel */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

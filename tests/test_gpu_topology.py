@@ -1,0 +1,163 @@
+"""GPU parity of the topology path against the oracle: bit-exact node
+pools, child lists, atlas map and point insertion (through the C-ABI)."""
+import numpy as np
+import pytest
+
+from _helpers import assert_nodes_equal, make_oracle, shell_points
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_volume(gvdb2_mod, pts, cfg=(3, 3, 3, 3, 3), chans=(0,), apron=1):
+    import torch
+    v = gvdb2_mod.VolumeGVDB(0)
+    v.Configure(*cfg)
+    for c in chans:
+        v.AddChannel(c, gvdb2_mod.T_FLOAT, apron)
+    t = torch.from_numpy(np.ascontiguousarray(pts, np.float32)).cuda()
+    v.SetPoints(t)
+    v._pts = t
+    return v
+
+
+def compare_topology(v, o):
+    inf = v.info()
+    d = o.depth()
+    assert inf.depth == d
+    assert inf.top_level == o.top_level()
+    a, b = o.bbox()
+    assert np.array_equal(np.array(inf.posmin[:], np.float32), a)
+    assert np.array_equal(np.array(inf.posmax[:], np.float32), b)
+    for lev in range(5):
+        assert inf.pool_count[lev] == o.pool_count(lev), f"pool count level {lev}"
+    assert inf.used_leaves == o.used_leaves()
+    for lev in range(d + 1):
+        assert_nodes_equal(v.nodes(lev), o.nodes(lev), lev)
+        if lev >= 1:
+            assert np.array_equal(v.childlists(lev), o.childlists(lev)), f"child lists level {lev}"
+
+
+@pytest.mark.parametrize("cfg,radius,n", [
+    ((3, 3, 3, 3, 3), 2.0, 200_000),
+    ((3, 3, 3, 3, 3), 0.0, 50_000),
+    ((3, 3, 3, 3, 3), 1.0, 50_000),
+    ((3, 3, 3, 4, 4), 2.0, 100_000),
+    ((3, 3, 3, 3, 2), 1.5, 30_000),
+])
+def test_full_rebuild_bit_exact(gvdb2_mod, oracle_mod, cfg, radius, n):
+    pts = shell_points(n, seed=0)
+    o = make_oracle(oracle_mod, cfg)
+    assert o.rebuild_topology(pts, radius) == 0
+    o.update_atlas()
+    v = gpu_volume(gvdb2_mod, pts, cfg)
+    v.RebuildTopology(n, radius)
+    v.UpdateAtlas()
+    compare_topology(v, o)
+    inf = v.info()
+    assert inf.atlas_slots == o.atlas_slots()
+    assert tuple(inf.atlas_subdim) == o.atlas_subdim()
+    assert np.array_equal(v.atlas_map(), o.atlas_map())
+
+
+def test_translation_and_negative_points(gvdb2_mod, oracle_mod):
+    rng = np.random.default_rng(21)
+    pts = shell_points(40_000, seed=1, r_in=30, r_out=34, center=(40.0, 40.0, 40.0))
+    pts[:500] -= 60.0  # some points land at negative coordinates (lev-255 keys)
+    orig = (3.25, 1.0, 0.5)
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, 2.0, orig) == 0
+    o.update_atlas()
+    v = gpu_volume(gvdb2_mod, pts)
+    v.RebuildTopology(len(pts), 2.0, orig)
+    v.UpdateAtlas()
+    compare_topology(v, o)
+    del rng
+
+
+def test_second_rebuild_is_full_again(gvdb2_mod, oracle_mod):
+    # mCurrDepth starts at -1, so the second call also takes the full path
+    pts = shell_points(30_000, seed=2)
+    o = make_oracle(oracle_mod)
+    v = gpu_volume(gvdb2_mod, pts)
+    for _ in range(2):
+        assert o.rebuild_topology(pts, 2.0) == 0
+        v.RebuildTopology(len(pts), 2.0)
+    o.update_atlas()
+    v.UpdateAtlas()
+    compare_topology(v, o)
+
+
+def test_depth_errors(gvdb2_mod):
+    pts = np.full((100, 3), 3.0, np.float32)  # extents inside one brick
+    v = gpu_volume(gvdb2_mod, pts)
+    with pytest.raises(gvdb2_mod.GvdbError) as e:
+        v.RebuildTopology(100, 0.0)
+    assert e.value.status == 2
+
+
+def test_empty_point_set(gvdb2_mod):
+    v = gpu_volume(gvdb2_mod, np.zeros((1, 3), np.float32))
+    with pytest.raises(gvdb2_mod.GvdbError):
+        v.RebuildTopology(0, 2.0)  # empty extents: smaller than one brick
+
+
+def test_insert_points(gvdb2_mod, oracle_mod):
+    pts = shell_points(100_000, seed=3)
+    pts[::1000, 2] = 1.0e10  # NOHIT
+    pts[1::1000] += 500.0    # outside every brick
+    o = make_oracle(oracle_mod)
+    keep = np.ones(len(pts), bool)
+    keep[::1000] = False
+    keep[1::1000] = False
+    good = pts[keep]  # the topology is built without the NOHIT and far-away points
+    assert o.rebuild_topology(good, 2.0) == 0
+    o.update_atlas()
+    v = gpu_volume(gvdb2_mod, good)
+    v.RebuildTopology(len(good), 2.0)
+    v.UpdateAtlas()
+    import torch
+    t = torch.from_numpy(pts).cuda()
+    v.SetPoints(t)
+    v.InsertPoints(len(pts), (0, 0, 0), prefix=True)
+    pnode, poff, gcnt = v.point_nodes(len(pts))
+    opnode, _, ogcnt = o.insert_points(pts)
+    assert np.array_equal(pnode, opnode)
+    assert np.array_equal(gcnt, ogcnt)
+    # poff is an atomic order inside each leaf: a permutation of 0..count-1
+    ok = pnode >= 0
+    order = np.lexsort((poff[ok], pnode[ok]))
+    leaves = pnode[ok][order]
+    starts = np.concatenate([[0], np.cumsum(np.bincount(leaves, minlength=len(gcnt)))[:-1]])
+    expect = np.arange(len(leaves)) - starts[leaves]
+    assert np.array_equal(poff[ok][order], expect)
+
+
+def test_neighbor_table(gvdb2_mod, oracle_mod):
+    pts = shell_points(50_000, seed=4)
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, 2.0) == 0
+    o.update_atlas()
+    o.update_neighbors()
+    v = gpu_volume(gvdb2_mod, pts)
+    v.RebuildTopology(len(pts), 2.0)
+    v.UpdateAtlas()
+    v.UpdateNeighbors()
+    assert np.array_equal(v.neighbors(), o.neighbors())
+
+
+def test_subcells(gvdb2_mod, oracle_mod):
+    pts = shell_points(60_000, seed=5)
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, 2.0) == 0
+    o.update_atlas()
+    v = gpu_volume(gvdb2_mod, pts)
+    v.RebuildTopology(len(pts), 2.0)
+    v.UpdateAtlas()
+    ln = v.InsertPointsSubcell(4, len(pts), 2.0)
+    oln = o.insert_points_subcell(4, pts, 2.0)
+    assert ln == oln
+    cnt, nid, pos = v.subcells(o.used_leaves() * 8)
+    ocnt, onid, opos = o.subcells()
+    assert np.array_equal(cnt, ocnt)
+    assert np.array_equal(nid, onid)
+    assert np.array_equal(pos, opos)

@@ -1,0 +1,322 @@
+"""CPU checks of the oracle itself: independent numpy restatements of the
+topology rules, conservation and partition-of-unity of the kernel splats,
+apron self-consistency and finite-difference checks of the adjoints."""
+import numpy as np
+import pytest
+
+from _helpers import UNDEF64, apron_self_consistent, interior, make_oracle, rel_err, shell_points
+
+
+def _levels_numpy(pts, radius, depth, ranges, rootpos, root_range, kmax=2.0):
+    """Base and box node sets per level, restated from gvdbCalcBrickId
+    (P:352-382) and gvdbCalcExtraBrickId (P:467-512) with the root clamp."""
+    w = pts.astype(np.float32)
+    ok = np.all(w >= 0, axis=1)
+    w = w[ok]
+    base, box = [], []
+    iw = w.astype(np.int32)
+    bmin = (iw.astype(np.float32) - np.float32(radius)).astype(np.int32)
+    bmax = (iw.astype(np.float32) + np.float32(kmax * radius)).astype(np.int32)
+    for lev in range(depth):
+        r = ranges[lev]
+        b = set(map(tuple, (iw // r).tolist()))
+        base.append(b)
+        x = set()
+        if radius >= 1:
+            lo = np.maximum(bmin, 0) // r
+            hi = bmax // r
+            rlo = np.asarray(rootpos) // r
+            rhi = (np.asarray(rootpos) + root_range) // r - 1
+            lo = np.maximum(lo, rlo)
+            hi = np.minimum(hi, rhi)
+            for l, h in zip(lo, hi):
+                for xx in range(l[0], h[0] + 1):
+                    for yy in range(l[1], h[1] + 1):
+                        for zz in range(l[2], h[2] + 1):
+                            x.add((xx, yy, zz))
+        box.append(x - b)
+    return base, box
+
+
+@pytest.mark.parametrize("radius", [0.0, 2.0])
+def test_full_rebuild_node_sets(oracle_mod, radius):
+    pts = shell_points(20000, seed=5)
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, radius) == 0
+    d = o.depth()
+    assert d == 2
+    ranges = [o.range(l) for l in range(5)]
+    root = o.nodes(d)[0]
+    base, extra = _levels_numpy(pts, radius, d, ranges, root["mPos"], ranges[d])
+    for lev in range(d):
+        nd = o.nodes(lev)
+        keys = [tuple(p // ranges[lev]) for p in nd["mPos"]]
+        nb = len(base[lev])
+        assert keys[:nb] == sorted(base[lev]), f"level {lev} base keys"
+        assert keys[nb:] == sorted(extra[lev]), f"level {lev} extra keys"
+        assert np.all(nd["mFlags"] == 1)
+        assert np.all(nd["mLev"] == lev)
+
+
+def test_links_consistent(oracle_mod):
+    pts = shell_points(20000, seed=6)
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, 2.0) == 0
+    d = o.depth()
+    for lev in range(d):
+        nd = o.nodes(lev)
+        par = o.nodes(lev + 1)
+        cl = o.childlists(lev + 1)
+        res, prange = o.res(lev + 1), o.range(lev + 1)
+        for i, n in enumerate(nd):
+            pid = int(n["mParent"]) >> 16
+            assert (int(n["mParent"]) >> 8) & 0xFF == lev + 1
+            p = par[pid]
+            loc = (n["mPos"] - p["mPos"]) * res // prange
+            assert np.all((loc >= 0) & (loc < res))
+            bit = (loc[2] * res + loc[1]) * res + loc[0]
+            assert int(cl[pid, bit]) == (i << 16) | (lev << 8)
+        # every set child slot points back at a node of this level
+        setslots = cl[cl != UNDEF64]
+        assert len(setslots) == len(nd)
+
+
+def _dense_reference(pts, kernel, active_bricks, res0, weights=None):
+    """Dense FP64 restatement of the kernel scatter: every voxel of an active
+    brick receives sum_p w_p W(v + 0.5 - x_p)."""
+    out = {}
+    for i, x in enumerate(pts.astype(np.float64)):
+        if tuple((x.astype(np.int64)) // res0) not in active_bricks:
+            continue
+        u = x - 0.5
+        b = np.floor(u)
+        t = u - b
+        if kernel == 1:
+            first = b.astype(int)
+            w = [np.array([1 - tt, tt]) for tt in t]
+        else:
+            first = b.astype(int) - 1
+            w = []
+            for tt in t:
+                s = 1 - tt
+                w.append(np.array([s ** 3 / 6, (3 * tt ** 3 - 6 * tt ** 2 + 4) / 6,
+                                   (-3 * tt ** 3 + 3 * tt ** 2 + 3 * tt + 1) / 6, tt ** 3 / 6]))
+        wt = 1.0 if weights is None else float(weights[i])
+        k = len(w[0])
+        for a in range(k):
+            for bb in range(k):
+                for c in range(k):
+                    v = (first[0] + a, first[1] + bb, first[2] + c)
+                    if tuple(np.array(v) // res0) in active_bricks:
+                        out[v] = out.get(v, 0.0) + wt * w[0][a] * w[1][bb] * w[2][c]
+    return out
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_scatter_matches_dense_numpy(oracle_mod, kernel):
+    pts = shell_points(600, seed=7, r_in=20, r_out=24, center=(40.0, 40.0, 40.0))
+    wts = np.random.default_rng(1).uniform(0.5, 1.5, len(pts)).astype(np.float32)
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, 2.0) == 0
+    o.update_atlas()
+    o.scatter_kernel(kernel, pts, [0], weight=wts)
+    nodes = o.nodes(0)
+    res0 = o.res(0)
+    active = {tuple(p // res0) for p in nodes["mPos"]}
+    ref = _dense_reference(pts, kernel, active, res0, wts)
+    tiles = o.atlas(0)
+    got = {}
+    a = o.apron()
+    for s, p in enumerate(nodes["mPos"]):
+        it = interior(tiles[s:s + 1], a)[0]
+        for (z, y, x), val in np.ndenumerate(it):
+            if val != 0.0:
+                got[(p[0] + x, p[1] + y, p[2] + z)] = val
+    keys = sorted(set(ref) | set(got))
+    g = np.array([got.get(k, 0.0) for k in keys])
+    r = np.array([ref.get(k, 0.0) for k in keys])
+    assert rel_err(g, r) < 1e-12
+    # mass: every stencil lies in active bricks (extra-brick box covers it)
+    assert abs(g.sum() - wts.astype(np.float64).sum()) < 1e-8 * wts.sum()
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_gather_partition_of_unity(oracle_mod, kernel):
+    pts = shell_points(2000, seed=8, r_in=20, r_out=24, center=(40.0, 40.0, 40.0))
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, 2.0) == 0
+    o.update_atlas()
+    tiles = o.atlas(0)
+    # set every interior voxel of every active brick to 3.0 through the
+    # public path: scatter of zero weight then direct fill is not exposed,
+    # so use the FP64 atlas pointer.
+    import ctypes
+    s, t = tiles.shape[0], tiles.shape[1]
+    buf = (ctypes.c_double * (s * t ** 3)).from_address(o.L.orc_atlas(o.h, 0))
+    arr = np.frombuffer(buf, np.float64).reshape(s, t, t, t)
+    arr[:] = 3.0
+    g = o.gather_kernel(kernel, pts, [0])
+    assert np.allclose(g, 3.0, rtol=0, atol=1e-12)
+
+
+def test_apron_copies(oracle_mod):
+    pts = shell_points(3000, seed=9, r_in=20, r_out=24, center=(40.0, 40.0, 40.0))
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, 2.0) == 0
+    o.update_atlas()
+    o.scatter_kernel(2, pts, [0])
+    o.update_apron(0, 0.0)
+    tiles = o.atlas(0).astype(np.float32)
+    pos = o.nodes(0)["mPos"]
+    n = apron_self_consistent(tiles, None, [tuple(p) for p in pos], o.res(0), o.apron())
+    assert n == len(pos) * (10 ** 3 - 8 ** 3)
+
+
+def test_apron_faces_only_touch_faces(oracle_mod):
+    pts = shell_points(3000, seed=10, r_in=20, r_out=24, center=(40.0, 40.0, 40.0))
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, 2.0) == 0
+    o.update_atlas()
+    o.scatter_kernel(1, pts, [0])
+    before = o.atlas(0)
+    o.update_neighbors()
+    o.update_apron_faces(0)
+    after = o.atlas(0)
+    changed = np.argwhere(before != after)
+    for s, z, y, x in changed:
+        edge = sum(int(c in (0, 9)) for c in (x, y, z))
+        assert edge == 1, "UpdateApronFaces writes face voxels only"
+    o.update_apron(0)
+    full = o.atlas(0)
+    # face voxels agree with the full apron update
+    mask = np.zeros((10, 10, 10), bool)
+    for c in range(1, 9):
+        for d in range(1, 9):
+            mask[0, c, d] = mask[9, c, d] = mask[c, 0, d] = mask[c, 9, d] = mask[c, d, 0] = mask[c, d, 9] = True
+    nb = o.neighbors()
+    for s in range(after.shape[0]):
+        if np.all(nb[s] >= 0):
+            assert np.array_equal(after[s][mask], full[s][mask])
+
+
+def test_distfunc_negative_weights(oracle_mod):
+    # a single point far from its voxel corner gets a negative weight (P:516-523)
+    pts = np.array([[20.9, 20.9, 20.9]] + [[12.5 + i, 12.5, 12.5] for i in range(20)], np.float32)
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, 0.0) == 0
+    o.update_atlas()
+    o.clear_channel(0)
+    pnode, poff, gcnt = o.insert_points(pts)
+    assert gcnt.sum() == len(pts)
+    o.scatter_density(pts, 1.0, 1.0, (0, 0, 0), False, pnode)
+    tiles = o.atlas(0)
+    assert tiles.min() < 0
+
+
+def test_incremental_invariants(oracle_mod):
+    import gvdb2.workloads as wl
+    p, vel = wl.dam_block(sites=(32, 8, 32), origin=(40.0, 40.0, 40.0), seed=11)
+    o = make_oracle(oracle_mod, chans=(0,))
+    for step in range(4):
+        assert o.rebuild_topology(p, 2.0) == 0
+        nd = o.nodes(0)
+        linked = nd["mParent"] != UNDEF64
+        assert np.all(nd["mFlags"][linked] == 1)
+        assert np.all(nd["mFlags"][~linked] == 0)
+        assert o.used_leaves() == int(linked.sum())
+        for x in p[::97]:
+            leaf = o.leaf_of_point(*x)
+            assert leaf >= 0 and nd["mFlags"][leaf] == 1
+        p = p + np.array([6.0, 0.0, 0.0], np.float32) + np.float32(0.2) * vel  # drift empties trailing bricks
+    assert o.pool_count(0) > o.used_leaves(), "incremental steps leave stale leaves in the pool"
+
+
+def test_subcell_lists(oracle_mod):
+    pts = shell_points(500, seed=12, r_in=20, r_out=24, center=(40.0, 40.0, 40.0))
+    o = make_oracle(oracle_mod)
+    assert o.rebuild_topology(pts, 2.0) == 0
+    o.update_atlas()
+    ln = o.insert_points_subcell(4, pts, 2.0)
+    cnt, nid, pos = o.subcells()
+    assert cnt.sum() == ln
+    # each point listed once per existing subcell of its box (P:286-291)
+    expect = 0
+    leaves = {tuple(p) for p in o.nodes(0)["mPos"]}
+    for x in pts:
+        mn = (np.floor(x - 2.0).astype(int) // 4) * 4
+        mx = (np.floor(x + 3.0).astype(int) // 4) * 4
+        for a in range(mn[0], mx[0] + 1, 4):
+            for b in range(mn[1], mx[1] + 1, 4):
+                for c in range(mn[2], mx[2] + 1, 4):
+                    if (a // 8 * 8, b // 8 * 8, c // 8 * 8) in leaves:
+                        expect += 1
+    assert expect == ln
+    o.gather_density(4, 1.0, 0)
+    o.gather_level_set(4, 1.0, 0, accum=False)
+
+
+def _loss_and_grad(o, kernel, pts, wts, cvox):
+    o.scatter_kernel(kernel, pts, [0], weight=wts)
+    tiles = o.atlas(0)
+    return float(np.sum(interior(tiles, o.apron()) * cvox))
+
+
+def test_scatter_adjoint_fd(oracle_mod):
+    pts = shell_points(300, seed=13, r_in=20, r_out=24, center=(40.0, 40.0, 40.0)).astype(np.float32)
+    wts = np.random.default_rng(2).uniform(0.5, 1.5, len(pts)).astype(np.float32)
+    o = make_oracle(oracle_mod, chans=(0, 1))
+    assert o.rebuild_topology(pts, 3.0) == 0
+    o.update_atlas()
+    s = o.atlas_slots()
+    rng = np.random.default_rng(3)
+    cvox = rng.standard_normal((s, 8, 8, 8))
+    # channel 1 holds dL/dG = cvox on interiors
+    import ctypes
+    t = o.tile_res()
+    buf = (ctypes.c_double * (s * t ** 3)).from_address(o.L.orc_atlas(o.h, 1))
+    g1 = np.frombuffer(buf, np.float64).reshape(s, t, t, t)
+    g1[:] = 0
+    g1[:, 1:9, 1:9, 1:9] = cvox
+    gpos, gw, ga = o.scatter_kernel_backward(2, pts, [0], [1], weight=wts)
+    h = 1e-3
+    for i in rng.choice(len(pts), 12, replace=False):
+        for k in range(3):
+            pp = pts.copy()
+            pm = pts.copy()
+            pp[i, k] += h
+            pm[i, k] -= h
+            fd = (_loss_and_grad(o, 2, pp, wts, cvox) - _loss_and_grad(o, 2, pm, wts, cvox)) / (
+                float(pp[i, k]) - float(pm[i, k]))
+            assert abs(fd - gpos[i, k]) <= 1e-4 * max(1.0, abs(gpos[:, k]).max()), (i, k, fd, gpos[i, k])
+        ww = wts.copy()
+        ww[i] += 0.25
+        fdw = (_loss_and_grad(o, 2, pts, ww, cvox) - _loss_and_grad(o, 2, pts, wts, cvox)) / (
+            float(ww[i]) - float(wts[i]))
+        assert abs(fdw - gw[i]) < 1e-9 * max(1.0, abs(gw).max())
+
+
+def test_gather_adjoint_fd(oracle_mod):
+    pts = shell_points(200, seed=14, r_in=20, r_out=24, center=(40.0, 40.0, 40.0)).astype(np.float32)
+    o = make_oracle(oracle_mod, chans=(0, 1))
+    assert o.rebuild_topology(pts, 3.0) == 0
+    o.update_atlas()
+    o.scatter_kernel(2, pts, [0])
+    o.update_apron(0)
+    rng = np.random.default_rng(4)
+    dout = rng.standard_normal((len(pts), 1))
+    gpos = o.gather_kernel_backward(2, pts, [0], dout, grad_chans=[1])
+    f = lambda q: float(np.sum(o.gather_kernel(2, q, [0]) * dout))
+    h = 1e-3
+    for i in rng.choice(len(pts), 10, replace=False):
+        for k in range(3):
+            pp = pts.copy()
+            pm = pts.copy()
+            pp[i, k] += h
+            pm[i, k] -= h
+            fd = (f(pp) - f(pm)) / (float(pp[i, k]) - float(pm[i, k]))
+            assert abs(fd - gpos[i, k]) <= 1e-4 * max(1.0, abs(gpos).max())
+    # dL/dG: <dL/dG, G'> equals <dout, gather(G')> for a field G'
+    gg = interior(o.atlas(1), o.apron())
+    lhs = float(np.sum(gg * interior(o.atlas(0), o.apron())))
+    rhs = float(np.sum(dout * o.gather_kernel(2, pts, [0])))
+    assert abs(lhs - rhs) < 1e-9 * max(1.0, abs(rhs))
