@@ -38,6 +38,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--incremental", action="store_true", help="reference state machine instead of full rebuilds")
+    ap.add_argument("--quick", action="store_true", help="timed steps only (no baseline, e2e or launch count)")
     return ap.parse_args()
 
 
@@ -261,7 +262,7 @@ def run_ours(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     pos, vel = wl.dam_block(sites=SITES)
     cpu = None
-    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not (a.no_cpu_baseline or a.quick):
         cpu = cpu_baseline(pos, vel)
 
     pipe = Pipeline(local, pos, vel, full_rebuild=not a.incremental)
@@ -294,6 +295,12 @@ def run_ours(a):
     clk = clocks.stop()
     ms = max_over_ranks(e0.elapsed_time(e1))
     value = n * a.steps * ws / (ms / 1e3)
+
+    if a.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
+                              "ms_per_step": ms / a.steps, "quick": True}), flush=True)
+        return 0
 
     # per-stage intervals (CUDA events on the launching stream), averaged
     geo = pipe.geometry()

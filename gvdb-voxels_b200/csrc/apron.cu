@@ -18,22 +18,29 @@ namespace gvdb2 {
 
 namespace {
 
-__global__ void __launch_bounds__(256) k_apron(float *chan, const int32_t *nbr27, int res, int apron, int tile,
+struct ApronChans {
+    float *chan[kMaxChan];
+    int nch;
+};
+
+// One CTA per slot; every channel of the call in one pass.
+__global__ void __launch_bounds__(256) k_apron(ApronChans C, const int32_t *nbr27, int res, int apron, int tile,
                                                int64_t tvox, float boundval) {
     const int64_t slot = blockIdx.x;
-    float *self = chan + slot * tvox;
-    const int32_t *nb27 = nbr27 + slot * 27;
+    __shared__ int32_t nbs[27];
+    if (threadIdx.x < 27) nbs[threadIdx.x] = nbr27[slot * 27 + threadIdx.x];
+    __syncthreads();
     for (int t = threadIdx.x; t < tvox; t += blockDim.x) {
-        int x = t % tile, y = (t / tile) % tile, z = t / (tile * tile);
-        int lx = x - apron, ly = y - apron, lz = z - apron;
-        int dx = floor_div(lx, res), dy = floor_div(ly, res), dz = floor_div(lz, res);
+        const int x = t % tile, y = (t / tile) % tile, z = t / (tile * tile);
+        const int lx = x - apron, ly = y - apron, lz = z - apron;
+        const int dx = lx < 0 ? -1 : (lx >= res ? 1 : 0), dy = ly < 0 ? -1 : (ly >= res ? 1 : 0),
+                  dz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
         if ((dx | dy | dz) == 0) continue; // interior voxel
-        int32_t nb = nb27[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
-        float val = boundval;
-        if (nb >= 0)
-            val = chan[(int64_t)nb * tvox +
-                       ((int64_t)(lz - dz * res + apron) * tile + (ly - dy * res + apron)) * tile + (lx - dx * res + apron)];
-        self[t] = val;
+        const int32_t nb = nbs[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
+        const int64_t src = (int64_t)nb * tvox +
+                            ((int64_t)(lz - dz * res + apron) * tile + (ly - dy * res + apron)) * tile +
+                            (lx - dx * res + apron);
+        for (int c = 0; c < C.nch; c++) C.chan[c][slot * tvox + t] = nb >= 0 ? C.chan[c][src] : boundval;
     }
 }
 
@@ -67,17 +74,20 @@ __global__ void __launch_bounds__(256) k_apron_faces(float *chan, const int32_t 
 gvdb2_status update_apron(Volume *v, int chan, float boundval) {
     if (v->apron == 0) return GVDB2_OK; // V:4421
     if (!v->atlas_valid) return fail(v, GVDB2_ERR_STATE, "UpdateAtlas must follow the topology rebuild");
+    ApronChans C;
+    C.nch = 0;
     for (int c = 0; c < kMaxChan; c++) {
         if (chan >= 0 && c != chan) continue;
         if (!v->has_chan[c]) {
             if (chan >= 0) return fail(v, GVDB2_ERR_ARG, "bad channel");
             continue;
         }
-        if (v->atlas_last == 0) continue;
-        k_apron<<<(unsigned)v->atlas_last, 256, 0, v->stream>>>(v->atlas[c].as<float>(), v->nbr27.as<int32_t>(), v->res(0),
-                                                                v->apron, v->tile_res(), v->tile_vox(), boundval);
-        GV_CUDA(v, cudaGetLastError());
+        C.chan[C.nch++] = v->atlas[c].as<float>();
     }
+    if (v->atlas_last == 0 || C.nch == 0) return GVDB2_OK;
+    k_apron<<<(unsigned)v->atlas_last, 256, 0, v->stream>>>(C, v->nbr27.as<int32_t>(), v->res(0), v->apron,
+                                                            v->tile_res(), v->tile_vox(), boundval);
+    GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
 

@@ -86,7 +86,7 @@ struct Volume {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
-    int deterministic = 0;
+    int deterministic = 0; // stable binning: kernel splats reproduce bit for bit
 
     // configuration (Configure, V:2364-2434)
     int nlev = 0;
@@ -152,6 +152,7 @@ struct Volume {
         PointsView pos{};
         float trans[3] = {0, 0, 0};
         uint64_t topo = 0;
+        bool det = false;
     } bin_key;
 
     // subcells (InsertPointsSubcell)

@@ -88,6 +88,15 @@ __global__ void k_bin_count(PointsView pos, int64_t n, float3 trans, LeafLookup 
     }
 }
 
+// keys for the stable (deterministic) binning: bin id, unbinned last
+__global__ void k_bin_keys(const int32_t *pbin, int64_t n, uint64_t *keys, int32_t *vals) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int32_t b = pbin[i];
+    keys[i] = b >= 0 ? (uint64_t)b : 0xFFFFFFFFull;
+    vals[i] = (int32_t)i;
+}
+
 __global__ void k_bin_fill(const int32_t *pbin, const int32_t *prank, int64_t n, const uint32_t *off, int32_t *perm) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -159,6 +168,7 @@ __global__ void k_sc_visit(ScArgs A, uint32_t *cnt, const uint32_t *cap, const u
                 } else {
                     uint32_t o = atomicAdd(&cnt[idx], 1u);
                     if (o >= cap[idx]) {
+                        atomicSub(&cnt[idx], 1u); // the list keeps its counted length
                         atomicOr(status, kDevCapacity);
                         continue;
                     }
@@ -221,7 +231,8 @@ gvdb2_status insert_points(Volume *v, int n, const float trans[3], int prefix) {
 
 gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     Volume::BinKey &k = v->bin_key;
-    if (k.valid && k.kernel == kernel && k.n == n && k.topo == v->topo_version && k.pos.base == v->pos.base &&
+    if (k.valid && k.kernel == kernel && k.n == n && k.topo == v->topo_version && k.det == (v->deterministic != 0) &&
+        k.pos.base == v->pos.base &&
         k.pos.stride == v->pos.stride && k.pos.offset == v->pos.offset && k.trans[0] == trans[0] &&
         k.trans[1] == trans[1] && k.trans[2] == trans[2])
         return GVDB2_OK;
@@ -250,12 +261,22 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
         GV_CUDA(v, cudaGetLastError());
     }
     GV_TRY(exclusive_scan_u32(v, v->bin_cnt.as<uint32_t>(), v->bin_off.as<uint32_t>(), nbins));
-    if (n > 0) {
+    if (n > 0 && v->deterministic) {
+        // stable counting sort: a radix sort of (bin, point index) keeps each
+        // bin's points in index order, independent of atomic timing
+        uint64_t *keys = nullptr;
+        GV_CUDA(v, cudaMallocAsync((void **)&keys, sizeof(uint64_t) * (size_t)n, s));
+        k_bin_keys<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pbin.as<int32_t>(), n, keys, v->perm.as<int32_t>());
+        gvdb2_status st = radix_sort_u64(v, keys, v->perm.as<int32_t>(), n, 0, 32);
+        cudaFreeAsync(keys, s);
+        GV_TRY(st);
+    } else if (n > 0) {
         k_bin_fill<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pbin.as<int32_t>(), v->prank.as<int32_t>(), n,
                                                                v->bin_off.as<uint32_t>(), v->perm.as<int32_t>());
         GV_CUDA(v, cudaGetLastError());
     }
     k.valid = true;
+    k.det = v->deterministic != 0;
     k.kernel = kernel;
     k.n = n;
     k.topo = v->topo_version;

@@ -146,121 +146,321 @@ __device__ __forceinline__ void neighbour_range(const SplatArgs &S, int64_t slot
     end = S.bin_off[base + xhi + 1];
 }
 
-template <int KERNEL, typename Acc>
-__device__ __forceinline__ void acc_add(Acc *a, float v);
-template <>
-__device__ __forceinline__ void acc_add<GVDB2_KERNEL_TENT1, float>(float *a, float v) { atomicAdd(a, v); }
-template <>
-__device__ __forceinline__ void acc_add<GVDB2_KERNEL_CUBIC2, float>(float *a, float v) { atomicAdd(a, v); }
-template <>
-__device__ __forceinline__ void acc_add<GVDB2_KERNEL_TENT1, unsigned long long>(unsigned long long *a, float v) {
-    atomicAdd(a, (unsigned long long)__float2ll_rn(v * 4294967296.0f));
-}
-template <>
-__device__ __forceinline__ void acc_add<GVDB2_KERNEL_CUBIC2, unsigned long long>(unsigned long long *a, float v) {
-    atomicAdd(a, (unsigned long long)__float2ll_rn(v * 4294967296.0f));
-}
-__device__ __forceinline__ float acc_value(float a) { return a; }
-__device__ __forceinline__ float acc_value(unsigned long long a) {
-    return (float)((double)(long long)a * (1.0 / 4294967296.0));
-}
-
-// One CTA per atlas slot.  Acc = float (default) or 64-bit fixed point
-// (deterministic: integer addition is associative, so the result does not
-// depend on the order of the shared-memory atomics).
-template <int KERNEL, typename Acc>
-__global__ void __launch_bounds__(256) k_scatter_tile(SplatArgs S) {
-    using T = Taps<KERNEL>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int res = S.res0, res3 = res * res * res;
-    Acc *acc = reinterpret_cast<Acc *>(smem_raw);
-    __shared__ uint32_t r_beg[kRangeSlots], r_pre[kRangeSlots + 1];
-    __shared__ uint32_t warp_tot[9];
-    const int64_t slot = blockIdx.x;
-
-    for (int i = threadIdx.x; i < S.nch * res3; i += blockDim.x) acc[i] = Acc(0);
-    // range table + exclusive prefix of range lengths
-    uint32_t len = 0;
-    if (threadIdx.x < kRangeSlots) {
-        uint32_t b, e;
-        neighbour_range(S, slot, threadIdx.x, b, e);
-        r_beg[threadIdx.x] = b;
-        len = e - b;
+// Block-wide exclusive scan of one value per thread (warp_tot: 33 words).
+__device__ __forceinline__ uint32_t block_scan_excl(uint32_t x, uint32_t *warp_tot, uint32_t &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
     }
-    {
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        uint32_t x = len;
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nw ? warp_tot[lane] : 0u;
+        uint32_t wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
         }
-        if (lane == 31) warp_tot[warp] = x;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t run = 0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
-                uint32_t t = warp_tot[w];
-                warp_tot[w] = run;
-                run += t;
-            }
-            warp_tot[8] = run;
-        }
-        __syncthreads();
-        if (threadIdx.x < kRangeSlots) r_pre[threadIdx.x] = warp_tot[warp] + x - len;
-        if (threadIdx.x == 0) r_pre[kRangeSlots] = warp_tot[8];
-        __syncthreads();
+        if (lane < nw) warp_tot[lane] = wi - w;
+        if (lane == 31) warp_tot[32] = wi;
     }
-    const uint32_t total = r_pre[kRangeSlots];
+    __syncthreads();
+    uint32_t ex = warp_tot[warp] + inc - x;
+    total = warp_tot[32];
+    __syncthreads();
+    return ex;
+}
+
+// Per-channel max |weight * attr| over all points (bounds the fixed-point
+// scale of k_scatter_fixed).  out[c] holds the float bits (>= 0 orders as int).
+template <int NCH>
+__global__ void k_absmax(SplatArgs S, int64_t n, int32_t *out) {
+    float m[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) m[c] = 0.0f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float wt = fabsf(S.has_weight ? load_f1(S.weight, i) : S.wconst);
+#pragma unroll
+        for (int c = 0; c < NCH; c++) m[c] = fmaxf(m[c], ((S.attr_mask >> c) & 1) ? wt * fabsf(load_f1(S.attr[c], i)) : wt);
+    }
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        float x = m[c];
+        for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(out + c, __float_as_int(x));
+    }
+}
+
+// Default scatter: one CTA per atlas slot accumulates its 8^3 interior in
+// shared memory from its own points and the boundary regions of its 26
+// neighbours, then writes the interior once with coalesced stores.  Every
+// (point, voxel) pair is added exactly once, by the CTA owning the voxel.
+//
+// Accumulation is fixed point in two int32 words per voxel: a contribution
+// v becomes x = rint(v * 2^s) (64-bit), split into hi = x >> L and
+// lo = x & (2^L - 1), each added with a native shared-memory integer atomic
+// (B200 runs float shared atomics as compare-and-swap loops, integer ones in
+// hardware).  L = 31 - ceil(log2(records + 1)) keeps the lo sums below 2^31;
+// s is chosen so that records * max|a| * 2^s < 2^(29 + L), which bounds the
+// hi sums below 2^30.  Integer sums do not depend on the order of the
+// atomics, so the result is bit-reproducible run to run; each contribution
+// is rounded once (to float, as a float splat would) and the sum is exact.
+constexpr int kAtomicThreads = 256;
+constexpr int kAccPlane = 72; // 8x8 plane padded by 8 words: z-neighbours fall in other banks
+
+template <int KERNEL, int NCH>
+__global__ void __launch_bounds__(kAtomicThreads, 6) k_scatter_fixed(SplatArgs S, const int32_t *absmax) {
+    using T = Taps<KERNEL>;
+    constexpr int N = T::N, RES = 8, ACC = RES * kAccPlane;
+    __shared__ int32_t acc_hi[NCH * ACC], acc_lo[NCH * ACC];
+    __shared__ uint32_t r_beg[kRangeSlots], r_pre[kRangeSlots + 1];
+    __shared__ uint32_t wtot[33];
+    const int64_t slot = blockIdx.x;
+    for (int i = threadIdx.x; i < NCH * ACC; i += blockDim.x) acc_hi[i] = acc_lo[i] = 0;
+    uint32_t b = 0, e = 0;
+    if (threadIdx.x < kRangeSlots) neighbour_range(S, slot, threadIdx.x, b, e);
+    uint32_t total;
+    const uint32_t ex = block_scan_excl(e - b, wtot, total); // ends with a barrier
+    if (threadIdx.x < kRangeSlots) {
+        r_beg[threadIdx.x] = b;
+        r_pre[threadIdx.x] = ex;
+    }
+    __syncthreads();
+    const int L = 31 - (32 - __clz((int)total + 1));
+    __shared__ float scale_s[NCH];
+    float scale[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        const float bound = (float)total * __int_as_float(absmax[c]);
+        int ex2 = 0;
+        frexpf(bound, &ex2); // bound < 2^ex2
+        scale[c] = bound > 0.0f ? ldexpf(1.0f, 29 + L - ex2) : 0.0f;
+        if (threadIdx.x == 0) scale_s[c] = scale[c];
+    }
     const Node &nd = S.leaves[S.slot_leaf[slot]];
     const int ox = nd.mPos[0], oy = nd.mPos[1], oz = nd.mPos[2];
-
+    const long long lmask = (1ll << L) - 1;
     for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
-        int lo = 0, hi = kRangeSlots - 1; // last r with r_pre[r] <= j
+        int lo = 0, hi = kRangeSlots - 1; // last range with r_pre <= j
         while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
+            const int mid = (lo + hi + 1) >> 1;
             if (r_pre[mid] <= j) lo = mid;
             else hi = mid - 1;
         }
-        int32_t pidx = S.perm[r_beg[lo] + (j - r_pre[lo])];
-        float3 p = load_f3(S.pos, pidx);
-        float w[3] = {p.x + S.trans.x, p.y + S.trans.y, p.z + S.trans.z};
-        float wt = S.has_weight ? load_f1(S.weight, pidx) : S.wconst;
-        float amt[kMaxSplatChan];
+        const int32_t p = S.perm[r_beg[lo] + (j - r_pre[lo])];
+        const float3 q = load_f3(S.pos, p);
+        float wx[N], wy[N], wz[N];
+        const int fx = T::eval(q.x + S.trans.x, wx) - ox;
+        const int fy = T::eval(q.y + S.trans.y, wy) - oy;
+        const int fz = T::eval(q.z + S.trans.z, wz) - oz;
+        const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
+        float amt[NCH];
 #pragma unroll
-        for (int c = 0; c < kMaxSplatChan; c++)
-            if (c < S.nch) amt[c] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], pidx) : wt;
-        float wx[T::N], wy[T::N], wz[T::N];
-        int fx = T::eval(w[0], wx) - ox, fy = T::eval(w[1], wy) - oy, fz = T::eval(w[2], wz) - oz;
+        for (int c = 0; c < NCH; c++) amt[c] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt;
 #pragma unroll
-        for (int tz = 0; tz < T::N; tz++) {
-            int lz = fz + tz;
-            if (lz < 0 || lz >= res) continue;
+        for (int c = 0; c < NCH; c++) amt[c] *= scale[c];
+        // z taps in a rolled loop (the weights rotate through registers) keep
+        // the unrolled body small enough for the instruction cache
+#pragma unroll 1
+        for (int tz = 0; tz < N; tz++) {
+            const int lz = fz + tz;
+            const float wzt = wz[0];
 #pragma unroll
-            for (int ty = 0; ty < T::N; ty++) {
-                int ly = fy + ty;
-                if (ly < 0 || ly >= res) continue;
-                float wyz = wy[ty] * wz[tz];
-                int row = (lz * res + ly) * res;
+            for (int k = 0; k + 1 < N; k++) wz[k] = wz[k + 1];
+            if ((unsigned)lz >= (unsigned)RES) continue;
 #pragma unroll
-                for (int tx = 0; tx < T::N; tx++) {
-                    int lx = fx + tx;
-                    if (lx < 0 || lx >= res) continue;
-                    float wgt = wx[tx] * wyz;
+            for (int ty = 0; ty < N; ty++) {
+                const int ly = fy + ty;
+                if ((unsigned)ly >= (unsigned)RES) continue;
+                const float wyz = wy[ty] * wzt;
+                const int row = lz * kAccPlane + ly * RES;
 #pragma unroll
-                    for (int c = 0; c < kMaxSplatChan; c++)
-                        if (c < S.nch) acc_add<KERNEL, Acc>(&acc[c * res3 + row + lx], amt[c] * wgt);
+                for (int tx = 0; tx < N; tx++) {
+                    const int lx = fx + tx;
+                    if ((unsigned)lx >= (unsigned)RES) continue;
+                    const float w = wx[tx] * wyz;
+#pragma unroll
+                    for (int c = 0; c < NCH; c++) {
+                        const long long xv = __float2ll_rn(amt[c] * w);
+                        atomicAdd(&acc_hi[c * ACC + row + lx], (int)(xv >> L));
+                        atomicAdd(&acc_lo[c * ACC + row + lx], (int)(xv & lmask));
+                    }
                 }
             }
         }
     }
     __syncthreads();
     const int a = S.apron, tl = S.tile;
-    for (int i = threadIdx.x; i < S.nch * res3; i += blockDim.x) {
-        int c = i / res3, v = i - c * res3;
-        int lx = v % res, ly = (v / res) % res, lz = v / (res * res);
-        S.chan[c][slot * S.tvox + ((int64_t)(lz + a) * tl + (ly + a)) * tl + (lx + a)] = acc_value(acc[i]);
+    for (int i = threadIdx.x; i < NCH * RES * RES * RES; i += blockDim.x) {
+        const int c = i >> 9, v = i & 511;
+        const int lx = v & 7, ly = (v >> 3) & 7, lz = v >> 6;
+        const int k = c * ACC + lz * kAccPlane + ly * RES + lx;
+        const long long sum = ((long long)acc_hi[k] << L) + (long long)acc_lo[k];
+        const float sc = scale_s[c];
+        const float val = sc > 0.0f ? (float)((double)sum / (double)sc) : 0.0f;
+        if (c < S.nch) S.chan[c][slot * S.tvox + ((int64_t)(lz + a) * tl + (ly + a)) * tl + (lx + a)] = val;
     }
+}
+
+constexpr int kScatterThreads = 512; // one thread per interior voxel of an 8^3 brick
+constexpr int kScatterRes = 8;
+
+// Shared-memory bytes of k_scatter_tile for a record capacity `cap`.
+__host__ __device__ constexpr size_t scatter_smem_bytes(int ntaps, int nch, int cap) {
+    return (size_t)cap * (3 * ntaps + nch + 1) * 4 + (size_t)cap * 6 +
+           (size_t)((kScatterRes + ntaps - 1) * (kScatterRes + ntaps - 1) * (kScatterRes + ntaps - 1) + 1) * 4;
+}
+
+// Scatter as a gather over shared memory: one CTA per atlas slot, one
+// thread per interior voxel.  The CTA stages the records of every point
+// whose stencil reaches the brick (its own points and the boundary regions
+// of its 26 neighbours): per-axis tap weights, weighted attributes and the
+// point index.  Records are counting-sorted by the stencil's first tap
+// (a cell of (8+N-1)^3) and each cell's records are ordered by point index.
+// A voxel then sums the N^3 cells whose stencils cover it in a fixed order:
+// no atomics on the accumulators, and the sum order does not depend on the
+// order in which points were binned (bit-reproducible while a brick's
+// records fit one chunk; the deterministic option also makes the binning
+// stable so multi-chunk bricks reproduce too).
+template <int KERNEL, int NCH>
+__global__ void __launch_bounds__(kScatterThreads, 3) k_scatter_tile(SplatArgs S, int cap) {
+    using T = Taps<KERNEL>;
+    constexpr int N = T::N, RES = kScatterRes, CA = RES + N - 1, C3 = CA * CA * CA;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *wgt = reinterpret_cast<float *>(smem_raw); // [3*N][cap]
+    float *att = wgt + 3 * N * cap;                    // [NCH][cap]
+    int32_t *pid = reinterpret_cast<int32_t *>(att + NCH * cap);
+    uint16_t *cellof = reinterpret_cast<uint16_t *>(pid + cap);
+    uint16_t *order = cellof + cap;
+    uint32_t *coff = reinterpret_cast<uint32_t *>(order + cap); // [C3 + 1]
+    uint8_t *tx0 = reinterpret_cast<uint8_t *>(coff + C3 + 1); // first x tap (cell coordinate)
+    __shared__ uint32_t r_beg[kRangeSlots], r_pre[kRangeSlots + 1];
+    __shared__ uint32_t wtot[33];
+    const int64_t slot = blockIdx.x;
+
+    uint32_t b = 0, e = 0;
+    if (threadIdx.x < kRangeSlots) neighbour_range(S, slot, threadIdx.x, b, e);
+    uint32_t total;
+    uint32_t ex = block_scan_excl(e - b, wtot, total);
+    if (threadIdx.x < kRangeSlots) {
+        r_beg[threadIdx.x] = b;
+        r_pre[threadIdx.x] = ex;
+    }
+    if (threadIdx.x == 0) r_pre[kRangeSlots] = total;
+    const Node &nd = S.leaves[S.slot_leaf[slot]];
+    const int ox = nd.mPos[0], oy = nd.mPos[1], oz = nd.mPos[2];
+    const int vx = threadIdx.x & 7, vy = (threadIdx.x >> 3) & 7, vz = threadIdx.x >> 6;
+    float acc[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) acc[c] = 0.0f;
+
+    for (uint32_t base = 0; base < total; base += cap) {
+        const int cnt = (int)min((uint32_t)cap, total - base);
+        for (int i = threadIdx.x; i <= C3; i += blockDim.x) coff[i] = 0;
+        __syncthreads();
+        // stage records
+        for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+            const uint32_t j = base + r;
+            int lo = 0, hi = kRangeSlots - 1; // last range with r_pre <= j
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (r_pre[mid] <= j) lo = mid;
+                else hi = mid - 1;
+            }
+            const int32_t p = S.perm[r_beg[lo] + (j - r_pre[lo])];
+            const float3 q = load_f3(S.pos, p);
+            float wx[N], wy[N], wz[N];
+            const int tx = T::eval(q.x + S.trans.x, wx) - ox + N - 1;
+            const int ty = T::eval(q.y + S.trans.y, wy) - oy + N - 1;
+            const int tz = T::eval(q.z + S.trans.z, wz) - oz + N - 1;
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                wgt[(0 * N + k) * cap + r] = wx[k];
+                wgt[(1 * N + k) * cap + r] = wy[k];
+                wgt[(2 * N + k) * cap + r] = wz[k];
+            }
+            const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
+#pragma unroll
+            for (int c = 0; c < NCH; c++) att[c * cap + r] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt;
+            pid[r] = p;
+            const bool ok = tx >= 0 && tx < CA && ty >= 0 && ty < CA && tz >= 0 && tz < CA;
+            const int cell = ok ? (tz * CA + ty) * CA + tx : C3;
+            cellof[r] = (uint16_t)cell;
+            tx0[r] = (uint8_t)tx;
+            if (ok) atomicAdd(&coff[cell], 1u);
+        }
+        __syncthreads();
+        // exclusive scan of the cell counts: thread t owns cells [t*K, t*K+K)
+        {
+            constexpr int K = (C3 + kScatterThreads - 1) / kScatterThreads;
+            uint32_t loc[K], sum = 0;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                int i = threadIdx.x * K + k;
+                loc[k] = i < C3 ? coff[i] : 0u;
+                sum += loc[k];
+            }
+            uint32_t tot;
+            uint32_t run = block_scan_excl(sum, wtot, tot);
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                int i = threadIdx.x * K + k;
+                if (i < C3) coff[i] = run;
+                run += loc[k];
+            }
+        }
+        __syncthreads();
+        // place; afterwards coff[c] is the end of cell c (start = coff[c-1])
+        for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+            const int cell = cellof[r];
+            if (cell < C3) order[atomicAdd(&coff[cell], 1u)] = (uint16_t)r;
+        }
+        __syncthreads();
+        // order each cell's records by point index
+        for (int c = threadIdx.x; c < C3; c += blockDim.x) {
+            const int s0 = c ? (int)coff[c - 1] : 0, s1 = (int)coff[c];
+            for (int k = s0 + 1; k < s1; k++) {
+                const uint16_t rk = order[k];
+                const int32_t pk = pid[rk];
+                int m = k - 1;
+                while (m >= s0 && pid[order[m]] > pk) {
+                    order[m + 1] = order[m];
+                    m--;
+                }
+                order[m + 1] = rk;
+            }
+        }
+        __syncthreads();
+        // this thread's voxel sums the records whose stencils cover it.  For
+        // fixed (dz, dy) the N cells of x offsets 0..N-1 are adjacent in the
+        // sorted order, so each row is one contiguous range of records.
+#pragma unroll 1
+        for (int dz = 0; dz < N; dz++) {
+#pragma unroll 1
+            for (int dy = 0; dy < N; dy++) {
+                const int chi = ((vz - dz + N - 1) * CA + (vy - dy + N - 1)) * CA + (vx + N - 1);
+                const int clo = chi - (N - 1);
+                const int s0 = clo ? (int)coff[clo - 1] : 0, s1 = (int)coff[chi];
+                for (int k = s0; k < s1; k++) {
+                    const int r = order[k];
+                    const int dx = vx + N - 1 - tx0[r];
+                    const float w = wgt[(0 * N + dx) * cap + r] * wgt[(1 * N + dy) * cap + r] * wgt[(2 * N + dz) * cap + r];
+#pragma unroll
+                    for (int c = 0; c < NCH; c++) acc[c] = fmaf(att[c * cap + r], w, acc[c]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    const int a = S.apron, tl = S.tile;
+    const int64_t at = slot * S.tvox + ((int64_t)(vz + a) * tl + (vy + a)) * tl + (vx + a);
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+        if (c < S.nch) S.chan[c][at] = acc[c];
 }
 
 // ---------------------------------------------------------------------
@@ -291,67 +491,72 @@ struct GatherArgs {
     int64_t tvox;
 };
 
-template <int KERNEL, int MODE>
+template <int KERNEL, int MODE, int NCH>
 __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
     using T = Taps<KERNEL>;
     constexpr int H = T::N / 2;
+    constexpr int N = T::N;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *tile = reinterpret_cast<float *>(smem_raw);
+    __shared__ int32_t nbs[27];
     const int res = G.res0, ht = res + 2 * H, ht3 = ht * ht * ht;
     const int64_t slot = blockIdx.x;
     const int a = G.apron, tl = G.tile;
+    if (threadIdx.x < 27) nbs[threadIdx.x] = G.nbr27[slot * 27 + threadIdx.x];
+    __syncthreads();
     // halo tile from the interiors of this brick and its neighbours
-    for (int i = threadIdx.x; i < G.nch * ht3; i += blockDim.x) {
-        int c = i / ht3, v = i - c * ht3;
-        int lx = v % ht - H, ly = (v / ht) % ht - H, lz = v / (ht * ht) - H;
-        int dx = floor_div(lx, res), dy = floor_div(ly, res), dz = floor_div(lz, res);
-        int32_t nb = G.nbr27[slot * 27 + (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
-        float val = 0.0f;
-        if (nb >= 0)
-            val = G.chan[c][(int64_t)nb * G.tvox +
-                            ((int64_t)(lz - dz * res + a) * tl + (ly - dy * res + a)) * tl + (lx - dx * res + a)];
-        tile[i] = val;
+    for (int i = threadIdx.x; i < ht3; i += blockDim.x) {
+        const int lx = i % ht - H, ly = (i / ht) % ht - H, lz = i / (ht * ht) - H;
+        const int dx = lx < 0 ? -1 : (lx >= res ? 1 : 0), dy = ly < 0 ? -1 : (ly >= res ? 1 : 0),
+                  dz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
+        const int32_t nb = nbs[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
+        const int64_t off = (int64_t)nb * G.tvox +
+                            ((int64_t)(lz - dz * res + a) * tl + (ly - dy * res + a)) * tl + (lx - dx * res + a);
+#pragma unroll
+        for (int c = 0; c < NCH; c++) tile[c * ht3 + i] = nb >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
     }
     __syncthreads();
     const Node &nd = G.leaves[G.slot_leaf[slot]];
     const int ox = nd.mPos[0] - H, oy = nd.mPos[1] - H, oz = nd.mPos[2] - H;
     const uint32_t beg = G.bin_off[slot * 27], end = G.bin_off[slot * 27 + 27];
     for (uint32_t j = beg + threadIdx.x; j < end; j += blockDim.x) {
-        int32_t pidx = G.perm[j];
-        float3 p = load_f3(G.pos, pidx);
-        float w[3] = {p.x + G.trans.x, p.y + G.trans.y, p.z + G.trans.z};
-        float wx[T::N], wy[T::N], wz[T::N], dx[T::N], dy[T::N], dz[T::N];
+        const int32_t pidx = G.perm[j];
+        const float3 p = load_f3(G.pos, pidx);
+        float wx[N], wy[N], wz[N], dx[N], dy[N], dz[N];
         int fx, fy, fz;
         if (MODE == kFwd) {
-            fx = T::eval(w[0], wx) - ox;
-            fy = T::eval(w[1], wy) - oy;
-            fz = T::eval(w[2], wz) - oz;
+            fx = T::eval(p.x + G.trans.x, wx) - ox;
+            fy = T::eval(p.y + G.trans.y, wy) - oy;
+            fz = T::eval(p.z + G.trans.z, wz) - oz;
         } else {
-            fx = T::eval_d(w[0], wx, dx) - ox;
-            fy = T::eval_d(w[1], wy, dy) - oy;
-            fz = T::eval_d(w[2], wz, dz) - oz;
+            fx = T::eval_d(p.x + G.trans.x, wx, dx) - ox;
+            fy = T::eval_d(p.y + G.trans.y, wy, dy) - oy;
+            fz = T::eval_d(p.z + G.trans.z, wz, dz) - oz;
         }
-        float sum[kMaxSplatChan], gx[kMaxSplatChan], gy[kMaxSplatChan], gz[kMaxSplatChan];
+        float sum[NCH], gx[NCH], gy[NCH], gz[NCH];
 #pragma unroll
-        for (int c = 0; c < kMaxSplatChan; c++) sum[c] = gx[c] = gy[c] = gz[c] = 0.0f;
+        for (int c = 0; c < NCH; c++) sum[c] = gx[c] = gy[c] = gz[c] = 0.0f;
 #pragma unroll
-        for (int tz = 0; tz < T::N; tz++) {
+        for (int tz = 0; tz < N; tz++) {
 #pragma unroll
-            for (int ty = 0; ty < T::N; ty++) {
-                int row = ((fz + tz) * ht + (fy + ty)) * ht + fx;
+            for (int ty = 0; ty < N; ty++) {
+                const int row = ((fz + tz) * ht + (fy + ty)) * ht + fx;
+                const float wyz = wy[ty] * wz[tz];
+                float dyz = 0.0f, ydz = 0.0f;
+                if (MODE != kFwd) {
+                    dyz = dy[ty] * wz[tz];
+                    ydz = wy[ty] * dz[tz];
+                }
 #pragma unroll
-                for (int tx = 0; tx < T::N; tx++) {
-                    float wyz = wy[ty] * wz[tz];
-                    float wgt = wx[tx] * wyz;
+                for (int tx = 0; tx < N; tx++) {
 #pragma unroll
-                    for (int c = 0; c < kMaxSplatChan; c++) {
-                        if (c >= G.nch) continue;
-                        float g = tile[c * ht3 + row + tx];
-                        if (MODE == kFwd || MODE == kScatterBwd) sum[c] += g * wgt;
+                    for (int c = 0; c < NCH; c++) {
+                        const float g = tile[c * ht3 + row + tx];
+                        if (MODE != kGatherBwd) sum[c] = fmaf(g, wx[tx] * wyz, sum[c]);
                         if (MODE != kFwd) {
-                            gx[c] += g * (dx[tx] * wyz);
-                            gy[c] += g * (wx[tx] * dy[ty] * wz[tz]);
-                            gz[c] += g * (wx[tx] * wy[ty] * dz[tz]);
+                            gx[c] = fmaf(g, dx[tx] * wyz, gx[c]);
+                            gy[c] = fmaf(g, wx[tx] * dyz, gy[c]);
+                            gz[c] = fmaf(g, wx[tx] * ydz, gz[c]);
                         }
                     }
                 }
@@ -359,17 +564,15 @@ __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
         }
         if (MODE == kFwd) {
 #pragma unroll
-            for (int c = 0; c < kMaxSplatChan; c++)
-                if (c < G.nch) G.out[(int64_t)pidx * G.out_stride + c] = sum[c];
+            for (int c = 0; c < NCH; c++) G.out[(int64_t)pidx * G.out_stride + c] = sum[c];
         } else if (MODE == kScatterBwd) {
-            float wt = G.has_weight ? load_f1(G.weight, pidx) : G.wconst;
+            const float wt = G.has_weight ? load_f1(G.weight, pidx) : G.wconst;
             float gw = 0.0f, gp0 = 0.0f, gp1 = 0.0f, gp2 = 0.0f;
 #pragma unroll
-            for (int c = 0; c < kMaxSplatChan; c++) {
-                if (c >= G.nch) continue;
-                bool has = (G.attr_mask >> c) & 1;
-                float at = has ? load_f1(G.attr[c], pidx) : 1.0f;
-                if (G.grad_attr) G.grad_attr[(int64_t)pidx * G.nch + c] = has ? wt * sum[c] : 0.0f;
+            for (int c = 0; c < NCH; c++) {
+                const bool has = (G.attr_mask >> c) & 1;
+                const float at = has ? load_f1(G.attr[c], pidx) : 1.0f;
+                if (G.grad_attr) G.grad_attr[(int64_t)pidx * NCH + c] = has ? wt * sum[c] : 0.0f;
                 gw += at * sum[c];
                 gp0 += wt * at * gx[c];
                 gp1 += wt * at * gy[c];
@@ -384,9 +587,8 @@ __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
         } else {
             float gp0 = 0.0f, gp1 = 0.0f, gp2 = 0.0f;
 #pragma unroll
-            for (int c = 0; c < kMaxSplatChan; c++) {
-                if (c >= G.nch) continue;
-                float go = G.grad_out[(int64_t)pidx * G.nch + c];
+            for (int c = 0; c < NCH; c++) {
+                const float go = G.grad_out[(int64_t)pidx * NCH + c];
                 gp0 += go * gx[c];
                 gp1 += go * gy[c];
                 gp2 += go * gz[c];
@@ -447,57 +649,95 @@ gvdb2_status launch_smem(Volume *v, K kernel, size_t smem, const char *what) {
     return GVDB2_OK;
 }
 
-gvdb2_status run_scatter(Volume *v, int kernel, const SplatArgs &S) {
-    if (v->atlas_last == 0) return GVDB2_OK;
-    const int res3 = v->res(0) * v->res(0) * v->res(0);
-    const unsigned g = (unsigned)v->atlas_last;
-    cudaStream_t s = v->stream;
-    if (v->deterministic) {
-        size_t smem = sizeof(unsigned long long) * (size_t)S.nch * res3;
-        if (kernel == GVDB2_KERNEL_TENT1) {
-            auto k = k_scatter_tile<GVDB2_KERNEL_TENT1, unsigned long long>;
-            GV_TRY(launch_smem(v, k, smem, "scatter"));
-            k<<<g, 256, smem, s>>>(S);
-        } else {
-            auto k = k_scatter_tile<GVDB2_KERNEL_CUBIC2, unsigned long long>;
-            GV_TRY(launch_smem(v, k, smem, "scatter"));
-            k<<<g, 256, smem, s>>>(S);
-        }
-    } else {
-        size_t smem = sizeof(float) * (size_t)S.nch * res3;
-        if (kernel == GVDB2_KERNEL_TENT1) {
-            auto k = k_scatter_tile<GVDB2_KERNEL_TENT1, float>;
-            GV_TRY(launch_smem(v, k, smem, "scatter"));
-            k<<<g, 256, smem, s>>>(S);
-        } else {
-            auto k = k_scatter_tile<GVDB2_KERNEL_CUBIC2, float>;
-            GV_TRY(launch_smem(v, k, smem, "scatter"));
-            k<<<g, 256, smem, s>>>(S);
-        }
+template <int KERNEL, int NCH>
+gvdb2_status launch_scatter(Volume *v, const SplatArgs &S) {
+    if (!v->deterministic) {
+        int32_t *absmax = nullptr;
+        GV_CUDA(v, cudaMallocAsync((void **)&absmax, sizeof(int32_t) * NCH, v->stream));
+        GV_CUDA(v, cudaMemsetAsync(absmax, 0, sizeof(int32_t) * NCH, v->stream));
+        const int64_t n = v->bin_key.n;
+        if (n > 0)
+            k_absmax<NCH><<<std::min(grid_for(n, 256), 4 * kSmCount), 256, 0, v->stream>>>(S, n, absmax);
+        k_scatter_fixed<KERNEL, NCH><<<(unsigned)v->atlas_last, kAtomicThreads, 0, v->stream>>>(S, absmax);
+        cudaError_t e = cudaGetLastError();
+        cudaFreeAsync(absmax, v->stream);
+        if (e != cudaSuccess) return cuda_fail(v, e, "k_scatter_fixed");
+        return GVDB2_OK;
     }
+    const int cap = NCH <= 4 ? 768 : 512;
+    const size_t smem = scatter_smem_bytes(Taps<KERNEL>::N, NCH, cap);
+    auto k = k_scatter_tile<KERNEL, NCH>;
+    GV_TRY(launch_smem(v, k, smem, "scatter"));
+    k<<<(unsigned)v->atlas_last, kScatterThreads, smem, v->stream>>>(S, cap);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
+}
+
+template <int KERNEL>
+gvdb2_status launch_scatter_n(Volume *v, const SplatArgs &S) {
+    switch (S.nch) {
+    case 1: return launch_scatter<KERNEL, 1>(v, S);
+    case 2: return launch_scatter<KERNEL, 2>(v, S);
+    case 3: return launch_scatter<KERNEL, 3>(v, S);
+    case 4: return launch_scatter<KERNEL, 4>(v, S);
+    default: return launch_scatter<KERNEL, 8>(v, S);
+    }
+}
+
+gvdb2_status run_scatter(Volume *v, int kernel, const SplatArgs &S) {
+    if (v->atlas_last == 0) return GVDB2_OK;
+    if (v->res(0) != kScatterRes)
+        return fail(v, GVDB2_ERR_UNSUPPORTED, "kernel splats need 8^3 bricks (Configure(...,3))");
+    return kernel == GVDB2_KERNEL_TENT1 ? launch_scatter_n<GVDB2_KERNEL_TENT1>(v, S)
+                                        : launch_scatter_n<GVDB2_KERNEL_CUBIC2>(v, S);
+}
+
+template <int KERNEL, int MODE, int NCH>
+gvdb2_status launch_gather(Volume *v, const GatherArgs &G) {
+    constexpr int H = Taps<KERNEL>::N / 2;
+    const int ht = v->res(0) + 2 * H;
+    const size_t smem = sizeof(float) * (size_t)NCH * ht * ht * ht;
+    auto k = k_gather_tile<KERNEL, MODE, NCH>;
+    GV_TRY(launch_smem(v, k, smem, "gather"));
+    k<<<(unsigned)v->atlas_last, 256, smem, v->stream>>>(G);
+    GV_CUDA(v, cudaGetLastError());
+    return GVDB2_OK;
+}
+
+template <int KERNEL, int MODE>
+gvdb2_status launch_gather_n(Volume *v, const GatherArgs &G) {
+    switch (G.nch) {
+    case 1: return launch_gather<KERNEL, MODE, 1>(v, G);
+    case 2: return launch_gather<KERNEL, MODE, 2>(v, G);
+    case 3: return launch_gather<KERNEL, MODE, 3>(v, G);
+    case 4: return launch_gather<KERNEL, MODE, 4>(v, G);
+    default: break;
+    }
+    // 5..8 channels: two passes over channel groups (4 + rest)
+    GatherArgs A = G, B = G;
+    A.nch = 4;
+    B.nch = G.nch - 4;
+    for (int c = 0; c < 4; c++) {
+        B.chan[c] = G.chan[4 + c];
+        B.attr[c] = G.attr[4 + c];
+    }
+    B.attr_mask = G.attr_mask >> 4;
+    if (MODE == kFwd) B.out = G.out + 4;
+    if (MODE != kFwd) return fail(v, GVDB2_ERR_UNSUPPORTED, "adjoints take at most 4 channels per call");
+    GV_TRY((launch_gather<KERNEL, MODE, 4>(v, A)));
+    switch (B.nch) {
+    case 1: return launch_gather<KERNEL, MODE, 1>(v, B);
+    case 2: return launch_gather<KERNEL, MODE, 2>(v, B);
+    case 3: return launch_gather<KERNEL, MODE, 3>(v, B);
+    default: return launch_gather<KERNEL, MODE, 4>(v, B);
+    }
 }
 
 template <int MODE>
 gvdb2_status run_gather(Volume *v, int kernel, const GatherArgs &G) {
     if (v->atlas_last == 0) return GVDB2_OK;
-    const int res = v->res(0);
-    const int h = kernel == GVDB2_KERNEL_TENT1 ? 1 : 2;
-    const int ht = res + 2 * h;
-    size_t smem = sizeof(float) * (size_t)G.nch * ht * ht * ht;
-    const unsigned g = (unsigned)v->atlas_last;
-    if (kernel == GVDB2_KERNEL_TENT1) {
-        auto k = k_gather_tile<GVDB2_KERNEL_TENT1, MODE>;
-        GV_TRY(launch_smem(v, k, smem, "gather"));
-        k<<<g, 256, smem, v->stream>>>(G);
-    } else {
-        auto k = k_gather_tile<GVDB2_KERNEL_CUBIC2, MODE>;
-        GV_TRY(launch_smem(v, k, smem, "gather"));
-        k<<<g, 256, smem, v->stream>>>(G);
-    }
-    GV_CUDA(v, cudaGetLastError());
-    return GVDB2_OK;
+    return kernel == GVDB2_KERNEL_TENT1 ? launch_gather_n<GVDB2_KERNEL_TENT1, MODE>(v, G)
+                                        : launch_gather_n<GVDB2_KERNEL_CUBIC2, MODE>(v, G);
 }
 
 gvdb2_status splat_prologue(Volume *v, int kernel, int n, const float trans[3]) {
