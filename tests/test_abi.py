@@ -76,3 +76,24 @@ def test_product_does_not_import_oracle():
             if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
                 txt = open(os.path.join(dirpath, f)).read()
                 assert "import oracle" not in txt and "liboracle" not in txt and "gvdb_oracle" not in txt, f
+
+
+def test_cpp_facade_compiles_and_links(built_lib, tmp_path):
+    """The C++ drop-in facade compiles against the header and links to the library."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("no g++")
+    src = tmp_path / "use.cpp"
+    src.write_text(
+        '#include "gvdb2_volume.hpp"\n'
+        "int main(int argc, char**) {\n"
+        "  if (argc > 5) { gvdb2::VolumeGVDB v(0); v.Configure(3,3,3,3,3); v.AddChannel(0, GVDB2_T_FLOAT, 1);\n"
+        "    v.RebuildTopology(0, 2.0f); v.UpdateAtlas(); v.UpdateApron(); }\n"
+        "  return 0; }\n")
+    out = tmp_path / "use"
+    libdir = os.path.dirname(built_lib)
+    r = subprocess.run([gxx, "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(out),
+                        "-L", libdir, "-lgvdb2", f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
