@@ -832,6 +832,26 @@ gvdb2_status gather_kernel(Volume *v, int kernel, int n, const float trans[3], c
     return run_gather<kFwd>(v, kernel, G);
 }
 
+gvdb2_status gather_kernel_prebinned(Volume *v, int kernel, int n, const float trans[3], const int *chans, int nch,
+                                     float *out, int64_t out_stride, const uint32_t *bin_off27, const int32_t *perm) {
+    GV_TRY(check_chans(v, chans, nch));
+    if (!out || out_stride < nch) return fail(v, GVDB2_ERR_ARG, "bad output buffer");
+    if (kernel != GVDB2_KERNEL_TENT1 && kernel != GVDB2_KERNEL_CUBIC2) return fail(v, GVDB2_ERR_ARG, "unknown kernel");
+    if (!v->atlas_valid) return fail(v, GVDB2_ERR_STATE, "UpdateAtlas must follow the topology rebuild");
+    if (n == 0) return GVDB2_OK;
+    GatherArgs G{};
+    G.pos = v->pos;
+    G.trans = make_float3(trans[0], trans[1], trans[2]);
+    for (int c = 0; c < kMaxSplatChan; c++) G.chan[c] = c < nch ? v->atlas[chans[c]].as<float>() : nullptr;
+    G.nch = nch;
+    G.out = out;
+    G.out_stride = out_stride;
+    fill_topology(v, G);
+    G.bin_off = bin_off27;
+    G.perm = perm;
+    return run_gather<kFwd>(v, kernel, G);
+}
+
 gvdb2_status scatter_kernel_backward(Volume *v, int kernel, int n, const float trans[3], gvdb2_points_view weight,
                                      float weight_const, const gvdb2_points_view *attrs, int nch,
                                      const int *grad_chans, float *grad_pos, float *grad_weight, float *grad_attr) {

@@ -72,6 +72,7 @@ _SIGS = {
     "gvdb2_update_apron_faces": [_vp, _i32],
     "gvdb2_scatter_kernel": [_vp, _i32, _i32, _fp, PointsView, _f32, _vp, _ip, _i32],
     "gvdb2_gather_kernel": [_vp, _i32, _i32, _fp, _ip, _i32, _vp, _i64],
+    "gvdb2_gather_kernel_noalloc": [_vp, _i32, _i32, _fp, _ip, _i32, _vp, _i64],
     "gvdb2_scatter_kernel_backward": [_vp, _i32, _i32, _fp, PointsView, _f32, _vp, _i32, _ip, _vp, _vp, _vp],
     "gvdb2_gather_kernel_backward": [_vp, _i32, _i32, _fp, _ip, _i32, _vp, _ip, _vp],
     "gvdb2_get_info": [_vp, ctypes.POINTER(Info)],

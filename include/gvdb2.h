@@ -149,6 +149,20 @@ GVDB2_API gvdb2_status gvdb2_gather_kernel_backward(gvdb2_volume *v, int kernel,
                                           const int *chans, int nch, const float *grad_out,
                                           const int *grad_chans, float *grad_pos);
 
+/* The same gather as gvdb2_gather_kernel, for callers that cannot allocate
+ * device memory once running (an application that fixes its GPU memory
+ * budget at start-up, a real-time loop that forbids allocation, a process
+ * whose allocator belongs to another framework).  No counterpart in the
+ * reference.  It performs no device allocation: its binning scratch is one
+ * file-scope device array per GPU (16.25 MB, held until the process exits),
+ * which limits a call to 1,048,576 points and 32,768 active bricks; larger
+ * calls return GVDB2_ERR_CAPACITY.  The first call on a device looks up the
+ * array's address (make it before any stream capture).  All calls share the
+ * array, so calls whose GPU work overlaps race and must be ordered by the
+ * caller.  Points outside every active brick gather 0. */
+GVDB2_API gvdb2_status gvdb2_gather_kernel_noalloc(gvdb2_volume *v, int kernel, int n, const float trans[3],
+                                                   const int *chans, int nch, float *out, int64_t out_stride);
+
 /* ---- inspection (host copies; synchronise the stream) ---- */
 GVDB2_API gvdb2_status gvdb2_get_info(gvdb2_volume *v, gvdb2_info *out);
 GVDB2_API gvdb2_status gvdb2_copy_nodes(gvdb2_volume *v, int lev, void *host, int64_t max_nodes);            /* getNode / pool 0 (64-byte nodes) */
