@@ -39,6 +39,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--incremental", action="store_true", help="reference state machine instead of full rebuilds")
     ap.add_argument("--quick", action="store_true", help="timed steps only (no baseline, e2e or launch count)")
+    ap.add_argument("--sites", default="256,64,256", help="lattice sites x,y,z (smaller cases for profiling)")
     return ap.parse_args()
 
 
@@ -231,6 +232,44 @@ def run_reference(a):
 # ----------------------------------------------------------------------------
 # our arm
 # ----------------------------------------------------------------------------
+def stage_times(pipe, reps=7):
+    """Median device time of each stage (one launch each for the splats)."""
+    import statistics as st
+    import torch
+    v, n, K = pipe.v, pipe.n, pipe.gvdb2.KERNEL_CUBIC2
+
+    def timed(f):
+        f()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            f()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return st.median(ts)
+
+    def topo():
+        v.RequestFullRebuild(True)
+        v.RebuildTopology(n, RADIUS)
+        v.UpdateAtlas()
+
+    out = {"topology": timed(topo)}
+    v.GatherKernel(K, n, [1, 2, 3], out=pipe.out)  # bins for the stages below
+    out["scatter"] = timed(lambda: v.ScatterKernel(K, n, [0, 1, 2, 3], weight=1.0, attrs=pipe.attrs))
+    out["apron"] = timed(lambda: v.UpdateApron(-1, 0.0))
+    out["gather"] = timed(lambda: v.GatherKernel(K, n, [1, 2, 3], out=pipe.out))
+
+    def rebin_gather():
+        v.SetPoints(pipe.pos)  # drops the cached binning
+        v.GatherKernel(K, n, [1, 2, 3], out=pipe.out)
+    out["binning"] = max(timed(rebin_gather) - out["gather"], 0.0)
+    return out
+
+
 def count_launches(pipe):
     """Kernels of libgvdb2 in one step (names in the gvdb2 namespace)."""
     import torch
@@ -260,7 +299,8 @@ def run_ours(a):
     if ws > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    pos, vel = wl.dam_block(sites=SITES)
+    sites = tuple(int(x) for x in a.sites.split(","))
+    pos, vel = wl.dam_block(sites=sites)
     cpu = None
     if rank == 0 and ws == 1 and not (a.no_cpu_baseline or a.quick):
         cpu = cpu_baseline(pos, vel)
@@ -302,27 +342,19 @@ def run_ours(a):
                               "ms_per_step": ms / a.steps, "quick": True}), flush=True)
         return 0
 
-    # per-stage intervals (CUDA events on the launching stream), averaged
+    # per-stage device times: each stage repeated on the launching stream,
+    # CUDA events around it, median of `reps`
     geo = pipe.geometry()
-    stage_ms = {}
-    reps = 3
-    for _ in range(reps):
-        ev = []
-        pipe.step(events=ev)
-        torch.cuda.synchronize()
-        for (n0, a0), (n1, a1) in zip(ev[:-1], ev[1:]):
-            stage_ms[n1] = stage_ms.get(n1, 0.0) + a0.elapsed_time(a1) / reps
+    stage_ms = stage_times(pipe)
     sb = metrics.stage_bytes(N=n, B=geo["B"], U=geo["U"], C=4, Cw=4, G=3, T=geo["T"], R3=geo["R3"], CL=geo["CL"])
-    launches_per_stage = {"scatter": 1, "gather": 1, "apron": 4}
     peak, peak_kind = peaks()
     stages = {}
     for k in ("topology", "binning", "scatter", "apron", "gather"):
         gbs = sb[k] / (stage_ms[k] / 1e3) / 1e9 if stage_ms.get(k) else None
         stages[k] = {"ms": round(stage_ms.get(k, 0.0), 4), "alg_bytes": sb[k], "GBps": gbs}
     dom = max(("scatter", "gather", "apron"), key=lambda k: stage_ms.get(k, 0.0))
-    per_launch_ms = stage_ms[dom] / launches_per_stage[dom]
-    achieved = sb[dom] / launches_per_stage[dom] / (per_launch_ms / 1e3) / 1e9
-    kernel_name = {"scatter": "k_scatter_tile<cubic,float>", "gather": "k_gather_tile<cubic,fwd>",
+    achieved = sb[dom] / (stage_ms[dom] / 1e3) / 1e9
+    kernel_name = {"scatter": "k_scatter_fixed<cubic,4>", "gather": "k_gather_tile<cubic,fwd,3>",
                    "apron": "k_apron"}[dom]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": TRAFFIC.get(dom), "kernel": kernel_name, "peak_source": peak_kind}
