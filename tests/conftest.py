@@ -4,7 +4,8 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-for p in (os.path.join(ROOT, "oracle"), os.path.join(ROOT, "gvdb-voxels_b200"), ROOT, os.path.dirname(__file__)):
+for p in (os.path.join(ROOT, "oracle"), os.path.join(ROOT, "gvdb-voxels_b200"), ROOT, os.path.dirname(__file__),
+          os.path.join(os.path.dirname(__file__), "golden")):
     if p not in sys.path:
         sys.path.insert(0, p)
 
