@@ -123,12 +123,9 @@ struct Volume {
     DevBuf clist[kMaxLev];    // uint64 child lists (lev >= 1)
     uint64_t topo_version = 0;
 
-    // leaf lookup: level-0 key -> leaf pool index (linked leaves only)
+    // leaf lookup: level-0 key -> leaf pool index (flagged, i.e. linked, leaves only)
     DevBuf leafmap_keys, leafmap_vals;
     uint32_t leafmap_mask = 0;
-    // per-level maps of linked interior nodes (incremental rebuild)
-    DevBuf levmap_keys[kMaxLev], levmap_vals[kMaxLev];
-    uint32_t levmap_mask[kMaxLev] = {0};
 
     // scratch for the rebuild
     DevBuf hs_keys[2];        // hash sets (base, box)

@@ -601,6 +601,8 @@ gvdb2_status full_rebuild(Volume *v, int n, float radius, const float orig[3]) {
     return GVDB2_OK;
 }
 
+gvdb2_status incremental_activate(Volume *v, int n, float radius, const float orig[3], bool accum);
+
 // DetermineDepth (V:821-837) with GetCoveringNode (V:2915-2931).
 int determine_depth(const Volume *v, int rootpos[3]) {
     for (int lev = 0; lev < kMaxLev; lev++) {
@@ -706,12 +708,9 @@ gvdb2_status rebuild_topology(Volume *v, int n, float radius, const float orig[3
     return incremental_rebuild(v, n, radius, orig, false);
 }
 
+// ActivateIncreBricksGPU (V:1020-1156); kernels in the incremental section.
 gvdb2_status incremental_rebuild(Volume *v, int n, float radius, const float orig[3], bool accum) {
-    (void)n;
-    (void)radius;
-    (void)orig;
-    (void)accum;
-    return fail(v, GVDB2_ERR_UNSUPPORTED, "incremental rebuild not built yet");
+    return incremental_activate(v, n, radius, orig, accum);
 }
 
 // Atlas growth along Z with content preserved by slot (AtlasResize, A:622-650).
@@ -808,6 +807,408 @@ gvdb2_status clear_channel(Volume *v, int chan) {
     GV_CUDA(v, cudaMemsetAsync(v->atlas[chan].p, 0, (size_t)v->atlas_cap * v->tile_vox() * sizeof(float), v->stream));
     return GVDB2_OK;
 }
+
+
+// ---- incremental rebuild ------------------------------------------------
+//
+// ActivateIncreBricksGPU (V:1020-1156) keeps the pools and appends:
+//   1. every point visits the level-l node corners of its box
+//      [int(w)-r, int(w)+r] (gvdbCalcIncreExtraBrickId, P:420-465); a corner
+//      the tree cannot reach becomes a new key, a reachable leaf is marked;
+//   2. no new key: nothing changes (V:1065);
+//   3. leaf flags := marks; new nodes are appended per level in key order;
+//   4. link top-down (N:470-505), delink unmarked leaves (N:401-429) and
+//      childless interior nodes bottom-up (N:431-467);
+//   5. used leaves = flagged leaves (V:1144-1147).
+// "Reachable" is the reference's tree walk through the child lists
+// (getPosParent / getParent), so a leaf delinked earlier is not found again:
+// a point returning there gets a new leaf and the old one stays unflagged in
+// the pool, as in the reference.  The leaf map is rebuilt from the flagged
+// leaves, which are the ones a tree walk reaches.
+namespace {
+
+struct TreeView {
+    Node *nodes[kMaxLev];
+    uint64_t *clist[kMaxLev];
+    int64_t cnt[kMaxLev];
+    int res[kMaxLev];
+    int64_t range[kMaxLev];
+    int top, depth;
+};
+
+TreeView tree_view(Volume *v) {
+    TreeView T;
+    for (int l = 0; l < kMaxLev; l++) {
+        T.nodes[l] = v->pool_ptr(l);
+        T.clist[l] = v->clist[l].as<uint64_t>();
+        T.cnt[l] = v->pool_cnt[l];
+        T.res[l] = l < v->nlev ? v->res(l) : 1;
+        T.range[l] = l < v->nlev ? v->range(l) : 1;
+    }
+    T.top = v->top_level();
+    T.depth = v->depth;
+    return T;
+}
+
+// getChild (N:115-124): child index, or -1 for an empty slot
+__device__ int64_t tv_child(const TreeView &T, const Node *nd, int64_t bit) {
+    uint64_t listid = nd->mChildList;
+    if (listid == kUndefL) return -1;
+    int clev = (int)((listid >> 8) & 0xFF);
+    int64_t cndx = (int64_t)(listid >> 16);
+    if (clev <= 0 || clev >= kMaxLev || cndx >= T.cnt[clev]) return -1;
+    int64_t r3 = (int64_t)T.res[clev] * T.res[clev] * T.res[clev];
+    if (bit < 0 || bit >= r3) return -1;
+    uint64_t c = T.clist[clev][cndx * r3 + bit];
+    return (int64_t)(int32_t)(uint32_t)(c >> 16);
+}
+
+// posInNode (N:313-319) with the bit index; false outside the node
+__device__ bool tv_bit(const TreeView &T, int lev, const int32_t np[3], const int pos[3], int64_t *bit) {
+    int res = T.res[lev];
+    int64_t p[3];
+    for (int a = 0; a < 3; a++) {
+        int64_t d = (int64_t)pos[a] - np[a];
+        p[a] = d * res / T.range[lev];
+        if (d < 0 || p[a] >= res) return false;
+    }
+    *bit = (p[2] * res + p[1]) * res + p[0];
+    return true;
+}
+
+// getPosParent (N:303-348): node of level stopLev containing pos, or -1
+__device__ int64_t tv_pos_parent(const TreeView &T, const int pos[3], int stopLev) {
+    if (T.cnt[T.top] < 1) return -1;
+    const Node *nd = &T.nodes[T.top][0];
+    int l = nd->mLev;
+    if (l == 0) return 0;
+    while (l > 0) {
+        int64_t bit;
+        if (!tv_bit(T, l, nd->mPos, pos, &bit)) return -1;
+        int64_t c = tv_child(T, nd, bit);
+        l--;
+        if (c == -1) return -1;
+        if (l == stopLev) return c;
+        if (c < 0 || c >= T.cnt[l]) return -1;
+        nd = &T.nodes[l][c];
+    }
+    return -1;
+}
+
+// getParent (N:350-397): as getPosParent, but 0 when the top node is
+// unflagged or already at stopLev
+__device__ int64_t tv_parent(const TreeView &T, int stopLev, const int pos[3]) {
+    if (T.cnt[T.top] < 1) return -1;
+    const Node *nd = &T.nodes[T.top][0];
+    if (!nd->mFlags) return 0;
+    int l = nd->mLev;
+    if (l == stopLev) return 0;
+    while (l > stopLev) {
+        int64_t bit;
+        if (!tv_bit(T, l, nd->mPos, pos, &bit)) return -1;
+        l--;
+        int64_t c = tv_child(T, nd, bit);
+        if (c == -1) return -1;
+        if (l == stopLev) return c;
+        if (c < 0 || c >= T.cnt[l]) return -1;
+        nd = &T.nodes[l][c];
+    }
+    return -1;
+}
+
+// child slot of a node at level lev inside its parent pn (level lev+1)
+__device__ bool tv_slot(const TreeView &T, int plev, const Node *pn, const int32_t pos[3], int64_t *bit, bool strict) {
+    int res = T.res[plev];
+    int p[3];
+    for (int a = 0; a < 3; a++) p[a] = (int)((int64_t)(pos[a] - pn->mPos[a]) * res / T.range[plev]);
+    if (strict && (p[0] > res || p[0] < 0 || p[1] > res || p[1] < 0 || p[2] > res || p[2] < 0)) return false;
+    *bit = ((int64_t)p[2] * res + p[1]) * res + p[0];
+    return true;
+}
+
+// Step 1: marks and new keys.  A new key is lev<<3b | x<<2b | y<<b | z in
+// units of the level's range, which sorts like the reference's keys.
+__global__ void k_incre_mark(PointsView pos, int64_t n, float3 orig, float radius, TreeView T, int b, uint64_t *hs,
+                             uint32_t mask, int32_t *marker, int64_t total, int32_t *count, int32_t *status) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 p = load_f3(pos, i);
+    float w[3] = {p.x + orig.x, p.y + orig.y, p.z + orig.z};
+    if (w[0] < 0 || w[1] < 0 || w[2] < 0) return;
+    if (T.cnt[T.depth] < 1) return;
+    const Node *root = &T.nodes[T.depth][0];
+    const int64_t rr_root = T.range[T.depth];
+    int bmin[3], bmax[3];
+    for (int a = 0; a < 3; a++) {
+        int iw = (int)w[a];
+        bmin[a] = (int)((float)iw - radius);
+        bmax[a] = (int)((float)iw + radius);
+    }
+    for (int lev = 0; lev < T.depth; lev++) {
+        const int rr = (int)T.range[lev];
+        int nd[3];
+        for (nd[0] = bmin[0] / rr * rr; nd[0] <= bmax[0] / rr * rr; nd[0] += rr)
+            for (nd[1] = bmin[1] / rr * rr; nd[1] <= bmax[1] / rr * rr; nd[1] += rr)
+                for (nd[2] = bmin[2] / rr * rr; nd[2] <= bmax[2] / rr * rr; nd[2] += rr) {
+                    bool out = false;
+                    for (int a = 0; a < 3; a++)
+                        out |= nd[a] < root->mPos[a] || (int64_t)nd[a] >= root->mPos[a] + rr_root;
+                    if (out) continue;
+                    int64_t pid = tv_pos_parent(T, nd, lev);
+                    if (pid == -1) {
+                        uint64_t key = ((uint64_t)lev << (3 * b)) | pack_key(nd[0] / rr, nd[1] / rr, nd[2] / rr, b);
+                        int r = hs_insert(hs, mask, key);
+                        if (r > 0) atomicAdd(count, 1);
+                        if (r < 0) atomicOr(status, kDevHashFull);
+                    } else if (lev == 0 && pid >= 0 && pid < total) {
+                        marker[pid] = 1;
+                    }
+                }
+    }
+}
+
+__global__ void k_init_markers(const Node *leaves, int64_t total, int accum, int32_t *marker) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < total) marker[i] = accum ? (int32_t)leaves[i].mFlags : 0;
+}
+
+__global__ void k_level_count(const uint64_t *keys, int64_t n, int b, int32_t *lev_cnt) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(&lev_cnt[(int)(keys[i] >> (3 * b))], 1);
+}
+
+// V:1078-1081: leaf flags := marks
+__global__ void k_apply_markers(Node *leaves, int64_t total, const int32_t *marker) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < total) leaves[i].mFlags = (uint8_t)(marker[i] ? 1 : 0);
+}
+
+struct NewNodes {
+    const uint64_t *keys;
+    int64_t n;
+    int b;
+    int64_t start[kMaxLev], old_cnt[kMaxLev], range[kMaxLev];
+    Node *nodes[kMaxLev];
+};
+
+// PoolAlloc + SetupNode for the appended nodes (V:1088-1111); the child
+// list of an interior node has the node's own pool index.
+__global__ void k_new_nodes(NewNodes A) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    uint64_t key = A.keys[i];
+    int lev = (int)(key >> (3 * A.b));
+    int x, y, z;
+    unpack_key(key, A.b, x, y, z);
+    int64_t idx = A.old_cnt[lev] + (i - A.start[lev]);
+    Node nd;
+    memset(&nd, 0, sizeof(nd));
+    nd.mLev = (uint8_t)lev;
+    nd.mFlags = 1;
+    nd.mPos[0] = (int32_t)(x * A.range[lev]);
+    nd.mPos[1] = (int32_t)(y * A.range[lev]);
+    nd.mPos[2] = (int32_t)(z * A.range[lev]);
+    nd.mValue[0] = nd.mValue[1] = nd.mValue[2] = -1;
+    nd.mParent = kUndefL;
+    nd.mChildList = lev > 0 ? elem(1, lev, (uint64_t)idx) : kUndefL;
+    A.nodes[lev][idx] = nd;
+}
+
+// gvdbLinkBricks (N:470-505) for one level
+__global__ void k_link_level(TreeView T, int lev) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.cnt[lev]) return;
+    Node *nd = &T.nodes[lev][i];
+    if (!nd->mFlags) return;
+    int pos[3] = {nd->mPos[0], nd->mPos[1], nd->mPos[2]};
+    const int pl = lev + 1;
+    int64_t pid = tv_parent(T, pl, pos);
+    if (pid < 0 || pid >= T.cnt[pl]) return;
+    const Node *pn = &T.nodes[pl][pid];
+    int64_t bit;
+    if (!tv_slot(T, pl, pn, nd->mPos, &bit, true)) return;
+    nd->mParent = ((uint64_t)pid << 16) | ((uint64_t)pl << 8);
+    int64_t cndx = (int64_t)(pn->mChildList >> 16);
+    int64_t r3 = (int64_t)T.res[pl] * T.res[pl] * T.res[pl];
+    if (cndx >= T.cnt[pl] || bit >= r3) return;
+    T.clist[pl][cndx * r3 + bit] = ((uint64_t)i << 16) | ((uint64_t)lev << 8);
+}
+
+// gvdbDelinkLeafBricks (N:401-429)
+__global__ void k_delink_leaves(TreeView T) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.cnt[0]) return;
+    Node *nd = &T.nodes[0][i];
+    if (nd->mFlags || nd->mParent == kUndef64) return;
+    int pos[3] = {nd->mPos[0], nd->mPos[1], nd->mPos[2]};
+    int64_t pid = tv_parent(T, 1, pos);
+    nd->mParent = kUndef64;
+    if (pid < 0 || pid >= T.cnt[1]) return;
+    const Node *pn = &T.nodes[1][pid];
+    int64_t bit;
+    tv_slot(T, 1, pn, nd->mPos, &bit, false);
+    int64_t r3 = (int64_t)T.res[1] * T.res[1] * T.res[1];
+    int64_t cndx = (int64_t)(pn->mChildList >> 16);
+    if (bit >= 0 && bit < r3 && cndx < T.cnt[1]) T.clist[1][cndx * r3 + bit] = kUndef64;
+}
+
+// gvdbDelinkBricks (N:431-467) for one interior level
+__global__ void k_delink_level(TreeView T, int lev) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.cnt[lev]) return;
+    Node *nd = &T.nodes[lev][i];
+    if (nd->mParent == kUndef64) {
+        nd->mFlags = 0;
+        return;
+    }
+    int64_t r3 = (int64_t)T.res[lev] * T.res[lev] * T.res[lev];
+    const uint64_t *cl = T.clist[lev] + i * r3;
+    for (int64_t c = 0; c < r3; c++)
+        if (cl[c] != kUndef64) {
+            nd->mFlags = 1;
+            return;
+        }
+    nd->mFlags = 0;
+    int pos[3] = {nd->mPos[0], nd->mPos[1], nd->mPos[2]};
+    int64_t pid = tv_parent(T, lev + 1, pos);
+    nd->mParent = kUndef64;
+    if (pid < 0 || pid >= T.cnt[lev + 1]) return;
+    const Node *pn = &T.nodes[lev + 1][pid];
+    int64_t bit;
+    tv_slot(T, lev + 1, pn, nd->mPos, &bit, false);
+    int64_t pr3 = (int64_t)T.res[lev + 1] * T.res[lev + 1] * T.res[lev + 1];
+    int64_t cndx = (int64_t)(pn->mChildList >> 16);
+    if (bit >= 0 && bit < pr3 && cndx < T.cnt[lev + 1]) T.clist[lev + 1][cndx * pr3 + bit] = kUndef64;
+}
+
+// leaf map of the flagged leaves; counts them into *used
+__global__ void k_leafmap_fill(const Node *leaves, int64_t n, KeyGeom g, uint64_t *lk, int32_t *lv, uint32_t mask,
+                               int32_t *used, int32_t *status) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Node &nd = leaves[i];
+    if (!nd.mFlags) return;
+    atomicAdd(used, 1);
+    uint64_t key = pack_key(nd.mPos[0] >> g.log2r0, nd.mPos[1] >> g.log2r0, nd.mPos[2] >> g.log2r0, g.b);
+    if (hm_insert(lk, lv, mask, key, (int32_t)i) < 0) atomicOr(status, kDevHashFull);
+}
+
+} // namespace
+
+namespace {
+
+gvdb2_status ensure_pool_keep(Volume *v, int lev, int64_t cnt) {
+    GV_CUDA(v, v->pool[lev].ensure(sizeof(Node) * (size_t)std::max<int64_t>(cnt, 1), v->stream, true));
+    if (lev > 0)
+        GV_CUDA(v, v->clist[lev].ensure(sizeof(uint64_t) * (size_t)(std::max<int64_t>(cnt, 1) * v->res3(lev)),
+                                        v->stream, true));
+    return GVDB2_OK;
+}
+
+gvdb2_status incremental_activate(Volume *v, int n, float radius, const float orig[3], bool accum) {
+    const int64_t total = v->pool_cnt[0];
+    if (total == 0) return GVDB2_OK; // V:1022
+    cudaStream_t s = v->stream;
+    const int depth = v->depth;
+    if (v->pool_cnt[depth] < 1) return fail(v, GVDB2_ERR_STATE, "incremental rebuild without a root at this depth");
+    KeyGeom g = key_geom(v);
+    if (3 * g.b + 4 > 64) return fail(v, GVDB2_ERR_UNSUPPORTED, "root too large for packed level keys");
+    const int b = g.b;
+    GV_CUDA(v, v->tmp_c.ensure(sizeof(int32_t) * (size_t)total, s));
+    int32_t *marker = v->tmp_c.as<int32_t>();
+
+    // 1. marks and new keys, into a hash set sized from the pool (grown on overflow)
+    uint32_t cap = next_pow2((uint64_t)std::max<int64_t>(4 * total, 1 << 16));
+    int64_t nnew = 0;
+    for (int attempt = 0;; attempt++) {
+        GV_CUDA(v, v->hs_keys[0].ensure(sizeof(uint64_t) * cap, s));
+        GV_CUDA(v, cudaMemsetAsync(v->hs_keys[0].p, 0xFF, sizeof(uint64_t) * cap, s));
+        GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count, 0, sizeof(int32_t) * 8 + sizeof(int32_t), s));
+        k_init_markers<<<grid_for(total, 256, 1ll << 31), 256, 0, s>>>(v->pool_ptr(0), total, accum ? 1 : 0, marker);
+        if (n > 0)
+            k_incre_mark<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(
+                v->pos, n, make_float3(orig[0], orig[1], orig[2]), radius, tree_view(v), b, v->hs_keys[0].as<uint64_t>(),
+                cap - 1, marker, total, dev_words(v)->count, &dev_words(v)->status);
+        GV_CUDA(v, cudaGetLastError());
+        GV_TRY(read_words(v));
+        nnew = host_words(v)->count[0];
+        bool full = (host_words(v)->status & kDevHashFull) || 2 * nnew > (int64_t)cap;
+        if (!full) break;
+        if (attempt == 3) return fail(v, GVDB2_ERR_CAPACITY, "new-node hash set overflow");
+        cap = next_pow2((uint64_t)cap * 4);
+    }
+    // 2. nothing new: pools and flags stay as they are (V:1065)
+    if (nnew == 0) return GVDB2_OK;
+
+    // sorted new keys and their count per level
+    GV_CUDA(v, v->tmp_a.ensure(sizeof(uint64_t) * (size_t)nnew, s));
+    uint64_t *keys = v->tmp_a.as<uint64_t>();
+    GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count + 2, 0, sizeof(int32_t), s));
+    k_compact_set<<<grid_for(cap, 256, 4096), 256, 0, s>>>(v->hs_keys[0].as<uint64_t>(), cap, keys,
+                                                           dev_words(v)->count + 2);
+    GV_TRY(radix_sort_u64(v, keys, nullptr, nnew, 0, 3 * b + 3));
+    GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count, 0, sizeof(int32_t) * 8, s));
+    k_level_count<<<grid_for(nnew, 256, 1ll << 31), 256, 0, s>>>(keys, nnew, b, dev_words(v)->count);
+    GV_CUDA(v, cudaGetLastError());
+    GV_TRY(read_words(v));
+    int64_t add[kMaxLev] = {0};
+    for (int l = 0; l < depth && l < 8; l++) add[l] = host_words(v)->count[l];
+
+    // 3. flags := marks, then append the new nodes level by level
+    k_apply_markers<<<grid_for(total, 256, 1ll << 31), 256, 0, s>>>(v->pool_ptr(0), total, marker);
+    NewNodes A;
+    A.keys = keys;
+    A.n = nnew;
+    A.b = b;
+    int64_t start = 0;
+    for (int l = 0; l < kMaxLev; l++) {
+        A.start[l] = start;
+        A.old_cnt[l] = v->pool_cnt[l];
+        A.range[l] = l < v->nlev ? v->range(l) : 1;
+        start += add[l];
+    }
+    for (int l = 0; l < depth; l++) {
+        if (!add[l]) continue;
+        GV_TRY(ensure_pool_keep(v, l, v->pool_cnt[l] + add[l]));
+        if (l > 0)
+            GV_CUDA(v, cudaMemsetAsync(v->clist[l].as<uint64_t>() + v->pool_cnt[l] * v->res3(l), 0xFF,
+                                       sizeof(uint64_t) * (size_t)(add[l] * v->res3(l)), s));
+    }
+    for (int l = 0; l < kMaxLev; l++) A.nodes[l] = v->pool_ptr(l);
+    k_new_nodes<<<grid_for(nnew, 256, 1ll << 31), 256, 0, s>>>(A);
+    for (int l = 0; l < depth; l++) v->pool_cnt[l] += add[l];
+
+    // 4. link top-down, delink bottom-up (top level from the new counts,
+    // as PrepareVDBPartially sets it)
+    TreeView T = tree_view(v);
+    for (int l = depth - 1; l >= 0; l--)
+        if (T.cnt[l] > 0) k_link_level<<<grid_for(T.cnt[l], 256, 1ll << 31), 256, 0, s>>>(T, l);
+    k_delink_leaves<<<grid_for(T.cnt[0], 256, 1ll << 31), 256, 0, s>>>(T);
+    for (int l = 1; l < depth; l++)
+        if (T.cnt[l] > 0) k_delink_level<<<grid_for(T.cnt[l], 256, 1ll << 31), 256, 0, s>>>(T, l);
+    GV_CUDA(v, cudaGetLastError());
+
+    // 5. leaf map of the flagged leaves; used leaves
+    uint32_t lcap = next_pow2((uint64_t)std::max<int64_t>(2 * v->pool_cnt[0], 1 << 12));
+    GV_CUDA(v, v->leafmap_keys.ensure(sizeof(uint64_t) * lcap, s));
+    GV_CUDA(v, v->leafmap_vals.ensure(sizeof(int32_t) * lcap, s));
+    GV_CUDA(v, cudaMemsetAsync(v->leafmap_keys.p, 0xFF, sizeof(uint64_t) * lcap, s));
+    v->leafmap_mask = lcap - 1;
+    GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count, 0, sizeof(int32_t) * 8 + sizeof(int32_t), s));
+    k_leafmap_fill<<<grid_for(v->pool_cnt[0], 256, 1ll << 31), 256, 0, s>>>(
+        v->pool_ptr(0), v->pool_cnt[0], g, v->leafmap_keys.as<uint64_t>(), v->leafmap_vals.as<int32_t>(),
+        v->leafmap_mask, dev_words(v)->count, &dev_words(v)->status);
+    GV_CUDA(v, cudaGetLastError());
+    GV_TRY(read_words(v));
+    if (host_words(v)->status & kDevHashFull) return fail(v, GVDB2_ERR_CAPACITY, "leaf map overflow");
+    v->used_leaves = host_words(v)->count[0];
+    v->lev_count[0][0] = v->pool_cnt[0];
+    v->lev_count[0][1] = 0;
+    v->atlas_valid = false;
+    return GVDB2_OK;
+}
+
+} // namespace
 
 
 } // namespace gvdb2

@@ -161,3 +161,78 @@ def test_subcells(gvdb2_mod, oracle_mod):
     assert np.array_equal(cnt, ocnt)
     assert np.array_equal(nid, onid)
     assert np.array_equal(pos, opos)
+
+
+def _drift_steps(pts, vel, steps):
+    for _ in range(steps):
+        yield pts
+        pts = pts + np.array([6.0, 0.0, 0.0], np.float32) + np.float32(0.2) * vel  # empties trailing bricks
+
+
+@pytest.mark.parametrize("radius", [2.0, 0.5])
+def test_incremental_rebuild_bit_exact(gvdb2_mod, oracle_mod, radius):
+    """Third and later RebuildTopology calls take the incremental branch
+    (V:1212-1217): appended nodes, flags, links and delinks match the oracle
+    bit for bit, stale leaves included."""
+    import gvdb2.workloads as wl
+    p, vel = wl.dam_block(sites=(48, 12, 48), origin=(40.0, 40.0, 40.0), seed=11)
+    o = make_oracle(oracle_mod)
+    v = gpu_volume(gvdb2_mod, p)
+    stale_seen = False
+    for step, q in enumerate(_drift_steps(p, vel, 5)):
+        assert o.rebuild_topology(q, radius) == 0
+        import torch
+        t = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+        v.SetPoints(t)
+        v._pts = t
+        v.RebuildTopology(len(q), radius)
+        compare_topology(v, o)
+        o.update_atlas()
+        v.UpdateAtlas()
+        assert np.array_equal(v.atlas_map(), o.atlas_map())
+        assert_nodes_equal(v.nodes(0), o.nodes(0), 0)
+        stale_seen |= o.pool_count(0) > o.used_leaves()
+    assert stale_seen
+
+
+def test_accumulate_topology_bit_exact(gvdb2_mod, oracle_mod):
+    """AccumulateTopology (V:1158-1178) keeps the flags of earlier leaves."""
+    a = shell_points(20_000, seed=7, r_in=20, r_out=24, center=(60.0, 60.0, 60.0))
+    b = shell_points(20_000, seed=8, r_in=20, r_out=24, center=(90.0, 60.0, 60.0))
+    o = make_oracle(oracle_mod)
+    v = gpu_volume(gvdb2_mod, a)
+    import torch
+    for q in (a, a, b):
+        assert o.accumulate_topology(q, 2.0, (0, 0, 0), 1) == 0
+        t = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+        v.SetPoints(t)
+        v._pts = t
+        v.AccumulateTopology(len(q), 2.0, (0, 0, 0), 1)
+        compare_topology(v, o)
+
+
+def test_splat_after_incremental(gvdb2_mod, oracle_mod):
+    """Splat and gather see only the linked leaves once stale leaves exist."""
+    import gvdb2.workloads as wl
+    import torch
+    from _helpers import REL_TOL, rel_err
+    p, vel = wl.dam_block(sites=(32, 8, 32), origin=(40.0, 40.0, 40.0), seed=12)
+    o = make_oracle(oracle_mod)
+    v = gpu_volume(gvdb2_mod, p)
+    for q in _drift_steps(p, vel, 4):
+        assert o.rebuild_topology(q, 2.0) == 0
+        t = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+        v.SetPoints(t)
+        v._pts = t
+        v.RebuildTopology(len(q), 2.0)
+    assert o.pool_count(0) > o.used_leaves()
+    o.update_atlas()
+    v.UpdateAtlas()
+    o.clear_channel(0)
+    v.ClearChannel(0)
+    o.scatter_kernel(gvdb2_mod.KERNEL_TENT1, q, [0])
+    v.ScatterKernel(gvdb2_mod.KERNEL_TENT1, len(q), [0])
+    assert rel_err(v.atlas(0), o.atlas(0)) <= REL_TOL
+    got = v.GatherKernel(gvdb2_mod.KERNEL_TENT1, len(q), [0]).cpu().numpy()
+    want = o.gather_kernel(gvdb2_mod.KERNEL_TENT1, q, [0])
+    assert rel_err(got, want) <= REL_TOL
