@@ -102,6 +102,69 @@ __global__ void k_gather_voxels(int64_t num_sc, int scpb, int sc, float radius, 
     chan[idx] = val;
 }
 
+// The same gathers for 4^3 subcells, one warp per subcell.  Each lane owns
+// two x-adjacent voxels of one (y, z) column, so the y/z part of a squared
+// distance is shared.  The subcell's points are staged through shared memory
+// in chunks of 64 (one float4 broadcast per point).  The minimum squared
+// distance is reduced first and the square root taken once: sqrt and the
+// subtraction of the radius are monotonic, so max(r - c) = r - sqrt(min d^2)
+// and min(c - r) = sqrt(min d^2) - r, as in P:725-728 / P:764-767.
+constexpr int kGvWarps = 8;
+template <bool LEVELSET>
+__global__ void __launch_bounds__(32 * kGvWarps) k_gather_voxels_sc4(int64_t num_sc, float radius,
+                                                                     const int32_t *sc_nid, const uint32_t *sc_cnt,
+                                                                     const uint32_t *sc_off, const int32_t *sc_pos,
+                                                                     const float *pnt, const Node *leaves, AtlasGeom A,
+                                                                     float *chan, int accum) {
+    __shared__ float4 buf[kGvWarps][64];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t sid = (int64_t)blockIdx.x * kGvWarps + warp;
+    if (sid >= num_sc) return;
+    const int col = lane >> 1, tx = (lane & 1) * 2, ty = col & 3, tz = col >> 2;
+    const int wx = sc_pos[3 * sid + 0] + tx, wy = sc_pos[3 * sid + 1] + ty, wz = sc_pos[3 * sid + 2] + tz;
+    const Node &nd = leaves[sc_nid[sid]];
+    const int64_t idx = atlas_index(A, nd.mValue[0] + wx - nd.mPos[0], nd.mValue[1] + wy - nd.mPos[1],
+                                    nd.mValue[2] + wz - nd.mPos[2]);
+    const float init = LEVELSET ? 3.0f : 0.0f;
+    float v0 = init, v1 = init;
+    if (accum && idx >= 0) {
+        v0 = chan[idx];
+        v1 = chan[idx + 1];
+    }
+    const uint32_t beg = sc_off[sid], cnt = sc_cnt[sid];
+    const float fx0 = (float)wx, fx1 = (float)(wx + 1), fy = (float)wy, fz = (float)wz;
+    float m0 = INFINITY, m1 = INFINITY;
+    float4 *wb = buf[warp];
+    for (uint32_t base = 0; base < cnt; base += 64) {
+        const uint32_t m = min(64u, cnt - base);
+        for (uint32_t k = lane; k < m; k += 32) {
+            const float *q = pnt + 3 * (int64_t)(beg + base + k);
+            wb[k] = make_float4(q[0], q[1], q[2], 0.0f);
+        }
+        __syncwarp();
+        for (uint32_t j = 0; j < m; j++) {
+            const float4 q = wb[j];
+            const float dy = q.y - fy, dz = q.z - fz;
+            const float syz = fmaf(dy, dy, dz * dz);
+            const float dx0 = q.x - fx0, dx1 = q.x - fx1;
+            m0 = fminf(m0, fmaf(dx0, dx0, syz));
+            m1 = fminf(m1, fmaf(dx1, dx1, syz));
+        }
+        __syncwarp();
+    }
+    if (idx < 0) return;
+    const float c0 = sqrtf(m0), c1 = sqrtf(m1);
+    if (LEVELSET) {
+        v0 = fminf(v0, c0 - radius);
+        v1 = fminf(v1, c1 - radius);
+    } else {
+        v0 = fmaxf(v0, radius - c0);
+        v1 = fmaxf(v1, radius - c1);
+    }
+    chan[idx] = v0;
+    chan[idx + 1] = v1;
+}
+
 // ---------------------------------------------------------------------
 // kernel splats
 // ---------------------------------------------------------------------
@@ -782,6 +845,19 @@ gvdb2_status gather_voxels(Volume *v, int sc, float radius, int chan, int accum,
     int64_t blocks = (v->num_sc + v->sc_per_brick - 1) / v->sc_per_brick;
     if (blocks == 0) return GVDB2_OK;
     const float *pnt = v->sc_len > 0 ? v->sc_pnt.as<float>() : nullptr;
+    if (sc == 4) {
+        const unsigned g = (unsigned)((v->num_sc + kGvWarps - 1) / kGvWarps);
+        if (levelset)
+            k_gather_voxels_sc4<true><<<g, 32 * kGvWarps, 0, v->stream>>>(
+                v->num_sc, radius, v->sc_nid.as<int32_t>(), v->sc_cnt.as<uint32_t>(), v->sc_off.as<uint32_t>(),
+                v->sc_pos.as<int32_t>(), pnt, v->pool_ptr(0), atlas_geom(v), v->atlas[chan].as<float>(), accum);
+        else
+            k_gather_voxels_sc4<false><<<g, 32 * kGvWarps, 0, v->stream>>>(
+                v->num_sc, radius, v->sc_nid.as<int32_t>(), v->sc_cnt.as<uint32_t>(), v->sc_off.as<uint32_t>(),
+                v->sc_pos.as<int32_t>(), pnt, v->pool_ptr(0), atlas_geom(v), v->atlas[chan].as<float>(), accum);
+        GV_CUDA(v, cudaGetLastError());
+        return GVDB2_OK;
+    }
     if (levelset)
         k_gather_voxels<true><<<(unsigned)blocks, threads, 0, v->stream>>>(
             v->num_sc, v->sc_per_brick, sc, radius, v->sc_nid.as<int32_t>(), v->sc_cnt.as<uint32_t>(),

@@ -864,6 +864,12 @@ RD_API int rd_rebuild_topology(void *h, int n, float radius, const float orig[3]
     return 0;
 }
 
+// RequestFullRebuild(true) (gvdb_volume_gvdb.h:343)
+RD_API int rd_request_full_rebuild(void *h) {
+    ((RefVolume *)h)->rebuild = true;
+    return 0;
+}
+
 RD_API int rd_update_atlas(void *h) { return update_atlas((RefVolume *)h); }
 
 RD_API int rd_clear_channel(void *h, int chan) {

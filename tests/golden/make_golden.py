@@ -134,6 +134,7 @@ class Ref:
             "rd_configure": (i32, [vp, i32, i32, i32, i32, i32]), "rd_add_channel": (i32, [vp, i32, i32]),
             "rd_set_points": (i32, [vp, vp, i32]), "rd_rebuild_topology": (i32, [vp, i32, f32, fp]),
             "rd_update_atlas": (i32, [vp]), "rd_clear_channel": (i32, [vp, i32]),
+            "rd_request_full_rebuild": (i32, [vp]),
             "rd_insert_points": (i32, [vp, i32, fp]),
             "rd_copy_point_nodes": (i32, [vp, vp, vp, i32, vp, i32]),
             "rd_scatter_density": (i32, [vp, i32, f32, f32, fp, i32]),
