@@ -14,8 +14,11 @@ namespace gvdb2 {
 
 cudaError_t DevBuf::ensure(size_t need, cudaStream_t s, bool preserve) {
     if (need <= bytes && p) return cudaSuccess;
-    size_t grow = bytes + bytes / 4;
+    // geometric growth: a buffer that tracks a slowly growing topology (the
+    // atlas, the splat scratch) is re-allocated O(log) times, not every step
+    size_t grow = bytes + bytes / 2;
     size_t nb = std::max(need, grow);
+    if (!p && need >= (size_t(1) << 24)) nb = need + need / 4; // large first allocations get headroom
     nb = (nb + 255) & ~size_t(255);
     void *np = nullptr;
     cudaError_t e = cudaMallocAsync(&np, nb, s);

@@ -122,6 +122,7 @@ struct Volume {
     DevBuf pool[kMaxLev];     // Node arrays
     DevBuf clist[kMaxLev];    // uint64 child lists (lev >= 1)
     uint64_t topo_version = 0;
+    int64_t pool_reserved_for = 0; // point count the stream-ordered pool was grown for
 
     // leaf lookup: level-0 key -> leaf pool index (flagged, i.e. linked, leaves only)
     DevBuf leafmap_keys, leafmap_vals;
@@ -229,10 +230,10 @@ gvdb2_status scatter_kernel(Volume *v, int kernel, int n, const float trans[3], 
                             float weight_const, const gvdb2_points_view *attrs, const int *chans, int nch);
 gvdb2_status gather_kernel(Volume *v, int kernel, int n, const float trans[3], const int *chans, int nch, float *out,
                            int64_t out_stride);
-// gather_kernel with the binning supplied by the caller: bin_off27[s*27] is
-// the first entry of slot s in perm and bin_off27[s*27 + 27] one past its last
+// gather_kernel with the binning supplied by the caller: bin_off[s] is the
+// first entry of slot s in perm and bin_off[s + 1] one past its last
 gvdb2_status gather_kernel_prebinned(Volume *v, int kernel, int n, const float trans[3], const int *chans, int nch,
-                                     float *out, int64_t out_stride, const uint32_t *bin_off27, const int32_t *perm);
+                                     float *out, int64_t out_stride, const uint32_t *bin_off, const int32_t *perm);
 gvdb2_status scatter_kernel_backward(Volume *v, int kernel, int n, const float trans[3], gvdb2_points_view weight,
                                      float weight_const, const gvdb2_points_view *attrs, int nch,
                                      const int *grad_chans, float *grad_pos, float *grad_weight, float *grad_attr);

@@ -33,11 +33,11 @@ namespace {
 
 constexpr int64_t kNoAllocMaxPoints = 1 << 20; // 1,048,576 points
 constexpr int64_t kNoAllocMaxSlots = 1 << 15;  // 32,768 active bricks
-constexpr int64_t kOff27Words = 27 * kNoAllocMaxSlots + 1;
-constexpr int64_t kScratchWords = 3 * kNoAllocMaxPoints + kNoAllocMaxSlots + kOff27Words; // 16.25 MB
+constexpr int64_t kOffWords = kNoAllocMaxSlots + 1;
+constexpr int64_t kScratchWords = 3 * kNoAllocMaxPoints + kNoAllocMaxSlots + kOffWords; // 12.25 MB
 
 // [0, P) point slots, [P, 2P) ranks, [2P, 3P) brick-ordered point list,
-// [3P, 3P+S) per-brick counts, then 27-strided per-brick offsets.
+// [3P, 3P+S) per-brick counts, then S+1 per-brick offsets.
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kScratchWords];
 
 constexpr int kMaxDevices = 64;
@@ -72,9 +72,9 @@ __global__ void k_na_bin(PointsView pos, int64_t n, float3 trans, LeafLookup L, 
     if (slot >= 0) prank[i] = atomicAdd(&counts[slot], 1u);
 }
 
-// One CTA: exclusive scan of the per-brick counts into 27-strided offsets.
+// One CTA: exclusive scan of the per-brick counts into offsets (S+1 words).
 constexpr int kNaScanThreads = 1024;
-__global__ void __launch_bounds__(kNaScanThreads) k_na_scan(const uint32_t *counts, int64_t nslots, uint32_t *off27) {
+__global__ void __launch_bounds__(kNaScanThreads) k_na_scan(const uint32_t *counts, int64_t nslots, uint32_t *off) {
     __shared__ uint32_t warp_sum[32];
     const int per = (int)((nslots + kNaScanThreads - 1) / kNaScanThreads);
     const int64_t first = (int64_t)threadIdx.x * per;
@@ -101,20 +101,20 @@ __global__ void __launch_bounds__(kNaScanThreads) k_na_scan(const uint32_t *coun
     uint32_t run = warp_sum[warp] + inc - local;
     for (int k = 0; k < per; k++) {
         if (first + k < nslots) {
-            off27[(first + k) * 27] = run;
+            off[first + k] = run;
             run += counts[first + k];
         }
     }
-    if (first < nslots && first + per >= nslots) off27[nslots * 27] = run; // the thread holding the last brick
+    if (first < nslots && first + per >= nslots) off[nslots] = run; // the thread holding the last brick
 }
 
-__global__ void k_na_fill(const int32_t *pslot, const uint32_t *prank, int64_t n, const uint32_t *off27, int32_t *perm,
+__global__ void k_na_fill(const int32_t *pslot, const uint32_t *prank, int64_t n, const uint32_t *off, int32_t *perm,
                           float *out, int64_t out_stride, int nch) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int32_t s = pslot[i];
     if (s >= 0) {
-        perm[off27[(int64_t)s * 27] + prank[i]] = (int32_t)i;
+        perm[off[s] + prank[i]] = (int32_t)i;
     } else {
         for (int c = 0; c < nch; c++) out[i * out_stride + c] = 0.0f; // outside every active brick
     }
@@ -150,7 +150,7 @@ extern "C" gvdb2_status gvdb2_gather_kernel_noalloc(gvdb2_volume *h, int kernel,
     uint32_t *prank = base + kNoAllocMaxPoints;
     int32_t *perm = reinterpret_cast<int32_t *>(base + 2 * kNoAllocMaxPoints);
     uint32_t *counts = base + 3 * kNoAllocMaxPoints;
-    uint32_t *off27 = counts + kNoAllocMaxSlots;
+    uint32_t *off = counts + kNoAllocMaxSlots;
     const int64_t nslots = v->atlas_last;
     if (n == 0 || nslots == 0) {
         if (n > 0) // no active brick: every point gathers zero
@@ -162,8 +162,8 @@ extern "C" gvdb2_status gvdb2_gather_kernel_noalloc(gvdb2_volume *h, int kernel,
     const float3 t = make_float3(trans[0], trans[1], trans[2]);
     const int g = grid_for(n, 256, 1ll << 31);
     k_na_bin<<<g, 256, 0, v->stream>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(), pslot, prank, counts);
-    k_na_scan<<<1, kNaScanThreads, 0, v->stream>>>(counts, nslots, off27);
-    k_na_fill<<<g, 256, 0, v->stream>>>(pslot, prank, n, off27, perm, out, out_stride, nch);
+    k_na_scan<<<1, kNaScanThreads, 0, v->stream>>>(counts, nslots, off);
+    k_na_fill<<<g, 256, 0, v->stream>>>(pslot, prank, n, off, perm, out, out_stride, nch);
     GV_CUDA(v, cudaGetLastError());
-    return gather_kernel_prebinned(v, kernel, n, trans, chans, nch, out, out_stride, off27, perm);
+    return gather_kernel_prebinned(v, kernel, n, trans, chans, nch, out, out_stride, off, perm);
 }

@@ -51,31 +51,17 @@ __global__ void k_sort_points(PointsView pos, int64_t n, float3 trans, const int
     out[3 * k + 2] = p.z + trans.z;
 }
 
-template <int KERNEL>
-__global__ void k_bin_count(PointsView pos, int64_t n, float3 trans, LeafLookup L, const int32_t *leaf_slot, int res0,
+// Bins every point by the atlas slot of the brick that contains it (-1 when
+// no active brick does); ranks come from warp-aggregated counters.
+__global__ void k_bin_count(PointsView pos, int64_t n, float3 trans, LeafLookup L, const int32_t *leaf_slot,
                             uint32_t *cnt, int32_t *pbin, int32_t *prank) {
-    using T = Taps<KERNEL>;
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int32_t bin = -1;
     if (i < n) {
         float3 p = load_f3(pos, i);
         if (p.z != kNoHit) {
-            float w[3] = {p.x + trans.x, p.y + trans.y, p.z + trans.z};
-            int32_t leaf = leaf_at(L, w[0], w[1], w[2]);
-            int32_t slot = leaf >= 0 ? leaf_slot[leaf] : -1;
-            if (slot >= 0) {
-                int code = 0, mul = 1;
-#pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    int bo = ((int)w[a] >> L.g.log2r0) * res0;
-                    int first = (int)floorf(w[a] - 0.5f) - T::LO - bo;
-                    int last = first + T::N - 1;
-                    int c = first < 0 ? 0 : (last >= res0 ? 2 : 1);
-                    code += c * mul;
-                    mul *= 3;
-                }
-                bin = slot * 27 + code;
-            }
+            int32_t leaf = leaf_at(L, p.x + trans.x, p.y + trans.y, p.z + trans.z);
+            bin = leaf >= 0 ? leaf_slot[leaf] : -1;
         }
     }
     unsigned act = __ballot_sync(0xffffffffu, bin >= 0);
@@ -231,7 +217,8 @@ gvdb2_status insert_points(Volume *v, int n, const float trans[3], int prefix) {
 
 gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     Volume::BinKey &k = v->bin_key;
-    if (k.valid && k.kernel == kernel && k.n == n && k.topo == v->topo_version && k.det == (v->deterministic != 0) &&
+    (void)kernel; // the bins (slot of each point) do not depend on the kernel
+    if (k.valid && k.n == n && k.topo == v->topo_version && k.det == (v->deterministic != 0) &&
         k.pos.base == v->pos.base &&
         k.pos.stride == v->pos.stride && k.pos.offset == v->pos.offset && k.trans[0] == trans[0] &&
         k.trans[1] == trans[1] && k.trans[2] == trans[2])
@@ -239,7 +226,7 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     if (!v->atlas_valid) return fail(v, GVDB2_ERR_STATE, "UpdateAtlas must follow the topology rebuild");
     if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count))) return fail(v, GVDB2_ERR_ARG, "bad point count");
     cudaStream_t s = v->stream;
-    int64_t nbins = 27 * v->atlas_last;
+    int64_t nbins = v->atlas_last;
     GV_CUDA(v, v->pbin.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
     GV_CUDA(v, v->prank.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
     GV_CUDA(v, v->perm.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
@@ -249,15 +236,9 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     float3 t = make_float3(trans[0], trans[1], trans[2]);
     LeafLookup L = make_lookup(v);
     if (n > 0) {
-        int g = grid_for(n, 256, 1ll << 31);
-        if (kernel == GVDB2_KERNEL_TENT1)
-            k_bin_count<GVDB2_KERNEL_TENT1><<<g, 256, 0, s>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(), v->res(0),
-                                                              v->bin_cnt.as<uint32_t>(), v->pbin.as<int32_t>(),
-                                                              v->prank.as<int32_t>());
-        else
-            k_bin_count<GVDB2_KERNEL_CUBIC2><<<g, 256, 0, s>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(), v->res(0),
-                                                               v->bin_cnt.as<uint32_t>(), v->pbin.as<int32_t>(),
-                                                               v->prank.as<int32_t>());
+        k_bin_count<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(),
+                                                                v->bin_cnt.as<uint32_t>(), v->pbin.as<int32_t>(),
+                                                                v->prank.as<int32_t>());
         GV_CUDA(v, cudaGetLastError());
     }
     GV_TRY(exclusive_scan_u32(v, v->bin_cnt.as<uint32_t>(), v->bin_off.as<uint32_t>(), nbins));

@@ -187,59 +187,8 @@ struct SplatArgs {
     int64_t tvox;
 };
 
-// The bins of neighbour k = (dx,dy,dz) whose points reach this brick:
-// along an axis with d = 0 every region, d = -1 the neighbour's high
-// region (2), d = +1 its low region (0).  Ranges are listed per (cz, cy)
-// row: up to 9 per neighbour, 243 per brick.
-constexpr int kRangeSlots = 27 * 9;
-
-__device__ __forceinline__ void neighbour_range(const SplatArgs &S, int64_t slot, int t, uint32_t &beg, uint32_t &end) {
-    beg = end = 0;
-    int k = t / 9, r = t % 9;
-    int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
-    int32_t nb = S.nbr27[slot * 27 + k];
-    if (nb < 0) return;
-    int ylo = dy == 0 ? 0 : (dy < 0 ? 2 : 0), yn = dy == 0 ? 3 : 1;
-    int zlo = dz == 0 ? 0 : (dz < 0 ? 2 : 0), zn = dz == 0 ? 3 : 1;
-    int xlo = dx == 0 ? 0 : (dx < 0 ? 2 : 0), xhi = dx == 0 ? 2 : xlo;
-    if (r >= yn * zn) return;
-    int cy = ylo + r % yn, cz = zlo + r / yn;
-    int64_t base = (int64_t)nb * 27 + (cz * 3 + cy) * 3;
-    beg = S.bin_off[base + xlo];
-    end = S.bin_off[base + xhi + 1];
-}
-
-// Block-wide exclusive scan of one value per thread (warp_tot: 33 words).
-__device__ __forceinline__ uint32_t block_scan_excl(uint32_t x, uint32_t *warp_tot, uint32_t &total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    uint32_t inc = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
-    }
-    if (lane == 31) warp_tot[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = lane < nw ? warp_tot[lane] : 0u;
-        uint32_t wi = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += y;
-        }
-        if (lane < nw) warp_tot[lane] = wi - w;
-        if (lane == 31) warp_tot[32] = wi;
-    }
-    __syncthreads();
-    uint32_t ex = warp_tot[warp] + inc - x;
-    total = warp_tot[32];
-    __syncthreads();
-    return ex;
-}
-
 // Per-channel max |weight * attr| over all points (bounds the fixed-point
-// scale of k_scatter_fixed).  out[c] holds the float bits (>= 0 orders as int).
+// scale of k_scatter_own).  out[c] holds the float bits (>= 0 orders as int).
 template <int NCH>
 __global__ void k_absmax(SplatArgs S, int64_t n, int32_t *out) {
     float m[NCH];
@@ -258,273 +207,209 @@ __global__ void k_absmax(SplatArgs S, int64_t n, int32_t *out) {
     }
 }
 
-// Default scatter: one CTA per atlas slot accumulates its 8^3 interior in
-// shared memory from its own points and the boundary regions of its 26
-// neighbours, then writes the interior once with coalesced stores.  Every
-// (point, voxel) pair is added exactly once, by the CTA owning the voxel.
+// ---- two-phase scatter ---------------------------------------------------
 //
-// Accumulation is fixed point in two int32 words per voxel: a contribution
-// v becomes x = rint(v * 2^s) (64-bit), split into hi = x >> L and
-// lo = x & (2^L - 1), each added with a native shared-memory integer atomic
-// (B200 runs float shared atomics as compare-and-swap loops, integer ones in
-// hardware).  L = 31 - ceil(log2(records + 1)) keeps the lo sums below 2^31;
-// s is chosen so that records * max|a| * 2^s < 2^(29 + L), which bounds the
-// hi sums below 2^30.  Integer sums do not depend on the order of the
-// atomics, so the result is bit-reproducible run to run; each contribution
-// is rounded once (to float, as a float splat would) and the sum is exact.
-constexpr int kAtomicThreads = 256;
-constexpr int kAccPlane = 72; // 8x8 plane padded by 8 words: z-neighbours fall in other banks
+// Phase 1 (k_scatter_own): one CTA per atlas slot splats only the points
+// binned to its brick, with unclipped stencils, into an extended tile that
+// covers every tap of those points: [-H, RES+H)^3 with H = N/2 (12^3 for the
+// cubic B-spline, 10^3 for the tent).  The tile is then written out as float
+// partial sums.
+// Phase 2 (k_scatter_merge): one thread per interior voxel adds, in a
+// fixed neighbour order, the partials of every brick whose extended tile
+// covers the voxel, and writes the channel once.
+//
+// Accumulation in phase 1 is exact: each contribution x (in units of 2^-s)
+// is rounded to an integer and split as rint(x) = hi * 2^L + lo, both parts
+// obtained with the float "magic number" rounding (t = x*2^-L + 1.5*2^23
+// holds rint(x*2^-L) in its low mantissa bits; the remainder x - hi*2^L is
+// exact), and added with native int32 shared-memory atomics.  The integer
+// sums do not depend on the order of the atomics, and the merge sums a fixed
+// sequence of floats, so the result is bit-reproducible run to run.
+// Bounds (R = points of the brick, max|a| = largest weighted amount):
+//   L = min(22, 31 - bits(R+1))      -> |sum lo| <= R * 2^(L-1) < 2^31
+//   max|a| * 2^s < 2^(21+L)          -> |x * 2^-L| < 2^22 (magic range)
+//   R * max|a| * 2^s < 2^(29+L)      -> |sum hi| < 2^29 + R/2
+template <int KERNEL>
+struct ExtTile {
+    static constexpr int N = Taps<KERNEL>::N;
+    static constexpr int H = N / 2;
+    static constexpr int E = 8 + N;                 // 12 (cubic) or 10 (tent)
+    static constexpr int RS = E;                    // row stride (words)
+    static constexpr int PS = N == 4 ? E * E + 8 : E * E; // plane stride: 152 puts a warp's 32 taps in 32 banks
+    static constexpr int CS = E * PS;               // channel stride
+    static constexpr int E3 = E * E * E;            // floats per channel in the global partial
+};
+constexpr int kOwnThreads = 256;
+constexpr int kOwnChunk = 128; // points staged per pass
 
 template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(kAtomicThreads, 6) k_scatter_fixed(SplatArgs S, const int32_t *absmax) {
+constexpr size_t own_smem_bytes() {
+    return sizeof(int32_t) * 2 * NCH * ExtTile<KERNEL>::CS +
+           sizeof(float) * (3 * Taps<KERNEL>::N + NCH) * kOwnChunk + sizeof(int32_t) * kOwnChunk;
+}
+
+__device__ __forceinline__ void fixed_add(int32_t *hi_acc, int32_t *lo_acc, int idx, float x, float inv2L, float two2L) {
+    const float M = 12582912.0f; // 1.5 * 2^23
+    const float t = fmaf(x, inv2L, M);
+    const int hi = __float_as_int(t) - 0x4B400000;
+    const float r = fmaf(t - M, -two2L, x);
+    const int lo = __float_as_int(r + M) - 0x4B400000;
+    atomicAdd(hi_acc + idx, hi);
+    atomicAdd(lo_acc + idx, lo);
+}
+
+template <int KERNEL, int NCH>
+__global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, const int32_t *absmax, float *ext) {
     using T = Taps<KERNEL>;
-    constexpr int N = T::N, RES = 8, ACC = RES * kAccPlane;
-    __shared__ int32_t acc_hi[NCH * ACC], acc_lo[NCH * ACC];
-    __shared__ uint32_t r_beg[kRangeSlots], r_pre[kRangeSlots + 1];
-    __shared__ uint32_t wtot[33];
+    using X = ExtTile<KERNEL>;
+    constexpr int N = T::N;
+    extern __shared__ __align__(16) unsigned char own_smem[];
+    int32_t *acc_hi = reinterpret_cast<int32_t *>(own_smem);
+    int32_t *acc_lo = acc_hi + NCH * X::CS;
+    float(*pw)[kOwnChunk] = reinterpret_cast<float(*)[kOwnChunk]>(acc_lo + NCH * X::CS);
+    float(*pa)[kOwnChunk] = pw + 3 * N;
+    int32_t *pb = reinterpret_cast<int32_t *>(pa + NCH);
+    __shared__ double inv_s[NCH];
     const int64_t slot = blockIdx.x;
-    for (int i = threadIdx.x; i < NCH * ACC; i += blockDim.x) acc_hi[i] = acc_lo[i] = 0;
-    uint32_t b = 0, e = 0;
-    if (threadIdx.x < kRangeSlots) neighbour_range(S, slot, threadIdx.x, b, e);
-    uint32_t total;
-    const uint32_t ex = block_scan_excl(e - b, wtot, total); // ends with a barrier
-    if (threadIdx.x < kRangeSlots) {
-        r_beg[threadIdx.x] = b;
-        r_pre[threadIdx.x] = ex;
-    }
-    __syncthreads();
-    const int L = 31 - (32 - __clz((int)total + 1));
-    __shared__ float scale_s[NCH];
+    for (int i = threadIdx.x; i < NCH * X::CS; i += kOwnThreads) acc_hi[i] = acc_lo[i] = 0;
+    const uint32_t beg = S.bin_off[slot], R = S.bin_off[slot + 1] - beg;
+    int L = 31 - (32 - __clz((int)R + 1));
+    L = L > 22 ? 22 : L;
+    const float inv2L = ldexpf(1.0f, -L), two2L = ldexpf(1.0f, L);
     float scale[NCH];
 #pragma unroll
     for (int c = 0; c < NCH; c++) {
-        const float bound = (float)total * __int_as_float(absmax[c]);
-        int ex2 = 0;
-        frexpf(bound, &ex2); // bound < 2^ex2
-        scale[c] = bound > 0.0f ? ldexpf(1.0f, 29 + L - ex2) : 0.0f;
-        if (threadIdx.x == 0) scale_s[c] = scale[c];
+        const float am = __int_as_float(absmax[c]);
+        int e1 = 0, e2 = 0;
+        frexpf(am, &e1);              // am < 2^e1
+        frexpf((float)R * am, &e2);  // R*am < 2^e2
+        const int sc = min(21 + L - e1, 29 + L - e2);
+        scale[c] = (am > 0.0f && R > 0) ? ldexpf(1.0f, sc) : 0.0f;
+        if (threadIdx.x == 0) inv_s[c] = scale[c] > 0.0f ? ldexp(1.0, -sc) : 0.0;
     }
     const Node &nd = S.leaves[S.slot_leaf[slot]];
-    const int ox = nd.mPos[0], oy = nd.mPos[1], oz = nd.mPos[2];
-    const long long lmask = (1ll << L) - 1;
-    for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
-        int lo = 0, hi = kRangeSlots - 1; // last range with r_pre <= j
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (r_pre[mid] <= j) lo = mid;
-            else hi = mid - 1;
+    const int ox = nd.mPos[0] - X::H, oy = nd.mPos[1] - X::H, oz = nd.mPos[2] - X::H;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t base = 0; base < R; base += kOwnChunk) {
+        const int cnt = (int)min((uint32_t)kOwnChunk, R - base);
+        __syncthreads(); // accumulators cleared / previous chunk consumed
+        if ((int)threadIdx.x < cnt) {
+            const int32_t p = S.perm[beg + base + threadIdx.x];
+            const float3 q = load_f3(S.pos, p);
+            float wx[N], wy[N], wz[N];
+            const int fx = T::eval(q.x + S.trans.x, wx) - ox;
+            const int fy = T::eval(q.y + S.trans.y, wy) - oy;
+            const int fz = T::eval(q.z + S.trans.z, wz) - oz;
+            // a binned point lies in the brick, so its first taps are in [0, 8];
+            // anything else (inconsistent input) is dropped, never written outside the tile
+            const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
+            pb[threadIdx.x] = ok ? (fx | (fy << 8) | (fz << 16)) : 0;
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                pw[k][threadIdx.x] = wx[k];
+                pw[N + k][threadIdx.x] = wy[k];
+                pw[2 * N + k][threadIdx.x] = wz[k];
+            }
+            const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
+#pragma unroll
+            for (int c = 0; c < NCH; c++)
+                pa[c][threadIdx.x] = ok ? (((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt) * scale[c] : 0.0f;
         }
-        const int32_t p = S.perm[r_beg[lo] + (j - r_pre[lo])];
-        const float3 q = load_f3(S.pos, p);
-        float wx[N], wy[N], wz[N];
-        const int fx = T::eval(q.x + S.trans.x, wx) - ox;
-        const int fy = T::eval(q.y + S.trans.y, wy) - oy;
-        const int fz = T::eval(q.z + S.trans.z, wz) - oz;
-        const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
-        float amt[NCH];
+        __syncthreads();
+        if constexpr (N == 4) {
+            // one point per warp step: lane = (tx, ty, z pair); two taps per lane
+            const int tx = lane & 3, ty = (lane >> 2) & 3, tz0 = (lane >> 4) * 2;
+            for (int j = warp; j < cnt; j += kOwnThreads / 32) {
+                const int b = pb[j];
+                const int a0 = ((b >> 16) + tz0) * X::PS + (((b >> 8) & 255) + ty) * X::RS + (b & 255) + tx;
+                const float wxv = pw[tx][j], wyv = pw[N + ty][j];
+                const float w0 = wxv * (wyv * pw[2 * N + tz0][j]);
+                const float w1 = wxv * (wyv * pw[2 * N + tz0 + 1][j]);
 #pragma unroll
-        for (int c = 0; c < NCH; c++) amt[c] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt;
-#pragma unroll
-        for (int c = 0; c < NCH; c++) amt[c] *= scale[c];
-        // z taps in a rolled loop (the weights rotate through registers) keep
-        // the unrolled body small enough for the instruction cache
-#pragma unroll 1
-        for (int tz = 0; tz < N; tz++) {
-            const int lz = fz + tz;
-            const float wzt = wz[0];
-#pragma unroll
-            for (int k = 0; k + 1 < N; k++) wz[k] = wz[k + 1];
-            if ((unsigned)lz >= (unsigned)RES) continue;
-#pragma unroll
-            for (int ty = 0; ty < N; ty++) {
-                const int ly = fy + ty;
-                if ((unsigned)ly >= (unsigned)RES) continue;
-                const float wyz = wy[ty] * wzt;
-                const int row = lz * kAccPlane + ly * RES;
-#pragma unroll
-                for (int tx = 0; tx < N; tx++) {
-                    const int lx = fx + tx;
-                    if ((unsigned)lx >= (unsigned)RES) continue;
-                    const float w = wx[tx] * wyz;
-#pragma unroll
-                    for (int c = 0; c < NCH; c++) {
-                        const long long xv = __float2ll_rn(amt[c] * w);
-                        atomicAdd(&acc_hi[c * ACC + row + lx], (int)(xv >> L));
-                        atomicAdd(&acc_lo[c * ACC + row + lx], (int)(xv & lmask));
-                    }
+                for (int c = 0; c < NCH; c++) {
+                    const float am = pa[c][j];
+                    fixed_add(acc_hi + c * X::CS, acc_lo + c * X::CS, a0, am * w0, inv2L, two2L);
+                    fixed_add(acc_hi + c * X::CS, acc_lo + c * X::CS, a0 + X::PS, am * w1, inv2L, two2L);
                 }
+            }
+        } else {
+            // four points per warp step, one tap per lane
+            const int sub = lane >> 3, tx = lane & 1, ty = (lane >> 1) & 1, tz = (lane >> 2) & 1;
+            for (int j0 = warp * 4; j0 < cnt; j0 += kOwnThreads / 8) {
+                const int j = j0 + sub;
+                if (j >= cnt) continue;
+                const int b = pb[j];
+                const int a = ((b >> 16) + tz) * X::PS + (((b >> 8) & 255) + ty) * X::RS + (b & 255) + tx;
+                const float w = pw[tx][j] * (pw[N + ty][j] * pw[2 * N + tz][j]);
+#pragma unroll
+                for (int c = 0; c < NCH; c++)
+                    fixed_add(acc_hi + c * X::CS, acc_lo + c * X::CS, a, pa[c][j] * w, inv2L, two2L);
             }
         }
     }
     __syncthreads();
-    const int a = S.apron, tl = S.tile;
-    for (int i = threadIdx.x; i < NCH * RES * RES * RES; i += blockDim.x) {
-        const int c = i >> 9, v = i & 511;
-        const int lx = v & 7, ly = (v >> 3) & 7, lz = v >> 6;
-        const int k = c * ACC + lz * kAccPlane + ly * RES + lx;
+    // thread t writes elements t, t+256, ... (coalesced); its (c, z, y, x)
+    // advances by the base-E digits of 256 instead of being divided out
+    constexpr int E = X::E, DZ = kOwnThreads / (E * E), DY = (kOwnThreads / E) % E, DX = kOwnThreads % E;
+    static_assert(DZ < E, "one wrap per step");
+    float *dst = ext + slot * (int64_t)NCH * X::E3;
+    int c = 0, z = threadIdx.x / (E * E), y = (threadIdx.x / E) % E, x = threadIdx.x % E;
+    for (int i = threadIdx.x; i < NCH * X::E3; i += kOwnThreads) {
+        const int k = c * X::CS + z * X::PS + y * X::RS + x;
+        // |sum| < 2^53: exact in double; the power-of-two scaling is exact
         const long long sum = ((long long)acc_hi[k] << L) + (long long)acc_lo[k];
-        const float sc = scale_s[c];
-        const float val = sc > 0.0f ? (float)((double)sum / (double)sc) : 0.0f;
-        if (c < S.nch) S.chan[c][slot * S.tvox + ((int64_t)(lz + a) * tl + (ly + a)) * tl + (lx + a)] = val;
+        dst[i] = (float)((double)sum * inv_s[c]);
+        x += DX;
+        if (x >= E) { x -= E; y++; }
+        y += DY;
+        if (y >= E) { y -= E; z++; }
+        z += DZ;
+        if (z >= E) { z -= E; c++; }
     }
 }
 
-constexpr int kScatterThreads = 512; // one thread per interior voxel of an 8^3 brick
-constexpr int kScatterRes = 8;
-
-// Shared-memory bytes of k_scatter_tile for a record capacity `cap`.
-__host__ __device__ constexpr size_t scatter_smem_bytes(int ntaps, int nch, int cap) {
-    return (size_t)cap * (3 * ntaps + nch + 1) * 4 + (size_t)cap * 6 +
-           (size_t)((kScatterRes + ntaps - 1) * (kScatterRes + ntaps - 1) * (kScatterRes + ntaps - 1) + 1) * 4;
-}
-
-// Scatter as a gather over shared memory: one CTA per atlas slot, one
-// thread per interior voxel.  The CTA stages the records of every point
-// whose stencil reaches the brick (its own points and the boundary regions
-// of its 26 neighbours): per-axis tap weights, weighted attributes and the
-// point index.  Records are counting-sorted by the stencil's first tap
-// (a cell of (8+N-1)^3) and each cell's records are ordered by point index.
-// A voxel then sums the N^3 cells whose stencils cover it in a fixed order:
-// no atomics on the accumulators, and the sum order does not depend on the
-// order in which points were binned (bit-reproducible while a brick's
-// records fit one chunk; the deterministic option also makes the binning
-// stable so multi-chunk bricks reproduce too).
+// Phase 2: interior voxel v of the slot sums, in a fixed order, the partial
+// of every brick whose extended tile covers v.
 template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(kScatterThreads, 3) k_scatter_tile(SplatArgs S, int cap) {
-    using T = Taps<KERNEL>;
-    constexpr int N = T::N, RES = kScatterRes, CA = RES + N - 1, C3 = CA * CA * CA;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float *wgt = reinterpret_cast<float *>(smem_raw); // [3*N][cap]
-    float *att = wgt + 3 * N * cap;                    // [NCH][cap]
-    int32_t *pid = reinterpret_cast<int32_t *>(att + NCH * cap);
-    uint16_t *cellof = reinterpret_cast<uint16_t *>(pid + cap);
-    uint16_t *order = cellof + cap;
-    uint32_t *coff = reinterpret_cast<uint32_t *>(order + cap); // [C3 + 1]
-    uint8_t *tx0 = reinterpret_cast<uint8_t *>(coff + C3 + 1); // first x tap (cell coordinate)
-    __shared__ uint32_t r_beg[kRangeSlots], r_pre[kRangeSlots + 1];
-    __shared__ uint32_t wtot[33];
+__global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S, const float *ext) {
+    using X = ExtTile<KERNEL>;
+    __shared__ int32_t nb[27];
     const int64_t slot = blockIdx.x;
-
-    uint32_t b = 0, e = 0;
-    if (threadIdx.x < kRangeSlots) neighbour_range(S, slot, threadIdx.x, b, e);
-    uint32_t total;
-    uint32_t ex = block_scan_excl(e - b, wtot, total);
-    if (threadIdx.x < kRangeSlots) {
-        r_beg[threadIdx.x] = b;
-        r_pre[threadIdx.x] = ex;
-    }
-    if (threadIdx.x == 0) r_pre[kRangeSlots] = total;
-    const Node &nd = S.leaves[S.slot_leaf[slot]];
-    const int ox = nd.mPos[0], oy = nd.mPos[1], oz = nd.mPos[2];
+    if (threadIdx.x < 27) nb[threadIdx.x] = S.nbr27[slot * 27 + threadIdx.x];
+    __syncthreads();
     const int vx = threadIdx.x & 7, vy = (threadIdx.x >> 3) & 7, vz = threadIdx.x >> 6;
     float acc[NCH];
 #pragma unroll
     for (int c = 0; c < NCH; c++) acc[c] = 0.0f;
-
-    for (uint32_t base = 0; base < total; base += cap) {
-        const int cnt = (int)min((uint32_t)cap, total - base);
-        for (int i = threadIdx.x; i <= C3; i += blockDim.x) coff[i] = 0;
-        __syncthreads();
-        // stage records
-        for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
-            const uint32_t j = base + r;
-            int lo = 0, hi = kRangeSlots - 1; // last range with r_pre <= j
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (r_pre[mid] <= j) lo = mid;
-                else hi = mid - 1;
-            }
-            const int32_t p = S.perm[r_beg[lo] + (j - r_pre[lo])];
-            const float3 q = load_f3(S.pos, p);
-            float wx[N], wy[N], wz[N];
-            const int tx = T::eval(q.x + S.trans.x, wx) - ox + N - 1;
-            const int ty = T::eval(q.y + S.trans.y, wy) - oy + N - 1;
-            const int tz = T::eval(q.z + S.trans.z, wz) - oz + N - 1;
+    // Per axis the covering bricks are d = 0 and, within H of a face, the
+    // neighbour across it (e = -1 or +1; never both, H <= 4).  The up to 8
+    // combinations are read first (predicated), then summed in a fixed order.
+    const int ex = vx < X::H ? -1 : (vx >= 8 - X::H ? 1 : 0);
+    const int ey = vy < X::H ? -1 : (vy >= 8 - X::H ? 1 : 0);
+    const int ez = vz < X::H ? -1 : (vz >= 8 - X::H ? 1 : 0);
+    float part[8][NCH];
 #pragma unroll
-            for (int k = 0; k < N; k++) {
-                wgt[(0 * N + k) * cap + r] = wx[k];
-                wgt[(1 * N + k) * cap + r] = wy[k];
-                wgt[(2 * N + k) * cap + r] = wz[k];
-            }
-            const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
+    for (int m = 0; m < 8; m++) {
+        const int dx = (m & 1) ? ex : 0, dy = (m & 2) ? ey : 0, dz = (m & 4) ? ez : 0;
+        const bool used = (!(m & 1) || ex) && (!(m & 2) || ey) && (!(m & 4) || ez);
+        const int n = used ? nb[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] : -1;
+        const int ux = vx - 8 * dx + X::H, uy = vy - 8 * dy + X::H, uz = vz - 8 * dz + X::H;
+        const float *src = ext + (int64_t)max(n, 0) * NCH * X::E3 + (uz * X::E + uy) * X::E + ux;
 #pragma unroll
-            for (int c = 0; c < NCH; c++) att[c * cap + r] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt;
-            pid[r] = p;
-            const bool ok = tx >= 0 && tx < CA && ty >= 0 && ty < CA && tz >= 0 && tz < CA;
-            const int cell = ok ? (tz * CA + ty) * CA + tx : C3;
-            cellof[r] = (uint16_t)cell;
-            tx0[r] = (uint8_t)tx;
-            if (ok) atomicAdd(&coff[cell], 1u);
-        }
-        __syncthreads();
-        // exclusive scan of the cell counts: thread t owns cells [t*K, t*K+K)
-        {
-            constexpr int K = (C3 + kScatterThreads - 1) / kScatterThreads;
-            uint32_t loc[K], sum = 0;
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                int i = threadIdx.x * K + k;
-                loc[k] = i < C3 ? coff[i] : 0u;
-                sum += loc[k];
-            }
-            uint32_t tot;
-            uint32_t run = block_scan_excl(sum, wtot, tot);
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                int i = threadIdx.x * K + k;
-                if (i < C3) coff[i] = run;
-                run += loc[k];
-            }
-        }
-        __syncthreads();
-        // place; afterwards coff[c] is the end of cell c (start = coff[c-1])
-        for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
-            const int cell = cellof[r];
-            if (cell < C3) order[atomicAdd(&coff[cell], 1u)] = (uint16_t)r;
-        }
-        __syncthreads();
-        // order each cell's records by point index
-        for (int c = threadIdx.x; c < C3; c += blockDim.x) {
-            const int s0 = c ? (int)coff[c - 1] : 0, s1 = (int)coff[c];
-            for (int k = s0 + 1; k < s1; k++) {
-                const uint16_t rk = order[k];
-                const int32_t pk = pid[rk];
-                int m = k - 1;
-                while (m >= s0 && pid[order[m]] > pk) {
-                    order[m + 1] = order[m];
-                    m--;
-                }
-                order[m + 1] = rk;
-            }
-        }
-        __syncthreads();
-        // this thread's voxel sums the records whose stencils cover it.  For
-        // fixed (dz, dy) the N cells of x offsets 0..N-1 are adjacent in the
-        // sorted order, so each row is one contiguous range of records.
-#pragma unroll 1
-        for (int dz = 0; dz < N; dz++) {
-#pragma unroll 1
-            for (int dy = 0; dy < N; dy++) {
-                const int chi = ((vz - dz + N - 1) * CA + (vy - dy + N - 1)) * CA + (vx + N - 1);
-                const int clo = chi - (N - 1);
-                const int s0 = clo ? (int)coff[clo - 1] : 0, s1 = (int)coff[chi];
-                for (int k = s0; k < s1; k++) {
-                    const int r = order[k];
-                    const int dx = vx + N - 1 - tx0[r];
-                    const float w = wgt[(0 * N + dx) * cap + r] * wgt[(1 * N + dy) * cap + r] * wgt[(2 * N + dz) * cap + r];
-#pragma unroll
-                    for (int c = 0; c < NCH; c++) acc[c] = fmaf(att[c * cap + r], w, acc[c]);
-                }
-            }
-        }
-        __syncthreads();
+        for (int c = 0; c < NCH; c++) part[m][c] = n >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
     }
+#pragma unroll
+    for (int m = 0; m < 8; m++)
+#pragma unroll
+        for (int c = 0; c < NCH; c++) acc[c] += part[m][c];
     const int a = S.apron, tl = S.tile;
     const int64_t at = slot * S.tvox + ((int64_t)(vz + a) * tl + (vy + a)) * tl + (vx + a);
 #pragma unroll
     for (int c = 0; c < NCH; c++)
         if (c < S.nch) S.chan[c][at] = acc[c];
 }
+
+constexpr int kScatterRes = 8; // brick edge the kernel splats take
 
 // ---------------------------------------------------------------------
 // tiled gathers: forward, scatter adjoint, gather adjoint
@@ -581,7 +466,7 @@ __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
     __syncthreads();
     const Node &nd = G.leaves[G.slot_leaf[slot]];
     const int ox = nd.mPos[0] - H, oy = nd.mPos[1] - H, oz = nd.mPos[2] - H;
-    const uint32_t beg = G.bin_off[slot * 27], end = G.bin_off[slot * 27 + 27];
+    const uint32_t beg = G.bin_off[slot], end = G.bin_off[slot + 1];
     for (uint32_t j = beg + threadIdx.x; j < end; j += blockDim.x) {
         const int32_t pidx = G.perm[j];
         const float3 p = load_f3(G.pos, pidx);
@@ -712,47 +597,62 @@ gvdb2_status launch_smem(Volume *v, K kernel, size_t smem, const char *what) {
     return GVDB2_OK;
 }
 
+// Two-phase scatter of up to 4 channels (one group).
 template <int KERNEL, int NCH>
-gvdb2_status launch_scatter(Volume *v, const SplatArgs &S) {
-    if (!v->deterministic) {
-        int32_t *absmax = nullptr;
-        GV_CUDA(v, cudaMallocAsync((void **)&absmax, sizeof(int32_t) * NCH, v->stream));
-        GV_CUDA(v, cudaMemsetAsync(absmax, 0, sizeof(int32_t) * NCH, v->stream));
-        const int64_t n = v->bin_key.n;
-        if (n > 0)
-            k_absmax<NCH><<<std::min(grid_for(n, 256), 4 * kSmCount), 256, 0, v->stream>>>(S, n, absmax);
-        k_scatter_fixed<KERNEL, NCH><<<(unsigned)v->atlas_last, kAtomicThreads, 0, v->stream>>>(S, absmax);
-        cudaError_t e = cudaGetLastError();
-        cudaFreeAsync(absmax, v->stream);
-        if (e != cudaSuccess) return cuda_fail(v, e, "k_scatter_fixed");
-        return GVDB2_OK;
-    }
-    const int cap = NCH <= 4 ? 768 : 512;
-    const size_t smem = scatter_smem_bytes(Taps<KERNEL>::N, NCH, cap);
-    auto k = k_scatter_tile<KERNEL, NCH>;
-    GV_TRY(launch_smem(v, k, smem, "scatter"));
-    k<<<(unsigned)v->atlas_last, kScatterThreads, smem, v->stream>>>(S, cap);
+gvdb2_status scatter_group(Volume *v, const SplatArgs &S) {
+    using X = ExtTile<KERNEL>;
+    cudaStream_t s = v->stream;
+    const int64_t nslots = v->atlas_last;
+    GV_CUDA(v, v->scratch.ensure(sizeof(float) * (size_t)nslots * NCH * X::E3 + 256, s));
+    float *ext = v->scratch.as<float>();
+    GV_CUDA(v, v->tmp_b.ensure(sizeof(int32_t) * 8, s));
+    int32_t *absmax = v->tmp_b.as<int32_t>();
+    GV_CUDA(v, cudaMemsetAsync(absmax, 0, sizeof(int32_t) * NCH, s));
+    const int64_t n = v->bin_key.n;
+    if (n > 0) k_absmax<NCH><<<std::min(grid_for(n, 256), 4 * kSmCount), 256, 0, s>>>(S, n, absmax);
+    constexpr size_t smem = own_smem_bytes<KERNEL, NCH>();
+    auto k1 = k_scatter_own<KERNEL, NCH>;
+    GV_TRY(launch_smem(v, k1, smem, "scatter"));
+    k1<<<(unsigned)nslots, kOwnThreads, smem, s>>>(S, absmax, ext);
+    k_scatter_merge<KERNEL, NCH><<<(unsigned)nslots, 512, 0, s>>>(S, ext);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
 
-template <int KERNEL>
-gvdb2_status launch_scatter_n(Volume *v, const SplatArgs &S) {
-    switch (S.nch) {
-    case 1: return launch_scatter<KERNEL, 1>(v, S);
-    case 2: return launch_scatter<KERNEL, 2>(v, S);
-    case 3: return launch_scatter<KERNEL, 3>(v, S);
-    case 4: return launch_scatter<KERNEL, 4>(v, S);
-    default: return launch_scatter<KERNEL, 8>(v, S);
+// channels [first, first + count) of S as a group of their own
+SplatArgs channel_group(const SplatArgs &S, int first, int count) {
+    SplatArgs G = S;
+    G.attr_mask = (S.attr_mask >> first) & ((1u << count) - 1);
+    for (int c = 0; c < kMaxSplatChan; c++) {
+        const bool in = c < count;
+        G.chan[c] = in ? S.chan[first + c] : nullptr;
+        G.attr[c] = in ? S.attr[first + c] : PointsView{};
     }
+    G.nch = count;
+    return G;
+}
+
+template <int KERNEL>
+gvdb2_status scatter_two_phase(Volume *v, const SplatArgs &S) {
+    for (int first = 0; first < S.nch; first += 4) {
+        const int cnt = std::min(4, S.nch - first);
+        const SplatArgs G = channel_group(S, first, cnt);
+        switch (cnt) {
+        case 1: GV_TRY((scatter_group<KERNEL, 1>(v, G))); break;
+        case 2: GV_TRY((scatter_group<KERNEL, 2>(v, G))); break;
+        case 3: GV_TRY((scatter_group<KERNEL, 3>(v, G))); break;
+        default: GV_TRY((scatter_group<KERNEL, 4>(v, G))); break;
+        }
+    }
+    return GVDB2_OK;
 }
 
 gvdb2_status run_scatter(Volume *v, int kernel, const SplatArgs &S) {
     if (v->atlas_last == 0) return GVDB2_OK;
     if (v->res(0) != kScatterRes)
         return fail(v, GVDB2_ERR_UNSUPPORTED, "kernel splats need 8^3 bricks (Configure(...,3))");
-    return kernel == GVDB2_KERNEL_TENT1 ? launch_scatter_n<GVDB2_KERNEL_TENT1>(v, S)
-                                        : launch_scatter_n<GVDB2_KERNEL_CUBIC2>(v, S);
+    return kernel == GVDB2_KERNEL_TENT1 ? scatter_two_phase<GVDB2_KERNEL_TENT1>(v, S)
+                                        : scatter_two_phase<GVDB2_KERNEL_CUBIC2>(v, S);
 }
 
 template <int KERNEL, int MODE, int NCH>
@@ -909,7 +809,7 @@ gvdb2_status gather_kernel(Volume *v, int kernel, int n, const float trans[3], c
 }
 
 gvdb2_status gather_kernel_prebinned(Volume *v, int kernel, int n, const float trans[3], const int *chans, int nch,
-                                     float *out, int64_t out_stride, const uint32_t *bin_off27, const int32_t *perm) {
+                                     float *out, int64_t out_stride, const uint32_t *bin_off, const int32_t *perm) {
     GV_TRY(check_chans(v, chans, nch));
     if (!out || out_stride < nch) return fail(v, GVDB2_ERR_ARG, "bad output buffer");
     if (kernel != GVDB2_KERNEL_TENT1 && kernel != GVDB2_KERNEL_CUBIC2) return fail(v, GVDB2_ERR_ARG, "unknown kernel");
@@ -923,7 +823,7 @@ gvdb2_status gather_kernel_prebinned(Volume *v, int kernel, int n, const float t
     G.out = out;
     G.out_stride = out_stride;
     fill_topology(v, G);
-    G.bin_off = bin_off27;
+    G.bin_off = bin_off;
     G.perm = perm;
     return run_gather<kFwd>(v, kernel, G);
 }

@@ -649,6 +649,28 @@ gvdb2_status sync_counts(Volume *v) {
     return GVDB2_OK;
 }
 
+// Grows the device's stream-ordered pool once per point-count high-water
+// mark, so that buffers tracking a spreading topology (atlas, splat scratch,
+// bins) are later carved from memory already mapped instead of mapping new
+// physical memory in the middle of a step.  About 1 KB per point covers the
+// rebuild, an atlas of 4 channels and the splat scratch; at most a quarter
+// of the free device memory is taken.
+void reserve_pool(Volume *v, int64_t n) {
+    if (n <= v->pool_reserved_for) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, v->device) != cudaSuccess) return;
+    uint64_t reserved = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return;
+    const uint64_t want = std::min<uint64_t>((uint64_t)n * 1024 + (256ull << 20), free_b / 4);
+    v->pool_reserved_for = n;
+    if (reserved >= want) return;
+    void *p = nullptr;
+    if (cudaMallocAsync(&p, want - reserved, v->stream) == cudaSuccess) cudaFreeAsync(p, v->stream);
+    cudaGetLastError(); // a failed reservation is only a missed optimisation
+}
+
 gvdb2_status rebuild_topology(Volume *v, int n, float radius, const float orig[3], bool accumulate, int min_depth) {
     if (v->nlev == 0) return fail(v, GVDB2_ERR_STATE, "Configure not called");
     if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count)))
@@ -658,6 +680,7 @@ gvdb2_status rebuild_topology(Volume *v, int n, float radius, const float orig[3
         GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), s));
         GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
     }
+    reserve_pool(v, n);
     // GetBoundingBox
     int32_t init[6];
     for (int a = 0; a < 3; a++) {

@@ -154,7 +154,7 @@ GVDB2_API gvdb2_status gvdb2_gather_kernel_backward(gvdb2_volume *v, int kernel,
  * budget at start-up, a real-time loop that forbids allocation, a process
  * whose allocator belongs to another framework).  No counterpart in the
  * reference.  It performs no device allocation: its binning scratch is one
- * file-scope device array per GPU (16.25 MB, held until the process exits),
+ * file-scope device array per GPU (12.25 MB, held until the process exits),
  * which limits a call to 1,048,576 points and 32,768 active bricks; larger
  * calls return GVDB2_ERR_CAPACITY.  The first call on a device looks up the
  * array's address (make it before any stream capture).  All calls share the
