@@ -12,6 +12,8 @@
 //     neighbour table of UpdateNeighbors (V:2527-2556).  A missing
 //     neighbour is -1 here; the reference stores 0xFFFF and then fails to
 //     recognise it (O:51).
+#include <vector>
+
 #include "dev_common.cuh"
 
 namespace gvdb2 {
@@ -23,24 +25,31 @@ struct ApronChans {
     int nch;
 };
 
-// One CTA per slot; every channel of the call in one pass.
-__global__ void __launch_bounds__(256) k_apron(ApronChans C, const int32_t *nbr27, int res, int apron, int tile,
+// One CTA per slot; every channel of the call in one pass.  `list` holds,
+// in tile order, every apron voxel of a tile: its tile offset and the
+// neighbour k (0..26) that owns it with the offset of the owner's interior
+// voxel, so the kernel does no index arithmetic.  For each voxel all loads
+// (up to 4 channels at a time) are issued before the stores.
+__global__ void __launch_bounds__(256) k_apron(ApronChans C, const int32_t *nbr27, const int2 *list, int nlist,
                                                int64_t tvox, float boundval) {
     const int64_t slot = blockIdx.x;
     __shared__ int32_t nbs[27];
     if (threadIdx.x < 27) nbs[threadIdx.x] = nbr27[slot * 27 + threadIdx.x];
     __syncthreads();
-    for (int t = threadIdx.x; t < tvox; t += blockDim.x) {
-        const int x = t % tile, y = (t / tile) % tile, z = t / (tile * tile);
-        const int lx = x - apron, ly = y - apron, lz = z - apron;
-        const int dx = lx < 0 ? -1 : (lx >= res ? 1 : 0), dy = ly < 0 ? -1 : (ly >= res ? 1 : 0),
-                  dz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
-        if ((dx | dy | dz) == 0) continue; // interior voxel
-        const int32_t nb = nbs[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
-        const int64_t src = (int64_t)nb * tvox +
-                            ((int64_t)(lz - dz * res + apron) * tile + (ly - dy * res + apron)) * tile +
-                            (lx - dx * res + apron);
-        for (int c = 0; c < C.nch; c++) C.chan[c][slot * tvox + t] = nb >= 0 ? C.chan[c][src] : boundval;
+    for (int i = threadIdx.x; i < nlist; i += blockDim.x) {
+        const int2 e = list[i];
+        const int32_t nb = nbs[e.y >> 24];
+        const int64_t src = (int64_t)nb * tvox + (e.y & 0xFFFFFF);
+        const int64_t dst = slot * tvox + e.x;
+        for (int c0 = 0; c0 < C.nch; c0 += 4) {
+            float val[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                val[j] = (c0 + j < C.nch && nb >= 0) ? __ldcg(C.chan[c0 + j] + src) : boundval;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (c0 + j < C.nch) C.chan[c0 + j][dst] = val[j];
+        }
     }
 }
 
@@ -69,6 +78,33 @@ __global__ void __launch_bounds__(256) k_apron_faces(float *chan, const int32_t 
     }
 }
 
+// The apron voxels of a tile in tile order (built once per brick geometry):
+// x = tile offset; y = owning neighbour k << 24 | offset of its interior voxel.
+gvdb2_status apron_list(Volume *v) {
+    const int res = v->res(0), a = v->apron, t = v->tile_res();
+    const int key = res * 64 + a;
+    if (v->apron_list_key == key && v->apron_list.p) return GVDB2_OK;
+    std::vector<int2> h;
+    for (int z = 0; z < t; z++)
+        for (int y = 0; y < t; y++)
+            for (int x = 0; x < t; x++) {
+                const int lx = x - a, ly = y - a, lz = z - a;
+                const int dx = lx < 0 ? -1 : (lx >= res ? 1 : 0), dy = ly < 0 ? -1 : (ly >= res ? 1 : 0),
+                          dz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
+                if ((dx | dy | dz) == 0) continue;
+                const int k = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+                const int src = ((lz - dz * res + a) * t + (ly - dy * res + a)) * t + (lx - dx * res + a);
+                h.push_back(make_int2((z * t + y) * t + x, (k << 24) | src));
+            }
+    if ((int64_t)t * t * t >= (1 << 24)) return fail(v, GVDB2_ERR_UNSUPPORTED, "brick tile too large for the apron list");
+    GV_CUDA(v, v->apron_list.ensure(sizeof(int2) * h.size(), v->stream));
+    GV_CUDA(v, cudaMemcpyAsync(v->apron_list.p, h.data(), sizeof(int2) * h.size(), cudaMemcpyHostToDevice, v->stream));
+    GV_CUDA(v, cudaStreamSynchronize(v->stream)); // h is released on return
+    v->apron_list_n = (int)h.size();
+    v->apron_list_key = key;
+    return GVDB2_OK;
+}
+
 } // namespace
 
 gvdb2_status update_apron(Volume *v, int chan, float boundval) {
@@ -85,8 +121,9 @@ gvdb2_status update_apron(Volume *v, int chan, float boundval) {
         C.chan[C.nch++] = v->atlas[c].as<float>();
     }
     if (v->atlas_last == 0 || C.nch == 0) return GVDB2_OK;
-    k_apron<<<(unsigned)v->atlas_last, 256, 0, v->stream>>>(C, v->nbr27.as<int32_t>(), v->res(0), v->apron,
-                                                            v->tile_res(), v->tile_vox(), boundval);
+    GV_TRY(apron_list(v));
+    k_apron<<<(unsigned)v->atlas_last, 256, 0, v->stream>>>(C, v->nbr27.as<int32_t>(), v->apron_list.as<int2>(),
+                                                            v->apron_list_n, v->tile_vox(), boundval);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }

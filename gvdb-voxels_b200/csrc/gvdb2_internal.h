@@ -105,6 +105,8 @@ struct Volume {
     DevBuf leaf_slot;         // int32 per pool leaf: slot or -1
     DevBuf nbr27;             // int32 per slot x 27: neighbour slots
     DevBuf nbr6;              // int32 per pool leaf x 6 (UpdateNeighbors)
+    DevBuf apron_list;        // int2 per apron voxel of a tile (UpdateApron)
+    int apron_list_n = 0, apron_list_key = -1;
     bool nbr6_valid = false;
     bool atlas_valid = false; // slots assigned for the current topology
 
