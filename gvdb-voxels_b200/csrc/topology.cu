@@ -441,12 +441,15 @@ gvdb2_status ensure_pool(Volume *v, int lev, int64_t cnt) {
     return GVDB2_OK;
 }
 
-// ActivateBricksGPU (+ ActivateExtraBricksGPU when radius >= 1).
-gvdb2_status full_rebuild(Volume *v, int n, float radius, const float orig[3]) {
+gvdb2_status build_from_keys(Volume *v, const int64_t nB[], const int64_t nE[], const KeyGeom &g);
+
+// Node key sets of the full rebuild through hash sets and radix sorts (any
+// extent): lev_keys[l][0] = sorted base keys (nB[l]), lev_keys[l][1] =
+// sorted extra keys (nE[l]).
+gvdb2_status key_sets_hash(Volume *v, int n, float radius, const float orig[3], const KeyGeom &g, int64_t nB[],
+                           int64_t nE[]) {
     cudaStream_t s = v->stream;
     const int depth = v->depth;
-    KeyGeom g = key_geom(v);
-    if (g.span > 65536) return fail(v, GVDB2_ERR_UNSUPPORTED, "root spans more than 65536 bricks per axis");
     const int kbits = 3 * g.b;
     const bool do_box = radius >= 1.0f;
 
@@ -493,7 +496,8 @@ gvdb2_status full_rebuild(Volume *v, int n, float radius, const float orig[3]) {
         k_compact_set<<<grid_for(cap, 256, 4096), 256, 0, s>>>(v->hs_keys[1].as<uint64_t>(), cap,
                                                                v->tmp_a.as<uint64_t>(), dev_words(v)->count + 3);
     GV_CUDA(v, cudaGetLastError());
-    int64_t nB[kMaxLev] = {0}, nX[kMaxLev] = {0}, nE[kMaxLev] = {0};
+    int64_t nX[kMaxLev] = {0};
+    for (int l = 0; l < kMaxLev; l++) nB[l] = nE[l] = 0;
     GV_TRY(radix_sort_u64(v, v->lev_keys[0][0].as<uint64_t>(), nullptr, nb, 0, kbits));
     nB[0] = nb;
     uint64_t *xkeys[kMaxLev] = {nullptr};
@@ -544,7 +548,13 @@ gvdb2_status full_rebuild(Volume *v, int n, float radius, const float orig[3]) {
         }
     }
     for (int q = 0; q < kMaxLev; q++) xbuf[q].release();
+    return GVDB2_OK;
+}
 
+// Pools, child lists, links and the leaf map from the sorted key sets.
+gvdb2_status build_from_keys(Volume *v, const int64_t nB[], const int64_t nE[], const KeyGeom &g) {
+    cudaStream_t s = v->stream;
+    const int depth = v->depth;
     // pools: level l < depth holds [B[l], E[l]]; the root sits at `depth`
     for (int l = 0; l < kMaxLev; l++) v->pool_cnt[l] = 0;
     for (int l = 0; l < depth; l++) v->pool_cnt[l] = nB[l] + nE[l];
@@ -602,6 +612,340 @@ gvdb2_status full_rebuild(Volume *v, int n, float radius, const float orig[3]) {
 }
 
 gvdb2_status incremental_activate(Volume *v, int n, float radius, const float orig[3], bool accum);
+
+// ---- full rebuild over brick bitmaps --------------------------------------
+//
+// For a cloud whose bounding box (in level-0 bricks, widened by the
+// activation box) holds at most 2^31 bricks, the node sets of every level are
+// bitmaps over that box instead of hash sets.  Bit (x, y, z) sits at
+// ((x-ox)*dy + (y-oy))*dz + (z-oz), i.e. in the order of the packed keys, so
+// an ordered compaction of the set bits yields the sorted unique keys with
+// no sort.  Parent levels are the OR of their children's bits, and the extra
+// (box-only) set of a level is box & ~base.  The result is the same node
+// sets, in the same order, as the hash path below.
+struct BitGrid {
+    int o[3];       // first brick per axis (absolute, in this level's units)
+    int d[3];       // bricks per axis
+    uint32_t *base; // bitmaps, ceil(d0*d1*d2 / 32) words each
+    uint32_t *box;
+    int64_t words;
+};
+
+__device__ __forceinline__ int64_t bg_bit(const BitGrid &G, int x, int y, int z) {
+    return ((int64_t)(x - G.o[0]) * G.d[1] + (y - G.o[1])) * G.d[2] + (z - G.o[2]);
+}
+__device__ __forceinline__ bool bg_in(const BitGrid &G, int x, int y, int z) {
+    return x >= G.o[0] && x < G.o[0] + G.d[0] && y >= G.o[1] && y < G.o[1] + G.d[1] && z >= G.o[2] &&
+           z < G.o[2] + G.d[2];
+}
+__device__ __forceinline__ void bg_set(uint32_t *bits, int64_t bit) {
+    uint32_t *w = bits + (bit >> 5);
+    const uint32_t m = 1u << (bit & 31);
+    if (!(__ldcg(w) & m)) atomicOr(w, m);
+}
+
+// Level-0 base brick and activation-box bricks of every point, with the
+// same rules as k_mark_keys.  A brick outside the grid sets kDevCapacity
+// (the host then takes the hash path).  With SMEM the CTA first marks a
+// shared copy of both bitmaps (grid-stride over the points) and then ORs
+// its non-zero words into the global ones: a small grid would otherwise
+// put every point's atomics on the same few L2 lines.
+template <bool SMEM>
+__global__ void k_mark_bits(PointsView pos, int64_t n, float3 orig, float radius, float kmax, int do_box, KeyGeom g,
+                            BitGrid G, int32_t *status) {
+    extern __shared__ uint32_t sbits[]; // [2 * words] when SMEM
+    uint32_t *base = G.base, *box = G.box;
+    if (SMEM) {
+        for (int64_t i = threadIdx.x; i < 2 * G.words; i += blockDim.x) sbits[i] = 0;
+        __syncthreads();
+        base = sbits;
+        box = sbits + G.words;
+    }
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t iters = (n + stride - 1) / stride; // uniform per warp: whole warps take part in match_any
+    for (int64_t it = 0; it < iters; it++) {
+        const int64_t i = it * stride + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        bool valid = i < n;
+        float w[3] = {0, 0, 0};
+        if (valid) {
+            float3 p = load_f3(pos, i);
+            w[0] = p.x + orig.x;
+            w[1] = p.y + orig.y;
+            w[2] = p.z + orig.z;
+            if (w[0] < 0 || w[1] < 0 || w[2] < 0) valid = false;
+        }
+        int64_t bit = -1;
+        int bx = 0, by = 0, bz = 0;
+        if (valid) {
+            bx = (int)w[0] >> g.log2r0;
+            by = (int)w[1] >> g.log2r0;
+            bz = (int)w[2] >> g.log2r0;
+            if (brick_in_root(g, bx, by, bz)) {
+                if (bg_in(G, bx, by, bz)) bit = bg_bit(G, bx, by, bz);
+                else atomicOr(status, kDevCapacity);
+            }
+        }
+        // one atomic per distinct bit per warp
+        const unsigned peers = __match_any_sync(0xffffffffu, (unsigned long long)bit);
+        if (bit >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1) {
+            if (SMEM) atomicOr(base + (bit >> 5), 1u << (bit & 31));
+            else bg_set(base, bit);
+        }
+        if (!valid || !do_box) continue;
+        int lo[3], hi[3];
+        for (int a = 0; a < 3; a++) {
+            const int iw = (int)w[a];
+            const int bmin = (int)((float)iw - radius);
+            const int bmax = (int)((float)iw + kmax * radius);
+            lo[a] = max((bmin < 0 ? 0 : bmin) >> g.log2r0, g.lo[a]);
+            hi[a] = min(bmax >> g.log2r0, g.lo[a] + g.span - 1);
+        }
+        for (int x = lo[0]; x <= hi[0]; x++)
+            for (int y = lo[1]; y <= hi[1]; y++)
+                for (int z = lo[2]; z <= hi[2]; z++) {
+                    if (!bg_in(G, x, y, z)) {
+                        atomicOr(status, kDevCapacity);
+                        continue;
+                    }
+                    const int64_t bb = bg_bit(G, x, y, z);
+                    if (SMEM) {
+                        const uint32_t m = 1u << (bb & 31);
+                        if (!(box[bb >> 5] & m)) atomicOr(box + (bb >> 5), m);
+                    } else {
+                        bg_set(box, bb);
+                    }
+                }
+    }
+    if (SMEM) {
+        __syncthreads();
+        for (int64_t k = threadIdx.x; k < 2 * G.words; k += blockDim.x) {
+            const uint32_t m = sbits[k];
+            if (m) atomicOr((k < G.words ? G.base + k : G.box + (k - G.words)), m);
+        }
+    }
+}
+
+// Parent bit = OR of its children's bits (shift sh per axis).
+__global__ void k_parent_bits(BitGrid C, BitGrid P, int sh) {
+    const int64_t nbits = (int64_t)P.d[0] * P.d[1] * P.d[2];
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nbits; t += (int64_t)gridDim.x * blockDim.x) {
+        const int Z = (int)(t % P.d[2]) + P.o[2], Y = (int)((t / P.d[2]) % P.d[1]) + P.o[1],
+                  X = (int)(t / ((int64_t)P.d[1] * P.d[2])) + P.o[0];
+        const int r = 1 << sh;
+        int lo[3] = {max(X << sh, C.o[0]), max(Y << sh, C.o[1]), max(Z << sh, C.o[2])};
+        int hi[3] = {min((X << sh) + r, C.o[0] + C.d[0]), min((Y << sh) + r, C.o[1] + C.d[1]),
+                     min((Z << sh) + r, C.o[2] + C.d[2])};
+        bool b0 = false, b1 = false;
+        for (int x = lo[0]; x < hi[0] && !(b0 && b1); x++)
+            for (int y = lo[1]; y < hi[1] && !(b0 && b1); y++)
+                for (int z = lo[2]; z < hi[2]; z++) {
+                    const int64_t cb = bg_bit(C, x, y, z);
+                    const uint32_t m = 1u << (cb & 31);
+                    b0 |= (C.base[cb >> 5] & m) != 0;
+                    b1 |= (C.box[cb >> 5] & m) != 0;
+                }
+        const int64_t pb = bg_bit(P, X, Y, Z);
+        if (b0) atomicOr(P.base + (pb >> 5), 1u << (pb & 31));
+        if (b1) atomicOr(P.box + (pb >> 5), 1u << (pb & 31));
+    }
+}
+
+// Ordered compaction of bitmap sets into packed keys: CTA j compacts set j
+// (a & ~mask) of `sets`, one thread per 32-bit word in rounds of the block,
+// decoding the brick of each set bit incrementally from its word's first
+// bit.  count[j] receives the number of keys; out == nullptr only counts.
+constexpr int kCompactThreads = 1024;
+struct CompactSet {
+    const uint32_t *a, *mask;
+    BitGrid G;
+    uint64_t *out;
+    int32_t *count;
+};
+struct CompactSets {
+    CompactSet set[2 * kMaxLev];
+    int b;
+};
+__global__ void __launch_bounds__(kCompactThreads) k_bits_compact(CompactSets S) {
+    __shared__ uint32_t warp_sum[32];
+    __shared__ uint32_t round_total;
+    const CompactSet &C = S.set[blockIdx.x];
+    const BitGrid &G = C.G;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nbits = G.d[0] * G.d[1] * G.d[2]; // <= 2^28
+    uint32_t running = 0;
+    for (int64_t round = 0; round < G.words; round += kCompactThreads) {
+        const int64_t wi = round + threadIdx.x;
+        uint32_t x = 0;
+        if (wi < G.words) {
+            x = C.a[wi];
+            if (C.mask) x &= ~C.mask[wi];
+        }
+        const uint32_t local = __popc(x);
+        uint32_t inc = local;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) warp_sum[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t ws = warp_sum[lane];
+            uint32_t wsum = ws;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, wsum, o);
+                if (lane >= o) wsum += y;
+            }
+            warp_sum[lane] = wsum - ws;
+            if (lane == 31) round_total = wsum;
+        }
+        __syncthreads();
+        if (C.out && x) {
+            uint32_t pos = running + warp_sum[warp] + inc - local;
+            const int b0 = (int)(wi << 5);
+            int z = b0 % G.d[2], t = b0 / G.d[2];
+            int y = t % G.d[1], xx = t / G.d[1];
+            int prev = 0;
+            while (x) {
+                const int j = __ffs(x) - 1;
+                x &= x - 1;
+                if (b0 + j >= nbits) break;
+                z += j - prev; // advance (x, y, z) from bit b0 + prev to b0 + j
+                prev = j;
+                while (z >= G.d[2]) {
+                    z -= G.d[2];
+                    if (++y >= G.d[1]) {
+                        y = 0;
+                        xx++;
+                    }
+                }
+                C.out[pos++] = pack_key(xx + G.o[0], y + G.o[1], z + G.o[2], S.b);
+            }
+        }
+        running += round_total;
+        __syncthreads(); // warp_sum / round_total are rewritten next round
+    }
+    if (threadIdx.x == 0) *C.count = (int32_t)running;
+}
+
+constexpr int64_t kMaxGridBits = 1ll << 28; // bitmap path up to 2^28 bricks (32 MB per bitmap)
+
+// Node key sets through brick bitmaps; *used = false when the grid would be
+// too large or a brick fell outside it (then nothing was changed).
+gvdb2_status key_sets_bitmap(Volume *v, int n, float radius, const float orig[3], const KeyGeom &g, int64_t nB[],
+                             int64_t nE[], bool *used) {
+    *used = false;
+    cudaStream_t s = v->stream;
+    const int depth = v->depth;
+    const bool do_box = radius >= 1.0f;
+    const float r = do_box ? radius : 0.0f;
+    BitGrid G[kMaxLev];
+    int64_t off[kMaxLev + 1];
+    off[0] = 0;
+    int lo0[3], hi0[3];
+    for (int a = 0; a < 3; a++) {
+        const float lo_v = std::max(0.0f, std::floor(v->posmin[a] - r - 2.0f));
+        const float hi_v = v->posmax[a] + 2.0f * r + 2.0f;
+        if (!(hi_v < 2.0e9f)) return GVDB2_OK;
+        lo0[a] = std::max(g.lo[a], (int)lo_v >> g.log2r0);
+        hi0[a] = std::min(g.lo[a] + g.span - 1, (int)hi_v >> g.log2r0);
+        if (hi0[a] < lo0[a]) hi0[a] = lo0[a];
+    }
+    int sh = 0;
+    for (int l = 0; l < depth; l++) {
+        if (l > 0) sh += v->logdim[l];
+        int64_t nbits = 1;
+        for (int a = 0; a < 3; a++) {
+            G[l].o[a] = lo0[a] >> sh;
+            G[l].d[a] = (hi0[a] >> sh) - G[l].o[a] + 1;
+            nbits *= G[l].d[a];
+        }
+        if (nbits > kMaxGridBits) return GVDB2_OK;
+        G[l].words = (nbits + 31) / 32;
+        off[l + 1] = off[l] + 2 * G[l].words;
+    }
+    GV_CUDA(v, v->bits.ensure(sizeof(uint32_t) * (size_t)off[depth], s));
+    GV_CUDA(v, cudaMemsetAsync(v->bits.p, 0, sizeof(uint32_t) * (size_t)off[depth], s));
+    for (int l = 0; l < depth; l++) {
+        G[l].base = v->bits.as<uint32_t>() + off[l];
+        G[l].box = G[l].base + G[l].words;
+    }
+    GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count, 0, sizeof(int32_t) * 8 + sizeof(int32_t), s));
+    const float3 t3 = make_float3(orig[0], orig[1], orig[2]);
+    constexpr int64_t kSmemWords = 24576; // both level-0 bitmaps in 96 KB of shared memory
+    if (n > 0 && 2 * G[0].words <= kSmemWords) {
+        const size_t smem = sizeof(uint32_t) * 2 * (size_t)G[0].words;
+        auto k = k_mark_bits<true>;
+        if (smem > 48 * 1024) GV_CUDA(v, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k<<<std::min(grid_for(n, 256), 2 * kSmCount), 256, smem, s>>>(v->pos, n, t3, radius, 2.0f, do_box ? 1 : 0, g,
+                                                                       G[0], &dev_words(v)->status);
+    } else if (n > 0) {
+        k_mark_bits<false><<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t3, radius, 2.0f, do_box ? 1 : 0, g,
+                                                                        G[0], &dev_words(v)->status);
+    }
+    for (int l = 1; l < depth; l++) {
+        const int64_t nbits = (int64_t)G[l].d[0] * G[l].d[1] * G[l].d[2];
+        k_parent_bits<<<grid_for(nbits, 256, 8 * kSmCount), 256, 0, s>>>(G[l - 1], G[l], v->logdim[l]);
+    }
+    // compaction of every (level, set) in one launch; for small grids the key
+    // arrays are sized by the grid and a single pass both counts and writes
+    CompactSets C;
+    C.b = g.b;
+    int nsets = 0;
+    int64_t maxbits = 0;
+    for (int l = 0; l < depth; l++) {
+        maxbits = std::max<int64_t>(maxbits, (int64_t)G[l].d[0] * G[l].d[1] * G[l].d[2]);
+        C.set[nsets++] = CompactSet{G[l].base, nullptr, G[l], nullptr, dev_words(v)->count + 2 * l};
+        if (do_box) C.set[nsets++] = CompactSet{G[l].box, G[l].base, G[l], nullptr, dev_words(v)->count + 2 * l + 1};
+    }
+    const bool one_pass = maxbits <= (1ll << 22);
+    if (one_pass) {
+        int k = 0;
+        for (int l = 0; l < depth; l++) {
+            const int64_t nbits = (int64_t)G[l].d[0] * G[l].d[1] * G[l].d[2];
+            GV_CUDA(v, v->lev_keys[l][0].ensure(sizeof(uint64_t) * (size_t)nbits, s));
+            C.set[k++].out = v->lev_keys[l][0].as<uint64_t>();
+            if (do_box) {
+                GV_CUDA(v, v->lev_keys[l][1].ensure(sizeof(uint64_t) * (size_t)nbits, s));
+                C.set[k++].out = v->lev_keys[l][1].as<uint64_t>();
+            } else {
+                GV_CUDA(v, v->lev_keys[l][1].ensure(sizeof(uint64_t), s));
+            }
+        }
+    }
+    k_bits_compact<<<nsets, kCompactThreads, 0, s>>>(C);
+    GV_CUDA(v, cudaGetLastError());
+    GV_TRY(read_words(v));
+    if (host_words(v)->status & kDevCapacity) return GVDB2_OK; // a brick outside the grid: hash path
+    for (int l = 0; l < kMaxLev; l++) nB[l] = nE[l] = 0;
+    for (int l = 0; l < depth; l++) {
+        nB[l] = host_words(v)->count[2 * l];
+        nE[l] = do_box ? host_words(v)->count[2 * l + 1] : 0;
+    }
+    if (!one_pass) {
+        int k = 0;
+        for (int l = 0; l < depth; l++) {
+            GV_CUDA(v, v->lev_keys[l][0].ensure(sizeof(uint64_t) * (size_t)std::max<int64_t>(nB[l], 1), s));
+            GV_CUDA(v, v->lev_keys[l][1].ensure(sizeof(uint64_t) * (size_t)std::max<int64_t>(nE[l], 1), s));
+            C.set[k++].out = v->lev_keys[l][0].as<uint64_t>();
+            if (do_box) C.set[k++].out = v->lev_keys[l][1].as<uint64_t>();
+        }
+        k_bits_compact<<<nsets, kCompactThreads, 0, s>>>(C);
+        GV_CUDA(v, cudaGetLastError());
+    }
+    *used = true;
+    return GVDB2_OK;
+}
+
+// ActivateBricksGPU (+ ActivateExtraBricksGPU when radius >= 1).
+gvdb2_status full_rebuild(Volume *v, int n, float radius, const float orig[3]) {
+    KeyGeom g = key_geom(v);
+    if (g.span > 65536) return fail(v, GVDB2_ERR_UNSUPPORTED, "root spans more than 65536 bricks per axis");
+    int64_t nB[kMaxLev] = {0}, nE[kMaxLev] = {0};
+    bool used = false;
+    GV_TRY(key_sets_bitmap(v, n, radius, orig, g, nB, nE, &used));
+    if (!used) GV_TRY(key_sets_hash(v, n, radius, orig, g, nB, nE));
+    return build_from_keys(v, nB, nE, g);
+}
 
 // DetermineDepth (V:821-837) with GetCoveringNode (V:2915-2931).
 int determine_depth(const Volume *v, int rootpos[3]) {

@@ -236,3 +236,21 @@ def test_splat_after_incremental(gvdb2_mod, oracle_mod):
     got = v.GatherKernel(gvdb2_mod.KERNEL_TENT1, len(q), [0]).cpu().numpy()
     want = o.gather_kernel(gvdb2_mod.KERNEL_TENT1, q, [0])
     assert rel_err(got, want) <= REL_TOL
+
+
+def test_sparse_extent_takes_hash_path(gvdb2_mod, oracle_mod):
+    """Two clusters 100,000 voxels apart: the level-0 brick grid of their
+    bounding box (12,500^3 bricks) is far past the bitmap limit, so the
+    rebuild takes the hash-set path; topology still matches bit for bit."""
+    a = shell_points(20_000, seed=31, r_in=20, r_out=24, center=(200.0, 200.0, 200.0))
+    b = shell_points(20_000, seed=32, r_in=20, r_out=24, center=(100_200.0, 100_200.0, 100_200.0))
+    pts = np.concatenate([a, b]).astype(np.float32)
+    cfg = (4, 4, 4, 4, 3)
+    o = make_oracle(oracle_mod, cfg)
+    assert o.rebuild_topology(pts, 2.0) == 0
+    o.update_atlas()
+    v = gpu_volume(gvdb2_mod, pts, cfg)
+    v.RebuildTopology(len(pts), 2.0)
+    v.UpdateAtlas()
+    compare_topology(v, o)
+    assert np.array_equal(v.atlas_map(), o.atlas_map())
