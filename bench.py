@@ -124,6 +124,12 @@ class Pipeline:
     def reset(self):
         self.pos.copy_(self.pos0)
 
+    def use_buffers(self, pos, vel, out):
+        """Run the next steps on these device buffers (positions, velocities, gather output)."""
+        self.pos, self.vel, self.out = pos, vel, out
+        self.attrs = [None, (vel, 0), (vel, 1), (vel, 2)]
+        self.v.SetPoints(pos)
+
     def step(self, events=None):
         v, n, K = self.v, self.n, self.gvdb2.KERNEL_CUBIC2
         rec = (lambda name: events.append((name, self._ev()))) if events is not None else (lambda name: None)
@@ -285,6 +291,66 @@ def count_launches(pipe):
     return ours
 
 
+def e2e_pipelined(pipe, pos, vel, steps, barrier):
+    """Device time of `steps` end-to-end steps with double-buffered copies.
+
+    Step k computes on buffer set k % 2 on the volume's own stream.  The
+    inputs of step k+1 are copied into the other set on a copy stream, after
+    step k-1 has finished with that set.  Step k's gathered velocities go
+    back to pinned host memory on a third stream.  Returns the time from the
+    first input copy to the last read-back.
+    """
+    import torch
+    n = pipe.n
+    hpos = torch.from_numpy(pos).pin_memory()
+    hvel = torch.from_numpy(vel).pin_memory()
+    hout = [torch.empty((n, 3), dtype=torch.float32).pin_memory() for _ in range(2)]
+    bufs = [(torch.empty_like(pipe.pos), torch.empty_like(pipe.vel), torch.empty_like(pipe.out)) for _ in range(2)]
+    compute, h2d, d2h = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    pipe.v.SetStream(compute)
+
+    def run(k_steps, e0=None, e1=None):
+        in_ready = [torch.cuda.Event() for _ in range(2)]
+        done = [torch.cuda.Event() for _ in range(2)]
+        read = [torch.cuda.Event() for _ in range(2)]
+        with torch.cuda.stream(h2d):
+            if e0 is not None:
+                e0.record(h2d)
+            bufs[0][0].copy_(hpos, non_blocking=True)
+            bufs[0][1].copy_(hvel, non_blocking=True)
+            in_ready[0].record(h2d)
+        for k in range(k_steps):
+            cur, nxt = k % 2, (k + 1) % 2
+            if k + 1 < k_steps:  # next step's inputs, once step k-1 is done with that set
+                with torch.cuda.stream(h2d):
+                    if k >= 1:
+                        h2d.wait_event(done[nxt])
+                    bufs[nxt][0].copy_(hpos, non_blocking=True)
+                    bufs[nxt][1].copy_(hvel, non_blocking=True)
+                    in_ready[nxt].record(h2d)
+            compute.wait_event(in_ready[cur])
+            if k >= 2:
+                compute.wait_event(read[cur])  # step k-2's result has left this buffer
+            with torch.cuda.stream(compute):
+                pipe.use_buffers(*bufs[cur])
+                pipe.step()
+                done[cur].record(compute)
+            with torch.cuda.stream(d2h):
+                d2h.wait_event(done[cur])
+                hout[cur].copy_(bufs[cur][2], non_blocking=True)
+                read[cur].record(d2h)
+        if e1 is not None:
+            e1.record(d2h)
+
+    run(3)  # warm-up
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    run(steps, e0, e1)
+    barrier()
+    return e0.elapsed_time(e1)
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -356,33 +422,25 @@ def run_ours(a):
         stages[k] = {"ms": round(stage_ms.get(k, 0.0), 4), "alg_bytes": sb[k], "GBps": gbs}
     dom = max(("scatter", "gather", "apron"), key=lambda k: stage_ms.get(k, 0.0))
     achieved = sb[dom] / (stage_ms[dom] / 1e3) / 1e9
-    kernel_name = {"scatter": "k_scatter_own<cubic,4> + k_scatter_merge<cubic,4>",
+    kernel_name = {"scatter": "scatter stage: k_absmax + k_scatter_own<cubic,4> + k_scatter_merge<cubic,4>",
                    "gather": "k_gather_tile<cubic,fwd,3>", "apron": "k_apron"}[dom]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": TRAFFIC.get(dom), "kernel": kernel_name, "peak_source": peak_kind}
+                "traffic": TRAFFIC_PER_BRICK[dom] * geo["B"] if dom in TRAFFIC_PER_BRICK else None,
+                "kernel": kernel_name, "peak_source": peak_kind,
+                "traffic_source": "ncu capture of a 2,097,152-point block, scaled by bricks"}
 
-    # end to end through the public API: pinned host inputs in, gathered velocities out
-    pipe.reset()
-    hpos = torch.from_numpy(pos).pin_memory()
-    hvel = torch.from_numpy(vel).pin_memory()
-    hout = torch.empty((n, 3), dtype=torch.float32).pin_memory()
-    for _ in range(2):
-        pipe.pos.copy_(hpos, non_blocking=True)
-        pipe.vel.copy_(hvel, non_blocking=True)
-        pipe.step()
-        hout.copy_(pipe.out, non_blocking=True)
+    # end to end through the public API: every step copies its inputs from
+    # pinned host memory and reads its gathered velocities back.  Two device
+    # buffer sets alternate, so the copies of one step run on their own
+    # streams while the neighbouring step computes.
     barrier()
-    e0.record()
-    for _ in range(a.steps):
-        pipe.pos.copy_(hpos, non_blocking=True)
-        pipe.vel.copy_(hvel, non_blocking=True)
-        pipe.step()
-        hout.copy_(pipe.out, non_blocking=True)
-    e1.record()
-    barrier()
-    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    e2e_ms = e2e_pipelined(pipe, pos, vel, a.steps, barrier)
+    ms_e2e = max_over_ranks(e2e_ms)
     e2e = {"value": n * a.steps * ws / (ms_e2e / 1e3), "unit": "points/s", "h2d_bytes_per_step": 24 * n,
-           "d2h_bytes_per_step": 12 * n}
+           "d2h_bytes_per_step": 12 * n, "overlap": "double-buffered: H2D, compute and D2H on separate streams"}
+    pipe.use_buffers(pipe.pos, pipe.vel, pipe.out)
+    pipe.v.SetStream(0)
+    barrier()
     launches = count_launches(pipe) * a.steps
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
@@ -402,8 +460,14 @@ def run_ours(a):
     return 0
 
 
-# DRAM bytes per launch from ncu captures (profiles/*.md); None until captured.
-TRAFFIC = {}
+# DRAM bytes (read + write) per brick of each stage's kernels, from the ncu
+# capture of a 2,097,152-point block larger than L2 (11,016 bricks; summary in
+# profiles/k_scatter_own_merge_gather_dam2m.md).  Traffic grows with the brick
+# count, so a launch moves about this many bytes x bricks.
+TRAFFIC_PER_BRICK = {
+    "scatter": (59.4e6 + 244.3e6 + 556.0e6 + 116.3e6) / 11016,
+    "gather": (159.9e6 + 21.2e6) / 11016,
+}
 
 
 def main():
