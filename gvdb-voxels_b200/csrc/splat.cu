@@ -187,25 +187,6 @@ struct SplatArgs {
     int64_t tvox;
 };
 
-// Per-channel max |weight * attr| over all points (bounds the fixed-point
-// scale of k_scatter_own).  out[c] holds the float bits (>= 0 orders as int).
-template <int NCH>
-__global__ void k_absmax(SplatArgs S, int64_t n, int32_t *out) {
-    float m[NCH];
-#pragma unroll
-    for (int c = 0; c < NCH; c++) m[c] = 0.0f;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const float wt = fabsf(S.has_weight ? load_f1(S.weight, i) : S.wconst);
-#pragma unroll
-        for (int c = 0; c < NCH; c++) m[c] = fmaxf(m[c], ((S.attr_mask >> c) & 1) ? wt * fabsf(load_f1(S.attr[c], i)) : wt);
-    }
-#pragma unroll
-    for (int c = 0; c < NCH; c++) {
-        float x = m[c];
-        for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, o));
-        if ((threadIdx.x & 31) == 0) atomicMax(out + c, __float_as_int(x));
-    }
-}
 
 // ---- two-phase scatter ---------------------------------------------------
 //
@@ -225,7 +206,8 @@ __global__ void k_absmax(SplatArgs S, int64_t n, int32_t *out) {
 // exact), and added with native int32 shared-memory atomics.  The integer
 // sums do not depend on the order of the atomics, and the merge sums a fixed
 // sequence of floats, so the result is bit-reproducible run to run.
-// Bounds (R = points of the brick, max|a| = largest weighted amount):
+// Bounds (R = points of the brick, max|a| = largest |weighted amount| among
+// them, so a brick's result depends on its own points only):
 //   L = min(22, 31 - bits(R+1))      -> |sum lo| <= R * 2^(L-1) < 2^31
 //   max|a| * 2^s < 2^(21+L)          -> |x * 2^-L| < 2^22 (magic range)
 //   R * max|a| * 2^s < 2^(29+L)      -> |sum hi| < 2^29 + R/2
@@ -259,7 +241,7 @@ __device__ __forceinline__ void fixed_add(int32_t *hi_acc, int32_t *lo_acc, int 
 }
 
 template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, const int32_t *absmax, float *ext) {
+__global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float *ext) {
     using T = Taps<KERNEL>;
     using X = ExtTile<KERNEL>;
     constexpr int N = T::N;
@@ -270,16 +252,79 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, const 
     float(*pa)[kOwnChunk] = pw + 3 * N;
     int32_t *pb = reinterpret_cast<int32_t *>(pa + NCH);
     __shared__ double inv_s[NCH];
+    __shared__ int32_t amax_bits[NCH]; // max |weighted amount| of the brick's points, as float bits
     const int64_t slot = blockIdx.x;
     for (int i = threadIdx.x; i < NCH * X::CS; i += kOwnThreads) acc_hi[i] = acc_lo[i] = 0;
+    if (threadIdx.x < NCH) amax_bits[threadIdx.x] = 0;
     const uint32_t beg = S.bin_off[slot], R = S.bin_off[slot + 1] - beg;
+    const Node &nd = S.leaves[S.slot_leaf[slot]];
+    const int ox = nd.mPos[0] - X::H, oy = nd.mPos[1] - X::H, oz = nd.mPos[2] - X::H;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    // Stage one point as record r of the current chunk (amounts times `scale`).
+    auto stage = [&](uint32_t j, int r, const float *scale, float *amt_out) {
+        const int32_t p = S.perm[beg + j];
+        const float3 q = load_f3(S.pos, p);
+        float wx[N], wy[N], wz[N];
+        const int fx = T::eval(q.x + S.trans.x, wx) - ox;
+        const int fy = T::eval(q.y + S.trans.y, wy) - oy;
+        const int fz = T::eval(q.z + S.trans.z, wz) - oz;
+        // a binned point lies in the brick, so its first taps are in [0, 8];
+        // anything else (inconsistent input) is dropped, never written outside the tile
+        const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
+        pb[r] = ok ? (fx | (fy << 8) | (fz << 16)) : 0;
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            pw[k][r] = wx[k];
+            pw[N + k][r] = wy[k];
+            pw[2 * N + k][r] = wz[k];
+        }
+        const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            const float am = ok ? (((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt) : 0.0f;
+            amt_out[c] = am;
+            pa[c][r] = am * scale[c];
+        }
+    };
+
+    // Pass over all the brick's points: the first chunk is staged unscaled
+    // and every amount enters the brick's max, which sets the scale (so the
+    // result depends only on this brick's points).
+    float one[NCH], mx[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        one[c] = 1.0f;
+        mx[c] = 0.0f;
+    }
+    __syncthreads(); // amax_bits cleared
+    for (uint32_t j = threadIdx.x; j < R; j += kOwnThreads) {
+        float am[NCH];
+        if (j < (uint32_t)kOwnChunk) {
+            stage(j, (int)j, one, am);
+        } else {
+            const int32_t p = S.perm[beg + j];
+            const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
+#pragma unroll
+            for (int c = 0; c < NCH; c++) am[c] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt;
+        }
+#pragma unroll
+        for (int c = 0; c < NCH; c++) mx[c] = fmaxf(mx[c], fabsf(am[c]));
+    }
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        float x = mx[c];
+        for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, o));
+        if (lane == 0 && x > 0.0f) atomicMax(&amax_bits[c], __float_as_int(x));
+    }
+    __syncthreads();
     int L = 31 - (32 - __clz((int)R + 1));
     L = L > 22 ? 22 : L;
     const float inv2L = ldexpf(1.0f, -L), two2L = ldexpf(1.0f, L);
     float scale[NCH];
 #pragma unroll
     for (int c = 0; c < NCH; c++) {
-        const float am = __int_as_float(absmax[c]);
+        const float am = __int_as_float(amax_bits[c]);
         int e1 = 0, e2 = 0;
         frexpf(am, &e1);              // am < 2^e1
         frexpf((float)R * am, &e2);  // R*am < 2^e2
@@ -287,33 +332,18 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, const 
         scale[c] = (am > 0.0f && R > 0) ? ldexpf(1.0f, sc) : 0.0f;
         if (threadIdx.x == 0) inv_s[c] = scale[c] > 0.0f ? ldexp(1.0, -sc) : 0.0;
     }
-    const Node &nd = S.leaves[S.slot_leaf[slot]];
-    const int ox = nd.mPos[0] - X::H, oy = nd.mPos[1] - X::H, oz = nd.mPos[2] - X::H;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    { // scale the staged first chunk
+        const int cnt0 = (int)min((uint32_t)kOwnChunk, R);
+        for (int r = threadIdx.x; r < cnt0; r += kOwnThreads)
+#pragma unroll
+            for (int c = 0; c < NCH; c++) pa[c][r] *= scale[c];
+    }
     for (uint32_t base = 0; base < R; base += kOwnChunk) {
         const int cnt = (int)min((uint32_t)kOwnChunk, R - base);
-        __syncthreads(); // accumulators cleared / previous chunk consumed
-        if ((int)threadIdx.x < cnt) {
-            const int32_t p = S.perm[beg + base + threadIdx.x];
-            const float3 q = load_f3(S.pos, p);
-            float wx[N], wy[N], wz[N];
-            const int fx = T::eval(q.x + S.trans.x, wx) - ox;
-            const int fy = T::eval(q.y + S.trans.y, wy) - oy;
-            const int fz = T::eval(q.z + S.trans.z, wz) - oz;
-            // a binned point lies in the brick, so its first taps are in [0, 8];
-            // anything else (inconsistent input) is dropped, never written outside the tile
-            const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
-            pb[threadIdx.x] = ok ? (fx | (fy << 8) | (fz << 16)) : 0;
-#pragma unroll
-            for (int k = 0; k < N; k++) {
-                pw[k][threadIdx.x] = wx[k];
-                pw[N + k][threadIdx.x] = wy[k];
-                pw[2 * N + k][threadIdx.x] = wz[k];
-            }
-            const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
-#pragma unroll
-            for (int c = 0; c < NCH; c++)
-                pa[c][threadIdx.x] = ok ? (((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt) * scale[c] : 0.0f;
+        if (base > 0) {
+            __syncthreads(); // previous chunk consumed
+            float am[NCH];
+            if ((int)threadIdx.x < cnt) stage(base + threadIdx.x, (int)threadIdx.x, scale, am);
         }
         __syncthreads();
         if constexpr (N == 4) {
@@ -605,15 +635,10 @@ gvdb2_status scatter_group(Volume *v, const SplatArgs &S) {
     const int64_t nslots = v->atlas_last;
     GV_CUDA(v, v->scratch.ensure(sizeof(float) * (size_t)nslots * NCH * X::E3 + 256, s));
     float *ext = v->scratch.as<float>();
-    GV_CUDA(v, v->tmp_b.ensure(sizeof(int32_t) * 8, s));
-    int32_t *absmax = v->tmp_b.as<int32_t>();
-    GV_CUDA(v, cudaMemsetAsync(absmax, 0, sizeof(int32_t) * NCH, s));
-    const int64_t n = v->bin_key.n;
-    if (n > 0) k_absmax<NCH><<<std::min(grid_for(n, 256), 4 * kSmCount), 256, 0, s>>>(S, n, absmax);
     constexpr size_t smem = own_smem_bytes<KERNEL, NCH>();
     auto k1 = k_scatter_own<KERNEL, NCH>;
     GV_TRY(launch_smem(v, k1, smem, "scatter"));
-    k1<<<(unsigned)nslots, kOwnThreads, smem, s>>>(S, absmax, ext);
+    k1<<<(unsigned)nslots, kOwnThreads, smem, s>>>(S, ext);
     k_scatter_merge<KERNEL, NCH><<<(unsigned)nslots, 512, 0, s>>>(S, ext);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
