@@ -196,6 +196,24 @@ gvdb2_status gvdb2_set_points(gvdb2_volume *h, gvdb2_points_view pos, gvdb2_poin
     v->vel = gvdb2::to_view(vel);
     v->clr = gvdb2::to_view(clr);
     v->bin_key.valid = false;
+    v->batch_clouds = 0;
+    return GVDB2_OK;
+}
+
+gvdb2_status gvdb2_batch_points(gvdb2_volume *h, const gvdb2_points_view *clouds, int ncloud, int space_log2,
+                                int64_t *first) {
+    CHECK_HANDLE(h);
+    return gvdb2::batch_points(VOL(h), clouds, ncloud, space_log2, first);
+}
+
+gvdb2_status gvdb2_batch_origin(gvdb2_volume *h, int cloud, int32_t out[3]) {
+    CHECK_HANDLE(h);
+    Volume *v = VOL(h);
+    if (v->batch_clouds == 0) return gvdb2::fail(v, GVDB2_ERR_STATE, "no batch set");
+    if (cloud < 0 || cloud >= v->batch_clouds || !out) return gvdb2::fail(v, GVDB2_ERR_ARG, "bad cloud index");
+    int o[3];
+    gvdb2::batch_origin(cloud, v->batch_clouds, v->batch_space_log2, o);
+    for (int a = 0; a < 3; a++) out[a] = o[a];
     return GVDB2_OK;
 }
 

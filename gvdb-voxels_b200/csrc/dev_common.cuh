@@ -15,6 +15,12 @@ __device__ __forceinline__ float3 load_f3(const PointsView &w, int64_t i) {
     const float *p = reinterpret_cast<const float *>(w.base + i * (int64_t)w.stride + w.offset);
     return make_float3(p[0], p[1], p[2]);
 }
+// Integer voxel origin of point i's cloud (zero outside a batch).
+__device__ __forceinline__ int3 point_origin(const PointsView &w, int64_t i) {
+    if (!w.cloud) return make_int3(0, 0, 0);
+    const int32_t *o = w.origin + 3 * (int64_t)w.cloud[i];
+    return make_int3(o[0], o[1], o[2]);
+}
 __device__ __forceinline__ float load_f1(const PointsView &w, int64_t i) {
     return *reinterpret_cast<const float *>(w.base + i * (int64_t)w.stride + w.offset);
 }
@@ -140,6 +146,12 @@ __device__ __forceinline__ int32_t leaf_at(const LeafLookup &L, float wx, float 
 __device__ __forceinline__ int32_t leaf_at_brick(const LeafLookup &L, int bx, int by, int bz) {
     if (!brick_in_root(L.g, bx, by, bz)) return -1;
     return hm_lookup(L.keys, L.vals, L.mask, pack_key(bx, by, bz, L.g.b));
+}
+
+// leaf_at for a point of a batched cloud: w in the cloud's own space, o its origin.
+__device__ __forceinline__ int32_t leaf_at_o(const LeafLookup &L, float wx, float wy, float wz, int3 o) {
+    if (!(wx >= 0.0f && wy >= 0.0f && wz >= 0.0f)) return -1;
+    return leaf_at_brick(L, ((int)wx + o.x) >> L.g.log2r0, ((int)wy + o.y) >> L.g.log2r0, ((int)wz + o.z) >> L.g.log2r0);
 }
 
 __device__ __forceinline__ bool hs_contains(const uint64_t *keys, uint32_t mask, uint64_t key) {

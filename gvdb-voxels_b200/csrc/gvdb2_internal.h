@@ -46,10 +46,16 @@ struct AtlasNode {
 static_assert(sizeof(AtlasNode) == 16, "AtlasNode is 16 bytes");
 
 struct PointsView {
-    const char *base;
-    int64_t count;
-    int32_t stride;
-    int32_t offset;
+    const char *base = nullptr;
+    int64_t count = 0;
+    int32_t stride = 0;
+    int32_t offset = 0;
+    // batched clouds: per-point cloud index and per-cloud integer voxel
+    // origin (3 ints).  Positions stay in the cloud's own index space; the
+    // origin is added to integer grid coordinates only, after floor and
+    // fraction are taken, so no position bit is lost to the offset.
+    const int32_t *cloud = nullptr;
+    const int32_t *origin = nullptr;
 };
 
 // Open-addressed hash set / map of 64-bit brick keys (linear probing).
@@ -139,6 +145,10 @@ struct Volume {
     DevBuf tmp_a, tmp_b, tmp_c, scratch;
     DevBuf dev_small;         // small device words: counters, status, bbox
     void *host_small = nullptr; // pinned mirror of dev_small
+
+    // batched clouds (gvdb2_batch_points): the packed positions
+    DevBuf batch_pos, batch_cloud, batch_origin;
+    int batch_clouds = 0, batch_space_log2 = 0;
 
     // InsertPoints results
     DevBuf pnode, poff, gcnt, goff, psorted;
@@ -242,6 +252,11 @@ gvdb2_status scatter_kernel_backward(Volume *v, int kernel, int n, const float t
                                      const int *grad_chans, float *grad_pos, float *grad_weight, float *grad_attr);
 gvdb2_status gather_kernel_backward(Volume *v, int kernel, int n, const float trans[3], const int *chans, int nch,
                                     const float *grad_out, const int *grad_chans, float *grad_pos);
+
+// ---- batch.cu ----
+int batch_grid(int ncloud);
+void batch_origin(int cloud, int ncloud, int space_log2, int32_t out[3]);
+gvdb2_status batch_points(Volume *v, const gvdb2_points_view *clouds, int ncloud, int space_log2, int64_t *first);
 
 // ---- apron.cu ----
 gvdb2_status update_apron(Volume *v, int chan, float boundval);

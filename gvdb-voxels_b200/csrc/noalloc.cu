@@ -65,7 +65,7 @@ __global__ void k_na_bin(PointsView pos, int64_t n, float3 trans, LeafLookup L, 
     float3 p = load_f3(pos, i);
     int32_t slot = -1;
     if (p.z != kNoHit) {
-        int32_t leaf = leaf_at(L, p.x + trans.x, p.y + trans.y, p.z + trans.z);
+        int32_t leaf = leaf_at_o(L, p.x + trans.x, p.y + trans.y, p.z + trans.z, point_origin(pos, i));
         slot = leaf >= 0 ? leaf_slot[leaf] : -1;
     }
     pslot[i] = slot;

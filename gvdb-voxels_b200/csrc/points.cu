@@ -60,7 +60,7 @@ __global__ void k_bin_count(PointsView pos, int64_t n, float3 trans, LeafLookup 
     if (i < n) {
         float3 p = load_f3(pos, i);
         if (p.z != kNoHit) {
-            int32_t leaf = leaf_at(L, p.x + trans.x, p.y + trans.y, p.z + trans.z);
+            int32_t leaf = leaf_at_o(L, p.x + trans.x, p.y + trans.y, p.z + trans.z, point_origin(pos, i));
             bin = leaf >= 0 ? leaf_slot[leaf] : -1;
         }
     }
@@ -186,6 +186,7 @@ __global__ void k_sc_pos(const Node *leaves, int64_t n, const uint32_t *mapping,
 } // namespace
 
 gvdb2_status insert_points(Volume *v, int n, const float trans[3], int prefix) {
+    if (v->pos.cloud) return fail(v, GVDB2_ERR_UNSUPPORTED, "batched clouds: the reference-mode point operations (InsertPoints, InsertPointsSubcell) take one cloud per volume");
     if (v->pool_cnt[0] == 0) return fail(v, GVDB2_ERR_STATE, "no topology");
     if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count))) return fail(v, GVDB2_ERR_ARG, "bad point count");
     cudaStream_t s = v->stream;
@@ -267,6 +268,7 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
 }
 
 gvdb2_status insert_points_subcell(Volume *v, int sc, int n, float radius, const float trans[3], int *len) {
+    if (v->pos.cloud) return fail(v, GVDB2_ERR_UNSUPPORTED, "batched clouds: the reference-mode point operations (InsertPoints, InsertPointsSubcell) take one cloud per volume");
     int res0 = v->res(0);
     if (sc <= 0 || res0 % sc) return fail(v, GVDB2_ERR_ARG, "subcell size must divide the brick resolution");
     if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count))) return fail(v, GVDB2_ERR_ARG, "bad point count");

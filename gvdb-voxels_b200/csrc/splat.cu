@@ -265,10 +265,11 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
     auto stage = [&](uint32_t j, int r, const float *scale, float *amt_out) {
         const int32_t p = S.perm[beg + j];
         const float3 q = load_f3(S.pos, p);
+        const int3 o = point_origin(S.pos, p);
         float wx[N], wy[N], wz[N];
-        const int fx = T::eval(q.x + S.trans.x, wx) - ox;
-        const int fy = T::eval(q.y + S.trans.y, wy) - oy;
-        const int fz = T::eval(q.z + S.trans.z, wz) - oz;
+        const int fx = T::eval(q.x + S.trans.x, wx) + o.x - ox;
+        const int fy = T::eval(q.y + S.trans.y, wy) + o.y - oy;
+        const int fz = T::eval(q.z + S.trans.z, wz) + o.z - oz;
         // a binned point lies in the brick, so its first taps are in [0, 8];
         // anything else (inconsistent input) is dropped, never written outside the tile
         const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
@@ -500,16 +501,17 @@ __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
     for (uint32_t j = beg + threadIdx.x; j < end; j += blockDim.x) {
         const int32_t pidx = G.perm[j];
         const float3 p = load_f3(G.pos, pidx);
+        const int3 o = point_origin(G.pos, pidx);
         float wx[N], wy[N], wz[N], dx[N], dy[N], dz[N];
         int fx, fy, fz;
         if (MODE == kFwd) {
-            fx = T::eval(p.x + G.trans.x, wx) - ox;
-            fy = T::eval(p.y + G.trans.y, wy) - oy;
-            fz = T::eval(p.z + G.trans.z, wz) - oz;
+            fx = T::eval(p.x + G.trans.x, wx) + o.x - ox;
+            fy = T::eval(p.y + G.trans.y, wy) + o.y - oy;
+            fz = T::eval(p.z + G.trans.z, wz) + o.z - oz;
         } else {
-            fx = T::eval_d(p.x + G.trans.x, wx, dx) - ox;
-            fy = T::eval_d(p.y + G.trans.y, wy, dy) - oy;
-            fz = T::eval_d(p.z + G.trans.z, wz, dz) - oz;
+            fx = T::eval_d(p.x + G.trans.x, wx, dx) + o.x - ox;
+            fy = T::eval_d(p.y + G.trans.y, wy, dy) + o.y - oy;
+            fz = T::eval_d(p.z + G.trans.z, wz, dz) + o.z - oz;
         }
         float sum[NCH], gx[NCH], gy[NCH], gz[NCH];
 #pragma unroll

@@ -51,7 +51,8 @@ __global__ void k_bbox(PointsView pos, int64_t n, float3 t, int32_t *bbox) {
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         float3 p = load_f3(pos, i);
-        float w[3] = {p.x + t.x, p.y + t.y, p.z + t.z};
+        const int3 o = point_origin(pos, i); // batched clouds: the bounds are only sizes, so float is enough
+        float w[3] = {p.x + t.x + (float)o.x, p.y + t.y + (float)o.y, p.z + t.z + (float)o.z};
 #pragma unroll
         for (int a = 0; a < 3; a++) {
             mn[a] = fminf(mn[a], w[a]);
@@ -99,16 +100,21 @@ __global__ void k_mark_keys(PointsView pos, int64_t n, float3 orig, float radius
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = i < n;
     float w[3] = {0, 0, 0};
+    int oo[3] = {0, 0, 0};
     if (valid) {
         float3 p = load_f3(pos, i);
         w[0] = p.x + orig.x;
         w[1] = p.y + orig.y;
         w[2] = p.z + orig.z;
         if (w[0] < 0 || w[1] < 0 || w[2] < 0) valid = false;
+        const int3 o = point_origin(pos, i);
+        oo[0] = o.x;
+        oo[1] = o.y;
+        oo[2] = o.z;
     }
     unsigned act = __ballot_sync(0xffffffffu, valid);
     if (!valid) return;
-    int bx = (int)w[0] >> g.log2r0, by = (int)w[1] >> g.log2r0, bz = (int)w[2] >> g.log2r0;
+    int bx = ((int)w[0] + oo[0]) >> g.log2r0, by = ((int)w[1] + oo[1]) >> g.log2r0, bz = ((int)w[2] + oo[2]) >> g.log2r0;
     bool inside = bx >= g.lo[0] && bx < g.lo[0] + g.span && by >= g.lo[1] && by < g.lo[1] + g.span &&
                   bz >= g.lo[2] && bz < g.lo[2] + g.span;
     uint64_t key = inside ? pack_key(bx, by, bz, g.b) : kEmptyKey;
@@ -125,8 +131,8 @@ __global__ void k_mark_keys(PointsView pos, int64_t n, float3 orig, float radius
         int iw = (int)w[a];
         int bmin = (int)((float)iw - radius);
         int bmax = (int)((float)iw + kmax * radius);
-        int l = (bmin < 0 ? 0 : bmin) >> g.log2r0;
-        int h = bmax >> g.log2r0;
+        int l = ((bmin < 0 ? 0 : bmin) + oo[a]) >> g.log2r0; // clamped in the cloud's own space
+        int h = (bmax + oo[a]) >> g.log2r0;
         l = max(l, g.lo[a]);
         h = min(h, g.lo[a] + g.span - 1);
         lo[a] = l;
@@ -667,19 +673,24 @@ __global__ void k_mark_bits(PointsView pos, int64_t n, float3 orig, float radius
         const int64_t i = it * stride + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
         bool valid = i < n;
         float w[3] = {0, 0, 0};
+        int oo[3] = {0, 0, 0};
         if (valid) {
             float3 p = load_f3(pos, i);
             w[0] = p.x + orig.x;
             w[1] = p.y + orig.y;
             w[2] = p.z + orig.z;
             if (w[0] < 0 || w[1] < 0 || w[2] < 0) valid = false;
+            const int3 o = point_origin(pos, i);
+            oo[0] = o.x;
+            oo[1] = o.y;
+            oo[2] = o.z;
         }
         int64_t bit = -1;
         int bx = 0, by = 0, bz = 0;
         if (valid) {
-            bx = (int)w[0] >> g.log2r0;
-            by = (int)w[1] >> g.log2r0;
-            bz = (int)w[2] >> g.log2r0;
+            bx = ((int)w[0] + oo[0]) >> g.log2r0;
+            by = ((int)w[1] + oo[1]) >> g.log2r0;
+            bz = ((int)w[2] + oo[2]) >> g.log2r0;
             if (brick_in_root(g, bx, by, bz)) {
                 if (bg_in(G, bx, by, bz)) bit = bg_bit(G, bx, by, bz);
                 else atomicOr(status, kDevCapacity);
@@ -697,8 +708,8 @@ __global__ void k_mark_bits(PointsView pos, int64_t n, float3 orig, float radius
             const int iw = (int)w[a];
             const int bmin = (int)((float)iw - radius);
             const int bmax = (int)((float)iw + kmax * radius);
-            lo[a] = max((bmin < 0 ? 0 : bmin) >> g.log2r0, g.lo[a]);
-            hi[a] = min(bmax >> g.log2r0, g.lo[a] + g.span - 1);
+            lo[a] = max(((bmin < 0 ? 0 : bmin) + oo[a]) >> g.log2r0, g.lo[a]); // clamped in the cloud's own space
+            hi[a] = min((bmax + oo[a]) >> g.log2r0, g.lo[a] + g.span - 1);
         }
         for (int x = lo[0]; x <= hi[0]; x++)
             for (int y = lo[1]; y <= hi[1]; y++)
@@ -1303,6 +1314,8 @@ __global__ void k_incre_mark(PointsView pos, int64_t n, float3 orig, float radiu
     float w[3] = {p.x + orig.x, p.y + orig.y, p.z + orig.z};
     if (w[0] < 0 || w[1] < 0 || w[2] < 0) return;
     if (T.cnt[T.depth] < 1) return;
+    const int3 o3 = point_origin(pos, i);
+    const int o[3] = {o3.x, o3.y, o3.z};
     const Node *root = &T.nodes[T.depth][0];
     const int64_t rr_root = T.range[T.depth];
     int bmin[3], bmax[3];
@@ -1313,10 +1326,23 @@ __global__ void k_incre_mark(PointsView pos, int64_t n, float3 orig, float radiu
     }
     for (int lev = 0; lev < T.depth; lev++) {
         const int rr = (int)T.range[lev];
+        // node corners in absolute coordinates; for a batched cloud whose
+        // origin is a multiple of the range they are the cloud's own corners
+        // (C truncation included) shifted by the origin
+        int clo[3], chi[3];
+        for (int a = 0; a < 3; a++) {
+            if (o[a] % rr == 0) {
+                clo[a] = bmin[a] / rr * rr + o[a];
+                chi[a] = bmax[a] / rr * rr + o[a];
+            } else {
+                clo[a] = (max(bmin[a], 0) + o[a]) / rr * rr;
+                chi[a] = (bmax[a] + o[a]) / rr * rr;
+            }
+        }
         int nd[3];
-        for (nd[0] = bmin[0] / rr * rr; nd[0] <= bmax[0] / rr * rr; nd[0] += rr)
-            for (nd[1] = bmin[1] / rr * rr; nd[1] <= bmax[1] / rr * rr; nd[1] += rr)
-                for (nd[2] = bmin[2] / rr * rr; nd[2] <= bmax[2] / rr * rr; nd[2] += rr) {
+        for (nd[0] = clo[0]; nd[0] <= chi[0]; nd[0] += rr)
+            for (nd[1] = clo[1]; nd[1] <= chi[1]; nd[1] += rr)
+                for (nd[2] = clo[2]; nd[2] <= chi[2]; nd[2] += rr) {
                     bool out = false;
                     for (int a = 0; a < 3; a++)
                         out |= nd[a] < root->mPos[a] || (int64_t)nd[a] >= root->mPos[a] + rr_root;

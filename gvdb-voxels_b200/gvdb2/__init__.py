@@ -101,6 +101,26 @@ class VolumeGVDB:
         self._keep["points"] = (pos, vel, clr)
         self._check(self._L.gvdb2_set_points(self._h, view_of(pos), view_of(vel), view_of(clr)), "SetPoints")
 
+    def BatchPoints(self, clouds, space_log2):
+        """Packs several clouds (CUDA (N,3) float32 tensors, each in its own
+        [0, 2**space_log2)^3 index space) into this volume's point set.
+        Returns numpy int64 first-index offsets (len = clouds + 1); later
+        per-point arrays are in that packed order."""
+        import numpy as np
+        n = len(clouds)
+        views = (PointsView * n)(*[view_of(c) for c in clouds])
+        first = np.zeros(n + 1, np.int64)
+        self._keep["batch"] = (clouds, views)
+        self._check(self._L.gvdb2_batch_points(self._h, views, n, int(space_log2),
+                                               first.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))), "BatchPoints")
+        return first
+
+    def BatchOrigin(self, cloud):
+        """Voxel offset of a cloud in the packed batch."""
+        o = (ctypes.c_int32 * 3)()
+        self._check(self._L.gvdb2_batch_origin(self._h, int(cloud), o), "BatchOrigin")
+        return tuple(o[:])
+
     # -- topology ---------------------------------------------------------
     def RequestFullRebuild(self, flag=True):
         self._check(self._L.gvdb2_request_full_rebuild(self._h, 1 if flag else 0), "RequestFullRebuild")

@@ -56,6 +56,8 @@ _SIGS = {
     "gvdb2_add_channel": [_vp, _i32, _i32, _i32],
     "gvdb2_set_points": [_vp, PointsView, PointsView, PointsView],
     "gvdb2_request_full_rebuild": [_vp, _i32],
+    "gvdb2_batch_points": [_vp, ctypes.POINTER(PointsView), _i32, _i32, ctypes.POINTER(ctypes.c_int64)],
+    "gvdb2_batch_origin": [_vp, _i32, ctypes.POINTER(ctypes.c_int32)],
     "gvdb2_rebuild_topology": [_vp, _i32, _f32, _fp],
     "gvdb2_accumulate_topology": [_vp, _i32, _f32, _fp, _i32],
     "gvdb2_finish_topology": [_vp, _i32, _i32],

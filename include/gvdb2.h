@@ -95,6 +95,25 @@ GVDB2_API gvdb2_status gvdb2_add_channel(gvdb2_volume *v, int chan, int dtype, i
 /* ---- points (SetPoints VH:541 / V:4900-4908) ---- */
 GVDB2_API gvdb2_status gvdb2_set_points(gvdb2_volume *v, gvdb2_points_view pos, gvdb2_points_view vel, gvdb2_points_view clr);
 
+/* Batched clouds (no counterpart in the reference, which holds one cloud
+ * per VolumeGVDB).  Packs `ncloud` clouds, each with positions in its own
+ * index space [0, 2^space_log2)^3, into one point set owned by the volume and
+ * makes it the volume's points (velocity and colour views are cleared).  The
+ * following calls with the total count process every cloud at once;
+ * per-point inputs and outputs (attributes, weights, gathered values) are in
+ * packed order, cloud after cloud.  first[c] receives the packed index of
+ * cloud c's first point (first[ncloud] = total; pass NULL to skip).  Cloud c
+ * is placed at the integer voxel origin gvdb2_batch_origin(c); positions
+ * keep their own coordinates (the origin is added to grid indices, not to
+ * the floats), so a cloud's bricks, voxel values and gathered values equal,
+ * bit for bit, those of a volume of its own.  InsertPoints and
+ * InsertPointsSubcell take one cloud per volume and return
+ * GVDB2_ERR_UNSUPPORTED for a batch. */
+GVDB2_API gvdb2_status gvdb2_batch_points(gvdb2_volume *v, const gvdb2_points_view *clouds, int ncloud, int space_log2,
+                                          int64_t *first);
+/* Voxel offset of cloud `cloud` in the packed set of gvdb2_batch_points. */
+GVDB2_API gvdb2_status gvdb2_batch_origin(gvdb2_volume *v, int cloud, int32_t out[3]);
+
 /* ---- topology ---- */
 GVDB2_API gvdb2_status gvdb2_request_full_rebuild(gvdb2_volume *v, int flag);                     /* RequestFullRebuild, VH:432 */
 GVDB2_API gvdb2_status gvdb2_rebuild_topology(gvdb2_volume *v, int n, float radius, const float orig[3]);  /* RebuildTopology, V:1181-1218 */

@@ -13,6 +13,7 @@
 
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "gvdb2.h"
 
@@ -25,6 +26,9 @@ struct Error : std::runtime_error {
 
 struct Vec3F {
     float x = 0, y = 0, z = 0;
+};
+struct Vec3I {
+    int x = 0, y = 0, z = 0;
 };
 
 class VolumeGVDB {
@@ -53,6 +57,20 @@ class VolumeGVDB {
     void SetPoints(gvdb2_points_view pos, gvdb2_points_view vel = gvdb2_points_view{},
                    gvdb2_points_view clr = gvdb2_points_view{}) {
         check(gvdb2_set_points(v_, pos, vel, clr), "SetPoints");
+    }
+
+    // Batched clouds (no reference counterpart): packs the clouds, each in
+    // its own [0, 2^space_log2)^3 space, into this volume's point set and
+    // returns each cloud's first packed index (plus the total at the end).
+    std::vector<long long> BatchPoints(const std::vector<gvdb2_points_view> &clouds, int space_log2) {
+        std::vector<int64_t> first(clouds.size() + 1, 0);
+        check(gvdb2_batch_points(v_, clouds.data(), (int)clouds.size(), space_log2, first.data()), "BatchPoints");
+        return std::vector<long long>(first.begin(), first.end());
+    }
+    Vec3I BatchOrigin(int cloud) {
+        int32_t o[3] = {0, 0, 0};
+        check(gvdb2_batch_origin(v_, cloud, o), "BatchOrigin");
+        return Vec3I{o[0], o[1], o[2]};
     }
 
     void RequestFullRebuild(bool tf) { check(gvdb2_request_full_rebuild(v_, tf ? 1 : 0), "RequestFullRebuild"); }
