@@ -24,6 +24,7 @@ sys.path.insert(0, os.path.join(ROOT, "gvdb-voxels_b200"))
 
 METRIC = "points/s rebuild+scatter+gather at <=1e-5 err, % HBM peak; adjoint & batched vs plain"
 WORKLOAD = "dynamic SPH-like step: 4,194,304-pt jittered lattice, cubic B-spline r=2, density+3 vel channels"
+WORKLOAD_16M = "dynamic SPH-like step: 16,777,216-pt jittered lattice (spacing 1,0.5,1), cubic B-spline r=2, 4 channels"
 N_POINTS = 4_194_304
 SITES = (256, 64, 256)
 DT = 0.1
@@ -40,6 +41,10 @@ def parse():
     ap.add_argument("--incremental", action="store_true", help="reference state machine instead of full rebuilds")
     ap.add_argument("--quick", action="store_true", help="timed steps only (no baseline, e2e or launch count)")
     ap.add_argument("--sites", default="256,64,256", help="lattice sites x,y,z (smaller cases for profiling)")
+    ap.add_argument("--workload", default="dam", choices=["dam", "dam16m", "batched", "adjoint"],
+                    help="dam: the contract line (dynamic step, 4,194,304 points); dam16m: the same step on "
+                         "16,777,216 points; batched: 64 clouds, batch vs per-cloud loop; adjoint: the "
+                         "differentiable splat, adjoint vs forward")
     return ap.parse_args()
 
 
@@ -365,8 +370,11 @@ def run_ours(a):
     if ws > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    sites = tuple(int(x) for x in a.sites.split(","))
-    pos, vel = wl.dam_block(sites=sites)
+    if a.workload == "dam16m":  # 256x256x256 sites at spacing (1, 0.5, 1): the same block, 4x denser
+        pos, vel = wl.dam_block(sites=(256, 256, 256), spacing=(1.0, 0.5, 1.0))
+    else:
+        sites = tuple(int(x) for x in a.sites.split(","))
+        pos, vel = wl.dam_block(sites=sites)
     cpu = None
     if rank == 0 and ws == 1 and not (a.no_cpu_baseline or a.quick):
         cpu = cpu_baseline(pos, vel)
@@ -446,7 +454,8 @@ def run_ours(a):
         line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
                 "warmup": max(3, a.warmup), "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "points_per_gpu": n, "bricks": geo["B"], "nodes": geo["U"],
+                "config": {"workload": WORKLOAD if a.workload == "dam" else WORKLOAD_16M,
+                           "points_per_gpu": n, "bricks": geo["B"], "nodes": geo["U"],
                            "rebuild": "incremental state machine" if a.incremental else "full rebuild every step",
                            "l2": "inputs larger than L2 (positions+velocities 100 MB, atlas "
                                  f"{4 * 4 * geo['B'] * geo['T'] / 1e6:.0f} MB per step)",
@@ -470,10 +479,177 @@ TRAFFIC_PER_BRICK = {
 }
 
 
+# ----------------------------------------------------------------------------
+# batched clouds: one batched pass vs a per-cloud loop of the plain path
+# ----------------------------------------------------------------------------
+BATCH_SPACE_LOG2 = 10
+
+
+def batched_step(v, K, n, chans_fwd, grad_chan, go):
+    """Forward (rebuild, splat, apron, gather) and adjoint (gather adjoint into
+    the gradient channel, then the splat adjoint) over the volume's points."""
+    v.RequestFullRebuild(True)
+    v.RebuildTopology(n, RADIUS)
+    v.UpdateAtlas()
+    v.ScatterKernel(K, n, chans_fwd, weight=1.0)
+    v.UpdateApron(-1, 0.0)
+    out = v.GatherKernel(K, n, chans_fwd, out=go[0])
+    v.GatherDensityBackward(K, n, chans_fwd, out, grad_chans=[grad_chan], grad_pos=go[1])
+    v.ScatterDensityBackward(K, n, [grad_chan], weight=1.0, grad_pos=go[2], grad_weight=go[3], grad_attr=go[4])
+
+
+def run_batched(a):
+    import numpy as np
+    import torch
+    import gvdb2
+    import gvdb2.workloads as wl
+    clouds, _ = wl.batched_clouds()
+    dev = [torch.from_numpy(c).cuda() for c in clouds]
+    total = sum(len(c) for c in clouds)
+    K = gvdb2.KERNEL_CUBIC2
+
+    def volume():
+        v = gvdb2.VolumeGVDB(0)
+        v.Configure(3, 3, 3, 3, 3)
+        for c in range(2):
+            v.AddChannel(c, gvdb2.T_FLOAT, 1)
+        return v
+
+    def outs(n):
+        return [torch.empty((n, 1), device="cuda"), torch.empty((n, 3), device="cuda"),
+                torch.empty((n, 3), device="cuda"), torch.empty((n,), device="cuda"),
+                torch.empty((n, 1), device="cuda")]
+
+    vb = volume()
+    gob = outs(total)
+
+    def step_batched():
+        vb.BatchPoints(dev, BATCH_SPACE_LOG2)
+        batched_step(vb, K, total, [0], 1, gob)
+
+    vl = volume()
+    gol = [outs(len(c)) for c in clouds]
+
+    def step_loop():
+        for c, t in enumerate(dev):
+            vl.SetPoints(t)
+            batched_step(vl, K, len(t), [0], 1, gol[c])
+
+    def timed(f, steps):
+        for _ in range(max(1, a.warmup)):
+            f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    clocks = Clocks(0)
+    clocks.start()
+    ms_b = timed(step_batched, a.steps)
+    ms_l = timed(step_loop, max(1, a.steps // 4))
+    clk = clocks.stop()
+    # identical results, cloud by cloud
+    first = vb.BatchPoints(dev, BATCH_SPACE_LOG2)
+    batched_step(vb, K, total, [0], 1, gob)
+    step_loop()
+    same = all(bool(torch.equal(gob[0][first[c]:first[c + 1]], gol[c][0])) and
+               bool(torch.equal(gob[2][first[c]:first[c + 1]], gol[c][2])) for c in range(len(clouds)))
+    line = {"metric": METRIC, "workload": f"batched: {len(clouds)} Gaussian clouds, {total} points, sizes log-uniform "
+            "in [1e4, 2e6], each in its own 1024^3 space; cubic B-spline r=2, density; forward + adjoint",
+            "value": total / (ms_b / 1e3), "unit": "points/s", "ms_per_step": ms_b,
+            "per_cloud_loop": {"value": total / (ms_l / 1e3), "ms_per_step": ms_l},
+            "speedup_vs_loop": ms_l / ms_b, "identical_to_loop": same, "n_gpus": 1, "steps": a.steps,
+            "data": "synthetic", "dtype": "f32", "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------
+# differentiable splat: adjoint step vs forward step
+# ----------------------------------------------------------------------------
+def run_adjoint(a):
+    """1,000,000 shell points splatted with the tent kernel into their own
+    topology; loss = sum over voxels of (rho - rho_target)^2 plus the sum of
+    the density gathered back at the points.  Forward = splat + loss +
+    gather; adjoint = gather adjoint + loss gradient + splat adjoint (grads
+    to positions and weights)."""
+    import torch
+    import gvdb2
+    import gvdb2.workloads as wl
+    K = gvdb2.KERNEL_TENT1
+    src = torch.from_numpy(wl.plain_small()).cuda()
+    tgt = torch.from_numpy(wl.diff_target()).cuda()
+    n, nt = len(src), len(tgt)
+    v = gvdb2.VolumeGVDB(0)
+    v.Configure(3, 3, 3, 3, 3)
+    for c in range(3):
+        v.AddChannel(c, gvdb2.T_FLOAT, 1)
+    v.SetPoints(src)
+    v.RebuildTopology(n, RADIUS)
+    v.UpdateAtlas()
+    for c in range(3):
+        v.ClearChannel(c)
+    v.SetPoints(tgt)
+    v.ScatterKernel(K, nt, [1])  # target density in the source topology (points outside it drop out)
+    v.SetPoints(src)
+    rho, rho_t, grad = v.atlas_tensor(0), v.atlas_tensor(1), v.atlas_tensor(2)
+    out = torch.empty((n, 1), device="cuda")
+    ones = torch.ones((n, 1), device="cuda")
+    gp_g = torch.empty((n, 3), device="cuda")
+    gp_s = torch.empty((n, 3), device="cuda")
+    gw = torch.empty((n,), device="cuda")
+    ga = torch.empty((n, 1), device="cuda")
+    loss = [None]
+
+    def forward():
+        v.ScatterKernel(K, n, [0])
+        loss[0] = torch.sum((rho - rho_t) ** 2)
+        v.GatherKernel(K, n, [0], out=out)
+
+    def adjoint():
+        v.GatherDensityBackward(K, n, [0], ones, grad_chans=[2], grad_pos=gp_g)  # d(sum gathered)/d rho
+        grad.add_(2.0 * (rho - rho_t))
+        v.ScatterDensityBackward(K, n, [2], weight=1.0, grad_pos=gp_s, grad_weight=gw, grad_attr=ga)
+
+    def timed(f):
+        for _ in range(max(3, a.warmup)):
+            f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / a.steps
+
+    clocks = Clocks(0)
+    clocks.start()
+    ms_f = timed(forward)
+    ms_b = timed(adjoint)
+    clk = clocks.stop()
+    line = {"metric": METRIC, "workload": "differentiable splat: 1,000,000 shell points (r 96-100) and a "
+            "1,000,000-point target (r 90-104), tent r=1, loss = sum (rho - rho_t)^2 + sum gathered",
+            "value": n / ((ms_f + ms_b) / 1e3), "unit": "points/s", "forward_ms": ms_f, "adjoint_ms": ms_b,
+            "adjoint_over_forward": ms_b / ms_f, "bricks": int(v.info().atlas_slots), "n_gpus": 1,
+            "steps": a.steps, "data": "synthetic", "dtype": "f32", "clocks": clk,
+            "loss": float(loss[0].item())}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "batched":
+        return run_batched(a)
+    if a.workload == "adjoint":
+        return run_adjoint(a)
     return run_ours(a)
 
 
