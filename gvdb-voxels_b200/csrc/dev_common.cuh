@@ -154,6 +154,34 @@ __device__ __forceinline__ int32_t leaf_at_o(const LeafLookup &L, float wx, floa
     return leaf_at_brick(L, ((int)wx + o.x) >> L.g.log2r0, ((int)wy + o.y) >> L.g.log2r0, ((int)wz + o.z) >> L.g.log2r0);
 }
 
+// The kernel splats and gathers work on cells: 8^3 blocks of a brick.  A
+// brick of res0 = 8m voxels holds m^3 cells; cell id = slot * m^3 +
+// (cz * m + cy) * m + cx.  For 8^3 bricks a cell is the brick.
+constexpr int kCell = 8;
+__device__ __forceinline__ void cell_coords(int64_t cell, int m, int m3, int64_t &slot, int &cx, int &cy, int &cz) {
+    if (m3 == 1) { // 8^3 bricks: the cell is the brick
+        slot = cell;
+        cx = cy = cz = 0;
+        return;
+    }
+    slot = cell / m3;
+    const int ci = (int)(cell - slot * m3);
+    cx = ci % m;
+    cy = (ci / m) % m;
+    cz = ci / (m * m);
+}
+// cell of a voxel inside its brick (local voxel coordinates in [0, res0))
+__device__ __forceinline__ int cell_of_local(int lx, int ly, int lz, int m) {
+    return ((lz >> 3) * m + (ly >> 3)) * m + (lx >> 3);
+}
+// brick-local coordinate that may lie in a neighbouring brick: the step to
+// that brick (-1, 0, 1) and the coordinate inside it
+__device__ __forceinline__ int brick_step(int L, int res0, int &local) {
+    const int d = L < 0 ? -1 : (L >= res0 ? 1 : 0);
+    local = L - d * res0;
+    return d;
+}
+
 __device__ __forceinline__ bool hs_contains(const uint64_t *keys, uint32_t mask, uint64_t key) {
     uint32_t h = hash_key(key) & mask;
     for (int probe = 0; probe < kMaxProbe; ++probe) {

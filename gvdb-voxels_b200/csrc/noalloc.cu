@@ -7,10 +7,11 @@
 // initialisation), a process whose allocator is owned by another framework,
 // or a caller holding a CUDA context in a state where an allocation would
 // synchronise the device at a bad time.  gvdb2_gather_kernel allocates its
-// per-call binning buffers (point -> brick ids, ranks, the brick-ordered
-// point list, per-brick offsets); this variant keeps them in one file-scope
-// device array instead, sized for at most kNoAllocMaxPoints points and
-// kNoAllocMaxSlots active bricks, and computes the same values.
+// per-call binning buffers (point -> bin ids, ranks, the bin-ordered point
+// list, per-bin offsets; a bin is an 8^3 cell of an active brick, the whole
+// brick for 8^3 bricks); this variant keeps them in one file-scope device
+// array instead, sized for at most kNoAllocMaxPoints points and
+// kNoAllocMaxBins bins, and computes the same values.
 //
 // The array exists once per GPU that loads the library and lives until the
 // process exits.  Every call shares it, and it keeps the last call's
@@ -32,12 +33,12 @@ namespace gvdb2 {
 namespace {
 
 constexpr int64_t kNoAllocMaxPoints = 1 << 20; // 1,048,576 points
-constexpr int64_t kNoAllocMaxSlots = 1 << 15;  // 32,768 active bricks
-constexpr int64_t kOffWords = kNoAllocMaxSlots + 1;
-constexpr int64_t kScratchWords = 3 * kNoAllocMaxPoints + kNoAllocMaxSlots + kOffWords; // 12.25 MB
+constexpr int64_t kNoAllocMaxBins = 1 << 15;   // 32,768 cells: active bricks of 8^3 (1/8 as many of 16^3)
+constexpr int64_t kOffWords = kNoAllocMaxBins + 1;
+constexpr int64_t kScratchWords = 3 * kNoAllocMaxPoints + kNoAllocMaxBins + kOffWords; // 12.25 MB
 
-// [0, P) point slots, [P, 2P) ranks, [2P, 3P) brick-ordered point list,
-// [3P, 3P+S) per-brick counts, then S+1 per-brick offsets.
+// [0, P) point bins, [P, 2P) ranks, [2P, 3P) bin-ordered point list,
+// [3P, 3P+S) per-bin counts, then S+1 per-bin offsets.
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kScratchWords];
 
 constexpr int kMaxDevices = 64;
@@ -58,18 +59,24 @@ gvdb2_status scratch_address(Volume *v, uint32_t **out) {
     return GVDB2_OK;
 }
 
-__global__ void k_na_bin(PointsView pos, int64_t n, float3 trans, LeafLookup L, const int32_t *leaf_slot,
+__global__ void k_na_bin(PointsView pos, int64_t n, float3 trans, LeafLookup L, const int32_t *leaf_slot, int m,
                          int32_t *pslot, uint32_t *prank, uint32_t *counts) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float3 p = load_f3(pos, i);
-    int32_t slot = -1;
+    int32_t bin = -1;
     if (p.z != kNoHit) {
-        int32_t leaf = leaf_at_o(L, p.x + trans.x, p.y + trans.y, p.z + trans.z, point_origin(pos, i));
-        slot = leaf >= 0 ? leaf_slot[leaf] : -1;
+        const float wx = p.x + trans.x, wy = p.y + trans.y, wz = p.z + trans.z;
+        const int3 o = point_origin(pos, i);
+        const int32_t leaf = leaf_at_o(L, wx, wy, wz, o);
+        const int32_t slot = leaf >= 0 ? leaf_slot[leaf] : -1;
+        if (slot >= 0) {
+            const int rm = (1 << L.g.log2r0) - 1; // local voxel = voxel mod res0
+            bin = slot * m * m * m + cell_of_local(((int)wx + o.x) & rm, ((int)wy + o.y) & rm, ((int)wz + o.z) & rm, m);
+        }
     }
-    pslot[i] = slot;
-    if (slot >= 0) prank[i] = atomicAdd(&counts[slot], 1u);
+    pslot[i] = bin;
+    if (bin >= 0) prank[i] = atomicAdd(&counts[bin], 1u);
 }
 
 // One CTA: exclusive scan of the per-brick counts into offsets (S+1 words).
@@ -139,8 +146,12 @@ extern "C" gvdb2_status gvdb2_gather_kernel_noalloc(gvdb2_volume *h, int kernel,
     if (n > kNoAllocMaxPoints)
         return fail(v, GVDB2_ERR_CAPACITY, "gvdb2_gather_kernel_noalloc takes at most 1,048,576 points per call");
     if (!v->atlas_valid) return fail(v, GVDB2_ERR_STATE, "UpdateAtlas must follow the topology rebuild");
-    if (v->atlas_last > kNoAllocMaxSlots)
-        return fail(v, GVDB2_ERR_CAPACITY, "gvdb2_gather_kernel_noalloc takes at most 32,768 active bricks");
+    const int m = v->res(0) / kCell; // cells per brick edge
+    if (m < 1 || v->res(0) % kCell)
+        return fail(v, GVDB2_ERR_UNSUPPORTED, "kernel gathers need bricks of a multiple of 8 voxels");
+    if (v->atlas_last * m * m * m > kNoAllocMaxBins)
+        return fail(v, GVDB2_ERR_CAPACITY,
+                    "gvdb2_gather_kernel_noalloc takes at most 32,768 active 8^3 cells (bricks of 8^3 voxels)");
     if (!out || out_stride < nch) return fail(v, GVDB2_ERR_ARG, "bad output buffer");
     const float zero[3] = {0, 0, 0};
     if (!trans) trans = zero;
@@ -150,19 +161,19 @@ extern "C" gvdb2_status gvdb2_gather_kernel_noalloc(gvdb2_volume *h, int kernel,
     uint32_t *prank = base + kNoAllocMaxPoints;
     int32_t *perm = reinterpret_cast<int32_t *>(base + 2 * kNoAllocMaxPoints);
     uint32_t *counts = base + 3 * kNoAllocMaxPoints;
-    uint32_t *off = counts + kNoAllocMaxSlots;
-    const int64_t nslots = v->atlas_last;
-    if (n == 0 || nslots == 0) {
+    uint32_t *off = counts + kNoAllocMaxBins;
+    const int64_t nbins = v->atlas_last * m * m * m;
+    if (n == 0 || nbins == 0) {
         if (n > 0) // no active brick: every point gathers zero
             GV_CUDA(v, cudaMemset2DAsync(out, sizeof(float) * out_stride, 0, sizeof(float) * nch, n, v->stream));
         return GVDB2_OK;
     }
-    GV_CUDA(v, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (size_t)nslots, v->stream));
+    GV_CUDA(v, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (size_t)nbins, v->stream));
     LeafLookup L = make_lookup(v);
     const float3 t = make_float3(trans[0], trans[1], trans[2]);
     const int g = grid_for(n, 256, 1ll << 31);
-    k_na_bin<<<g, 256, 0, v->stream>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(), pslot, prank, counts);
-    k_na_scan<<<1, kNaScanThreads, 0, v->stream>>>(counts, nslots, off);
+    k_na_bin<<<g, 256, 0, v->stream>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(), m, pslot, prank, counts);
+    k_na_scan<<<1, kNaScanThreads, 0, v->stream>>>(counts, nbins, off);
     k_na_fill<<<g, 256, 0, v->stream>>>(pslot, prank, n, off, perm, out, out_stride, nch);
     GV_CUDA(v, cudaGetLastError());
     return gather_kernel_prebinned(v, kernel, n, trans, chans, nch, out, out_stride, off, perm);

@@ -51,17 +51,25 @@ __global__ void k_sort_points(PointsView pos, int64_t n, float3 trans, const int
     out[3 * k + 2] = p.z + trans.z;
 }
 
-// Bins every point by the atlas slot of the brick that contains it (-1 when
-// no active brick does); ranks come from warp-aggregated counters.
-__global__ void k_bin_count(PointsView pos, int64_t n, float3 trans, LeafLookup L, const int32_t *leaf_slot,
+// Bins every point by the 8^3 cell that contains it, cell = slot * m^3 +
+// cell in the brick (-1 when no active brick contains it); ranks come from
+// warp-aggregated counters.
+__global__ void k_bin_count(PointsView pos, int64_t n, float3 trans, LeafLookup L, const int32_t *leaf_slot, int m,
                             uint32_t *cnt, int32_t *pbin, int32_t *prank) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int32_t bin = -1;
     if (i < n) {
         float3 p = load_f3(pos, i);
         if (p.z != kNoHit) {
-            int32_t leaf = leaf_at_o(L, p.x + trans.x, p.y + trans.y, p.z + trans.z, point_origin(pos, i));
-            bin = leaf >= 0 ? leaf_slot[leaf] : -1;
+            const float w[3] = {p.x + trans.x, p.y + trans.y, p.z + trans.z};
+            const int3 o = point_origin(pos, i);
+            const int32_t leaf = leaf_at_o(L, w[0], w[1], w[2], o);
+            const int32_t slot = leaf >= 0 ? leaf_slot[leaf] : -1;
+            if (slot >= 0) {
+                const int rm = (1 << L.g.log2r0) - 1; // local voxel = voxel mod res0
+                bin = slot * m * m * m + cell_of_local(((int)w[0] + o.x) & rm, ((int)w[1] + o.y) & rm,
+                                                       ((int)w[2] + o.z) & rm, m);
+            }
         }
     }
     unsigned act = __ballot_sync(0xffffffffu, bin >= 0);
@@ -227,7 +235,10 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     if (!v->atlas_valid) return fail(v, GVDB2_ERR_STATE, "UpdateAtlas must follow the topology rebuild");
     if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count))) return fail(v, GVDB2_ERR_ARG, "bad point count");
     cudaStream_t s = v->stream;
-    int64_t nbins = v->atlas_last;
+    const int m = v->res(0) / kCell; // cells per brick edge (bins are 8^3 cells)
+    if (m < 1 || v->res(0) % kCell) return fail(v, GVDB2_ERR_UNSUPPORTED, "kernel splats need bricks of a multiple of 8 voxels");
+    int64_t nbins = v->atlas_last * m * m * m;
+    if (nbins >= INT32_MAX) return fail(v, GVDB2_ERR_CAPACITY, "more than 2^31 cells of 8^3 voxels");
     GV_CUDA(v, v->pbin.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
     GV_CUDA(v, v->prank.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
     GV_CUDA(v, v->perm.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
@@ -237,7 +248,7 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     float3 t = make_float3(trans[0], trans[1], trans[2]);
     LeafLookup L = make_lookup(v);
     if (n > 0) {
-        k_bin_count<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(),
+        k_bin_count<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(), m,
                                                                 v->bin_cnt.as<uint32_t>(), v->pbin.as<int32_t>(),
                                                                 v->prank.as<int32_t>());
         GV_CUDA(v, cudaGetLastError());

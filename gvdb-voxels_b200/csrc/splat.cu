@@ -184,6 +184,7 @@ struct SplatArgs {
     const uint32_t *bin_off;
     const int32_t *perm;
     int res0, log2r0, apron, tile;
+    int m, m3; // cells per brick edge, per brick
     int64_t tvox;
 };
 
@@ -252,13 +253,17 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
     float(*pa)[kOwnChunk] = pw + 3 * N;
     int32_t *pb = reinterpret_cast<int32_t *>(pa + NCH);
     __shared__ double inv_s[NCH];
-    __shared__ int32_t amax_bits[NCH]; // max |weighted amount| of the brick's points, as float bits
-    const int64_t slot = blockIdx.x;
+    __shared__ int32_t amax_bits[NCH]; // max |weighted amount| of the cell's points, as float bits
+    const int64_t cell = blockIdx.x;
+    int64_t slot;
+    int cx, cy, cz;
+    cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
     for (int i = threadIdx.x; i < NCH * X::CS; i += kOwnThreads) acc_hi[i] = acc_lo[i] = 0;
     if (threadIdx.x < NCH) amax_bits[threadIdx.x] = 0;
-    const uint32_t beg = S.bin_off[slot], R = S.bin_off[slot + 1] - beg;
+    const uint32_t beg = S.bin_off[cell], R = S.bin_off[cell + 1] - beg;
     const Node &nd = S.leaves[S.slot_leaf[slot]];
-    const int ox = nd.mPos[0] - X::H, oy = nd.mPos[1] - X::H, oz = nd.mPos[2] - X::H;
+    const int ox = nd.mPos[0] + kCell * cx - X::H, oy = nd.mPos[1] + kCell * cy - X::H,
+              oz = nd.mPos[2] + kCell * cz - X::H;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     // Stage one point as record r of the current chunk (amounts times `scale`).
@@ -383,7 +388,7 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
     // advances by the base-E digits of 256 instead of being divided out
     constexpr int E = X::E, DZ = kOwnThreads / (E * E), DY = (kOwnThreads / E) % E, DX = kOwnThreads % E;
     static_assert(DZ < E, "one wrap per step");
-    float *dst = ext + slot * (int64_t)NCH * X::E3;
+    float *dst = ext + cell * (int64_t)NCH * X::E3;
     int c = 0, z = threadIdx.x / (E * E), y = (threadIdx.x / E) % E, x = threadIdx.x % E;
     for (int i = threadIdx.x; i < NCH * X::E3; i += kOwnThreads) {
         const int k = c * X::CS + z * X::PS + y * X::RS + x;
@@ -405,7 +410,10 @@ template <int KERNEL, int NCH>
 __global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S, const float *ext) {
     using X = ExtTile<KERNEL>;
     __shared__ int32_t nb[27];
-    const int64_t slot = blockIdx.x;
+    const int64_t cell = blockIdx.x;
+    int64_t slot;
+    int cx, cy, cz;
+    cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
     if (threadIdx.x < 27) nb[threadIdx.x] = S.nbr27[slot * 27 + threadIdx.x];
     __syncthreads();
     const int vx = threadIdx.x & 7, vy = (threadIdx.x >> 3) & 7, vz = threadIdx.x >> 6;
@@ -423,9 +431,17 @@ __global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S, const float 
     for (int m = 0; m < 8; m++) {
         const int dx = (m & 1) ? ex : 0, dy = (m & 2) ? ey : 0, dz = (m & 4) ? ez : 0;
         const bool used = (!(m & 1) || ex) && (!(m & 2) || ey) && (!(m & 4) || ez);
-        const int n = used ? nb[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] : -1;
+        // the covering cell: one step d from this cell, possibly in a neighbouring brick
+        int ncx = cx + dx, ncy = cy + dy, ncz = cz + dz;
+        const int bx = ncx < 0 ? -1 : (ncx >= S.m ? 1 : 0), by = ncy < 0 ? -1 : (ncy >= S.m ? 1 : 0),
+                  bz = ncz < 0 ? -1 : (ncz >= S.m ? 1 : 0);
+        ncx -= bx * S.m;
+        ncy -= by * S.m;
+        ncz -= bz * S.m;
+        const int ns = used ? nb[(bz + 1) * 9 + (by + 1) * 3 + (bx + 1)] : -1;
+        const int64_t n = ns >= 0 ? (int64_t)ns * S.m3 + (ncz * S.m + ncy) * S.m + ncx : -1;
         const int ux = vx - 8 * dx + X::H, uy = vy - 8 * dy + X::H, uz = vz - 8 * dz + X::H;
-        const float *src = ext + (int64_t)max(n, 0) * NCH * X::E3 + (uz * X::E + uy) * X::E + ux;
+        const float *src = ext + (n >= 0 ? n : 0) * (int64_t)NCH * X::E3 + (uz * X::E + uy) * X::E + ux;
 #pragma unroll
         for (int c = 0; c < NCH; c++) part[m][c] = n >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
     }
@@ -434,13 +450,13 @@ __global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S, const float 
 #pragma unroll
         for (int c = 0; c < NCH; c++) acc[c] += part[m][c];
     const int a = S.apron, tl = S.tile;
-    const int64_t at = slot * S.tvox + ((int64_t)(vz + a) * tl + (vy + a)) * tl + (vx + a);
+    const int Lx = kCell * cx + vx, Ly = kCell * cy + vy, Lz = kCell * cz + vz; // voxel in the brick
+    const int64_t at = slot * S.tvox + ((int64_t)(Lz + a) * tl + (Ly + a)) * tl + (Lx + a);
 #pragma unroll
     for (int c = 0; c < NCH; c++)
         if (c < S.nch) S.chan[c][at] = acc[c];
 }
 
-constexpr int kScatterRes = 8; // brick edge the kernel splats take
 
 // ---------------------------------------------------------------------
 // tiled gathers: forward, scatter adjoint, gather adjoint
@@ -467,6 +483,7 @@ struct GatherArgs {
     const uint32_t *bin_off;
     const int32_t *perm;
     int res0, apron, tile;
+    int m, m3; // cells per brick edge, per brick
     int64_t tvox;
 };
 
@@ -478,14 +495,20 @@ __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *tile = reinterpret_cast<float *>(smem_raw);
     __shared__ int32_t nbs[27];
-    const int res = G.res0, ht = res + 2 * H, ht3 = ht * ht * ht;
-    const int64_t slot = blockIdx.x;
+    // one CTA per 8^3 cell of a brick: the cell plus its halo is staged
+    const int res = G.res0, ht = kCell + 2 * H, ht3 = ht * ht * ht;
+    const int64_t cell = blockIdx.x;
+    int64_t slot;
+    int cx, cy, cz;
+    cell_coords(cell, G.m, G.m3, slot, cx, cy, cz);
     const int a = G.apron, tl = G.tile;
     if (threadIdx.x < 27) nbs[threadIdx.x] = G.nbr27[slot * 27 + threadIdx.x];
     __syncthreads();
     // halo tile from the interiors of this brick and its neighbours
     for (int i = threadIdx.x; i < ht3; i += blockDim.x) {
-        const int lx = i % ht - H, ly = (i / ht) % ht - H, lz = i / (ht * ht) - H;
+        // brick-local voxel of tile element i
+        const int lx = i % ht - H + kCell * cx, ly = (i / ht) % ht - H + kCell * cy,
+                  lz = i / (ht * ht) - H + kCell * cz;
         const int dx = lx < 0 ? -1 : (lx >= res ? 1 : 0), dy = ly < 0 ? -1 : (ly >= res ? 1 : 0),
                   dz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
         const int32_t nb = nbs[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
@@ -496,8 +519,8 @@ __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
     }
     __syncthreads();
     const Node &nd = G.leaves[G.slot_leaf[slot]];
-    const int ox = nd.mPos[0] - H, oy = nd.mPos[1] - H, oz = nd.mPos[2] - H;
-    const uint32_t beg = G.bin_off[slot], end = G.bin_off[slot + 1];
+    const int ox = nd.mPos[0] + kCell * cx - H, oy = nd.mPos[1] + kCell * cy - H, oz = nd.mPos[2] + kCell * cz - H;
+    const uint32_t beg = G.bin_off[cell], end = G.bin_off[cell + 1];
     for (uint32_t j = beg + threadIdx.x; j < end; j += blockDim.x) {
         const int32_t pidx = G.perm[j];
         const float3 p = load_f3(G.pos, pidx);
@@ -613,6 +636,8 @@ void fill_topology(Volume *v, Args &S) {
     S.bin_off = v->bin_off.as<uint32_t>();
     S.perm = v->perm.as<int32_t>();
     S.res0 = v->res(0);
+    S.m = v->res(0) / kCell;
+    S.m3 = S.m * S.m * S.m;
     S.apron = v->apron;
     S.tile = v->tile_res();
     S.tvox = v->tile_vox();
@@ -634,14 +659,14 @@ template <int KERNEL, int NCH>
 gvdb2_status scatter_group(Volume *v, const SplatArgs &S) {
     using X = ExtTile<KERNEL>;
     cudaStream_t s = v->stream;
-    const int64_t nslots = v->atlas_last;
-    GV_CUDA(v, v->scratch.ensure(sizeof(float) * (size_t)nslots * NCH * X::E3 + 256, s));
+    const int64_t ncells = v->atlas_last * S.m3;
+    GV_CUDA(v, v->scratch.ensure(sizeof(float) * (size_t)ncells * NCH * X::E3 + 256, s));
     float *ext = v->scratch.as<float>();
     constexpr size_t smem = own_smem_bytes<KERNEL, NCH>();
     auto k1 = k_scatter_own<KERNEL, NCH>;
     GV_TRY(launch_smem(v, k1, smem, "scatter"));
-    k1<<<(unsigned)nslots, kOwnThreads, smem, s>>>(S, ext);
-    k_scatter_merge<KERNEL, NCH><<<(unsigned)nslots, 512, 0, s>>>(S, ext);
+    k1<<<(unsigned)ncells, kOwnThreads, smem, s>>>(S, ext);
+    k_scatter_merge<KERNEL, NCH><<<(unsigned)ncells, 512, 0, s>>>(S, ext);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
@@ -676,8 +701,8 @@ gvdb2_status scatter_two_phase(Volume *v, const SplatArgs &S) {
 
 gvdb2_status run_scatter(Volume *v, int kernel, const SplatArgs &S) {
     if (v->atlas_last == 0) return GVDB2_OK;
-    if (v->res(0) != kScatterRes)
-        return fail(v, GVDB2_ERR_UNSUPPORTED, "kernel splats need 8^3 bricks (Configure(...,3))");
+    if (v->res(0) % kCell)
+        return fail(v, GVDB2_ERR_UNSUPPORTED, "kernel splats need bricks of a multiple of 8 voxels");
     return kernel == GVDB2_KERNEL_TENT1 ? scatter_two_phase<GVDB2_KERNEL_TENT1>(v, S)
                                         : scatter_two_phase<GVDB2_KERNEL_CUBIC2>(v, S);
 }
@@ -685,11 +710,11 @@ gvdb2_status run_scatter(Volume *v, int kernel, const SplatArgs &S) {
 template <int KERNEL, int MODE, int NCH>
 gvdb2_status launch_gather(Volume *v, const GatherArgs &G) {
     constexpr int H = Taps<KERNEL>::N / 2;
-    const int ht = v->res(0) + 2 * H;
+    constexpr int ht = kCell + 2 * H;
     const size_t smem = sizeof(float) * (size_t)NCH * ht * ht * ht;
     auto k = k_gather_tile<KERNEL, MODE, NCH>;
     GV_TRY(launch_smem(v, k, smem, "gather"));
-    k<<<(unsigned)v->atlas_last, 256, smem, v->stream>>>(G);
+    k<<<(unsigned)(v->atlas_last * G.m3), 256, smem, v->stream>>>(G);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
