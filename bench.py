@@ -41,10 +41,12 @@ def parse():
     ap.add_argument("--incremental", action="store_true", help="reference state machine instead of full rebuilds")
     ap.add_argument("--quick", action="store_true", help="timed steps only (no baseline, e2e or launch count)")
     ap.add_argument("--sites", default="256,64,256", help="lattice sites x,y,z (smaller cases for profiling)")
-    ap.add_argument("--workload", default="dam", choices=["dam", "dam16m", "batched", "adjoint"],
+    ap.add_argument("--workload", default="dam", choices=["dam", "dam16m", "batched", "adjoint", "sparse67m"],
                     help="dam: the contract line (dynamic step, 4,194,304 points); dam16m: the same step on "
                          "16,777,216 points; batched: 64 clouds, batch vs per-cloud loop; adjoint: the "
-                         "differentiable splat, adjoint vs forward")
+                         "differentiable splat, adjoint vs forward; sparse67m: the large sparse scene "
+                         "(67,108,864-point Gaussian mixture, 32^3 bricks, forward + adjoint)")
+    ap.add_argument("--points", type=int, default=0, help="sparse67m: fewer points (smaller cases for profiling)")
     return ap.parse_args()
 
 
@@ -642,6 +644,141 @@ def run_adjoint(a):
     return 0
 
 
+# ----------------------------------------------------------------------------
+# large sparse scene: 67M-point Gaussian mixture on 32^3 bricks
+# ----------------------------------------------------------------------------
+SPARSE_WORKLOAD = ("large sparse scene: 67,108,864-pt 32-component Gaussian mixture (sigma 8-64, means in 4096^3), "
+                   "Configure(3,3,3,4,5), cubic B-spline r=2, density+3 vel channels, full rebuild every step, "
+                   "forward + adjoint")
+
+
+def run_sparse(a):
+    """Each step: advect p += 0.1 v -> full RebuildTopology(N, 2) ->
+    UpdateAtlas -> scatter of mass and momentum (4 channels) -> UpdateApron
+    -> gather of the 3 velocity channels; then the adjoint of
+    L = sum(out * g) + sum over voxels of rho^2 for a fixed random g: the
+    gather adjoint (dL/dG into 3 channels, dL/dpos) and the scatter adjoint
+    (dL/dpos, dL/dweight, dL/dattr).  Per-kernel device times come from one
+    profiled step after the timed region; GB/s per kernel is algorithmic
+    bytes over that time."""
+    import numpy as np
+    import torch
+    import gvdb2
+    import gvdb2.workloads as wl
+    from torch.profiler import ProfilerActivity, profile
+    K = gvdb2.KERNEL_CUBIC2
+    n = a.points if a.points else 67_108_864
+    pos_h, vel_h = wl.gaussian_mixture(n=n)
+    pos = torch.from_numpy(pos_h).cuda()
+    vel = torch.from_numpy(vel_h).cuda()
+    del pos_h, vel_h
+    g_out = torch.randn((n, 3), device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+    out = torch.empty((n, 3), device="cuda")
+    gp_g = torch.empty((n, 3), device="cuda")
+    gp_s = torch.empty((n, 3), device="cuda")
+    gw = torch.empty((n,), device="cuda")
+    ga = torch.empty((n, 4), device="cuda")
+    v = gvdb2.VolumeGVDB(0)
+    v.Configure(3, 3, 3, 4, 5)
+    for c in range(8):
+        v.AddChannel(c, gvdb2.T_FLOAT, 1)
+    v.SetPoints(pos)
+    attrs = [None, (vel, 0), (vel, 1), (vel, 2)]
+    stage = {}
+
+    def rec(events, name):
+        if events is not None:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record()
+            events.append((name, e))
+
+    def step(events=None):
+        rec(events, "start")
+        pos.add_(vel, alpha=DT)
+        v.RequestFullRebuild(True)
+        v.RebuildTopology(n, RADIUS)
+        v.UpdateAtlas()
+        rec(events, "topology")
+        v.ScatterKernel(K, n, [0, 1, 2, 3], weight=1.0, attrs=attrs)
+        rec(events, "scatter")
+        for c in range(4):
+            v.UpdateApron(c, 0.0)
+        rec(events, "apron")
+        v.GatherKernel(K, n, [1, 2, 3], out=out)
+        rec(events, "gather")
+        v.GatherDensityBackward(K, n, [1, 2, 3], g_out, grad_chans=[5, 6, 7], grad_pos=gp_g)
+        rec(events, "gather_adjoint")
+        rho, g_rho = v.atlas_tensor(0), v.atlas_tensor(4)
+        torch.mul(rho, 2.0, out=g_rho)
+        v.ScatterDensityBackward(K, n, [4, 5, 6, 7], weight=1.0, attrs=attrs, grad_pos=gp_s, grad_weight=gw,
+                                 grad_attr=ga)
+        rec(events, "scatter_adjoint")
+
+    for _ in range(max(3, a.warmup)):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / a.steps
+    # per-stage device time (event pairs), median over 3 steps
+    per = {}
+    for _ in range(3):
+        ev = []
+        step(ev)
+        torch.cuda.synchronize()
+        for (_, x), (nm, y) in zip(ev, ev[1:]):
+            per.setdefault(nm, []).append(x.elapsed_time(y))
+    stage = {k: statistics.median(t) for k, t in per.items()}
+    # per-kernel device time from one profiled step
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        step()
+        torch.cuda.synchronize()
+    kt = {}
+    for e in prof.events():
+        if e.device_type == torch.autograd.DeviceType.CUDA:
+            nm = e.name.replace("(anonymous namespace)::", "").replace("gvdb2::", "").replace("void ", "")
+            nm = nm.split("(")[0]
+            d = kt.setdefault(nm, [0, 0.0])
+            d[0] += 1
+            d[1] += e.device_time / 1e3
+    inf = v.info()
+    slots = int(inf.atlas_slots)
+    ncell = slots * 64
+    busy = int(inf.splat_cells) if int(inf.splat_cells) >= 0 else None
+    T3, R3, E3 = int(inf.tile_res) ** 3, 32 ** 3, 12 ** 3
+    # algorithmic bytes per launch (forward scatter 4 ch, gather 3 ch)
+    alg = {}
+    if busy is not None:
+        alg["k_scatter_own<2, 4>"] = n * 28 + busy * 4 * E3 * 4
+        alg["k_scatter_merge<2, 4>"] = busy * 4 * E3 * 4 + ncell * 512 * 4 * 4
+    alg["k_apron"] = slots * (T3 - R3) * 4 * 2
+    total_ms = sum(d[1] for d in kt.values())
+    kernels = []
+    for nm, (cnt, t) in sorted(kt.items(), key=lambda x: -x[1][1]):
+        row = {"kernel": nm, "launches": cnt, "ms": round(t, 3), "share": round(t / total_ms, 4)}
+        b = alg.get(nm)
+        if b is not None:
+            one = t / cnt  # ms per launch
+            row["alg_gb_per_launch"] = round(b / 1e9, 3)
+            row["gbs"] = round(b / (one / 1e3) / 1e9, 1)
+        kernels.append(row)
+    peak, src = peaks()
+    line = {"metric": METRIC, "workload": SPARSE_WORKLOAD, "value": n / (ms / 1e3), "unit": "points/s",
+            "ms_per_step": ms, "stage_ms": stage, "bricks": slots, "cells": ncell, "cells_with_points": busy,
+            "n_points": n, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "data": "synthetic", "dtype": "f32",
+            "hbm_peak_gbs": peak, "peak_source": src, "kernels": kernels[:16], "clocks": clk,
+            "device_mem_gb": round(torch.cuda.max_memory_allocated() / 1e9, 2)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -650,6 +787,8 @@ def main():
         return run_batched(a)
     if a.workload == "adjoint":
         return run_adjoint(a)
+    if a.workload == "sparse67m":
+        return run_sparse(a)
     return run_ours(a)
 
 

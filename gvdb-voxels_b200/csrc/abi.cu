@@ -376,6 +376,13 @@ gvdb2_status gvdb2_get_info(gvdb2_volume *h, gvdb2_info *out) {
         out->root_pos[a] = v->root_pos[a];
     }
     out->tile_res = v->tile_res();
+    out->splat_cells = -1;
+    if (v->bin_key.valid && v->cell_cnt.p) {
+        uint32_t c3[3] = {0, 0, 0};
+        e = cudaMemcpy(c3, v->cell_cnt.p, sizeof(c3), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return gvdb2::cuda_fail(v, e, "get_info");
+        out->splat_cells = (int64_t)c3[0] + c3[1] + c3[2];
+    }
     return GVDB2_OK;
 }
 

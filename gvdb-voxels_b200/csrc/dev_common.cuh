@@ -164,11 +164,39 @@ __device__ __forceinline__ void cell_coords(int64_t cell, int m, int m3, int64_t
         cx = cy = cz = 0;
         return;
     }
-    slot = cell / m3;
-    const int ci = (int)(cell - slot * m3);
-    cx = ci % m;
-    cy = (ci / m) % m;
-    cz = ci / (m * m);
+    const int lm = __ffs(m) - 1; // m = res0 / 8 is a power of two: shifts, no division
+    slot = cell >> (3 * lm);
+    const int ci = (int)(cell & (int64_t)(m3 - 1));
+    cx = ci & (m - 1);
+    cy = (ci >> lm) & (m - 1);
+    cz = ci >> (2 * lm);
+}
+// The cells that hold points fall in three classes by their point count k:
+// huge (k > kHeavyCell), heavy (kLightCell < k <= kHeavyCell) and light
+// (0 < k <= kLightCell).  The huge and heavy cells are listed in the order
+// of cell_at: huge cells first (list[0 .. cnt[0])), then the heavy ones,
+// stored from the back (list[ncell - 1], list[ncell - 2], ..., cnt[1] of
+// them).  Light cells are listed apart (light[0 .. cnt[2])).  The gather
+// stages a halo tile per huge or heavy cell and reads the taps of light
+// cells' points straight from the atlas, one warp per light cell; the
+// splat's own phase takes all three classes (order of own_cell_at).
+constexpr uint32_t kHeavyCell = 1024;
+constexpr uint32_t kLightCell = 32;
+// The i-th huge or heavy cell, or -1 past their end.
+__device__ __forceinline__ int64_t cell_at(int64_t i, const int32_t *list, const uint32_t *cnt, int64_t ncell) {
+    const int64_t h = cnt[0];
+    if (i < h) return list[i];
+    i -= h;
+    return i < (int64_t)cnt[1] ? list[ncell - 1 - i] : -1;
+}
+// The i-th cell of the splat's own order: the huge and heavy cells (order of
+// cell_at), then the light ones; -1 past the end.
+__device__ __forceinline__ int64_t own_cell_at(int64_t i, const int32_t *list, const int32_t *light,
+                                               const uint32_t *cnt, int64_t ncell) {
+    const int64_t hh = (int64_t)cnt[0] + cnt[1];
+    if (i < hh) return cell_at(i, list, cnt, ncell);
+    i -= hh;
+    return i < (int64_t)cnt[2] ? (int64_t)light[i] : -1;
 }
 // cell of a voxel inside its brick (local voxel coordinates in [0, res0))
 __device__ __forceinline__ int cell_of_local(int lx, int ly, int lz, int m) {

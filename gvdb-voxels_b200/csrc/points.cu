@@ -98,6 +98,50 @@ __global__ void k_bin_fill(const int32_t *pbin, const int32_t *prank, int64_t n,
     if (b >= 0) perm[off[b] + prank[i]] = (int32_t)i;
 }
 
+// List the cells that hold points by class (huge from the front of `list`,
+// heavy from its back, light in `light`; see cell_at).
+constexpr int64_t kCellCountReadback = 1 << 16; // cells
+
+__global__ void k_cell_list(const uint32_t *off, int64_t ncell, int32_t *list, int32_t *light, uint32_t *cnt) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t k = c < ncell ? off[c + 1] - off[c] : 0u;
+    const int cls = k == 0 ? -1 : (k > kHeavyCell ? 0 : (k > kLightCell ? 1 : 2));
+    const unsigned act = __ballot_sync(0xffffffffu, cls >= 0);
+    if (cls >= 0) {
+        const uint32_t r = warp_agg_inc(cnt, (uint32_t)cls, act);
+        if (cls == 2) light[r] = (int32_t)c;
+        else list[cls == 0 ? (int64_t)r : ncell - 1 - r] = (int32_t)c;
+    }
+}
+
+// ext[cell] = the cell's index in the splat's own order (own_cell_at);
+// ext was set to -1
+__global__ void k_cell_ext(const int32_t *list, const int32_t *light, const uint32_t *cnt, int64_t ncell,
+                           int32_t *ext) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ncell) return;
+    const int64_t c = own_cell_at(i, list, light, cnt, ncell);
+    if (c >= 0) ext[c] = (int32_t)i;
+}
+
+// nbr[cell * 27 + d] = the own-order index of neighbour cell d = (dz+1)*9 +
+// (dy+1)*3 + (dx+1) of the cell (its partial in the splat), -1 if it holds
+// no points or lies outside the active bricks.
+__global__ void k_cell_nbrs(int64_t ncell, const int32_t *nbr27, const int32_t *ext, int m, int m3, int32_t *nbr) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ncell * 27) return;
+    const int64_t cell = t < (1ll << 32) ? (int64_t)((uint32_t)t / 27u) : t / 27;
+    const int d = (int)(t - cell * 27);
+    int64_t slot;
+    int cx, cy, cz;
+    cell_coords(cell, m, m3, slot, cx, cy, cz);
+    int ncx = cx + d % 3 - 1, ncy = cy + (d / 3) % 3 - 1, ncz = cz + d / 9 - 1;
+    const int bx = ncx < 0 ? -1 : (ncx >= m ? 1 : 0), by = ncy < 0 ? -1 : (ncy >= m ? 1 : 0),
+              bz = ncz < 0 ? -1 : (ncz >= m ? 1 : 0);
+    const int32_t ns = nbr27[slot * 27 + (bz + 1) * 9 + (by + 1) * 3 + (bx + 1)];
+    nbr[t] = ns >= 0 ? ext[(int64_t)ns * m3 + ((ncz - bz * m) * m + (ncy - by * m)) * m + (ncx - bx * m)] : -1;
+}
+
 // gvdbSetFlagSubcell (P:109-118)
 __global__ void k_sc_flag(const Node *leaves, int64_t n, uint32_t *flag) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -267,6 +311,39 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
         k_bin_fill<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pbin.as<int32_t>(), v->prank.as<int32_t>(), n,
                                                                v->bin_off.as<uint32_t>(), v->perm.as<int32_t>());
         GV_CUDA(v, cudaGetLastError());
+    }
+    // the cells that hold points, by class
+    GV_CUDA(v, v->cell_list.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
+    GV_CUDA(v, v->cell_light.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
+    GV_CUDA(v, v->cell_ext.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
+    GV_CUDA(v, v->cell_cnt.ensure(sizeof(uint32_t) * 4, s));
+    GV_CUDA(v, cudaMemsetAsync(v->cell_cnt.p, 0, sizeof(uint32_t) * 4, s));
+    GV_CUDA(v, cudaMemsetAsync(v->cell_ext.p, 0xFF, sizeof(int32_t) * (size_t)nbins, s));
+    v->cell_grid = v->heavy_grid = v->light_grid = 0;
+    if (nbins > 0) {
+        const int g = grid_for(nbins, 256, 1ll << 31);
+        k_cell_list<<<g, 256, 0, s>>>(v->bin_off.as<uint32_t>(), nbins, v->cell_list.as<int32_t>(),
+                                      v->cell_light.as<int32_t>(), v->cell_cnt.as<uint32_t>());
+        k_cell_ext<<<g, 256, 0, s>>>(v->cell_list.as<int32_t>(), v->cell_light.as<int32_t>(),
+                                     v->cell_cnt.as<uint32_t>(), nbins, v->cell_ext.as<int32_t>());
+        GV_CUDA(v, cudaGetLastError());
+        // each cell's 27 neighbour partials, for the merge
+        GV_CUDA(v, v->cell_nbr.ensure(sizeof(int32_t) * 27 * (size_t)nbins, s));
+        k_cell_nbrs<<<grid_for(nbins * 27, 256, 1ll << 31), 256, 0, s>>>(nbins, v->nbr27.as<int32_t>(),
+                                                                        v->cell_ext.as<int32_t>(), m, m * m * m,
+                                                                        v->cell_nbr.as<int32_t>());
+        GV_CUDA(v, cudaGetLastError());
+        v->cell_grid = v->heavy_grid = v->light_grid = nbins;
+        if (nbins > kCellCountReadback) {
+            // many cells: size the splat scratch and the grids by the cells
+            // of each class (one 12-byte read) rather than by all cells
+            uint32_t c3[3] = {0, 0, 0};
+            GV_CUDA(v, cudaMemcpyAsync(c3, v->cell_cnt.p, sizeof(c3), cudaMemcpyDeviceToHost, s));
+            GV_CUDA(v, cudaStreamSynchronize(s));
+            v->heavy_grid = (int64_t)c3[0] + c3[1];
+            v->light_grid = c3[2];
+            v->cell_grid = v->heavy_grid + v->light_grid;
+        }
     }
     k.valid = true;
     k.det = v->deterministic != 0;

@@ -185,20 +185,28 @@ struct SplatArgs {
     const int32_t *perm;
     int res0, log2r0, apron, tile;
     int m, m3; // cells per brick edge, per brick
+    // huge and heavy cells (order of cell_at), light cells, each cell's index
+    // in the splat's own order; cell_list == nullptr: every cell, in cell order
+    const int32_t *cell_list, *cell_light, *cell_ext;
+    const uint32_t *cell_cnt;
+    int64_t ncell;
+    const int32_t *cell_nbr;      // per cell, the own-order index of its 27 neighbours (-1: none)
     int64_t tvox;
 };
 
 
 // ---- two-phase scatter ---------------------------------------------------
 //
-// Phase 1 (k_scatter_own): one CTA per atlas slot splats only the points
-// binned to its brick, with unclipped stencils, into an extended tile that
-// covers every tap of those points: [-H, RES+H)^3 with H = N/2 (12^3 for the
-// cubic B-spline, 10^3 for the tent).  The tile is then written out as float
-// partial sums.
-// Phase 2 (k_scatter_merge): one thread per interior voxel adds, in a
-// fixed neighbour order, the partials of every brick whose extended tile
-// covers the voxel, and writes the channel once.
+// The kernels work on cells, 8^3 blocks of a brick (the brick itself for
+// 8^3 bricks).
+// Phase 1 (k_scatter_own): one CTA per cell that holds points splats only
+// the points binned to it, with unclipped stencils, into an extended tile
+// that covers every tap of those points: [-H, 8+H)^3 with H = N/2 (12^3 for
+// the cubic B-spline, 10^3 for the tent).  The tile is then written out as
+// float partial sums.
+// Phase 2 (k_scatter_merge): one thread per interior voxel of every cell
+// adds, in a fixed neighbour order, the partials whose extended tile covers
+// the voxel, and writes the channel once.
 //
 // Accumulation in phase 1 is exact: each contribution x (in units of 2^-s)
 // is rounded to an integer and split as rint(x) = hi * 2^L + lo, both parts
@@ -231,6 +239,24 @@ constexpr size_t own_smem_bytes() {
            sizeof(float) * (3 * Taps<KERNEL>::N + NCH) * kOwnChunk + sizeof(int32_t) * kOwnChunk;
 }
 
+// Split step 2^L of the fixed-point sums of R points.
+__device__ __forceinline__ int fixed_level(uint32_t R) {
+    const int L = 31 - (32 - __clz((int)R + 1));
+    return L > 22 ? 22 : L;
+}
+
+// Scale 2^sc applied to the contributions of R points whose largest
+// |weighted amount| is am (0 when there is nothing to add); inv = 2^-sc.
+__device__ __forceinline__ float fixed_scale(uint32_t R, int L, float am, double &inv) {
+    int e1 = 0, e2 = 0;
+    frexpf(am, &e1);             // am < 2^e1
+    frexpf((float)R * am, &e2);  // R*am < 2^e2
+    const int sc = min(21 + L - e1, 29 + L - e2);
+    const bool on = am > 0.0f && R > 0;
+    inv = on ? ldexp(1.0, -sc) : 0.0;
+    return on ? ldexpf(1.0f, sc) : 0.0f;
+}
+
 __device__ __forceinline__ void fixed_add(int32_t *hi_acc, int32_t *lo_acc, int idx, float x, float inv2L, float two2L) {
     const float M = 12582912.0f; // 1.5 * 2^23
     const float t = fmaf(x, inv2L, M);
@@ -254,7 +280,9 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
     int32_t *pb = reinterpret_cast<int32_t *>(pa + NCH);
     __shared__ double inv_s[NCH];
     __shared__ int32_t amax_bits[NCH]; // max |weighted amount| of the cell's points, as float bits
-    const int64_t cell = blockIdx.x;
+    // the blockIdx.x-th cell that holds points; its partial goes to ext[blockIdx.x]
+    const int64_t cell = own_cell_at(blockIdx.x, S.cell_list, S.cell_light, S.cell_cnt, S.ncell);
+    if (cell < 0) return;
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
@@ -324,19 +352,14 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
         if (lane == 0 && x > 0.0f) atomicMax(&amax_bits[c], __float_as_int(x));
     }
     __syncthreads();
-    int L = 31 - (32 - __clz((int)R + 1));
-    L = L > 22 ? 22 : L;
+    const int L = fixed_level(R);
     const float inv2L = ldexpf(1.0f, -L), two2L = ldexpf(1.0f, L);
     float scale[NCH];
 #pragma unroll
     for (int c = 0; c < NCH; c++) {
-        const float am = __int_as_float(amax_bits[c]);
-        int e1 = 0, e2 = 0;
-        frexpf(am, &e1);              // am < 2^e1
-        frexpf((float)R * am, &e2);  // R*am < 2^e2
-        const int sc = min(21 + L - e1, 29 + L - e2);
-        scale[c] = (am > 0.0f && R > 0) ? ldexpf(1.0f, sc) : 0.0f;
-        if (threadIdx.x == 0) inv_s[c] = scale[c] > 0.0f ? ldexp(1.0, -sc) : 0.0;
+        double inv;
+        scale[c] = fixed_scale(R, L, __int_as_float(amax_bits[c]), inv);
+        if (threadIdx.x == 0) inv_s[c] = inv;
     }
     { // scale the staged first chunk
         const int cnt0 = (int)min((uint32_t)kOwnChunk, R);
@@ -388,7 +411,7 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
     // advances by the base-E digits of 256 instead of being divided out
     constexpr int E = X::E, DZ = kOwnThreads / (E * E), DY = (kOwnThreads / E) % E, DX = kOwnThreads % E;
     static_assert(DZ < E, "one wrap per step");
-    float *dst = ext + cell * (int64_t)NCH * X::E3;
+    float *dst = ext + (int64_t)blockIdx.x * NCH * X::E3;
     int c = 0, z = threadIdx.x / (E * E), y = (threadIdx.x / E) % E, x = threadIdx.x % E;
     for (int i = threadIdx.x; i < NCH * X::E3; i += kOwnThreads) {
         const int k = c * X::CS + z * X::PS + y * X::RS + x;
@@ -404,25 +427,22 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
     }
 }
 
-// Phase 2: interior voxel v of the slot sums, in a fixed order, the partial
-// of every brick whose extended tile covers v.
+// Phase 2 (k_scatter_merge): one thread per interior voxel of every cell,
+// with no shared memory or barrier, so that the SM keeps as many voxels in
+// flight as its registers allow.  Voxel v sums, in a fixed order, the
+// partials of the cells whose extended tile covers it: its own cell and,
+// within H of a face, the neighbours across it (per axis d = 0 and e = -1
+// or +1, never both, H <= 4), looked up in the cell's 27-entry neighbour
+// table.  The up to 8 partials are read first (predicated), then summed.
 template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S, const float *ext) {
+__global__ void __launch_bounds__(256) k_scatter_merge(SplatArgs S, const float *ext) {
     using X = ExtTile<KERNEL>;
-    __shared__ int32_t nb[27];
-    const int64_t cell = blockIdx.x;
-    int64_t slot;
-    int cx, cy, cz;
-    cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
-    if (threadIdx.x < 27) nb[threadIdx.x] = S.nbr27[slot * 27 + threadIdx.x];
-    __syncthreads();
-    const int vx = threadIdx.x & 7, vy = (threadIdx.x >> 3) & 7, vz = threadIdx.x >> 6;
-    float acc[NCH];
-#pragma unroll
-    for (int c = 0; c < NCH; c++) acc[c] = 0.0f;
-    // Per axis the covering bricks are d = 0 and, within H of a face, the
-    // neighbour across it (e = -1 or +1; never both, H <= 4).  The up to 8
-    // combinations are read first (predicated), then summed in a fixed order.
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t cell = i >> 9;
+    if (cell >= S.ncell) return;
+    const int v = (int)(i & 511);
+    const int vx = v & 7, vy = (v >> 3) & 7, vz = v >> 6;
+    const int32_t *ne = S.cell_nbr + cell * 27;
     const int ex = vx < X::H ? -1 : (vx >= 8 - X::H ? 1 : 0);
     const int ey = vy < X::H ? -1 : (vy >= 8 - X::H ? 1 : 0);
     const int ez = vz < X::H ? -1 : (vz >= 8 - X::H ? 1 : 0);
@@ -431,24 +451,22 @@ __global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S, const float 
     for (int m = 0; m < 8; m++) {
         const int dx = (m & 1) ? ex : 0, dy = (m & 2) ? ey : 0, dz = (m & 4) ? ez : 0;
         const bool used = (!(m & 1) || ex) && (!(m & 2) || ey) && (!(m & 4) || ez);
-        // the covering cell: one step d from this cell, possibly in a neighbouring brick
-        int ncx = cx + dx, ncy = cy + dy, ncz = cz + dz;
-        const int bx = ncx < 0 ? -1 : (ncx >= S.m ? 1 : 0), by = ncy < 0 ? -1 : (ncy >= S.m ? 1 : 0),
-                  bz = ncz < 0 ? -1 : (ncz >= S.m ? 1 : 0);
-        ncx -= bx * S.m;
-        ncy -= by * S.m;
-        ncz -= bz * S.m;
-        const int ns = used ? nb[(bz + 1) * 9 + (by + 1) * 3 + (bx + 1)] : -1;
-        const int64_t n = ns >= 0 ? (int64_t)ns * S.m3 + (ncz * S.m + ncy) * S.m + ncx : -1;
+        const int32_t e = used ? __ldg(ne + (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)) : -1;
         const int ux = vx - 8 * dx + X::H, uy = vy - 8 * dy + X::H, uz = vz - 8 * dz + X::H;
-        const float *src = ext + (n >= 0 ? n : 0) * (int64_t)NCH * X::E3 + (uz * X::E + uy) * X::E + ux;
+        const float *src = ext + (int64_t)(e >= 0 ? e : 0) * NCH * X::E3 + (uz * X::E + uy) * X::E + ux;
 #pragma unroll
-        for (int c = 0; c < NCH; c++) part[m][c] = n >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
+        for (int c = 0; c < NCH; c++) part[m][c] = e >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
     }
+    float acc[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) acc[c] = 0.0f;
 #pragma unroll
     for (int m = 0; m < 8; m++)
 #pragma unroll
         for (int c = 0; c < NCH; c++) acc[c] += part[m][c];
+    int64_t slot;
+    int cx, cy, cz;
+    cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
     const int a = S.apron, tl = S.tile;
     const int Lx = kCell * cx + vx, Ly = kCell * cy + vy, Lz = kCell * cz + vz; // voxel in the brick
     const int64_t at = slot * S.tvox + ((int64_t)(Lz + a) * tl + (Ly + a)) * tl + (Lx + a);
@@ -484,20 +502,123 @@ struct GatherArgs {
     const int32_t *perm;
     int res0, apron, tile;
     int m, m3; // cells per brick edge, per brick
+    // huge and heavy cells (order of cell_at), light cells, each cell's index
+    // in the splat's own order; cell_list == nullptr: every cell, in cell order
+    const int32_t *cell_list, *cell_light, *cell_ext;
+    const uint32_t *cell_cnt;
+    int64_t ncell;
+    const int32_t *cell_nbr; // (not used by the gathers)
     int64_t tvox;
 };
 
+// One point of a gather, in any mode.  fetch(x, y, z, g) gives g[c], the
+// value of channel c at tap (x, y, z) of the cell's extended frame, whose
+// origin (ox, oy, oz) is the cell's first voxel minus H.
+template <int KERNEL, int MODE, int NCH, class Fetch>
+__device__ __forceinline__ void gather_point(const GatherArgs &G, int32_t pidx, int ox, int oy, int oz,
+                                             const Fetch &fetch) {
+    using T = Taps<KERNEL>;
+    constexpr int N = T::N;
+    const float3 p = load_f3(G.pos, pidx);
+    const int3 o = point_origin(G.pos, pidx);
+    float wx[N], wy[N], wz[N], dx[N], dy[N], dz[N];
+    int fx, fy, fz;
+    if (MODE == kFwd) {
+        fx = T::eval(p.x + G.trans.x, wx) + o.x - ox;
+        fy = T::eval(p.y + G.trans.y, wy) + o.y - oy;
+        fz = T::eval(p.z + G.trans.z, wz) + o.z - oz;
+    } else {
+        fx = T::eval_d(p.x + G.trans.x, wx, dx) + o.x - ox;
+        fy = T::eval_d(p.y + G.trans.y, wy, dy) + o.y - oy;
+        fz = T::eval_d(p.z + G.trans.z, wz, dz) + o.z - oz;
+    }
+    // a binned point's first taps lie in [0, 8]; a point moved since the
+    // binning (positions changed in place) gathers 0 and reads nothing outside
+    if (!((unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u)) {
+        fx = fy = fz = 0;
+#pragma unroll
+        for (int k = 0; k < N; k++) wx[k] = wy[k] = wz[k] = dx[k] = dy[k] = dz[k] = 0.0f;
+    }
+    float sum[NCH], gx[NCH], gy[NCH], gz[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) sum[c] = gx[c] = gy[c] = gz[c] = 0.0f;
+#pragma unroll
+    for (int tz = 0; tz < N; tz++) {
+#pragma unroll
+        for (int ty = 0; ty < N; ty++) {
+            const float wyz = wy[ty] * wz[tz];
+            float dyz = 0.0f, ydz = 0.0f;
+            if (MODE != kFwd) {
+                dyz = dy[ty] * wz[tz];
+                ydz = wy[ty] * dz[tz];
+            }
+#pragma unroll
+            for (int tx = 0; tx < N; tx++) {
+                float gv[NCH];
+                fetch(fx + tx, fy + ty, fz + tz, gv);
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    const float g = gv[c];
+                    if (MODE != kGatherBwd) sum[c] = fmaf(g, wx[tx] * wyz, sum[c]);
+                    if (MODE != kFwd) {
+                        gx[c] = fmaf(g, dx[tx] * wyz, gx[c]);
+                        gy[c] = fmaf(g, wx[tx] * dyz, gy[c]);
+                        gz[c] = fmaf(g, wx[tx] * ydz, gz[c]);
+                    }
+                }
+            }
+        }
+    }
+    if (MODE == kFwd) {
+#pragma unroll
+        for (int c = 0; c < NCH; c++) G.out[(int64_t)pidx * G.out_stride + c] = sum[c];
+    } else if (MODE == kScatterBwd) {
+        const float wt = G.has_weight ? load_f1(G.weight, pidx) : G.wconst;
+        float gw = 0.0f, gp0 = 0.0f, gp1 = 0.0f, gp2 = 0.0f;
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            const bool has = (G.attr_mask >> c) & 1;
+            const float at = has ? load_f1(G.attr[c], pidx) : 1.0f;
+            if (G.grad_attr) G.grad_attr[(int64_t)pidx * NCH + c] = has ? wt * sum[c] : 0.0f;
+            gw += at * sum[c];
+            gp0 += wt * at * gx[c];
+            gp1 += wt * at * gy[c];
+            gp2 += wt * at * gz[c];
+        }
+        if (G.grad_weight) G.grad_weight[pidx] = gw;
+        if (G.grad_pos) {
+            G.grad_pos[3 * (int64_t)pidx + 0] = gp0;
+            G.grad_pos[3 * (int64_t)pidx + 1] = gp1;
+            G.grad_pos[3 * (int64_t)pidx + 2] = gp2;
+        }
+    } else {
+        float gp0 = 0.0f, gp1 = 0.0f, gp2 = 0.0f;
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            const float go = G.grad_out[(int64_t)pidx * NCH + c];
+            gp0 += go * gx[c];
+            gp1 += go * gy[c];
+            gp2 += go * gz[c];
+        }
+        G.grad_pos[3 * (int64_t)pidx + 0] = gp0;
+        G.grad_pos[3 * (int64_t)pidx + 1] = gp1;
+        G.grad_pos[3 * (int64_t)pidx + 2] = gp2;
+    }
+}
+
 template <int KERNEL, int MODE, int NCH>
 __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
-    using T = Taps<KERNEL>;
-    constexpr int H = T::N / 2;
-    constexpr int N = T::N;
+    constexpr int H = Taps<KERNEL>::N / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *tile = reinterpret_cast<float *>(smem_raw);
     __shared__ int32_t nbs[27];
     // one CTA per 8^3 cell of a brick: the cell plus its halo is staged
-    const int res = G.res0, ht = kCell + 2 * H, ht3 = ht * ht * ht;
-    const int64_t cell = blockIdx.x;
+    constexpr int ht = kCell + 2 * H, ht3 = ht * ht * ht;
+    const int res = G.res0;
+    const int64_t cell = G.cell_list ? cell_at(blockIdx.x, G.cell_list, G.cell_cnt, G.ncell) : (int64_t)blockIdx.x;
+    if (cell < 0) return;
+    const uint32_t beg = G.bin_off[cell], end = G.bin_off[cell + 1];
+    if (beg == end) return; // no points: nothing to stage
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, G.m, G.m3, slot, cx, cy, cz);
@@ -520,87 +641,46 @@ __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
     __syncthreads();
     const Node &nd = G.leaves[G.slot_leaf[slot]];
     const int ox = nd.mPos[0] + kCell * cx - H, oy = nd.mPos[1] + kCell * cy - H, oz = nd.mPos[2] + kCell * cz - H;
-    const uint32_t beg = G.bin_off[cell], end = G.bin_off[cell + 1];
-    for (uint32_t j = beg + threadIdx.x; j < end; j += blockDim.x) {
-        const int32_t pidx = G.perm[j];
-        const float3 p = load_f3(G.pos, pidx);
-        const int3 o = point_origin(G.pos, pidx);
-        float wx[N], wy[N], wz[N], dx[N], dy[N], dz[N];
-        int fx, fy, fz;
-        if (MODE == kFwd) {
-            fx = T::eval(p.x + G.trans.x, wx) + o.x - ox;
-            fy = T::eval(p.y + G.trans.y, wy) + o.y - oy;
-            fz = T::eval(p.z + G.trans.z, wz) + o.z - oz;
-        } else {
-            fx = T::eval_d(p.x + G.trans.x, wx, dx) + o.x - ox;
-            fy = T::eval_d(p.y + G.trans.y, wy, dy) + o.y - oy;
-            fz = T::eval_d(p.z + G.trans.z, wz, dz) + o.z - oz;
-        }
-        float sum[NCH], gx[NCH], gy[NCH], gz[NCH];
+    auto fetch = [&](int x, int y, int z, float g[NCH]) {
+        const int k = (z * ht + y) * ht + x;
 #pragma unroll
-        for (int c = 0; c < NCH; c++) sum[c] = gx[c] = gy[c] = gz[c] = 0.0f;
+        for (int c = 0; c < NCH; c++) g[c] = tile[c * ht3 + k];
+    };
+    for (uint32_t j = beg + threadIdx.x; j < end; j += blockDim.x)
+        gather_point<KERNEL, MODE, NCH>(G, G.perm[j], ox, oy, oz, fetch);
+}
+
+// The points of light cells: one warp per cell, one lane per point (a light
+// cell holds at most kLightCell = 32), taps read straight from the atlas; a
+// staged halo would cost 12^3 floats per channel for a few points.
+template <int KERNEL, int MODE, int NCH>
+__global__ void __launch_bounds__(256) k_gather_light(GatherArgs G) {
+    constexpr int H = Taps<KERNEL>::N / 2;
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= (int64_t)G.cell_cnt[2]) return;
+    const int64_t cell = G.cell_light[w];
+    const uint32_t beg = G.bin_off[cell], cnt = G.bin_off[cell + 1] - beg;
+    if ((uint32_t)lane >= cnt) return;
+    int64_t slot;
+    int cx, cy, cz;
+    cell_coords(cell, G.m, G.m3, slot, cx, cy, cz);
+    const Node &nd = G.leaves[G.slot_leaf[slot]];
+    const int fx0 = kCell * cx - H, fy0 = kCell * cy - H, fz0 = kCell * cz - H; // frame origin in the brick
+    const int res = G.res0, a = G.apron, tl = G.tile;
+    auto fetch = [&](int x, int y, int z, float g[NCH]) {
+        const int lx = fx0 + x, ly = fy0 + y, lz = fz0 + z; // brick-local, may step into a neighbour
+        const int sx = lx < 0 ? -1 : (lx >= res ? 1 : 0), sy = ly < 0 ? -1 : (ly >= res ? 1 : 0),
+                  sz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
+        const int d = (sz + 1) * 9 + (sy + 1) * 3 + (sx + 1);
+        const int64_t ns = d == 13 ? slot : (int64_t)G.nbr27[slot * 27 + d];
+        const int64_t off = ns * G.tvox + ((int64_t)(lz - sz * res + a) * tl + (ly - sy * res + a)) * tl +
+                            (lx - sx * res + a);
 #pragma unroll
-        for (int tz = 0; tz < N; tz++) {
-#pragma unroll
-            for (int ty = 0; ty < N; ty++) {
-                const int row = ((fz + tz) * ht + (fy + ty)) * ht + fx;
-                const float wyz = wy[ty] * wz[tz];
-                float dyz = 0.0f, ydz = 0.0f;
-                if (MODE != kFwd) {
-                    dyz = dy[ty] * wz[tz];
-                    ydz = wy[ty] * dz[tz];
-                }
-#pragma unroll
-                for (int tx = 0; tx < N; tx++) {
-#pragma unroll
-                    for (int c = 0; c < NCH; c++) {
-                        const float g = tile[c * ht3 + row + tx];
-                        if (MODE != kGatherBwd) sum[c] = fmaf(g, wx[tx] * wyz, sum[c]);
-                        if (MODE != kFwd) {
-                            gx[c] = fmaf(g, dx[tx] * wyz, gx[c]);
-                            gy[c] = fmaf(g, wx[tx] * dyz, gy[c]);
-                            gz[c] = fmaf(g, wx[tx] * ydz, gz[c]);
-                        }
-                    }
-                }
-            }
-        }
-        if (MODE == kFwd) {
-#pragma unroll
-            for (int c = 0; c < NCH; c++) G.out[(int64_t)pidx * G.out_stride + c] = sum[c];
-        } else if (MODE == kScatterBwd) {
-            const float wt = G.has_weight ? load_f1(G.weight, pidx) : G.wconst;
-            float gw = 0.0f, gp0 = 0.0f, gp1 = 0.0f, gp2 = 0.0f;
-#pragma unroll
-            for (int c = 0; c < NCH; c++) {
-                const bool has = (G.attr_mask >> c) & 1;
-                const float at = has ? load_f1(G.attr[c], pidx) : 1.0f;
-                if (G.grad_attr) G.grad_attr[(int64_t)pidx * NCH + c] = has ? wt * sum[c] : 0.0f;
-                gw += at * sum[c];
-                gp0 += wt * at * gx[c];
-                gp1 += wt * at * gy[c];
-                gp2 += wt * at * gz[c];
-            }
-            if (G.grad_weight) G.grad_weight[pidx] = gw;
-            if (G.grad_pos) {
-                G.grad_pos[3 * (int64_t)pidx + 0] = gp0;
-                G.grad_pos[3 * (int64_t)pidx + 1] = gp1;
-                G.grad_pos[3 * (int64_t)pidx + 2] = gp2;
-            }
-        } else {
-            float gp0 = 0.0f, gp1 = 0.0f, gp2 = 0.0f;
-#pragma unroll
-            for (int c = 0; c < NCH; c++) {
-                const float go = G.grad_out[(int64_t)pidx * NCH + c];
-                gp0 += go * gx[c];
-                gp1 += go * gy[c];
-                gp2 += go * gz[c];
-            }
-            G.grad_pos[3 * (int64_t)pidx + 0] = gp0;
-            G.grad_pos[3 * (int64_t)pidx + 1] = gp1;
-            G.grad_pos[3 * (int64_t)pidx + 2] = gp2;
-        }
-    }
+        for (int c = 0; c < NCH; c++) g[c] = ns >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
+    };
+    gather_point<KERNEL, MODE, NCH>(G, G.perm[beg + lane], nd.mPos[0] + fx0, nd.mPos[1] + fy0, nd.mPos[2] + fz0,
+                                    fetch);
 }
 
 // Points outside every active brick: gathers and gradients are zero.
@@ -638,6 +718,12 @@ void fill_topology(Volume *v, Args &S) {
     S.res0 = v->res(0);
     S.m = v->res(0) / kCell;
     S.m3 = S.m * S.m * S.m;
+    S.cell_list = v->cell_list.as<int32_t>();
+    S.cell_nbr = v->cell_nbr.as<int32_t>();
+    S.cell_light = v->cell_light.as<int32_t>();
+    S.cell_ext = v->cell_ext.as<int32_t>();
+    S.cell_cnt = v->cell_cnt.as<uint32_t>();
+    S.ncell = v->atlas_last * S.m3;
     S.apron = v->apron;
     S.tile = v->tile_res();
     S.tvox = v->tile_vox();
@@ -659,14 +745,15 @@ template <int KERNEL, int NCH>
 gvdb2_status scatter_group(Volume *v, const SplatArgs &S) {
     using X = ExtTile<KERNEL>;
     cudaStream_t s = v->stream;
-    const int64_t ncells = v->atlas_last * S.m3;
-    GV_CUDA(v, v->scratch.ensure(sizeof(float) * (size_t)ncells * NCH * X::E3 + 256, s));
+    // one partial per cell that holds points (at most cell_grid of them)
+    const int64_t nown = v->cell_grid;
+    GV_CUDA(v, v->scratch.ensure(sizeof(float) * (size_t)nown * NCH * X::E3 + 256, s));
     float *ext = v->scratch.as<float>();
     constexpr size_t smem = own_smem_bytes<KERNEL, NCH>();
     auto k1 = k_scatter_own<KERNEL, NCH>;
     GV_TRY(launch_smem(v, k1, smem, "scatter"));
-    k1<<<(unsigned)ncells, kOwnThreads, smem, s>>>(S, ext);
-    k_scatter_merge<KERNEL, NCH><<<(unsigned)ncells, 512, 0, s>>>(S, ext);
+    if (nown > 0) k1<<<(unsigned)nown, kOwnThreads, smem, s>>>(S, ext);
+    k_scatter_merge<KERNEL, NCH><<<(unsigned)(S.ncell * 2), 256, 0, s>>>(S, ext);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
@@ -714,7 +801,10 @@ gvdb2_status launch_gather(Volume *v, const GatherArgs &G) {
     const size_t smem = sizeof(float) * (size_t)NCH * ht * ht * ht;
     auto k = k_gather_tile<KERNEL, MODE, NCH>;
     GV_TRY(launch_smem(v, k, smem, "gather"));
-    k<<<(unsigned)(v->atlas_last * G.m3), 256, smem, v->stream>>>(G);
+    const int64_t grid = G.cell_list ? v->heavy_grid : G.ncell;
+    if (grid > 0) k<<<(unsigned)grid, 256, smem, v->stream>>>(G);
+    if (G.cell_list && v->light_grid > 0) // light cells: a warp each
+        k_gather_light<KERNEL, MODE, NCH><<<(unsigned)((v->light_grid + 7) / 8), 256, 0, v->stream>>>(G);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
@@ -877,6 +967,7 @@ gvdb2_status gather_kernel_prebinned(Volume *v, int kernel, int n, const float t
     fill_topology(v, G);
     G.bin_off = bin_off;
     G.perm = perm;
+    G.cell_list = nullptr; // bins supplied by the caller: every cell, in cell order
     return run_gather<kFwd>(v, kernel, G);
 }
 

@@ -227,7 +227,7 @@ class VolumeGVDB:
         """GatherKernel for callers that cannot allocate device memory once
         running: no device allocation at all (binning scratch is a fixed
         12.25 MB array per GPU; at most 1,048,576 points and 32,768 active
-        bricks per call).  `out` is a caller-owned (N, nch) float32 CUDA
+        8^3 cells per call: bricks of 8^3 voxels, or an eighth as many of 16^3).  `out` is a caller-owned (N, nch) float32 CUDA
         tensor.  Calls whose GPU work overlaps share the scratch and race."""
         self._check(self._L.gvdb2_gather_kernel_noalloc(self._h, kernel, int(num_pnts), _f3(trans), self._chans(chans),
                                                         len(chans), ctypes.c_void_p(out.data_ptr()), out.stride(0)),

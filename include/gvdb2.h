@@ -77,6 +77,8 @@ typedef struct gvdb2_info {
     float posmax[3];
     int32_t root_pos[3];
     int32_t tile_res;         /* res0 + 2*apron */
+    int64_t splat_cells;      /* 8^3 brick cells holding points at the last kernel-splat
+                                 binning, -1 before one (no counterpart in the reference) */
 } gvdb2_info;
 
 /* ---- lifetime (SetCudaDevice VH:325 / V:240-334, Initialize VH:326 / V:2320-2361) ---- */

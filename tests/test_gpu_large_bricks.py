@@ -41,6 +41,8 @@ def test_scatter_gather_large_bricks(gvdb2_mod, oracle_mod, cfg, kernel):
     tw, ta = torch.from_numpy(w).cuda(), torch.from_numpy(at).cuda()
     v.ScatterKernel(kernel, n, [0, 1], weight=tw, attrs=[None, ta])
     o.scatter_kernel(kernel, p, [0, 1], weight=w, attrs=[None, at])
+    # the splat takes only the 8^3 cells that hold points
+    assert int(v.info().splat_cells) == len(np.unique(np.floor(p).astype(np.int64) >> 3, axis=0))
     for c in (0, 1):
         g, r = interior(v.atlas(c), 1), interior(o.atlas(c), 1)
         assert g.shape[1] == res
