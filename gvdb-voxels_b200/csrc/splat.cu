@@ -199,8 +199,9 @@ struct SplatArgs {
 //
 // The kernels work on cells, 8^3 blocks of a brick (the brick itself for
 // 8^3 bricks).
-// Phase 1 (k_scatter_own): one CTA per cell that holds points splats only
-// the points binned to it, with unclipped stencils, into an extended tile
+// Phase 1 (k_scatter_own): one CTA per cell of more than kLightCell points
+// (k_scatter_own_light: one warp per lighter cell) splats only the points
+// binned to it, with unclipped stencils, into an extended tile
 // that covers every tap of those points: [-H, 8+H)^3 with H = N/2 (12^3 for
 // the cubic B-spline, 10^3 for the tent).  The tile is then written out as
 // float partial sums.
@@ -281,7 +282,8 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
     __shared__ double inv_s[NCH];
     __shared__ int32_t amax_bits[NCH]; // max |weighted amount| of the cell's points, as float bits
     // the blockIdx.x-th cell that holds points; its partial goes to ext[blockIdx.x]
-    const int64_t cell = own_cell_at(blockIdx.x, S.cell_list, S.cell_light, S.cell_cnt, S.ncell);
+    // the blockIdx.x-th huge or heavy cell (light cells: k_scatter_own_light)
+    const int64_t cell = cell_at(blockIdx.x, S.cell_list, S.cell_cnt, S.ncell);
     if (cell < 0) return;
     int64_t slot;
     int cx, cy, cz;
@@ -424,6 +426,106 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
         if (y >= E) { y -= E; z++; }
         z += DZ;
         if (z >= E) { z -= E; c++; }
+    }
+}
+
+// Phase 1 for light cells (at most kLightCell = 32 points): one warp per
+// cell, so that a CTA-sized tile and its barriers are not spent on a few
+// points.  The warp sorts its points by index, stages their taps in shared
+// memory (one lane per point), then per channel accumulates them into a
+// warp-private float tile in that order -- each point's taps are distinct
+// voxels, handled by distinct lanes, so plain adds suffice and every voxel
+// sums its contributions in index order: the partial is bit-reproducible --
+// and writes the tile out in the partial layout of phase 1.  A partial of
+// at most 32 points is accurate to float rounding.
+constexpr int kLightWarps = 8;
+
+template <int KERNEL, int NCH>
+constexpr size_t own_light_smem_bytes() {
+    return sizeof(float) * kLightWarps * (ExtTile<KERNEL>::E3 + 32 * (1 + 3 * Taps<KERNEL>::N + NCH));
+}
+
+template <int KERNEL, int NCH>
+__global__ void __launch_bounds__(32 * kLightWarps) k_scatter_own_light(SplatArgs S, float *ext) {
+    using T = Taps<KERNEL>;
+    using X = ExtTile<KERNEL>;
+    constexpr int N = T::N, E = X::E, E3 = X::E3;
+    extern __shared__ __align__(16) unsigned char light_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float *tile = reinterpret_cast<float *>(light_smem) + warp * E3;
+    float *stage = reinterpret_cast<float *>(light_smem) + kLightWarps * E3 + warp * 32 * (1 + 3 * N + NCH);
+    int32_t *pbase = reinterpret_cast<int32_t *>(stage); // packed first tap (x | y << 8 | z << 16)
+    float *pw = stage + 32;                              // pw[k * 32 + j]: weight k (x taps, y taps, z taps)
+    float *pa = pw + 3 * N * 32;                         // pa[c * 32 + j]: amount of channel c
+    const int64_t w = (int64_t)blockIdx.x * kLightWarps + warp;
+    if (w >= (int64_t)S.cell_cnt[2]) return;
+    const int64_t cell = S.cell_light[w];
+    const uint32_t beg = S.bin_off[cell], cnt = min(S.bin_off[cell + 1] - beg, 32u); // light: <= 32
+    // the cell's points in ascending index order (bitonic sort over the warp)
+    int32_t key = (uint32_t)lane < cnt ? S.perm[beg + lane] : INT32_MAX;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int32_t other = __shfl_xor_sync(0xffffffffu, key, j);
+            const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+            key = keep_min ? min(key, other) : max(key, other);
+        }
+    int64_t slot;
+    int cx, cy, cz;
+    cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
+    const Node &nd = S.leaves[S.slot_leaf[slot]];
+    const int ox = nd.mPos[0] + kCell * cx - X::H, oy = nd.mPos[1] + kCell * cy - X::H,
+              oz = nd.mPos[2] + kCell * cz - X::H;
+    if ((uint32_t)lane < cnt) {
+        const int32_t p = key;
+        const float3 q = load_f3(S.pos, p);
+        const int3 o = point_origin(S.pos, p);
+        float wx[N], wy[N], wz[N];
+        const int fx = T::eval(q.x + S.trans.x, wx) + o.x - ox;
+        const int fy = T::eval(q.y + S.trans.y, wy) + o.y - oy;
+        const int fz = T::eval(q.z + S.trans.z, wz) + o.z - oz;
+        // a binned point's first taps lie in [0, 8]; anything else is dropped
+        const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
+        pbase[lane] = ok ? (fx | (fy << 8) | (fz << 16)) : 0;
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            pw[k * 32 + lane] = wx[k];
+            pw[(N + k) * 32 + lane] = wy[k];
+            pw[(2 * N + k) * 32 + lane] = wz[k];
+        }
+        const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
+#pragma unroll
+        for (int c = 0; c < NCH; c++)
+            pa[c * 32 + lane] = ok ? (((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt) : 0.0f;
+    }
+    __syncwarp();
+    // own-order index of this light cell: after the huge and heavy cells
+    float *dst = ext + ((int64_t)S.cell_cnt[0] + S.cell_cnt[1] + w) * NCH * E3;
+    // taps of a point per lane: cubic, lane = (tx, ty, z pair) with two taps;
+    // tent, lanes 0-7 = (tx, ty, tz)
+    const int tx = N == 4 ? (lane & 3) : (lane & 1), ty = N == 4 ? ((lane >> 2) & 3) : ((lane >> 1) & 1);
+    const int tz0 = N == 4 ? (lane >> 4) * 2 : ((lane >> 2) & 1);
+    const bool tap_lane = N == 4 || lane < 8;
+#pragma unroll 1
+    for (int c = 0; c < NCH; c++) {
+        float4 *t4 = reinterpret_cast<float4 *>(tile);
+        for (int i = lane; i < E3 / 4; i += 32) t4[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        __syncwarp();
+        for (uint32_t j = 0; j < cnt; j++) {
+            if (tap_lane) {
+                const int b = pbase[j];
+                const int a0 = (((b >> 16) + tz0) * E + ((b >> 8) & 255) + ty) * E + (b & 255) + tx;
+                const float am = pa[c * 32 + j];
+                const float wxy = pw[tx * 32 + j], wyv = pw[(N + ty) * 32 + j];
+                tile[a0] += am * (wxy * (wyv * pw[(2 * N + tz0) * 32 + j]));
+                if (N == 4) tile[a0 + E * E] += am * (wxy * (wyv * pw[(2 * N + tz0 + 1) * 32 + j]));
+            }
+            __syncwarp();
+        }
+        float4 *d4 = reinterpret_cast<float4 *>(dst + c * E3);
+        for (int i = lane; i < E3 / 4; i += 32) d4[i] = t4[i];
+        __syncwarp();
     }
 }
 
@@ -752,7 +854,12 @@ gvdb2_status scatter_group(Volume *v, const SplatArgs &S) {
     constexpr size_t smem = own_smem_bytes<KERNEL, NCH>();
     auto k1 = k_scatter_own<KERNEL, NCH>;
     GV_TRY(launch_smem(v, k1, smem, "scatter"));
-    if (nown > 0) k1<<<(unsigned)nown, kOwnThreads, smem, s>>>(S, ext);
+    if (v->heavy_grid > 0) k1<<<(unsigned)v->heavy_grid, kOwnThreads, smem, s>>>(S, ext);
+    constexpr size_t smem_l = own_light_smem_bytes<KERNEL, NCH>();
+    auto k1l = k_scatter_own_light<KERNEL, NCH>;
+    GV_TRY(launch_smem(v, k1l, smem_l, "scatter"));
+    if (v->light_grid > 0)
+        k1l<<<(unsigned)((v->light_grid + kLightWarps - 1) / kLightWarps), 32 * kLightWarps, smem_l, s>>>(S, ext);
     k_scatter_merge<KERNEL, NCH><<<(unsigned)(S.ncell * 2), 256, 0, s>>>(S, ext);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
