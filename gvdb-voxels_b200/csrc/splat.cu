@@ -536,8 +536,11 @@ __global__ void __launch_bounds__(32 * kLightWarps) k_scatter_own_light(SplatArg
 // within H of a face, the neighbours across it (per axis d = 0 and e = -1
 // or +1, never both, H <= 4), looked up in the cell's 27-entry neighbour
 // table.  The up to 8 partials are read first (predicated), then summed.
-template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(256) k_scatter_merge(SplatArgs S, const float *ext) {
+// A launch merges channels [c0, c0 + CC) of the NCH-channel partials (all
+// of them: two launches of two channels each measured slower on the sparse
+// scene and no faster on the dense one).
+template <int KERNEL, int NCH, int CC>
+__global__ void __launch_bounds__(256) k_scatter_merge(SplatArgs S, const float *ext, int c0) {
     using X = ExtTile<KERNEL>;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t cell = i >> 9;
@@ -548,24 +551,24 @@ __global__ void __launch_bounds__(256) k_scatter_merge(SplatArgs S, const float 
     const int ex = vx < X::H ? -1 : (vx >= 8 - X::H ? 1 : 0);
     const int ey = vy < X::H ? -1 : (vy >= 8 - X::H ? 1 : 0);
     const int ez = vz < X::H ? -1 : (vz >= 8 - X::H ? 1 : 0);
-    float part[8][NCH];
+    float part[8][CC];
 #pragma unroll
     for (int m = 0; m < 8; m++) {
         const int dx = (m & 1) ? ex : 0, dy = (m & 2) ? ey : 0, dz = (m & 4) ? ez : 0;
         const bool used = (!(m & 1) || ex) && (!(m & 2) || ey) && (!(m & 4) || ez);
         const int32_t e = used ? __ldg(ne + (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)) : -1;
         const int ux = vx - 8 * dx + X::H, uy = vy - 8 * dy + X::H, uz = vz - 8 * dz + X::H;
-        const float *src = ext + (int64_t)(e >= 0 ? e : 0) * NCH * X::E3 + (uz * X::E + uy) * X::E + ux;
+        const float *src = ext + ((int64_t)(e >= 0 ? e : 0) * NCH + c0) * X::E3 + (uz * X::E + uy) * X::E + ux;
 #pragma unroll
-        for (int c = 0; c < NCH; c++) part[m][c] = e >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
+        for (int c = 0; c < CC; c++) part[m][c] = e >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
     }
-    float acc[NCH];
+    float acc[CC];
 #pragma unroll
-    for (int c = 0; c < NCH; c++) acc[c] = 0.0f;
+    for (int c = 0; c < CC; c++) acc[c] = 0.0f;
 #pragma unroll
     for (int m = 0; m < 8; m++)
 #pragma unroll
-        for (int c = 0; c < NCH; c++) acc[c] += part[m][c];
+        for (int c = 0; c < CC; c++) acc[c] += part[m][c];
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
@@ -573,8 +576,8 @@ __global__ void __launch_bounds__(256) k_scatter_merge(SplatArgs S, const float 
     const int Lx = kCell * cx + vx, Ly = kCell * cy + vy, Lz = kCell * cz + vz; // voxel in the brick
     const int64_t at = slot * S.tvox + ((int64_t)(Lz + a) * tl + (Ly + a)) * tl + (Lx + a);
 #pragma unroll
-    for (int c = 0; c < NCH; c++)
-        if (c < S.nch) S.chan[c][at] = acc[c];
+    for (int c = 0; c < CC; c++)
+        if (c0 + c < S.nch) S.chan[c0 + c][at] = acc[c];
 }
 
 
@@ -860,7 +863,7 @@ gvdb2_status scatter_group(Volume *v, const SplatArgs &S) {
     GV_TRY(launch_smem(v, k1l, smem_l, "scatter"));
     if (v->light_grid > 0)
         k1l<<<(unsigned)((v->light_grid + kLightWarps - 1) / kLightWarps), 32 * kLightWarps, smem_l, s>>>(S, ext);
-    k_scatter_merge<KERNEL, NCH><<<(unsigned)(S.ncell * 2), 256, 0, s>>>(S, ext);
+    k_scatter_merge<KERNEL, NCH, NCH><<<(unsigned)(S.ncell * 2), 256, 0, s>>>(S, ext, 0);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
