@@ -270,6 +270,18 @@ gvdb2_status gvdb2_insert_points_subcell(gvdb2_volume *h, int subcell, int n, fl
     return gvdb2::insert_points_subcell(VOL(h), subcell, n, radius, trans ? trans : zero, len);
 }
 
+gvdb2_status gvdb2_insert_points_subcell_fp16(gvdb2_volume *h, int subcell, int n, float radius, const float trans[3],
+                                              int *len) {
+    CHECK_HANDLE(h);
+    const float zero[3] = {0, 0, 0};
+    return gvdb2::insert_points_subcell(VOL(h), subcell, n, radius, trans ? trans : zero, len, true);
+}
+
+gvdb2_status gvdb2_get_min_max_vel(gvdb2_volume *h, int n) {
+    CHECK_HANDLE(h);
+    return gvdb2::get_min_max_vel(VOL(h), n);
+}
+
 gvdb2_status gvdb2_scatter_density(gvdb2_volume *h, int n, float radius, float amp, const float trans[3], int expand,
                                    int avg_color) {
     CHECK_HANDLE(h);
@@ -279,13 +291,22 @@ gvdb2_status gvdb2_scatter_density(gvdb2_volume *h, int n, float radius, float a
 }
 
 static gvdb2_status gather_common(gvdb2_volume *h, int subcell, float radius, int *len, int chan, int chan_clr,
-                                  int accum, bool levelset) {
+                                  int accum, bool levelset, bool fp16 = false) {
     CHECK_HANDLE(h);
     Volume *v = VOL(h);
     if (chan_clr >= 0 && chan_clr < gvdb2::kMaxChan && v->has_chan[chan_clr] && v->clr.base)
         return gvdb2::fail(v, GVDB2_ERR_UNSUPPORTED, "colour gathers are not on this path");
     if (len && *len == 0 && !levelset) return GVDB2_OK; // GatherDensity returns on an empty list (V:5321)
-    return gvdb2::gather_voxels(v, subcell, radius, chan, accum, levelset);
+    return gvdb2::gather_voxels(v, subcell, radius, chan, accum, levelset, fp16);
+}
+
+gvdb2_status gvdb2_gather_level_set_fp16(gvdb2_volume *h, int subcell, int n, float radius, const float trans[3],
+                                         int *len, int chan_levelset, int chan_clr) {
+    (void)n;
+    (void)trans;
+    CHECK_HANDLE(h);
+    if (VOL(h)->used_leaves == 0) return GVDB2_OK; // returns without bricks (V:5378-5379)
+    return gather_common(h, subcell, radius, len, chan_levelset, chan_clr, 0, true, true);
 }
 
 gvdb2_status gvdb2_gather_density(gvdb2_volume *h, int subcell, int n, float radius, const float trans[3], int *len,
@@ -452,6 +473,20 @@ gvdb2_status gvdb2_copy_subcells(gvdb2_volume *h, int32_t *cnt, int32_t *nid, in
     if (cnt) GV_TRY(copy_out(v, cnt, v->sc_cnt.p, (size_t)n * sizeof(int32_t)));
     if (nid) GV_TRY(copy_out(v, nid, v->sc_nid.p, (size_t)n * sizeof(int32_t)));
     if (pos3) GV_TRY(copy_out(v, pos3, v->sc_pos.p, (size_t)n * 3 * sizeof(int32_t)));
+    return GVDB2_OK;
+}
+
+gvdb2_status gvdb2_copy_subcell_points_fp16(gvdb2_volume *h, uint16_t *pos3, uint16_t *vel3, int64_t max_entries) {
+    CHECK_HANDLE(h);
+    Volume *v = VOL(h);
+    if (!v->sc_fp16) return gvdb2::fail(v, GVDB2_ERR_STATE, "the subcell lists are not the 16-bit ones");
+    int64_t n = std::min<int64_t>(v->sc_len, max_entries);
+    if (n <= 0) return GVDB2_OK;
+    if (pos3) GV_TRY(copy_out(v, pos3, v->sc_q.p, (size_t)n * 3 * sizeof(uint16_t)));
+    if (vel3) {
+        if (!v->sc_qvel_valid) return gvdb2::fail(v, GVDB2_ERR_STATE, "no velocity lists (SetPoints without velocities)");
+        GV_TRY(copy_out(v, vel3, v->sc_qvel.p, (size_t)n * 3 * sizeof(uint16_t)));
+    }
     return GVDB2_OK;
 }
 

@@ -174,6 +174,11 @@ struct Volume {
 
     // subcells (InsertPointsSubcell)
     DevBuf sc_map, sc_flag, sc_cnt, sc_off, sc_nid, sc_pos, sc_pnt;
+    // InsertPointsSubcell_FP16: 16-bit entries (3 per list entry) over the
+    // bounding box of the last rebuild; velocities over velmin/velrange
+    DevBuf sc_q, sc_qvel;
+    bool sc_fp16 = false, sc_qvel_valid = false;
+    float velmin[3] = {0, 0, 0}, velrange[3] = {0, 0, 0}; // GetMinMaxVel; zero until computed
     int sc_size = 0, sc_dim = 0, sc_per_brick = 0;
     int64_t num_sc = 0, sc_len = 0;
 
@@ -240,11 +245,13 @@ gvdb2_status sync_counts(Volume *v);
 // ---- points.cu ----
 gvdb2_status insert_points(Volume *v, int n, const float trans[3], int prefix);
 gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]);
-gvdb2_status insert_points_subcell(Volume *v, int sc, int n, float radius, const float trans[3], int *len);
+gvdb2_status insert_points_subcell(Volume *v, int sc, int n, float radius, const float trans[3], int *len,
+                                   bool fp16 = false);
+gvdb2_status get_min_max_vel(Volume *v, int n);
 
 // ---- splat.cu ----
 gvdb2_status scatter_density_ref(Volume *v, int n, float radius, float amp, const float trans[3], int expand);
-gvdb2_status gather_voxels(Volume *v, int sc, float radius, int chan, int accum, bool levelset);
+gvdb2_status gather_voxels(Volume *v, int sc, float radius, int chan, int accum, bool levelset, bool fp16 = false);
 gvdb2_status scatter_kernel(Volume *v, int kernel, int n, const float trans[3], gvdb2_points_view weight,
                             float weight_const, const gvdb2_points_view *attrs, const int *chans, int nch);
 gvdb2_status gather_kernel(Volume *v, int kernel, int n, const float trans[3], const int *chans, int nch, float *out,

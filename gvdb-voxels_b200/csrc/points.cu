@@ -160,21 +160,43 @@ struct ScArgs {
     const Node *leaves;
     int64_t nleaves;
     const uint32_t *mapping;
+    // pass 2 (InsertPointsSubcell_FP16): quantization ranges, velocities
+    float3 pmin, prange, vmin, vrange;
+    PointsView vel;
+    uint16_t *q, *qvel;
 };
 
+// gvdbInsertSubcell_fp16's 16-bit quantization (P:195-203): (x - lo) /
+// range * 65535 with the reference's approximate division, converted as a
+// float-to-unsigned-short conversion does: toward zero, clamped, NaN to 0.
+__device__ __forceinline__ uint16_t quantize16(float x, float lo, float range) {
+    const float t = __fdividef(x - lo, range) * 65535.0f;
+    if (!(t > 0.0f)) return 0; // also NaN
+    return t >= 65535.0f ? (uint16_t)65535 : (uint16_t)t;
+}
+
 // gvdbCountSubcell (P:275-315, pass 0) / gvdbInsertSubcell (P:218-273,
-// pass 1).  The count pass tests the sign after adding trans, the insert
-// pass before, as in the reference; an insert never writes past the
-// counted capacity of its subcell.
+// pass 1) / gvdbInsertSubcell_fp16 (P:154-216, pass 2).  The count pass
+// tests the sign after adding trans, the insert pass before, the fp16 insert
+// pass tests NOHIT and the sign on the translated position, all as in the
+// reference; an insert never writes past the counted capacity of its
+// subcell.
 template <int PASS>
 __global__ void k_sc_visit(ScArgs A, uint32_t *cnt, const uint32_t *cap, const uint32_t *off, float *pnt,
                            int32_t *status) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;
     float3 p = load_f3(A.pos, i);
-    if (p.z == kNoHit) return;
     float w[3];
-    if (PASS == 0) {
+    if (PASS == 2) {
+        w[0] = p.x + A.trans.x;
+        w[1] = p.y + A.trans.y;
+        w[2] = p.z + A.trans.z;
+        if (w[2] == kNoHit) return;
+        if (w[0] < 0 || w[1] < 0 || w[2] < 0) return;
+    } else if (p.z == kNoHit) {
+        return;
+    } else if (PASS == 0) {
         w[0] = p.x + A.trans.x;
         w[1] = p.y + A.trans.y;
         w[2] = p.z + A.trans.z;
@@ -211,9 +233,21 @@ __global__ void k_sc_visit(ScArgs A, uint32_t *cnt, const uint32_t *cap, const u
                         continue;
                     }
                     int64_t at = (int64_t)off[idx] + o;
-                    pnt[3 * at + 0] = w[0];
-                    pnt[3 * at + 1] = w[1];
-                    pnt[3 * at + 2] = w[2];
+                    if (PASS == 2) {
+                        A.q[3 * at + 0] = quantize16(w[0], A.pmin.x, A.prange.x);
+                        A.q[3 * at + 1] = quantize16(w[1], A.pmin.y, A.prange.y);
+                        A.q[3 * at + 2] = quantize16(w[2], A.pmin.z, A.prange.z);
+                        if (A.qvel) {
+                            const float3 u = load_f3(A.vel, i);
+                            A.qvel[3 * at + 0] = quantize16(u.x, A.vmin.x, A.vrange.x);
+                            A.qvel[3 * at + 1] = quantize16(u.y, A.vmin.y, A.vrange.y);
+                            A.qvel[3 * at + 2] = quantize16(u.z, A.vmin.z, A.vrange.z);
+                        }
+                    } else {
+                        pnt[3 * at + 0] = w[0];
+                        pnt[3 * at + 1] = w[1];
+                        pnt[3 * at + 2] = w[2];
+                    }
                 }
             }
 }
@@ -355,7 +389,8 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     return GVDB2_OK;
 }
 
-gvdb2_status insert_points_subcell(Volume *v, int sc, int n, float radius, const float trans[3], int *len) {
+gvdb2_status insert_points_subcell(Volume *v, int sc, int n, float radius, const float trans[3], int *len,
+                                   bool fp16) {
     if (v->pos.cloud) return fail(v, GVDB2_ERR_UNSUPPORTED, "batched clouds: the reference-mode point operations (InsertPoints, InsertPointsSubcell) take one cloud per volume");
     int res0 = v->res(0);
     if (sc <= 0 || res0 % sc) return fail(v, GVDB2_ERR_ARG, "subcell size must divide the brick resolution");
@@ -394,6 +429,14 @@ gvdb2_status insert_points_subcell(Volume *v, int sc, int n, float radius, const
     A.leaves = v->pool_ptr(0);
     A.nleaves = nmap;
     A.mapping = v->sc_map.as<uint32_t>();
+    A.pmin = make_float3(v->posmin[0], v->posmin[1], v->posmin[2]); // mPosMin, mPosRange (V:5452-5462)
+    A.prange = make_float3(v->posmax[0] - v->posmin[0], v->posmax[1] - v->posmin[1], v->posmax[2] - v->posmin[2]);
+    A.vmin = make_float3(v->velmin[0], v->velmin[1], v->velmin[2]);
+    A.vrange = make_float3(v->velrange[0], v->velrange[1], v->velrange[2]);
+    A.vel = v->vel;
+    A.q = A.qvel = nullptr;
+    v->sc_fp16 = fp16;
+    v->sc_qvel_valid = false;
     int32_t *status = nullptr;
     GV_CUDA(v, cudaMallocAsync((void **)&status, sizeof(int32_t), s));
     GV_CUDA(v, cudaMemsetAsync(status, 0, sizeof(int32_t), s));
@@ -405,12 +448,25 @@ gvdb2_status insert_points_subcell(Volume *v, int sc, int n, float radius, const
     v->sc_len = total;
     if (len) *len = (int)total;
     if (total > 0) {
-        GV_CUDA(v, v->sc_pnt.ensure(sizeof(float) * 3 * (size_t)total, s));
         GV_CUDA(v, cudaMemcpyAsync(cap, cnt, sizeof(uint32_t) * (size_t)num_sc, cudaMemcpyDeviceToDevice, s));
         GV_CUDA(v, cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (size_t)num_sc, s));
-        if (n > 0)
-            k_sc_visit<1><<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(A, cnt, cap, v->sc_off.as<uint32_t>(),
-                                                                     v->sc_pnt.as<float>(), status);
+        if (fp16) {
+            GV_CUDA(v, v->sc_q.ensure(sizeof(uint16_t) * 3 * (size_t)total, s));
+            A.q = v->sc_q.as<uint16_t>();
+            if (v->vel.base) { // velocities too, when SetPoints gave them (P:204-207)
+                GV_CUDA(v, v->sc_qvel.ensure(sizeof(uint16_t) * 3 * (size_t)total, s));
+                A.qvel = v->sc_qvel.as<uint16_t>();
+                v->sc_qvel_valid = true;
+            }
+            if (n > 0)
+                k_sc_visit<2><<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(A, cnt, cap, v->sc_off.as<uint32_t>(),
+                                                                         nullptr, status);
+        } else {
+            GV_CUDA(v, v->sc_pnt.ensure(sizeof(float) * 3 * (size_t)total, s));
+            if (n > 0)
+                k_sc_visit<1><<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(A, cnt, cap, v->sc_off.as<uint32_t>(),
+                                                                         v->sc_pnt.as<float>(), status);
+        }
     }
     k_sc_pos<<<grid_for(nmap, 256, 1ll << 31), 256, 0, s>>>(v->pool_ptr(0), nmap, v->sc_map.as<uint32_t>(), sc, scdim,
                                                             scpb, num_sc, v->sc_nid.as<int32_t>(),

@@ -73,11 +73,31 @@ __global__ void k_scatter_ref(PointsView pos, int64_t n, float radius, float3 tr
     }
 }
 
-// gvdbGatherDensity / gvdbGatherLevelSet: one CTA per mapped leaf, one
-// thread per voxel of its subcells.
-template <bool LEVELSET>
+// The entries of the subcell lists: float xyz (InsertPointsSubcell), or
+// 16-bit xyz over the rebuild's bounding box (InsertPointsSubcell_FP16),
+// read back as q / 65535 * range + min (gvdbGatherLevelSet_fp16, P:792-794).
+struct ScList {
+    const float *pnt;
+    const uint16_t *q;
+    float3 qmin, qrange;
+};
+template <bool FP16>
+__device__ __forceinline__ float3 sc_entry(const ScList &L, int64_t e) {
+    if (FP16) {
+        const uint16_t *q = L.q + 3 * e;
+        return make_float3(fmaf(__fdividef((float)q[0], 65535.0f), L.qrange.x, L.qmin.x),
+                           fmaf(__fdividef((float)q[1], 65535.0f), L.qrange.y, L.qmin.y),
+                           fmaf(__fdividef((float)q[2], 65535.0f), L.qrange.z, L.qmin.z));
+    }
+    const float *p = L.pnt + 3 * e;
+    return make_float3(p[0], p[1], p[2]);
+}
+
+// gvdbGatherDensity / gvdbGatherLevelSet (and gvdbGatherLevelSet_fp16): one
+// CTA per mapped leaf, one thread per voxel of its subcells.
+template <bool LEVELSET, bool FP16>
 __global__ void k_gather_voxels(int64_t num_sc, int scpb, int sc, float radius, const int32_t *sc_nid,
-                                const uint32_t *sc_cnt, const uint32_t *sc_off, const int32_t *sc_pos, const float *pnt,
+                                const uint32_t *sc_cnt, const uint32_t *sc_off, const int32_t *sc_pos, ScList pl,
                                 const Node *leaves, int apron, AtlasGeom A, float *chan, int accum) {
     int sc3 = sc * sc * sc;
     int64_t sid = (int64_t)blockIdx.x * scpb + threadIdx.x / sc3;
@@ -93,8 +113,8 @@ __global__ void k_gather_voxels(int64_t num_sc, int scpb, int sc, float radius, 
     uint32_t beg = sc_off[sid], cnt = sc_cnt[sid];
     float fx = (float)wx, fy = (float)wy, fz = (float)wz;
     for (uint32_t j = 0; j < cnt; j++) {
-        const float *p = pnt + 3 * (int64_t)(beg + j);
-        float dx = p[0] - fx, dy = p[1] - fy, dz = p[2] - fz;
+        const float3 p = sc_entry<FP16>(pl, (int64_t)(beg + j));
+        float dx = p.x - fx, dy = p.y - fy, dz = p.z - fz;
         float c = sqrtf(dx * dx + dy * dy + dz * dz);
         if (LEVELSET) val = fminf(val, c - radius);
         else val = fmaxf(val, radius - c);
@@ -110,11 +130,11 @@ __global__ void k_gather_voxels(int64_t num_sc, int scpb, int sc, float radius, 
 // subtraction of the radius are monotonic, so max(r - c) = r - sqrt(min d^2)
 // and min(c - r) = sqrt(min d^2) - r, as in P:725-728 / P:764-767.
 constexpr int kGvWarps = 8;
-template <bool LEVELSET>
+template <bool LEVELSET, bool FP16>
 __global__ void __launch_bounds__(32 * kGvWarps) k_gather_voxels_sc4(int64_t num_sc, float radius,
                                                                      const int32_t *sc_nid, const uint32_t *sc_cnt,
                                                                      const uint32_t *sc_off, const int32_t *sc_pos,
-                                                                     const float *pnt, const Node *leaves, AtlasGeom A,
+                                                                     ScList pl, const Node *leaves, AtlasGeom A,
                                                                      float *chan, int accum) {
     __shared__ float4 buf[kGvWarps][64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -138,8 +158,8 @@ __global__ void __launch_bounds__(32 * kGvWarps) k_gather_voxels_sc4(int64_t num
     for (uint32_t base = 0; base < cnt; base += 64) {
         const uint32_t m = min(64u, cnt - base);
         for (uint32_t k = lane; k < m; k += 32) {
-            const float *q = pnt + 3 * (int64_t)(beg + base + k);
-            wb[k] = make_float4(q[0], q[1], q[2], 0.0f);
+            const float3 q = sc_entry<FP16>(pl, (int64_t)(beg + base + k));
+            wb[k] = make_float4(q.x, q.y, q.z, 0.0f);
         }
         __syncwarp();
         for (uint32_t j = 0; j < m; j++) {
@@ -988,40 +1008,44 @@ gvdb2_status scatter_density_ref(Volume *v, int n, float radius, float amp, cons
     return GVDB2_OK;
 }
 
-gvdb2_status gather_voxels(Volume *v, int sc, float radius, int chan, int accum, bool levelset) {
-    if (chan < 0 || chan >= kMaxChan || !v->has_chan[chan]) return fail(v, GVDB2_ERR_ARG, "bad channel");
-    if (v->num_sc == 0 || sc != v->sc_size) return fail(v, GVDB2_ERR_STATE, "InsertPointsSubcell must precede the gather");
-    int sc3 = sc * sc * sc;
-    int threads = v->sc_per_brick * sc3;
-    if (threads > 1024) return fail(v, GVDB2_ERR_UNSUPPORTED, "brick has more than 1024 voxels");
-    int64_t blocks = (v->num_sc + v->sc_per_brick - 1) / v->sc_per_brick;
-    if (blocks == 0) return GVDB2_OK;
-    const float *pnt = v->sc_len > 0 ? v->sc_pnt.as<float>() : nullptr;
+template <bool LEVELSET, bool FP16>
+gvdb2_status launch_gather_voxels(Volume *v, int sc, float radius, int chan, int accum) {
+    ScList pl;
+    pl.pnt = (!FP16 && v->sc_len > 0) ? v->sc_pnt.as<float>() : nullptr;
+    pl.q = (FP16 && v->sc_len > 0) ? v->sc_q.as<uint16_t>() : nullptr;
+    pl.qmin = make_float3(v->posmin[0], v->posmin[1], v->posmin[2]);
+    pl.qrange = make_float3(v->posmax[0] - v->posmin[0], v->posmax[1] - v->posmin[1], v->posmax[2] - v->posmin[2]);
     if (sc == 4) {
         const unsigned g = (unsigned)((v->num_sc + kGvWarps - 1) / kGvWarps);
-        if (levelset)
-            k_gather_voxels_sc4<true><<<g, 32 * kGvWarps, 0, v->stream>>>(
-                v->num_sc, radius, v->sc_nid.as<int32_t>(), v->sc_cnt.as<uint32_t>(), v->sc_off.as<uint32_t>(),
-                v->sc_pos.as<int32_t>(), pnt, v->pool_ptr(0), atlas_geom(v), v->atlas[chan].as<float>(), accum);
-        else
-            k_gather_voxels_sc4<false><<<g, 32 * kGvWarps, 0, v->stream>>>(
-                v->num_sc, radius, v->sc_nid.as<int32_t>(), v->sc_cnt.as<uint32_t>(), v->sc_off.as<uint32_t>(),
-                v->sc_pos.as<int32_t>(), pnt, v->pool_ptr(0), atlas_geom(v), v->atlas[chan].as<float>(), accum);
-        GV_CUDA(v, cudaGetLastError());
-        return GVDB2_OK;
+        k_gather_voxels_sc4<LEVELSET, FP16><<<g, 32 * kGvWarps, 0, v->stream>>>(
+            v->num_sc, radius, v->sc_nid.as<int32_t>(), v->sc_cnt.as<uint32_t>(), v->sc_off.as<uint32_t>(),
+            v->sc_pos.as<int32_t>(), pl, v->pool_ptr(0), atlas_geom(v), v->atlas[chan].as<float>(), accum);
+    } else {
+        const int threads = v->sc_per_brick * sc * sc * sc;
+        const int64_t blocks = (v->num_sc + v->sc_per_brick - 1) / v->sc_per_brick;
+        k_gather_voxels<LEVELSET, FP16><<<(unsigned)blocks, threads, 0, v->stream>>>(
+            v->num_sc, v->sc_per_brick, sc, radius, v->sc_nid.as<int32_t>(), v->sc_cnt.as<uint32_t>(),
+            v->sc_off.as<uint32_t>(), v->sc_pos.as<int32_t>(), pl, v->pool_ptr(0), v->apron, atlas_geom(v),
+            v->atlas[chan].as<float>(), accum);
     }
-    if (levelset)
-        k_gather_voxels<true><<<(unsigned)blocks, threads, 0, v->stream>>>(
-            v->num_sc, v->sc_per_brick, sc, radius, v->sc_nid.as<int32_t>(), v->sc_cnt.as<uint32_t>(),
-            v->sc_off.as<uint32_t>(), v->sc_pos.as<int32_t>(), pnt, v->pool_ptr(0), v->apron, atlas_geom(v),
-            v->atlas[chan].as<float>(), accum);
-    else
-        k_gather_voxels<false><<<(unsigned)blocks, threads, 0, v->stream>>>(
-            v->num_sc, v->sc_per_brick, sc, radius, v->sc_nid.as<int32_t>(), v->sc_cnt.as<uint32_t>(),
-            v->sc_off.as<uint32_t>(), v->sc_pos.as<int32_t>(), pnt, v->pool_ptr(0), v->apron, atlas_geom(v),
-            v->atlas[chan].as<float>(), accum);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
+}
+
+gvdb2_status gather_voxels(Volume *v, int sc, float radius, int chan, int accum, bool levelset, bool fp16) {
+    if (chan < 0 || chan >= kMaxChan || !v->has_chan[chan]) return fail(v, GVDB2_ERR_ARG, "bad channel");
+    if (v->num_sc == 0 || sc != v->sc_size) return fail(v, GVDB2_ERR_STATE, "InsertPointsSubcell must precede the gather");
+    if (fp16 != v->sc_fp16)
+        return fail(v, GVDB2_ERR_STATE, fp16 ? "GatherLevelSet_FP16 needs the lists of InsertPointsSubcell_FP16"
+                                             : "the subcell lists hold 16-bit entries: use GatherLevelSet_FP16");
+    if (fp16 && !levelset) return fail(v, GVDB2_ERR_UNSUPPORTED, "16-bit lists serve the level set only");
+    // 4^3 subcells take a warp each; other sizes a CTA per brick
+    if (sc != 4 && v->sc_per_brick * sc * sc * sc > 1024)
+        return fail(v, GVDB2_ERR_UNSUPPORTED, "subcells other than 4^3 need bricks of at most 1024 voxels");
+    if ((v->num_sc + v->sc_per_brick - 1) / v->sc_per_brick == 0) return GVDB2_OK;
+    if (fp16) return launch_gather_voxels<true, true>(v, sc, radius, chan, 0);
+    return levelset ? launch_gather_voxels<true, false>(v, sc, radius, chan, accum)
+                    : launch_gather_voxels<false, false>(v, sc, radius, chan, accum);
 }
 
 gvdb2_status scatter_kernel(Volume *v, int kernel, int n, const float trans[3], gvdb2_points_view weight,

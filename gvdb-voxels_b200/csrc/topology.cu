@@ -1026,6 +1026,33 @@ void reserve_pool(Volume *v, int64_t n) {
     cudaGetLastError(); // a failed reservation is only a missed optimisation
 }
 
+// GetMinMaxVel (V:5469-5521): per axis min and max of the first n
+// velocities (the bounding-box reduction with no translation);
+// mVelRange = mVelMax - mVelMin.  Read by InsertPointsSubcell_FP16.
+gvdb2_status get_min_max_vel(Volume *v, int n) {
+    if (!v->vel.base || n <= 0 || n > v->vel.count) return fail(v, GVDB2_ERR_ARG, "GetMinMaxVel needs velocities");
+    cudaStream_t s = v->stream;
+    if (!v->dev_small.p) {
+        GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), s));
+        GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
+    }
+    int32_t init[6];
+    for (int a = 0; a < 3; a++) {
+        init[a] = 0x7F800000;              // ord(+inf)
+        init[3 + a] = (int32_t)0x807FFFFF; // ord(-inf)
+    }
+    GV_CUDA(v, cudaMemcpyAsync(dev_words(v)->bbox, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    k_bbox<<<std::min(grid_for(n, 256), 8 * kSmCount), 256, 0, s>>>(v->vel, n, make_float3(0.0f, 0.0f, 0.0f),
+                                                                    dev_words(v)->bbox);
+    GV_CUDA(v, cudaGetLastError());
+    GV_TRY(read_words(v));
+    for (int a = 0; a < 3; a++) {
+        v->velmin[a] = ord2f(host_words(v)->bbox[a]);
+        v->velrange[a] = ord2f(host_words(v)->bbox[3 + a]) - v->velmin[a];
+    }
+    return GVDB2_OK;
+}
+
 gvdb2_status rebuild_topology(Volume *v, int n, float radius, const float orig[3], bool accumulate, int min_depth) {
     if (v->nlev == 0) return fail(v, GVDB2_ERR_STATE, "Configure not called");
     if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count)))

@@ -161,6 +161,23 @@ class VolumeGVDB:
         self._check(self._L.gvdb2_scatter_density(self._h, int(num_pnts), float(radius), float(amp), _f3(trans),
                                                   1 if expand else 0, 1 if avgColor else 0), "ScatterDensity")
 
+    def InsertPointsSubcell_FP16(self, subcell_size, num_pnts, radius, trans=(0, 0, 0)):
+        """InsertPointsSubcell with 16-bit list entries (V:5094-5189); returns the list length."""
+        ln = ctypes.c_int(0)
+        self._check(self._L.gvdb2_insert_points_subcell_fp16(self._h, subcell_size, int(num_pnts), float(radius),
+                                                             _f3(trans), ctypes.byref(ln)), "InsertPointsSubcell_FP16")
+        return ln.value
+
+    def GetMinMaxVel(self, num_pnts):
+        """Velocity range used to quantize the 16-bit velocity lists (V:5469-5521)."""
+        self._check(self._L.gvdb2_get_min_max_vel(self._h, int(num_pnts)), "GetMinMaxVel")
+
+    def GatherLevelSet_FP16(self, subcell_size, num_pnts, radius, trans, sc_len, chanLevelset, chanClr=-1):
+        ln = ctypes.c_int(int(sc_len))
+        self._check(self._L.gvdb2_gather_level_set_fp16(self._h, subcell_size, int(num_pnts), float(radius),
+                                                        _f3(trans), ctypes.byref(ln), chanLevelset, chanClr),
+                    "GatherLevelSet_FP16")
+
     def _gather(self, fn, what, subcell_size, num_pnts, radius, trans, sc_len, chan, chan_clr, accum):
         ln = ctypes.c_int(int(sc_len))
         self._check(fn(self._h, subcell_size, int(num_pnts), float(radius), _f3(trans), ctypes.byref(ln), chan,
@@ -328,6 +345,16 @@ class VolumeGVDB:
         self._check(self._L.gvdb2_copy_point_nodes(self._h, pnode.ctypes.data, poff.ctypes.data, n,
                                                    gcnt.ctypes.data, nl), "copy_point_nodes")
         return pnode, poff, gcnt
+
+    def subcell_points_fp16(self, length, vel=False):
+        """The 16-bit list entries, (length, 3) uint16 (and velocities)."""
+        import numpy as np
+        q = np.zeros((max(length, 1), 3), np.uint16)
+        qv = np.zeros((max(length, 1), 3), np.uint16) if vel else None
+        self._check(self._L.gvdb2_copy_subcell_points_fp16(self._h, q.ctypes.data,
+                                                           qv.ctypes.data if vel else None, int(length)),
+                    "copy_subcell_points_fp16")
+        return (q[:length], qv[:length]) if vel else q[:length]
 
     def subcells(self, count):
         cnt = np.zeros(count, np.int32)

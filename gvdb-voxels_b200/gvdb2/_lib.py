@@ -66,6 +66,9 @@ _SIGS = {
     "gvdb2_update_neighbors": [_vp],
     "gvdb2_insert_points": [_vp, _i32, _fp, _i32],
     "gvdb2_insert_points_subcell": [_vp, _i32, _i32, _f32, _fp, _ip],
+    "gvdb2_insert_points_subcell_fp16": [_vp, _i32, _i32, _f32, _fp, _ip],
+    "gvdb2_get_min_max_vel": [_vp, _i32],
+    "gvdb2_gather_level_set_fp16": [_vp, _i32, _i32, _f32, _fp, _ip, _i32, _i32],
     "gvdb2_scatter_density": [_vp, _i32, _f32, _f32, _fp, _i32, _i32],
     "gvdb2_gather_density": [_vp, _i32, _i32, _f32, _fp, _ip, _i32, _i32, _i32],
     "gvdb2_gather_level_set": [_vp, _i32, _i32, _f32, _fp, _ip, _i32, _i32, _i32],
@@ -85,6 +88,7 @@ _SIGS = {
     "gvdb2_copy_neighbors": [_vp, _vp, _i64],
     "gvdb2_copy_point_nodes": [_vp, _vp, _vp, _i64, _vp, _i64],
     "gvdb2_copy_subcells": [_vp, _vp, _vp, _vp, _i64],
+    "gvdb2_copy_subcell_points_fp16": [_vp, _vp, _vp, _i64],
     "gvdb2_atlas_device_ptr": [_vp, _i32, ctypes.POINTER(_vp)],
 }
 

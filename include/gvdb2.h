@@ -129,6 +129,14 @@ GVDB2_API gvdb2_status gvdb2_update_neighbors(gvdb2_volume *v);                 
 GVDB2_API gvdb2_status gvdb2_insert_points(gvdb2_volume *v, int n, const float trans[3], int prefix);          /* InsertPoints, V:5219-5267 */
 GVDB2_API gvdb2_status gvdb2_insert_points_subcell(gvdb2_volume *v, int subcell, int n, float radius,
                                          const float trans[3], int *len);                    /* InsertPointsSubcell, V:4971-5092 */
+/* The same lists with 16-bit entries: positions quantized over the bounding
+ * box of the last rebuild, (p + trans - mPosMin) / mPosRange * 65535, and,
+ * when SetPoints gave velocities, velocities over the range of the last
+ * gvdb2_get_min_max_vel (zero before one).  NOHIT and negativity are tested
+ * on the translated position, as the reference's 16-bit insert does. */
+GVDB2_API gvdb2_status gvdb2_insert_points_subcell_fp16(gvdb2_volume *v, int subcell, int n, float radius,
+                                              const float trans[3], int *len);               /* InsertPointsSubcell_FP16, V:5094-5189 */
+GVDB2_API gvdb2_status gvdb2_get_min_max_vel(gvdb2_volume *v, int n);                          /* GetMinMaxVel, V:5469-5521 */
 
 /* ---- reference-mode splat / gathers / apron ---- */
 GVDB2_API gvdb2_status gvdb2_scatter_density(gvdb2_volume *v, int n, float radius, float amp, const float trans[3],
@@ -137,6 +145,11 @@ GVDB2_API gvdb2_status gvdb2_gather_density(gvdb2_volume *v, int subcell, int n,
                                   int *len, int chan_density, int chan_clr, int accum);       /* GatherDensity, V:5318-5344 */
 GVDB2_API gvdb2_status gvdb2_gather_level_set(gvdb2_volume *v, int subcell, int n, float radius, const float trans[3],
                                     int *len, int chan_levelset, int chan_clr, int accum);    /* GatherLevelSet, V:5348-5373 */
+/* GatherLevelSet over the 16-bit lists of gvdb2_insert_points_subcell_fp16
+ * (never accumulates, as in the reference). */
+GVDB2_API gvdb2_status gvdb2_gather_level_set_fp16(gvdb2_volume *v, int subcell, int n, float radius,
+                                         const float trans[3], int *len, int chan_levelset,
+                                         int chan_clr);                                       /* GatherLevelSet_FP16, V:5375-5402 */
 GVDB2_API gvdb2_status gvdb2_scatter_reduce_level_set(gvdb2_volume *v, int subcell, int n, float radius,
                                             const float trans[3], int *len, int chan_levelset,
                                             int chan_clr, int accum); /* same operation as GatherLevelSet, V:5348-5373 */
@@ -195,6 +208,10 @@ GVDB2_API gvdb2_status gvdb2_copy_neighbors(gvdb2_volume *v, int32_t *host, int6
 GVDB2_API gvdb2_status gvdb2_copy_point_nodes(gvdb2_volume *v, int32_t *pnode, int32_t *poff, int64_t n,
                                     int32_t *gcnt, int64_t ngcnt);                                /* InsertPoints results */
 GVDB2_API gvdb2_status gvdb2_copy_subcells(gvdb2_volume *v, int32_t *cnt, int32_t *nid, int32_t *pos3, int64_t max_subcells);
+/* the 16-bit list entries (3 per entry, grouped by subcell like the counts);
+ * vel3 may be NULL */
+GVDB2_API gvdb2_status gvdb2_copy_subcell_points_fp16(gvdb2_volume *v, uint16_t *pos3, uint16_t *vel3,
+                                                int64_t max_entries);
 GVDB2_API gvdb2_status gvdb2_atlas_device_ptr(gvdb2_volume *v, int chan, float **dev_ptr);                 /* device view of a channel */
 
 #ifdef __cplusplus

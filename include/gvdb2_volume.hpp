@@ -97,6 +97,12 @@ class VolumeGVDB {
         const float t[3] = {trans.x, trans.y, trans.z};
         check(gvdb2_insert_points_subcell(v_, subcell_size, num_pnts, radius, t, &pSCPntsLength), "InsertPointsSubcell");
     }
+    void InsertPointsSubcell_FP16(int subcell_size, int num_pnts, float radius, Vec3F trans, int &pSCPntsLength) {
+        const float t[3] = {trans.x, trans.y, trans.z};
+        check(gvdb2_insert_points_subcell_fp16(v_, subcell_size, num_pnts, radius, t, &pSCPntsLength),
+              "InsertPointsSubcell_FP16");
+    }
+    void GetMinMaxVel(int num_pnts) { check(gvdb2_get_min_max_vel(v_, num_pnts), "GetMinMaxVel"); }
     void ScatterDensity(int num_pnts, float radius, float amp, Vec3F trans, bool expand = true, bool avgColor = false) {
         const float t[3] = {trans.x, trans.y, trans.z};
         check(gvdb2_scatter_density(v_, num_pnts, radius, amp, t, expand ? 1 : 0, avgColor ? 1 : 0), "ScatterDensity");
@@ -114,6 +120,12 @@ class VolumeGVDB {
         check(gvdb2_gather_level_set(v_, subcell_size, num_pnts, radius, t, &pSCPntsLength, chanLevelset, chanClr,
                                      bAccum ? 1 : 0),
               "GatherLevelSet");
+    }
+    void GatherLevelSet_FP16(int subcell_size, int num_pnts, float radius, Vec3F trans, int &pSCPntsLength,
+                             int chanLevelSet, int chanClr) {
+        const float t[3] = {trans.x, trans.y, trans.z};
+        check(gvdb2_gather_level_set_fp16(v_, subcell_size, num_pnts, radius, t, &pSCPntsLength, chanLevelSet, chanClr),
+              "GatherLevelSet_FP16");
     }
     void UpdateApron() { check(gvdb2_update_apron(v_, -1, 0.0f), "UpdateApron"); }
     void UpdateApron(unsigned char chan, float boundval = 0.0f) {

@@ -49,8 +49,11 @@ struct orc_volume {
     int sc_size, sc_dim, sc_per_brick;
     int64_t num_sc;
     int32_t *sc_cnt, *sc_off, *sc_nid, *sc_pos;
-    float *sc_pnt; /* xyz per list entry */
+    float *sc_pnt; /* xyz per list entry (InsertPointsSubcell) */
     int64_t sc_len;
+    int sc_fp16;                 /* lists hold quantized entries (InsertPointsSubcell_FP16) */
+    uint16_t *sc_q, *sc_qvel;    /* 3 per entry: position, velocity (when set) */
+    float velmin[3], velrange[3]; /* GetMinMaxVel (V:5469-5521); zero until computed */
 };
 
 /* ------------------------------------------------------------------ */
@@ -305,8 +308,12 @@ static void free_subcells(orc_volume *v) {
     free(v->sc_nid);
     free(v->sc_pos);
     free(v->sc_pnt);
+    free(v->sc_q);
+    free(v->sc_qvel);
     v->sc_cnt = v->sc_off = v->sc_nid = v->sc_pos = NULL;
     v->sc_pnt = NULL;
+    v->sc_q = v->sc_qvel = NULL;
+    v->sc_fp16 = 0;
     v->num_sc = v->sc_len = 0;
 }
 
@@ -1074,10 +1081,26 @@ static void subcell_box(const float w[3], float radius, int sc, int mn[3], int m
     }
 }
 
+/* gvdbInsertSubcell_fp16's 16-bit quantization (P:195-203): (x - lo) /
+ * range * 65535, converted as a float-to-unsigned-short conversion on the
+ * GPU does: toward zero, clamped to [0, 65535], NaN to 0. */
+static uint16_t quantize16(float x, float lo, float range) {
+    float t = (x - lo) / range * 65535.0f;
+    if (t != t || t <= 0.0f) return 0;
+    if (t >= 65535.0f) return 65535;
+    return (uint16_t)t;
+}
+
 /* InsertPointsSubcell (V:4971-5092): gvdbSetFlagSubcell + PrefixSum ->
  * mapping, gvdbCountSubcell, PrefixSum, gvdbInsertSubcell (list order
- * follows point order here), gvdbCalcSubcellPos (P:677-694). */
-int orc_insert_points_subcell(orc_volume *v, int sc, orc_view pos, int n, float radius, const float trans[3], int *len) {
+ * follows point order here), gvdbCalcSubcellPos (P:677-694).
+ * InsertPointsSubcell_FP16 (V:5094-5189) runs the same count, then
+ * gvdbInsertSubcell_fp16 (P:154-216): both tests on the translated
+ * position (NOHIT on its z), entries quantized over the bounding box of the
+ * last rebuild (mPosMin, mPosRange = mPosMax - mPosMin) and, with
+ * velocities, over mVelMin/mVelRange. */
+static int insert_subcells(orc_volume *v, int sc, orc_view pos, orc_view vel, int n, float radius,
+                           const float trans[3], int *len, int fp16) {
     int res = res_of(v, 0);
     if (sc <= 0 || res % sc) return ORC_ERR_ARG;
     int64_t num_brick = v->used_leaves;
@@ -1121,8 +1144,20 @@ int orc_insert_points_subcell(orc_volume *v, int sc, orc_view pos, int n, float 
             v->sc_len = acc;
             memcpy(cap, v->sc_cnt, (size_t)v->num_sc * sizeof(int32_t));
             memset(v->sc_cnt, 0, (size_t)v->num_sc * sizeof(int32_t));
-            v->sc_pnt = (float *)malloc((size_t)(acc * 3 + 3) * sizeof(float));
-            if (!v->sc_pnt) {
+            int bad = 0;
+            if (fp16) {
+                v->sc_fp16 = 1;
+                v->sc_q = (uint16_t *)malloc((size_t)(acc * 3 + 3) * sizeof(uint16_t));
+                bad = !v->sc_q;
+                if (vel.base) {
+                    v->sc_qvel = (uint16_t *)malloc((size_t)(acc * 3 + 3) * sizeof(uint16_t));
+                    bad = bad || !v->sc_qvel;
+                }
+            } else {
+                v->sc_pnt = (float *)malloc((size_t)(acc * 3 + 3) * sizeof(float));
+                bad = !v->sc_pnt;
+            }
+            if (bad) {
                 free(mapping);
                 free(cap);
                 return ORC_ERR_NOMEM;
@@ -1130,12 +1165,17 @@ int orc_insert_points_subcell(orc_volume *v, int sc, orc_view pos, int n, float 
         }
         for (int64_t i = 0; i < n; i++) {
             const float *p = view_f3(pos, i);
-            if (p[2] == NOHIT) continue;
             float w[3];
             if (pass == 0) { /* count: trans added before the sign test (P:283-284) */
+                if (p[2] == NOHIT) continue;
                 for (int a = 0; a < 3; a++) w[a] = p[a] + trans[a];
                 if (w[0] < 0 || w[1] < 0 || w[2] < 0) continue;
+            } else if (fp16) { /* fp16 insert: both tests on the translated position (P:169-172) */
+                for (int a = 0; a < 3; a++) w[a] = p[a] + trans[a];
+                if (w[2] == NOHIT) continue;
+                if (w[0] < 0 || w[1] < 0 || w[2] < 0) continue;
             } else { /* insert: sign test before trans (P:231-233) */
+                if (p[2] == NOHIT) continue;
                 if (p[0] < 0 || p[1] < 0 || p[2] < 0) continue;
                 for (int a = 0; a < 3; a++) w[a] = p[a] + trans[a];
             }
@@ -1158,9 +1198,20 @@ int orc_insert_points_subcell(orc_volume *v, int sc, orc_view pos, int n, float 
                         } else {
                             if (v->sc_cnt[idx] >= cap[idx]) continue; /* never past the counted list */
                             int64_t at = v->sc_off[idx] + v->sc_cnt[idx]++;
-                            v->sc_pnt[at * 3 + 0] = w[0];
-                            v->sc_pnt[at * 3 + 1] = w[1];
-                            v->sc_pnt[at * 3 + 2] = w[2];
+                            if (fp16) {
+                                float range[3];
+                                for (int a = 0; a < 3; a++) range[a] = v->posmax[a] - v->posmin[a];
+                                for (int a = 0; a < 3; a++) v->sc_q[at * 3 + a] = quantize16(w[a], v->posmin[a], range[a]);
+                                if (v->sc_qvel) {
+                                    const float *u = view_f3(vel, i);
+                                    for (int a = 0; a < 3; a++)
+                                        v->sc_qvel[at * 3 + a] = quantize16(u[a], v->velmin[a], v->velrange[a]);
+                                }
+                            } else {
+                                v->sc_pnt[at * 3 + 0] = w[0];
+                                v->sc_pnt[at * 3 + 1] = w[1];
+                                v->sc_pnt[at * 3 + 2] = w[2];
+                            }
                         }
                     }
         }
@@ -1183,12 +1234,43 @@ int orc_insert_points_subcell(orc_volume *v, int sc, orc_view pos, int n, float 
     return ORC_OK;
 }
 
+int orc_insert_points_subcell(orc_volume *v, int sc, orc_view pos, int n, float radius, const float trans[3], int *len) {
+    orc_view none = {NULL, 0, 0, 0};
+    return insert_subcells(v, sc, pos, none, n, radius, trans, len, 0);
+}
+
+int orc_insert_points_subcell_fp16(orc_volume *v, int sc, orc_view pos, orc_view vel, int n, float radius,
+                                   const float trans[3], int *len) {
+    return insert_subcells(v, sc, pos, vel, n, radius, trans, len, 1);
+}
+
+/* GetMinMaxVel (V:5469-5521): per axis min and max of the velocities,
+ * mVelRange = mVelMax - mVelMin. */
+int orc_get_min_max_vel(orc_volume *v, orc_view vel, int n) {
+    if (!vel.base || n <= 0) return ORC_ERR_ARG;
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = 0; i < n; i++) {
+        const float *u = view_f3(vel, i);
+        for (int a = 0; a < 3; a++) {
+            if (u[a] < mn[a]) mn[a] = u[a];
+            if (u[a] > mx[a]) mx[a] = u[a];
+        }
+    }
+    for (int a = 0; a < 3; a++) {
+        v->velmin[a] = mn[a];
+        v->velrange[a] = mx[a] - mn[a];
+    }
+    return ORC_OK;
+}
+
 /* gvdbGatherDensity (P:696-733) / gvdbGatherLevelSet (P:736-773): each
  * voxel of each subcell reduces over that subcell's list with the integer
  * voxel corner as the sample position. */
 static int gather_voxels(orc_volume *v, int sc, float radius, int chan, int accum, int levelset) {
     if (chan < 0 || chan >= ORC_MAXCHAN || !v->has_chan[chan]) return ORC_ERR_ARG;
     if (!v->sc_cnt || sc != v->sc_size) return ORC_ERR_STATE;
+    float range[3];
+    for (int a = 0; a < 3; a++) range[a] = v->posmax[a] - v->posmin[a];
     int64_t tv = tile_vox(v);
     double *at = v->atlas[chan];
     int a = v->apron;
@@ -1206,7 +1288,13 @@ static int gather_voxels(orc_volume *v, int sc, float radius, int chan, int accu
                     double *dst = &at[slot * tv + tile_index(v, lc)];
                     double val = accum ? *dst : (levelset ? 3.0 : 0.0);
                     for (int32_t j = 0; j < v->sc_cnt[s]; j++) {
-                        const float *p = &v->sc_pnt[(int64_t)(v->sc_off[s] + j) * 3];
+                        const int64_t e = (int64_t)(v->sc_off[s] + j) * 3;
+                        float q[3];
+                        if (v->sc_fp16) /* gvdbGatherLevelSet_fp16 (P:792-794): q / 65535 * range + min */
+                            for (int k = 0; k < 3; k++) q[k] = (float)v->sc_q[e + k] / 65535.0f * range[k] + v->posmin[k];
+                        else
+                            for (int k = 0; k < 3; k++) q[k] = v->sc_pnt[e + k];
+                        const float *p = q;
                         float d[3] = {p[0] - (float)wp[0], p[1] - (float)wp[1], p[2] - (float)wp[2]};
                         double c = sqrt((double)d[0] * d[0] + (double)d[1] * d[1] + (double)d[2] * d[2]);
                         if (levelset) {
@@ -1223,10 +1311,18 @@ static int gather_voxels(orc_volume *v, int sc, float radius, int chan, int accu
     return ORC_OK;
 }
 int orc_gather_density(orc_volume *v, int sc, float radius, int chan, int accum) {
+    if (v->sc_fp16) return ORC_ERR_STATE; /* the lists hold quantized entries */
     return gather_voxels(v, sc, radius, chan, accum, 0);
 }
 int orc_gather_level_set(orc_volume *v, int sc, float radius, int chan, int accum) {
+    if (v->sc_fp16) return ORC_ERR_STATE; /* the lists hold quantized entries */
     return gather_voxels(v, sc, radius, chan, accum, 1);
+}
+/* GatherLevelSet_FP16 (V:5375-5402): the level set over quantized lists,
+ * never accumulating (P:775-811). */
+int orc_gather_level_set_fp16(orc_volume *v, int sc, float radius, int chan) {
+    if (!v->sc_fp16) return ORC_ERR_STATE;
+    return gather_voxels(v, sc, radius, chan, 0, 1);
 }
 
 /* ------------------------------------------------------------------ */
@@ -1512,3 +1608,8 @@ int64_t orc_subcell_count(const orc_volume *v) { return v->num_sc; }
 const int32_t *orc_subcell_cnt(const orc_volume *v) { return v->sc_cnt; }
 const int32_t *orc_subcell_nid(const orc_volume *v) { return v->sc_nid; }
 const int32_t *orc_subcell_pos(const orc_volume *v) { return v->sc_pos; }
+const int32_t *orc_subcell_off(const orc_volume *v) { return v->sc_off; }
+int64_t orc_subcell_len(const orc_volume *v) { return v->sc_len; }
+const float *orc_subcell_points(const orc_volume *v) { return v->sc_pnt; }
+const uint16_t *orc_subcell_points_fp16(const orc_volume *v) { return v->sc_q; }
+const uint16_t *orc_subcell_vel_fp16(const orc_volume *v) { return v->sc_qvel; }

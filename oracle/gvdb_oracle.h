@@ -91,6 +91,12 @@ int orc_update_apron_faces(orc_volume *v, int chan);
 int orc_insert_points_subcell(orc_volume *v, int sc, orc_view pos, int n, float radius, const float trans[3], int *len);
 int orc_gather_density(orc_volume *v, int sc, float radius, int chan, int accum);
 int orc_gather_level_set(orc_volume *v, int sc, float radius, int chan, int accum);
+/* InsertPointsSubcell_FP16 (V:5094-5189), GatherLevelSet_FP16 (V:5375-5402),
+ * GetMinMaxVel (V:5469-5521); vel.base == NULL: no velocity lists. */
+int orc_insert_points_subcell_fp16(orc_volume *v, int sc, orc_view pos, orc_view vel, int n, float radius,
+                                   const float trans[3], int *len);
+int orc_gather_level_set_fp16(orc_volume *v, int sc, float radius, int chan);
+int orc_get_min_max_vel(orc_volume *v, orc_view vel, int n);
 
 /* Kernel splats (no reference counterpart; specified mathematically).
  * channel chans[c] := sum_p weight_p * attr_c(p) * W(v + 0.5 - x_p) over the
@@ -129,6 +135,11 @@ int64_t orc_subcell_count(const orc_volume *v);
 const int32_t *orc_subcell_cnt(const orc_volume *v);
 const int32_t *orc_subcell_nid(const orc_volume *v);
 const int32_t *orc_subcell_pos(const orc_volume *v);
+const int32_t *orc_subcell_off(const orc_volume *v);
+int64_t orc_subcell_len(const orc_volume *v);
+const float *orc_subcell_points(const orc_volume *v);
+const uint16_t *orc_subcell_points_fp16(const orc_volume *v);
+const uint16_t *orc_subcell_vel_fp16(const orc_volume *v);
 int64_t orc_leaf_of_point(const orc_volume *v, float x, float y, float z);
 
 #ifdef __cplusplus

@@ -67,6 +67,9 @@ def lib():
             "orc_insert_points_subcell": (i32, [vp, i32, _View, i32, f32, fp, ip]),
             "orc_gather_density": (i32, [vp, i32, f32, i32, i32]),
             "orc_gather_level_set": (i32, [vp, i32, f32, i32, i32]),
+            "orc_insert_points_subcell_fp16": (i32, [vp, i32, _View, _View, i32, f32, fp, ip]),
+            "orc_gather_level_set_fp16": (i32, [vp, i32, f32, i32]),
+            "orc_get_min_max_vel": (i32, [vp, _View, i32]),
             "orc_scatter_kernel": (i32, [vp, i32, _View, i32, fp, _View, f32, vp, ip, i32]),
             "orc_gather_kernel": (i32, [vp, i32, _View, i32, fp, ip, i32, dp]),
             "orc_scatter_kernel_backward": (i32, [vp, i32, _View, i32, fp, _View, f32, vp, ip, i32, ip, dp, dp, dp]),
@@ -93,6 +96,11 @@ def lib():
             "orc_subcell_cnt": (vp, [vp]),
             "orc_subcell_nid": (vp, [vp]),
             "orc_subcell_pos": (vp, [vp]),
+            "orc_subcell_off": (vp, [vp]),
+            "orc_subcell_len": (i64, [vp]),
+            "orc_subcell_points": (vp, [vp]),
+            "orc_subcell_points_fp16": (vp, [vp]),
+            "orc_subcell_vel_fp16": (vp, [vp]),
             "orc_leaf_of_point": (i64, [vp, f32, f32, f32]),
         }
         for name, (res, args) in sig.items():
@@ -213,6 +221,24 @@ class Oracle:
 
     def gather_level_set(self, sc, radius, chan, accum=False):
         _check(self.L.orc_gather_level_set(self.h, sc, float(radius), chan, 1 if accum else 0), "gather_level_set")
+
+    def insert_points_subcell_fp16(self, sc, pos, radius, trans=(0, 0, 0), vel=None):
+        pos = np.ascontiguousarray(pos, dtype=np.float32)
+        vv = _View(None, 0, 0, 0)
+        if vel is not None:
+            vel = np.ascontiguousarray(vel, dtype=np.float32)
+            vv = view(vel)
+        ln = ctypes.c_int32(0)
+        _check(self.L.orc_insert_points_subcell_fp16(self.h, sc, view(pos), vv, pos.shape[0], float(radius),
+                                                     _f3(trans), ctypes.byref(ln)), "insert_points_subcell_fp16")
+        return ln.value
+
+    def gather_level_set_fp16(self, sc, radius, chan):
+        _check(self.L.orc_gather_level_set_fp16(self.h, sc, float(radius), chan), "gather_level_set_fp16")
+
+    def get_min_max_vel(self, vel):
+        vel = np.ascontiguousarray(vel, dtype=np.float32)
+        _check(self.L.orc_get_min_max_vel(self.h, view(vel), vel.shape[0]), "get_min_max_vel")
 
     def _attr_views(self, attrs, nch):
         arr = (_View * nch)()
@@ -370,6 +396,24 @@ class Oracle:
             return np.frombuffer(buf, np.int32, cnt).copy()
         return (arr(self.L.orc_subcell_cnt(self.h), m), arr(self.L.orc_subcell_nid(self.h), m),
                 arr(self.L.orc_subcell_pos(self.h), 3 * m).reshape(m, 3))
+
+    def subcell_lists(self):
+        """Offsets per subcell and the list entries: float xyz, or quantized
+        (uint16 xyz, uint16 velocity or None) after an FP16 insert."""
+        m = int(self.L.orc_subcell_count(self.h))
+        ln = int(self.L.orc_subcell_len(self.h))
+        off = np.frombuffer((ctypes.c_char * (4 * m)).from_address(self.L.orc_subcell_off(self.h)), np.int32).copy()
+
+        def arr(ptr, dtype, width):
+            if not ptr or ln == 0:
+                return None
+            n = ln * 3
+            return np.frombuffer((ctypes.c_char * (n * width)).from_address(ptr), dtype, n).copy().reshape(ln, 3)
+        pts = arr(self.L.orc_subcell_points(self.h), np.float32, 4)
+        if pts is not None:
+            return off, pts
+        return off, arr(self.L.orc_subcell_points_fp16(self.h), np.uint16, 2), \
+            arr(self.L.orc_subcell_vel_fp16(self.h), np.uint16, 2)
 
     def leaf_of_point(self, x, y, z):
         return int(self.L.orc_leaf_of_point(self.h, x, y, z))

@@ -147,7 +147,9 @@ struct RefVolume {
     DevArr scan_a1, scan_s1, scan_a2, scan_s2;
     DevArr pnode, poff, gcnt;
     DevArr sc_flag, sc_map, sc_cnt, sc_pre, sc_pnt, sc_pos, sc_nid, nbr;
+    DevArr sc_q; // ushort3 entries of InsertPointsSubcell_FP16
     int num_sc = 0, sc_size = 0, sc_len = 0;
+    bool sc_fp16 = false; // the last subcell insert was the FP16 one
     std::vector<int> nbr_host;
 
     int res(int l) const { return 1 << logdim[l]; }
@@ -694,8 +696,9 @@ int update_apron_faces(RefVolume *v, int chan) {
     return 0;
 }
 
-// InsertPointsSubcell (V:4971-5083) without velocities and colours
-int insert_points_subcell(RefVolume *v, int sc, int n, float radius, float3 trans, int *out_len) {
+// InsertPointsSubcell (V:4971-5083) and InsertPointsSubcell_FP16
+// (V:5094-5189) without velocities and colours
+int insert_points_subcell(RefVolume *v, int sc, int n, float radius, float3 trans, int *out_len, bool fp16) {
     *out_len = 0;
     int num_brick = (int)v->used_leaves;
     if (num_brick == 0) return 0;
@@ -722,11 +725,28 @@ int insert_points_subcell(RefVolume *v, int sc, int n, float radius, float3 tran
     v->sc_size = sc;
     v->num_sc = num_sc;
     v->sc_len = len;
+    v->sc_fp16 = fp16;
     if (len == 0) return 0;
-    if (v->sc_cnt.ensure((size_t)num_sc * 4, true) || v->sc_pnt.ensure((size_t)len * 12, false)) return -1;
-    gvdbInsertSubcell<<<n / 512 + 1, 512>>>(v->d_info, sc, per_brick, n, (int *)v->sc_cnt.p, (int *)v->sc_pre.p,
-                                            (int *)v->sc_map.p, range, trans, sc_dim, radius, v->pos.p, 0, 12,
-                                            (float3 *)v->sc_pnt.p, nullptr, 0, 0, nullptr, nullptr, 0, 0, nullptr);
+    if (v->sc_cnt.ensure((size_t)num_sc * 4, true)) return -1;
+    if (fp16) {
+        // mPosMin / mPosRange of the last GetBoundingBox; mVelMin / mVelRange
+        // are not used without velocities
+        if (v->sc_q.ensure((size_t)len * 6, false)) return -1;
+        const float3 pmin = make_float3(v->posmin[0], v->posmin[1], v->posmin[2]);
+        const float3 prange = make_float3(v->posmax[0] - v->posmin[0], v->posmax[1] - v->posmin[1],
+                                          v->posmax[2] - v->posmin[2]);
+        const float3 zero = make_float3(0.0f, 0.0f, 0.0f);
+        gvdbInsertSubcell_fp16<<<n / 512 + 1, 512>>>(v->d_info, sc, per_brick, n, (int *)v->sc_cnt.p,
+                                                     (int *)v->sc_pre.p, (int *)v->sc_map.p, pmin, prange, zero, zero,
+                                                     range, trans, sc_dim, radius, v->pos.p, 0, 12,
+                                                     (ushort3 *)v->sc_q.p, nullptr, 0, 0, nullptr, nullptr, 0, 0,
+                                                     nullptr);
+    } else {
+        if (v->sc_pnt.ensure((size_t)len * 12, false)) return -1;
+        gvdbInsertSubcell<<<n / 512 + 1, 512>>>(v->d_info, sc, per_brick, n, (int *)v->sc_cnt.p, (int *)v->sc_pre.p,
+                                                (int *)v->sc_map.p, range, trans, sc_dim, radius, v->pos.p, 0, 12,
+                                                (float3 *)v->sc_pnt.p, nullptr, 0, 0, nullptr, nullptr, 0, 0, nullptr);
+    }
     if (v->sc_pos.ensure((size_t)num_sc * 12, false) || v->sc_nid.ensure((size_t)num_sc * 4, false)) return -1;
     gvdbCalcSubcellPos<<<nmap / 512 + 1, 512>>>(v->d_info, (int *)v->sc_nid.p, (int3 *)v->sc_pos.p, nmap, sc_dim,
                                                 per_brick, sc, (int *)v->sc_map.p);
@@ -736,6 +756,7 @@ int insert_points_subcell(RefVolume *v, int sc, int n, float radius, float3 tran
 
 // GatherDensity / GatherLevelSet (V:5318-5373) without colours
 int gather(RefVolume *v, bool levelset, int n, float radius, int chan, bool accum) {
+    if (v->sc_fp16) return -4; // the lists hold ushort3 entries
     if (v->used_leaves == 0 || v->num_sc == 0) return 0;
     if (!levelset && v->sc_len == 0) return 0;
     if (prepare_vdb(v)) return -1;
@@ -748,6 +769,23 @@ int gather(RefVolume *v, bool levelset, int n, float radius, int chan, bool accu
         gvdbGatherDensity<<<v->num_sc, block>>>(v->d_info, n, v->num_sc, radius, (int *)v->sc_nid.p, (int *)v->sc_cnt.p,
                                                 (int *)v->sc_pre.p, (int3 *)v->sc_pos.p, (float3 *)v->sc_pnt.p, nullptr,
                                                 nullptr, chan, 0, accum);
+    RD_CHECK(cudaGetLastError());
+    return 0;
+}
+
+// GatherLevelSet_FP16 (V:5375-5402) without colours
+int gather_level_set_fp16(RefVolume *v, int n, float radius, int chan) {
+    if (!v->sc_fp16 && v->sc_len) return -4; // the lists hold float3 entries
+    if (v->used_leaves == 0 || v->num_sc == 0) return 0;
+    if (prepare_vdb(v)) return -1;
+    const float3 pmin = make_float3(v->posmin[0], v->posmin[1], v->posmin[2]);
+    const float3 prange = make_float3(v->posmax[0] - v->posmin[0], v->posmax[1] - v->posmin[1],
+                                      v->posmax[2] - v->posmin[2]);
+    const float3 zero = make_float3(0.0f, 0.0f, 0.0f);
+    dim3 block(v->sc_size, v->sc_size, v->sc_size);
+    gvdbGatherLevelSet_fp16<<<v->num_sc, block>>>(v->d_info, n, v->num_sc, radius, pmin, prange, zero, zero,
+                                                   (int *)v->sc_nid.p, (int *)v->sc_cnt.p, (int *)v->sc_pre.p,
+                                                   (int3 *)v->sc_pos.p, (ushort3 *)v->sc_q.p, nullptr, nullptr, chan, 0);
     RD_CHECK(cudaGetLastError());
     return 0;
 }
@@ -937,7 +975,34 @@ RD_API int rd_update_apron_faces(void *h, int chan) {
 RD_API int rd_insert_points_subcell(void *h, int sc, int n, float radius, const float trans[3], int *out_len) {
     RefVolume *v = (RefVolume *)h;
     if (sc <= 0 || v->res(0) % sc || sc * sc * sc > 1024) return -4;
-    int rc = insert_points_subcell(v, sc, n, radius, make_float3(trans[0], trans[1], trans[2]), out_len);
+    int rc = insert_points_subcell(v, sc, n, radius, make_float3(trans[0], trans[1], trans[2]), out_len, false);
+    if (rc) return rc;
+    RD_CHECK(cudaDeviceSynchronize());
+    return 0;
+}
+
+RD_API int rd_insert_points_subcell_fp16(void *h, int sc, int n, float radius, const float trans[3], int *out_len) {
+    RefVolume *v = (RefVolume *)h;
+    if (sc <= 0 || v->res(0) % sc || sc * sc * sc > 1024) return -4;
+    int rc = insert_points_subcell(v, sc, n, radius, make_float3(trans[0], trans[1], trans[2]), out_len, true);
+    if (rc) return rc;
+    RD_CHECK(cudaDeviceSynchronize());
+    return 0;
+}
+
+// the ushort3 entries of the FP16 lists, grouped by subcell like rd_copy_subcells
+RD_API int rd_copy_subcells_fp16(void *h, unsigned short *q, long long max_pnts) {
+    RefVolume *v = (RefVolume *)h;
+    if (v->sc_len > max_pnts) return -2;
+    if (!v->sc_fp16 || v->sc_q.bytes < (size_t)v->sc_len * 6) return -4;
+    if (v->sc_len) RD_CHECK(cudaMemcpy(q, v->sc_q.p, (size_t)v->sc_len * 6, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+RD_API int rd_gather_level_set_fp16(void *h, int n, float radius, int chan) {
+    RefVolume *v = (RefVolume *)h;
+    if (chan >= v->nchan) return -4;
+    int rc = gather_level_set_fp16(v, n, radius, chan);
     if (rc) return rc;
     RD_CHECK(cudaDeviceSynchronize());
     return 0;
@@ -953,7 +1018,9 @@ RD_API int rd_copy_subcells(void *h, int *cnt, int *off, int *nid, float *pnts, 
         RD_CHECK(cudaMemcpy(off, v->sc_pre.p, (size_t)v->num_sc * 4, cudaMemcpyDeviceToHost));
         RD_CHECK(cudaMemcpy(nid, v->sc_nid.p, (size_t)v->num_sc * 4, cudaMemcpyDeviceToHost));
     }
-    if (v->sc_len) RD_CHECK(cudaMemcpy(pnts, v->sc_pnt.p, (size_t)v->sc_len * 12, cudaMemcpyDeviceToHost));
+    // the float3 list only when the last insert wrote one
+    if (v->sc_len && !v->sc_fp16 && v->sc_pnt.bytes >= (size_t)v->sc_len * 12)
+        RD_CHECK(cudaMemcpy(pnts, v->sc_pnt.p, (size_t)v->sc_len * 12, cudaMemcpyDeviceToHost));
     return 0;
 }
 

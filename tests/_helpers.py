@@ -9,6 +9,22 @@ UNDEF64 = np.uint64(0xFFFFFFFFFFFFFFFF)
 REL_TOL = 1e-5
 
 
+def fp16_level_set_tol(pts, ref, units=0):
+    """Largest difference allowed between level sets gathered from 16-bit
+    subcell lists: two float spacings at the largest coordinate -- the
+    dequantized position q / 65535 * range + min is rounded to a float of
+    that magnitude, and the approximate division of a --use_fast_math build
+    rounds it differently from an exact one -- plus `units` quantization
+    steps (entries that may differ by that many units: an exact division
+    against an approximate one) plus REL_TOL of the values."""
+    import numpy as np
+    lo = np.maximum(pts.min(0) - 1.0, 0.0)  # the bounding box the entries are quantized over
+    hi = np.maximum(pts.max(0) + 2.0, 0.0)
+    step = float((hi - lo).max()) / 65535.0
+    return (2.0 * float(np.spacing(np.float32(np.abs(pts).max()))) + units * step +
+            REL_TOL * float(np.abs(ref).max()))
+
+
 def rel_err(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)

@@ -74,6 +74,9 @@ def cases():
              pts=[_box(300, 13, 100.0, 1400.0)], ops=["topology", "atlas", "insert"]),
         dict(name="deep_r0", cfg=(3, 3, 3, 3, 3), apron=1, chans=1, radius=0.0,
              pts=[_box(400, 14, 100.0, 5000.0)], ops=["topology", "atlas", "insert"]),
+        dict(name="blob_fp16", cfg=(3, 3, 3, 3, 3), apron=1, chans=1, radius=2.0,
+             pts=[_shell(800, 15, (511.7, 512.2, 512.9), 4.0, 24.0)],
+             ops=["topology", "atlas", "subcell_fp16", "levelset_fp16", "apron_levelset_fp16"]),
     ]
 
 
@@ -144,6 +147,9 @@ class Ref:
             "rd_copy_subcells": (i32, [vp, vp, vp, vp, vp, i64, i64]),
             "rd_gather_density": (i32, [vp, i32, f32, i32, i32]),
             "rd_gather_level_set": (i32, [vp, i32, f32, i32, i32]),
+            "rd_insert_points_subcell_fp16": (i32, [vp, i32, i32, f32, fp, ip]),
+            "rd_copy_subcells_fp16": (i32, [vp, vp, i64]),
+            "rd_gather_level_set_fp16": (i32, [vp, i32, f32, i32]),
             "rd_get_counts": (i32, [vp, vp]), "rd_copy_nodes": (i32, [vp, i32, vp, i64]),
             "rd_copy_childlists": (i32, [vp, i32, vp, i64]), "rd_copy_atlas_map": (i32, [vp, vp, i64]),
             "rd_copy_atlas_tiles": (i32, [vp, i32, vp, i64]),
@@ -273,6 +279,30 @@ def run_case(case, device):
         if "density" in ops:
             R("rd_gather_density", n, DENSITY["radius"], DENSITY["chan"], 0)
             out["tiles_density"] = R.tiles(DENSITY["chan"], slots, t)
+        if "subcell_fp16" in ops:
+            ln = ctypes.c_int(0)
+            R("rd_insert_points_subcell_fp16", SUBCELL["size"], n, SUBCELL["radius"], zero, ctypes.byref(ln))
+            per = (res[0] // SUBCELL["size"]) ** 3
+            m = per * int(cnt[5])
+            sc_cnt = np.zeros(m, np.int32)
+            sc_off = np.zeros(m, np.int32)
+            sc_nid = np.zeros(m, np.int32)
+            unused = np.zeros((1, 3), np.float32)  # the float lists are not written by the 16-bit insert
+            R("rd_copy_subcells", sc_cnt.ctypes.data, sc_off.ctypes.data, sc_nid.ctypes.data, unused.ctypes.data,
+              m, ln.value)
+            q = np.zeros((max(ln.value, 1), 3), np.uint16)
+            R("rd_copy_subcells_fp16", q.ctypes.data, len(q))
+            for s in range(m):  # order inside one subcell follows atomics
+                a, b = sc_off[s], sc_off[s] + sc_cnt[s]
+                blk = q[a:b]
+                q[a:b] = blk[np.lexsort(blk.T[::-1])]
+            out.update(sc16_len=ln.value, sc16_cnt=sc_cnt, sc16_off=sc_off, sc16_nid=sc_nid, sc16_q=q[:ln.value])
+        if "levelset_fp16" in ops:
+            R("rd_gather_level_set_fp16", n, LEVELSET["radius"], LEVELSET["chan"])
+            out["tiles_levelset_fp16"] = R.tiles(LEVELSET["chan"], slots, t)
+        if "apron_levelset_fp16" in ops:
+            R("rd_update_apron", LEVELSET["chan"], APRON_LEVELSET_BOUND)
+            out["tiles_apron_levelset_fp16"] = R.tiles(LEVELSET["chan"], slots, t)
     finally:
         R.close()
     return out
@@ -283,8 +313,11 @@ def main():
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--check-only", action="store_true", help="run the CPU input checks and exit")
+    ap.add_argument("--only", default=None, help="generate this case only")
     a = ap.parse_args()
     for case in cases():
+        if a.only and case["name"] != a.only:
+            continue
         if a.check_only:
             print(case["name"], "depths", check_inputs(case))
             continue

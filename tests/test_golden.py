@@ -8,8 +8,13 @@ same sequences through libgvdb2's C-ABI.
 Equality rules:
   - topology, atlas assignment, neighbour table, point->brick assignment and
     subcell lists are compared bit for bit;
+  - the 16-bit subcell entries of InsertPointsSubcell_FP16 too, for libgvdb2,
+    which quantizes with the same approximate division as the reference's
+    --use_fast_math build; the oracle divides exactly (IEEE), so an entry
+    may differ from the reference's by one unit there;
   - float channels are compared within REL_TOL. The reference is built with
-    --use_fast_math.
+    --use_fast_math. Level sets from 16-bit lists also allow two float
+    spacings at the coordinates' magnitude (fp16_level_set_tol).
   - the reference leaves two things undefined, so only their defined part is
     compared:
       - the brick coordinates of unused atlas-map entries;
@@ -22,7 +27,7 @@ import numpy as np
 import pytest
 
 import make_golden as mg
-from _helpers import REL_TOL, assert_nodes_equal, interior, rel_err
+from _helpers import REL_TOL, assert_nodes_equal, fp16_level_set_tol, interior, rel_err
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = {c["name"]: c for c in mg.cases()}
@@ -51,6 +56,17 @@ def assert_atlas_map_equal(got, want):
     assert np.array_equal(got["mLeafID"], want["mLeafID"])
     used = want["mLeafID"] >= 0
     assert np.array_equal(got["mPos"][used], want["mPos"][used])
+
+
+def sort_groups(entries, off, cnt, by_column=False):
+    """Entries of each subcell list in lexicographic order, or each column
+    sorted on its own (entries that may differ by one unit can swap places
+    in a lexicographic order; per column, sorting keeps |a - b| <= 1)."""
+    out = entries.copy()
+    for a, c in zip(off.tolist(), cnt.tolist()):
+        blk = out[a:a + c]
+        out[a:a + c] = np.sort(blk, axis=0) if by_column else blk[np.lexsort(blk.T[::-1])]
+    return out
 
 
 def assert_poff_permutation(pnode, poff):
@@ -90,6 +106,8 @@ class Steps:
         assert run.atlas_slots() == int(g["counts_atlas"][6])
         assert_nodes_equal(run.nodes(0), g["nodes0_atlas"], 0)
         assert_atlas_map_equal(run.atlas_map(), g["atlas_map"])
+        if "subcell_fp16" in self.ops:
+            self.check_fp16(run)
         if "insert" not in self.ops:
             return
         for c in range(self.case["chans"]):
@@ -120,7 +138,27 @@ class Steps:
         assert rel_err(interior(run.tiles(1), 1), interior(g["tiles_density"], 1)) <= REL_TOL
 
 
+    def check_fp16(self, run):
+        g = self.g
+        ln = run.subcell_fp16(self.pts)
+        assert ln == int(g["sc16_len"])
+        cnt, nid = run.subcell_lists(len(g["sc16_cnt"]))
+        assert np.array_equal(cnt, g["sc16_cnt"]) and np.array_equal(nid, g["sc16_nid"])
+        by_column = run.Q16_TOL > 0
+        q = sort_groups(run.fp16_entries(ln), g["sc16_off"], g["sc16_cnt"], by_column)
+        ref = sort_groups(g["sc16_q"], g["sc16_off"], g["sc16_cnt"], by_column)
+        diff = np.abs(q.astype(np.int32) - ref.astype(np.int32))
+        assert diff.max() <= run.Q16_TOL, f"16-bit entries differ by up to {diff.max()}"
+        run.levelset_fp16(ln)
+        want = interior(g["tiles_levelset_fp16"], 1)
+        tol = fp16_level_set_tol(self.pts, want, run.Q16_TOL)
+        assert np.abs(interior(run.tiles(0), 1) - want).max() <= tol
+        run.apron(mg.LEVELSET["chan"], mg.APRON_LEVELSET_BOUND)
+        assert np.abs(run.tiles(0) - g["tiles_apron_levelset_fp16"]).max() <= tol
+
+
 class OracleRun:
+    Q16_TOL = 1  # exact division against the reference's approximate one
     def __init__(self, oracle_mod, case):
         self.o = oracle_mod.Oracle()
         self.o.configure(*case["cfg"])
@@ -168,6 +206,15 @@ class OracleRun:
     def density(self, ln):
         self.o.gather_density(mg.SUBCELL["size"], mg.DENSITY["radius"], mg.DENSITY["chan"])
 
+    def subcell_fp16(self, pts):
+        return self.o.insert_points_subcell_fp16(mg.SUBCELL["size"], pts, mg.SUBCELL["radius"])
+
+    def fp16_entries(self, ln):
+        return self.o.subcell_lists()[1]
+
+    def levelset_fp16(self, ln):
+        self.o.gather_level_set_fp16(mg.SUBCELL["size"], mg.LEVELSET["radius"], mg.LEVELSET["chan"])
+
 
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_oracle_matches_reference(oracle_mod, name):
@@ -175,6 +222,8 @@ def test_oracle_matches_reference(oracle_mod, name):
 
 
 class GpuRun:
+    Q16_TOL = 0
+
     def __init__(self, gvdb2_mod, case):
         self.v = gvdb2_mod.VolumeGVDB(0)
         self.v.Configure(*case["cfg"])
@@ -259,6 +308,16 @@ class GpuRun:
     def density(self, ln):
         self.v.GatherDensity(mg.SUBCELL["size"], len(self._t), mg.DENSITY["radius"], (0, 0, 0), ln,
                              mg.DENSITY["chan"])
+
+    def subcell_fp16(self, pts):
+        return self.v.InsertPointsSubcell_FP16(mg.SUBCELL["size"], len(pts), mg.SUBCELL["radius"])
+
+    def fp16_entries(self, ln):
+        return self.v.subcell_points_fp16(ln)
+
+    def levelset_fp16(self, ln):
+        self.v.GatherLevelSet_FP16(mg.SUBCELL["size"], len(self._t), mg.LEVELSET["radius"], (0, 0, 0), ln,
+                                   mg.LEVELSET["chan"])
 
 
 @pytest.mark.gpu
