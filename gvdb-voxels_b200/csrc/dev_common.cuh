@@ -179,7 +179,9 @@ __device__ __forceinline__ void cell_coords(int64_t cell, int m, int m3, int64_t
 // them).  Light cells are listed apart (light[0 .. cnt[2])).  The gather
 // stages a halo tile per huge or heavy cell and reads the taps of light
 // cells' points straight from the atlas, one warp per light cell; the
-// splat's own phase takes all three classes (order of own_cell_at).
+// splat's own phase likewise gives a huge or heavy cell a CTA and a light
+// cell a warp.  Every cell with points has a partial, indexed by its rank
+// among those cells in cell order (cell_ext).
 constexpr uint32_t kHeavyCell = 1024;
 constexpr uint32_t kLightCell = 32;
 // The i-th huge or heavy cell, or -1 past their end.
@@ -188,15 +190,6 @@ __device__ __forceinline__ int64_t cell_at(int64_t i, const int32_t *list, const
     if (i < h) return list[i];
     i -= h;
     return i < (int64_t)cnt[1] ? list[ncell - 1 - i] : -1;
-}
-// The i-th cell of the splat's own order: the huge and heavy cells (order of
-// cell_at), then the light ones; -1 past the end.
-__device__ __forceinline__ int64_t own_cell_at(int64_t i, const int32_t *list, const int32_t *light,
-                                               const uint32_t *cnt, int64_t ncell) {
-    const int64_t hh = (int64_t)cnt[0] + cnt[1];
-    if (i < hh) return cell_at(i, list, cnt, ncell);
-    i -= hh;
-    return i < (int64_t)cnt[2] ? (int64_t)light[i] : -1;
 }
 // cell of a voxel inside its brick (local voxel coordinates in [0, res0))
 __device__ __forceinline__ int cell_of_local(int lx, int ly, int lz, int m) {

@@ -157,10 +157,11 @@ struct Volume {
     // kernel-splat binning
     DevBuf pbin, prank, bin_cnt, bin_off, perm;
     // cells that hold points: huge and heavy ones (order of cell_at), light
-    // ones, each cell's index in the splat's own order (-1 if empty), the
-    // three counts, each cell's 27 neighbour indices (cell_nbr); heavy_grid,
+    // ones, each cell's partial index (rank among the cells with points, in
+    // cell order; -1 if empty), the three counts, each cell's 27 neighbour
+    // partial indices (cell_nbr), scan scratch (cell_rank); heavy_grid,
     // light_grid and cell_grid bound the huge+heavy, light and all lists
-    DevBuf cell_list, cell_light, cell_ext, cell_cnt, cell_nbr;
+    DevBuf cell_list, cell_light, cell_ext, cell_cnt, cell_nbr, cell_rank;
     int64_t cell_grid = 0, heavy_grid = 0, light_grid = 0;
     struct BinKey {
         bool valid = false;

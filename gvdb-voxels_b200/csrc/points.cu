@@ -114,17 +114,21 @@ __global__ void k_cell_list(const uint32_t *off, int64_t ncell, int32_t *list, i
     }
 }
 
-// ext[cell] = the cell's index in the splat's own order (own_cell_at);
-// ext was set to -1
-__global__ void k_cell_ext(const int32_t *list, const int32_t *light, const uint32_t *cnt, int64_t ncell,
-                           int32_t *ext) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ncell) return;
-    const int64_t c = own_cell_at(i, list, light, cnt, ncell);
-    if (c >= 0) ext[c] = (int32_t)i;
+// flag[cell] = 1 if the cell holds points
+__global__ void k_cell_flags(const uint32_t *off, int64_t ncell, uint32_t *flag) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < ncell) flag[c] = off[c + 1] > off[c] ? 1u : 0u;
 }
 
-// nbr[cell * 27 + d] = the own-order index of neighbour cell d = (dz+1)*9 +
+// ext[cell] = the cell's partial index: its rank among the cells that hold
+// points, in cell order (so neighbouring cells' partials lie close together
+// whatever order the own phase runs them in); -1 if it holds none
+__global__ void k_cell_ext(const uint32_t *off, const uint32_t *rank, int64_t ncell, int32_t *ext) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < ncell) ext[c] = off[c + 1] > off[c] ? (int32_t)rank[c] : -1;
+}
+
+// nbr[cell * 27 + d] = the partial index of neighbour cell d = (dz+1)*9 +
 // (dy+1)*3 + (dx+1) of the cell (its partial in the splat), -1 if it holds
 // no points or lies outside the active bricks.
 __global__ void k_cell_nbrs(int64_t ncell, const int32_t *nbr27, const int32_t *ext, int m, int m3, int32_t *nbr) {
@@ -352,14 +356,17 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     GV_CUDA(v, v->cell_ext.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
     GV_CUDA(v, v->cell_cnt.ensure(sizeof(uint32_t) * 4, s));
     GV_CUDA(v, cudaMemsetAsync(v->cell_cnt.p, 0, sizeof(uint32_t) * 4, s));
-    GV_CUDA(v, cudaMemsetAsync(v->cell_ext.p, 0xFF, sizeof(int32_t) * (size_t)nbins, s));
+
     v->cell_grid = v->heavy_grid = v->light_grid = 0;
     if (nbins > 0) {
         const int g = grid_for(nbins, 256, 1ll << 31);
         k_cell_list<<<g, 256, 0, s>>>(v->bin_off.as<uint32_t>(), nbins, v->cell_list.as<int32_t>(),
                                       v->cell_light.as<int32_t>(), v->cell_cnt.as<uint32_t>());
-        k_cell_ext<<<g, 256, 0, s>>>(v->cell_list.as<int32_t>(), v->cell_light.as<int32_t>(),
-                                     v->cell_cnt.as<uint32_t>(), nbins, v->cell_ext.as<int32_t>());
+        GV_CUDA(v, v->cell_rank.ensure(sizeof(uint32_t) * 2 * (size_t)(nbins + 1), s));
+        uint32_t *flag = v->cell_rank.as<uint32_t>(), *rank = flag + nbins + 1;
+        k_cell_flags<<<g, 256, 0, s>>>(v->bin_off.as<uint32_t>(), nbins, flag);
+        GV_TRY(exclusive_scan_u32(v, flag, rank, nbins));
+        k_cell_ext<<<g, 256, 0, s>>>(v->bin_off.as<uint32_t>(), rank, nbins, v->cell_ext.as<int32_t>());
         GV_CUDA(v, cudaGetLastError());
         // each cell's 27 neighbour partials, for the merge
         GV_CUDA(v, v->cell_nbr.ensure(sizeof(int32_t) * 27 * (size_t)nbins, s));

@@ -301,8 +301,8 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
     int32_t *pb = reinterpret_cast<int32_t *>(pa + NCH);
     __shared__ double inv_s[NCH];
     __shared__ int32_t amax_bits[NCH]; // max |weighted amount| of the cell's points, as float bits
-    // the blockIdx.x-th cell that holds points; its partial goes to ext[blockIdx.x]
-    // the blockIdx.x-th huge or heavy cell (light cells: k_scatter_own_light)
+    // the blockIdx.x-th huge or heavy cell (light cells: k_scatter_own_light);
+    // its partial goes to ext[cell_ext[cell]]
     const int64_t cell = cell_at(blockIdx.x, S.cell_list, S.cell_cnt, S.ncell);
     if (cell < 0) return;
     int64_t slot;
@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
     // advances by the base-E digits of 256 instead of being divided out
     constexpr int E = X::E, DZ = kOwnThreads / (E * E), DY = (kOwnThreads / E) % E, DX = kOwnThreads % E;
     static_assert(DZ < E, "one wrap per step");
-    float *dst = ext + (int64_t)blockIdx.x * NCH * X::E3;
+    float *dst = ext + (int64_t)S.cell_ext[cell] * NCH * X::E3;
     int c = 0, z = threadIdx.x / (E * E), y = (threadIdx.x / E) % E, x = threadIdx.x % E;
     for (int i = threadIdx.x; i < NCH * X::E3; i += kOwnThreads) {
         const int k = c * X::CS + z * X::PS + y * X::RS + x;
@@ -520,8 +520,7 @@ __global__ void __launch_bounds__(32 * kLightWarps) k_scatter_own_light(SplatArg
             pa[c * 32 + lane] = ok ? (((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt) : 0.0f;
     }
     __syncwarp();
-    // own-order index of this light cell: after the huge and heavy cells
-    float *dst = ext + ((int64_t)S.cell_cnt[0] + S.cell_cnt[1] + w) * NCH * E3;
+    float *dst = ext + (int64_t)S.cell_ext[cell] * NCH * E3;
     // taps of a point per lane: cubic, lane = (tx, ty, z pair) with two taps;
     // tent, lanes 0-7 = (tx, ty, tz)
     const int tx = N == 4 ? (lane & 3) : (lane & 1), ty = N == 4 ? ((lane >> 2) & 3) : ((lane >> 1) & 1);
@@ -549,46 +548,38 @@ __global__ void __launch_bounds__(32 * kLightWarps) k_scatter_own_light(SplatArg
     }
 }
 
-// Phase 2 (k_scatter_merge): one thread per interior voxel of every cell,
-// with no shared memory or barrier, so that the SM keeps as many voxels in
-// flight as its registers allow.  Voxel v sums, in a fixed order, the
-// partials of the cells whose extended tile covers it: its own cell and,
-// within H of a face, the neighbours across it (per axis d = 0 and e = -1
-// or +1, never both, H <= 4), looked up in the cell's 27-entry neighbour
-// table.  The up to 8 partials are read first (predicated), then summed.
-// A launch merges channels [c0, c0 + CC) of the NCH-channel partials (all
-// of them: two launches of two channels each measured slower on the sparse
-// scene and no faster on the dense one).
-template <int KERNEL, int NCH, int CC>
-__global__ void __launch_bounds__(256) k_scatter_merge(SplatArgs S, const float *ext, int c0) {
+// Phase 2 (k_scatter_merge / k_scatter_merge_cta): voxel v of a cell sums,
+// in a fixed order, the partials of the cells whose extended tile covers
+// it: its own cell and, within H of a face, the neighbours across it (per
+// axis d = 0 and e = -1 or +1, never both, H <= 4), looked up in the cell's
+// 27-entry neighbour table.  The up to 8 partials are read first
+// (predicated), then summed, and the channel is written once.
+template <int KERNEL, int NCH>
+__device__ __forceinline__ void merge_voxel(const SplatArgs &S, const float *ext, const int32_t *ne, int64_t cell,
+                                            int v) {
     using X = ExtTile<KERNEL>;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t cell = i >> 9;
-    if (cell >= S.ncell) return;
-    const int v = (int)(i & 511);
     const int vx = v & 7, vy = (v >> 3) & 7, vz = v >> 6;
-    const int32_t *ne = S.cell_nbr + cell * 27;
     const int ex = vx < X::H ? -1 : (vx >= 8 - X::H ? 1 : 0);
     const int ey = vy < X::H ? -1 : (vy >= 8 - X::H ? 1 : 0);
     const int ez = vz < X::H ? -1 : (vz >= 8 - X::H ? 1 : 0);
-    float part[8][CC];
+    float part[8][NCH];
 #pragma unroll
     for (int m = 0; m < 8; m++) {
         const int dx = (m & 1) ? ex : 0, dy = (m & 2) ? ey : 0, dz = (m & 4) ? ez : 0;
         const bool used = (!(m & 1) || ex) && (!(m & 2) || ey) && (!(m & 4) || ez);
-        const int32_t e = used ? __ldg(ne + (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)) : -1;
+        const int32_t e = used ? ne[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] : -1;
         const int ux = vx - 8 * dx + X::H, uy = vy - 8 * dy + X::H, uz = vz - 8 * dz + X::H;
-        const float *src = ext + ((int64_t)(e >= 0 ? e : 0) * NCH + c0) * X::E3 + (uz * X::E + uy) * X::E + ux;
+        const float *src = ext + (int64_t)(e >= 0 ? e : 0) * NCH * X::E3 + (uz * X::E + uy) * X::E + ux;
 #pragma unroll
-        for (int c = 0; c < CC; c++) part[m][c] = e >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
+        for (int c = 0; c < NCH; c++) part[m][c] = e >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
     }
-    float acc[CC];
+    float acc[NCH];
 #pragma unroll
-    for (int c = 0; c < CC; c++) acc[c] = 0.0f;
+    for (int c = 0; c < NCH; c++) acc[c] = 0.0f;
 #pragma unroll
     for (int m = 0; m < 8; m++)
 #pragma unroll
-        for (int c = 0; c < CC; c++) acc[c] += part[m][c];
+        for (int c = 0; c < NCH; c++) acc[c] += part[m][c];
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
@@ -596,8 +587,30 @@ __global__ void __launch_bounds__(256) k_scatter_merge(SplatArgs S, const float 
     const int Lx = kCell * cx + vx, Ly = kCell * cy + vy, Lz = kCell * cz + vz; // voxel in the brick
     const int64_t at = slot * S.tvox + ((int64_t)(Lz + a) * tl + (Ly + a)) * tl + (Lx + a);
 #pragma unroll
-    for (int c = 0; c < CC; c++)
-        if (c0 + c < S.nch) S.chan[c0 + c][at] = acc[c];
+    for (int c = 0; c < NCH; c++)
+        if (c < S.nch) S.chan[c][at] = acc[c];
+}
+
+// Thread per voxel (sparse volumes): no shared memory or barrier, as many
+// voxels in flight as the registers allow; the neighbour row is read
+// through L1.
+template <int KERNEL, int NCH>
+__global__ void __launch_bounds__(256) k_scatter_merge(SplatArgs S, const float *ext) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t cell = i >> 9;
+    if (cell >= S.ncell) return;
+    merge_voxel<KERNEL, NCH>(S, ext, S.cell_nbr + cell * 27, cell, (int)(i & 511));
+}
+
+// CTA per cell (dense volumes, where nearly every cell has partials): the
+// neighbour row staged once in shared memory.
+template <int KERNEL, int NCH>
+__global__ void __launch_bounds__(512) k_scatter_merge_cta(SplatArgs S, const float *ext) {
+    __shared__ int32_t ne[27];
+    const int64_t cell = blockIdx.x;
+    if (threadIdx.x < 27) ne[threadIdx.x] = S.cell_nbr[cell * 27 + threadIdx.x];
+    __syncthreads();
+    merge_voxel<KERNEL, NCH>(S, ext, ne, cell, threadIdx.x);
 }
 
 
@@ -883,7 +896,10 @@ gvdb2_status scatter_group(Volume *v, const SplatArgs &S) {
     GV_TRY(launch_smem(v, k1l, smem_l, "scatter"));
     if (v->light_grid > 0)
         k1l<<<(unsigned)((v->light_grid + kLightWarps - 1) / kLightWarps), 32 * kLightWarps, smem_l, s>>>(S, ext);
-    k_scatter_merge<KERNEL, NCH, NCH><<<(unsigned)(S.ncell * 2), 256, 0, s>>>(S, ext, 0);
+    if (4 * nown >= 3 * S.ncell) // dense: most cells hold points
+        k_scatter_merge_cta<KERNEL, NCH><<<(unsigned)S.ncell, 512, 0, s>>>(S, ext);
+    else
+        k_scatter_merge<KERNEL, NCH><<<(unsigned)(S.ncell * 2), 256, 0, s>>>(S, ext);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
