@@ -220,7 +220,7 @@ struct SplatArgs {
 // The kernels work on cells, 8^3 blocks of a brick (the brick itself for
 // 8^3 bricks).
 // Phase 1 (k_scatter_own): one CTA per cell of more than kLightCell points
-// (k_scatter_own_light: one warp per lighter cell) splats only the points
+// (own_light, in the same launch: one warp per lighter cell) splats only the points
 // binned to it, with unclipped stencils, into an extended tile
 // that covers every tap of those points: [-H, 8+H)^3 with H = N/2 (12^3 for
 // the cubic B-spline, 10^3 for the tent).  The tile is then written out as
@@ -289,7 +289,7 @@ __device__ __forceinline__ void fixed_add(int32_t *hi_acc, int32_t *lo_acc, int 
 }
 
 template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float *ext) {
+__device__ __forceinline__ void own_heavy(const SplatArgs &S, float *ext, int64_t block) {
     using T = Taps<KERNEL>;
     using X = ExtTile<KERNEL>;
     constexpr int N = T::N;
@@ -301,9 +301,9 @@ __global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float 
     int32_t *pb = reinterpret_cast<int32_t *>(pa + NCH);
     __shared__ double inv_s[NCH];
     __shared__ int32_t amax_bits[NCH]; // max |weighted amount| of the cell's points, as float bits
-    // the blockIdx.x-th huge or heavy cell (light cells: k_scatter_own_light);
-    // its partial goes to ext[cell_ext[cell]]
-    const int64_t cell = cell_at(blockIdx.x, S.cell_list, S.cell_cnt, S.ncell);
+    // the block-th huge or heavy cell (light cells: own_light); its partial
+    // goes to ext[cell_ext[cell]]
+    const int64_t cell = cell_at(block, S.cell_list, S.cell_cnt, S.ncell);
     if (cell < 0) return;
     int64_t slot;
     int cx, cy, cz;
@@ -466,7 +466,7 @@ constexpr size_t own_light_smem_bytes() {
 }
 
 template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(32 * kLightWarps) k_scatter_own_light(SplatArgs S, float *ext) {
+__device__ __forceinline__ void own_light(const SplatArgs &S, float *ext, int64_t block) {
     using T = Taps<KERNEL>;
     using X = ExtTile<KERNEL>;
     constexpr int N = T::N, E = X::E, E3 = X::E3;
@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(32 * kLightWarps) k_scatter_own_light(SplatArg
     int32_t *pbase = reinterpret_cast<int32_t *>(stage); // packed first tap (x | y << 8 | z << 16)
     float *pw = stage + 32;                              // pw[k * 32 + j]: weight k (x taps, y taps, z taps)
     float *pa = pw + 3 * N * 32;                         // pa[c * 32 + j]: amount of channel c
-    const int64_t w = (int64_t)blockIdx.x * kLightWarps + warp;
+    const int64_t w = block * kLightWarps + warp;
     if (w >= (int64_t)S.cell_cnt[2]) return;
     const int64_t cell = S.cell_light[w];
     const uint32_t beg = S.bin_off[cell], cnt = min(S.bin_off[cell + 1] - beg, 32u); // light: <= 32
@@ -546,6 +546,16 @@ __global__ void __launch_bounds__(32 * kLightWarps) k_scatter_own_light(SplatArg
         for (int i = lane; i < E3 / 4; i += 32) d4[i] = t4[i];
         __syncwarp();
     }
+}
+
+// Phase 1 in one launch: blocks [0, heavy_blocks) take a huge or heavy cell
+// each, the rest kLightWarps light cells each (kOwnThreads = 32 *
+// kLightWarps), so the light cells run beside the heavy ones.
+static_assert(kOwnThreads == 32 * kLightWarps, "one block size for both kinds of cell");
+template <int KERNEL, int NCH>
+__global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float *ext, int64_t heavy_blocks) {
+    if ((int64_t)blockIdx.x < heavy_blocks) own_heavy<KERNEL, NCH>(S, ext, blockIdx.x);
+    else own_light<KERNEL, NCH>(S, ext, blockIdx.x - heavy_blocks);
 }
 
 // Phase 2 (k_scatter_merge / k_scatter_merge_cta): voxel v of a cell sums,
@@ -745,7 +755,7 @@ __device__ __forceinline__ void gather_point(const GatherArgs &G, int32_t pidx, 
 }
 
 template <int KERNEL, int MODE, int NCH>
-__global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
+__device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t block) {
     constexpr int H = Taps<KERNEL>::N / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *tile = reinterpret_cast<float *>(smem_raw);
@@ -753,7 +763,7 @@ __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
     // one CTA per 8^3 cell of a brick: the cell plus its halo is staged
     constexpr int ht = kCell + 2 * H, ht3 = ht * ht * ht;
     const int res = G.res0;
-    const int64_t cell = G.cell_list ? cell_at(blockIdx.x, G.cell_list, G.cell_cnt, G.ncell) : (int64_t)blockIdx.x;
+    const int64_t cell = G.cell_list ? cell_at(block, G.cell_list, G.cell_cnt, G.ncell) : block;
     if (cell < 0) return;
     const uint32_t beg = G.bin_off[cell], end = G.bin_off[cell + 1];
     if (beg == end) return; // no points: nothing to stage
@@ -792,9 +802,9 @@ __global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
 // cell holds at most kLightCell = 32), taps read straight from the atlas; a
 // staged halo would cost 12^3 floats per channel for a few points.
 template <int KERNEL, int MODE, int NCH>
-__global__ void __launch_bounds__(256) k_gather_light(GatherArgs G) {
+__device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t block) {
     constexpr int H = Taps<KERNEL>::N / 2;
-    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t w = (block * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= (int64_t)G.cell_cnt[2]) return;
     const int64_t cell = G.cell_light[w];
@@ -819,6 +829,19 @@ __global__ void __launch_bounds__(256) k_gather_light(GatherArgs G) {
     };
     gather_point<KERNEL, MODE, NCH>(G, G.perm[beg + lane], nd.mPos[0] + fx0, nd.mPos[1] + fy0, nd.mPos[2] + fz0,
                                     fetch);
+}
+
+// Two launches: a halo tile per huge or heavy cell (every cell, in cell
+// order, when no cell list is given), then the light cells, a warp each.
+// One fused launch measured slower: the light path's registers (66) halved
+// the tiles' occupancy.
+template <int KERNEL, int MODE, int NCH>
+__global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
+    gather_tile_cell<KERNEL, MODE, NCH>(G, blockIdx.x);
+}
+template <int KERNEL, int MODE, int NCH>
+__global__ void __launch_bounds__(256) k_gather_light(GatherArgs G) {
+    gather_light_cells<KERNEL, MODE, NCH>(G, blockIdx.x);
 }
 
 // Points outside every active brick: gathers and gradients are zero.
@@ -887,15 +910,11 @@ gvdb2_status scatter_group(Volume *v, const SplatArgs &S) {
     const int64_t nown = v->cell_grid;
     GV_CUDA(v, v->scratch.ensure(sizeof(float) * (size_t)nown * NCH * X::E3 + 256, s));
     float *ext = v->scratch.as<float>();
-    constexpr size_t smem = own_smem_bytes<KERNEL, NCH>();
+    constexpr size_t smem = std::max(own_smem_bytes<KERNEL, NCH>(), own_light_smem_bytes<KERNEL, NCH>());
     auto k1 = k_scatter_own<KERNEL, NCH>;
     GV_TRY(launch_smem(v, k1, smem, "scatter"));
-    if (v->heavy_grid > 0) k1<<<(unsigned)v->heavy_grid, kOwnThreads, smem, s>>>(S, ext);
-    constexpr size_t smem_l = own_light_smem_bytes<KERNEL, NCH>();
-    auto k1l = k_scatter_own_light<KERNEL, NCH>;
-    GV_TRY(launch_smem(v, k1l, smem_l, "scatter"));
-    if (v->light_grid > 0)
-        k1l<<<(unsigned)((v->light_grid + kLightWarps - 1) / kLightWarps), 32 * kLightWarps, smem_l, s>>>(S, ext);
+    const int64_t own_blocks = v->heavy_grid + (v->light_grid + kLightWarps - 1) / kLightWarps;
+    if (own_blocks > 0) k1<<<(unsigned)own_blocks, kOwnThreads, smem, s>>>(S, ext, v->heavy_grid);
     if (4 * nown >= 3 * S.ncell) // dense: most cells hold points
         k_scatter_merge_cta<KERNEL, NCH><<<(unsigned)S.ncell, 512, 0, s>>>(S, ext);
     else
@@ -947,9 +966,11 @@ gvdb2_status launch_gather(Volume *v, const GatherArgs &G) {
     const size_t smem = sizeof(float) * (size_t)NCH * ht * ht * ht;
     auto k = k_gather_tile<KERNEL, MODE, NCH>;
     GV_TRY(launch_smem(v, k, smem, "gather"));
-    const int64_t grid = G.cell_list ? v->heavy_grid : G.ncell;
-    if (grid > 0) k<<<(unsigned)grid, 256, smem, v->stream>>>(G);
-    if (G.cell_list && v->light_grid > 0) // light cells: a warp each
+    // tiles for the huge and heavy cells, then the light cells, a warp each
+    // (every cell gets a tile when the caller supplied the binning)
+    const int64_t heavy = G.cell_list ? v->heavy_grid : G.ncell;
+    if (heavy > 0) k<<<(unsigned)heavy, 256, smem, v->stream>>>(G);
+    if (G.cell_list && v->light_grid > 0)
         k_gather_light<KERNEL, MODE, NCH><<<(unsigned)((v->light_grid + 7) / 8), 256, 0, v->stream>>>(G);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
