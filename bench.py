@@ -432,8 +432,9 @@ def run_ours(a):
         stages[k] = {"ms": round(stage_ms.get(k, 0.0), 4), "alg_bytes": sb[k], "GBps": gbs}
     dom = max(("scatter", "gather", "apron"), key=lambda k: stage_ms.get(k, 0.0))
     achieved = sb[dom] / (stage_ms[dom] / 1e3) / 1e9
-    kernel_name = {"scatter": "scatter stage: k_absmax + k_scatter_own<cubic,4> + k_scatter_merge<cubic,4>",
-                   "gather": "k_gather_tile<cubic,fwd,3>", "apron": "k_apron"}[dom]
+    kernel_name = {"scatter": "scatter stage: k_scatter_own<cubic,4> (heavy and light cells) + "
+                              "k_scatter_merge_cta<cubic,4>",
+                   "gather": "k_gather_tile<cubic,fwd,3> + k_gather_light<cubic,fwd,3>", "apron": "k_apron"}[dom]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": TRAFFIC_PER_BRICK[dom] * geo["B"] if dom in TRAFFIC_PER_BRICK else None,
                 "kernel": kernel_name, "peak_source": peak_kind,

@@ -160,6 +160,43 @@ gvdb2_status gvdb2_configure(gvdb2_volume *h, int q4, int q3, int q2, int q1, in
     return GVDB2_OK;
 }
 
+gvdb2_status gvdb2_set_transform(gvdb2_volume *h, const float pretrans[3], const float scale[3], const float angs[3],
+                                 const float trans[3]) {
+    CHECK_HANDLE(h);
+    Volume *v = VOL(h);
+    if (!pretrans || !scale || !angs || !trans) return gvdb2::fail(v, GVDB2_ERR_ARG, "null transform part");
+    for (int a = 0; a < 3; a++) {
+        v->xf_pretrans[a] = pretrans[a];
+        v->xf_scale[a] = scale[a];
+        v->xf_angs[a] = angs[a];
+        v->xf_trans[a] = trans[a];
+    }
+    return GVDB2_OK;
+}
+
+gvdb2_status gvdb2_get_transform(gvdb2_volume *h, float pretrans[3], float scale[3], float angs[3], float trans[3]) {
+    CHECK_HANDLE(h);
+    Volume *v = VOL(h);
+    if (!pretrans || !scale || !angs || !trans) return gvdb2::fail(v, GVDB2_ERR_ARG, "null transform part");
+    for (int a = 0; a < 3; a++) {
+        pretrans[a] = v->xf_pretrans[a];
+        scale[a] = v->xf_scale[a];
+        angs[a] = v->xf_angs[a];
+        trans[a] = v->xf_trans[a];
+    }
+    return GVDB2_OK;
+}
+
+gvdb2_status gvdb2_save_vbx(gvdb2_volume *h, const char *path) {
+    CHECK_HANDLE(h);
+    return gvdb2::save_vbx(VOL(h), path);
+}
+
+gvdb2_status gvdb2_load_vbx(gvdb2_volume *h, const char *path) {
+    CHECK_HANDLE(h);
+    return gvdb2::load_vbx(VOL(h), path);
+}
+
 gvdb2_status gvdb2_set_channel_default(gvdb2_volume *h, int cx, int cy, int cz) {
     CHECK_HANDLE(h);
     if (cx < 1 || cy < 1 || cz < 1) return gvdb2::fail(VOL(h), GVDB2_ERR_ARG, "bad axis counts");

@@ -98,6 +98,9 @@ struct Volume {
     int nlev = 0;
     int logdim[kMaxLev] = {0};
     int default_axiscnt[3] = {16, 16, 1}; // SetChannelDefault(16,16,1), V:2348
+    // grid transform (SetTransform, V:5770; default V:77): kept and written
+    // to VBX files, not applied by the point path
+    float xf_pretrans[3] = {0, 0, 0}, xf_angs[3] = {0, 0, 0}, xf_scale[3] = {1, 1, 1}, xf_trans[3] = {0, 0, 0};
 
     // channels / atlas
     bool has_chan[kMaxChan] = {false};
@@ -239,6 +242,11 @@ gvdb2_status radix_sort_u64(Volume *v, uint64_t *keys, int32_t *vals, int64_t n,
 // ---- topology.cu ----
 gvdb2_status rebuild_topology(Volume *v, int n, float radius, const float orig[3], bool accumulate, int min_depth);
 gvdb2_status update_atlas(Volume *v);
+gvdb2_status alloc_channel_storage(Volume *v, int chan);
+gvdb2_status pool_reserve(Volume *v, int lev, int64_t cnt);
+gvdb2_status adopt_pools(Volume *v, int depth);
+gvdb2_status save_vbx(Volume *v, const char *path);
+gvdb2_status load_vbx(Volume *v, const char *path);
 gvdb2_status update_neighbors(Volume *v);
 gvdb2_status clear_channel(Volume *v, int chan);
 gvdb2_status sync_counts(Volume *v);

@@ -250,7 +250,46 @@ struct ExtTile {
     static constexpr int PS = N == 4 ? E * E + 8 : E * E; // plane stride: 152 puts a warp's 32 taps in 32 banks
     static constexpr int CS = E * PS;               // channel stride
     static constexpr int E3 = E * E * E;            // floats per channel in the global partial
+    // Position in the global partial of extended-tile voxel (ux, uy, uz) in
+    // [0, E)^3.  Per channel the partial holds 27 regions: the cell's 8^3
+    // interior first, then the halo beyond each face, edge and corner d in
+    // {-1,0,1}^3 (z-major order of d), each z-major with extent 8 along the
+    // axes where d is 0 and H where it is not.  The merge so reads whole
+    // 32-byte-aligned rows of the interior (8 floats) and packed rows of
+    // the halos, instead of 8 floats straddling two sectors of a 12-float
+    // row.  Region d starts, in the plain z-major order of the regions, at
+    // start_z E^2 + s_z start_y E + s_z s_y start_x, with start and s the
+    // region's first extended coordinate and extent along each axis.
+    __host__ __device__ static constexpr int part_index(int ux, int uy, int uz) {
+        const int dx = ux < H ? -1 : (ux >= 8 + H ? 1 : 0), dy = uy < H ? -1 : (uy >= 8 + H ? 1 : 0),
+                  dz = uz < H ? -1 : (uz >= 8 + H ? 1 : 0);
+        const int sx0 = dx < 0 ? 0 : (dx == 0 ? H : 8 + H), sy0 = dy < 0 ? 0 : (dy == 0 ? H : 8 + H),
+                  sz0 = dz < 0 ? 0 : (dz == 0 ? H : 8 + H);
+        const int ex = dx == 0 ? 8 : H, ey = dy == 0 ? 8 : H, ez = dz == 0 ? 8 : H;
+        const int local = ((uz - sz0) * ey + (uy - sy0)) * ex + (ux - sx0);
+        if ((dx | dy | dz) == 0) return local; // interior
+        const int r = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+        const int start = sz0 * E * E + ez * sy0 * E + ez * ey * sx0;
+        return 512 + start - (r > 13 ? 512 : 0) + local;
+    }
 };
+// The inverse of part_index: the extended-tile voxel (x | y << 4 | z << 8)
+// of each partial position, so that the own phase writes its partial in
+// order (coalesced) and looks the tile up.
+template <int KERNEL>
+struct PartMap {
+    uint16_t xyz[ExtTile<KERNEL>::E3];
+    constexpr PartMap() : xyz() {
+        constexpr int E = ExtTile<KERNEL>::E;
+        for (int z = 0; z < E; z++)
+            for (int y = 0; y < E; y++)
+                for (int x = 0; x < E; x++)
+                    xyz[ExtTile<KERNEL>::part_index(x, y, z)] = (uint16_t)(x | (y << 4) | (z << 8));
+    }
+};
+template <int KERNEL>
+__device__ constexpr PartMap<KERNEL> kPartMap{};
+
 constexpr int kOwnThreads = 256;
 constexpr int kOwnChunk = 128; // points staged per pass
 
@@ -429,23 +468,22 @@ __device__ __forceinline__ void own_heavy(const SplatArgs &S, float *ext, int64_
         }
     }
     __syncthreads();
-    // thread t writes elements t, t+256, ... (coalesced); its (c, z, y, x)
-    // advances by the base-E digits of 256 instead of being divided out
-    constexpr int E = X::E, DZ = kOwnThreads / (E * E), DY = (kOwnThreads / E) % E, DX = kOwnThreads % E;
-    static_assert(DZ < E, "one wrap per step");
+    // thread t writes partial positions t, t+256, ... (coalesced) of
+    // channel c, looking their tile voxel up in kPartMap
+    static_assert(kOwnThreads < X::E3, "one channel step per iteration");
     float *dst = ext + (int64_t)S.cell_ext[cell] * NCH * X::E3;
-    int c = 0, z = threadIdx.x / (E * E), y = (threadIdx.x / E) % E, x = threadIdx.x % E;
+    int c = 0, j = threadIdx.x;
     for (int i = threadIdx.x; i < NCH * X::E3; i += kOwnThreads) {
-        const int k = c * X::CS + z * X::PS + y * X::RS + x;
+        const int q = kPartMap<KERNEL>.xyz[j];
+        const int k = c * X::CS + (q >> 8) * X::PS + ((q >> 4) & 15) * X::RS + (q & 15);
         // |sum| < 2^53: exact in double; the power-of-two scaling is exact
         const long long sum = ((long long)acc_hi[k] << L) + (long long)acc_lo[k];
         dst[i] = (float)((double)sum * inv_s[c]);
-        x += DX;
-        if (x >= E) { x -= E; y++; }
-        y += DY;
-        if (y >= E) { y -= E; z++; }
-        z += DZ;
-        if (z >= E) { z -= E; c++; }
+        j += kOwnThreads;
+        if (j >= X::E3) {
+            j -= X::E3;
+            c++;
+        }
     }
 }
 
@@ -542,8 +580,11 @@ __device__ __forceinline__ void own_light(const SplatArgs &S, float *ext, int64_
             }
             __syncwarp();
         }
-        float4 *d4 = reinterpret_cast<float4 *>(dst + c * E3);
-        for (int i = lane; i < E3 / 4; i += 32) d4[i] = t4[i];
+        float *dc = dst + c * E3;
+        for (int i = lane; i < E3; i += 32) {
+            const int q = kPartMap<KERNEL>.xyz[i];
+            dc[i] = tile[((q >> 8) * E + ((q >> 4) & 15)) * E + (q & 15)];
+        }
         __syncwarp();
     }
 }
@@ -579,7 +620,7 @@ __device__ __forceinline__ void merge_voxel(const SplatArgs &S, const float *ext
         const bool used = (!(m & 1) || ex) && (!(m & 2) || ey) && (!(m & 4) || ez);
         const int32_t e = used ? ne[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] : -1;
         const int ux = vx - 8 * dx + X::H, uy = vy - 8 * dy + X::H, uz = vz - 8 * dz + X::H;
-        const float *src = ext + (int64_t)(e >= 0 ? e : 0) * NCH * X::E3 + (uz * X::E + uy) * X::E + ux;
+        const float *src = ext + (int64_t)(e >= 0 ? e : 0) * NCH * X::E3 + X::part_index(ux, uy, uz);
 #pragma unroll
         for (int c = 0; c < NCH; c++) part[m][c] = e >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
     }

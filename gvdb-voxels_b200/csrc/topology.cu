@@ -1630,5 +1630,51 @@ gvdb2_status incremental_activate(Volume *v, int n, float radius, const float or
 
 } // namespace
 
+// LoadVBX: room for `cnt` nodes (and their child lists) at level `lev`.
+gvdb2_status pool_reserve(Volume *v, int lev, int64_t cnt) { return ensure_pool(v, lev, cnt); }
+
+// LoadVBX (FinishTopology, V:636): the pools were filled from a file.
+// Derive what a rebuild leaves besides them: depth and root position, the
+// leaf map of the linked leaves and the used-leaf count.  The next
+// RebuildTopology starts over, as after Configure.
+gvdb2_status adopt_pools(Volume *v, int depth) {
+    cudaStream_t s = v->stream;
+    if (!v->dev_small.p) {
+        GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), s));
+        GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
+    }
+    Node root;
+    GV_CUDA(v, cudaMemcpy(&root, v->pool[depth].p, sizeof(Node), cudaMemcpyDeviceToHost));
+    v->depth = depth;
+    v->cur_depth = depth;
+    for (int a = 0; a < 3; a++) {
+        v->root_pos[a] = root.mPos[a];
+        v->posmin[a] = v->posmax[a] = 0.0f; // no bounding box in the file
+    }
+    const KeyGeom g = key_geom(v);
+    uint32_t lcap = next_pow2((uint64_t)std::max<int64_t>(2 * v->pool_cnt[0], 1 << 12));
+    GV_CUDA(v, v->leafmap_keys.ensure(sizeof(uint64_t) * lcap, s));
+    GV_CUDA(v, v->leafmap_vals.ensure(sizeof(int32_t) * lcap, s));
+    GV_CUDA(v, cudaMemsetAsync(v->leafmap_keys.p, 0xFF, sizeof(uint64_t) * lcap, s));
+    v->leafmap_mask = lcap - 1;
+    GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count, 0, sizeof(int32_t) * 8 + sizeof(int32_t), s));
+    if (v->pool_cnt[0] > 0)
+        k_leafmap_fill<<<grid_for(v->pool_cnt[0], 256, 1ll << 31), 256, 0, s>>>(
+            v->pool_ptr(0), v->pool_cnt[0], g, v->leafmap_keys.as<uint64_t>(), v->leafmap_vals.as<int32_t>(),
+            v->leafmap_mask, dev_words(v)->count, &dev_words(v)->status);
+    GV_CUDA(v, cudaGetLastError());
+    GV_TRY(read_words(v));
+    if (host_words(v)->status & kDevHashFull) return fail(v, GVDB2_ERR_CAPACITY, "leaf map overflow");
+    v->used_leaves = host_words(v)->count[0];
+    for (int l = 0; l < kMaxLev; l++) v->lev_count[l][0] = v->lev_count[l][1] = 0;
+    v->lev_count[0][0] = v->pool_cnt[0];
+    v->rebuild_topo = true;
+    v->topo_version++;
+    v->bin_key.valid = false;
+    v->nbr6_valid = false;
+    v->atlas_valid = false;
+    v->atlas_last = 0;
+    return GVDB2_OK;
+}
 
 } // namespace gvdb2

@@ -8,6 +8,7 @@ column of a 2-D tensor for per-point attributes.  PyTorch only supplies
 device memory and streams; all work runs in libgvdb2's CUDA kernels.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -160,6 +161,25 @@ class VolumeGVDB:
     def ScatterDensity(self, num_pnts, radius, amp, trans=(0, 0, 0), expand=True, avgColor=False):
         self._check(self._L.gvdb2_scatter_density(self._h, int(num_pnts), float(radius), float(amp), _f3(trans),
                                                   1 if expand else 0, 1 if avgColor else 0), "ScatterDensity")
+
+    def SetTransform(self, pretrans, scale, angs, trans):
+        """Grid transform (SetTransform, V:5770); stored in VBX files."""
+        self._check(self._L.gvdb2_set_transform(self._h, _f3(pretrans), _f3(scale), _f3(angs), _f3(trans)),
+                    "SetTransform")
+
+    def GetTransform(self):
+        """(pretrans, scale, angs, trans) as tuples."""
+        parts = [(ctypes.c_float * 3)() for _ in range(4)]
+        self._check(self._L.gvdb2_get_transform(self._h, *parts), "GetTransform")
+        return tuple(tuple(float(x) for x in p) for p in parts)
+
+    def SaveVBX(self, fname):
+        """Writes the volume as a VBX file (V:1626-1768)."""
+        self._check(self._L.gvdb2_save_vbx(self._h, os.fsencode(fname)), "SaveVBX")
+
+    def LoadVBX(self, fname):
+        """Replaces the volume with a VBX file's (V:507-685)."""
+        self._check(self._L.gvdb2_load_vbx(self._h, os.fsencode(fname)), "LoadVBX")
 
     def InsertPointsSubcell_FP16(self, subcell_size, num_pnts, radius, trans=(0, 0, 0)):
         """InsertPointsSubcell with 16-bit list entries (V:5094-5189); returns the list length."""

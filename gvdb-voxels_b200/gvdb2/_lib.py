@@ -68,6 +68,10 @@ _SIGS = {
     "gvdb2_insert_points_subcell": [_vp, _i32, _i32, _f32, _fp, _ip],
     "gvdb2_insert_points_subcell_fp16": [_vp, _i32, _i32, _f32, _fp, _ip],
     "gvdb2_get_min_max_vel": [_vp, _i32],
+    "gvdb2_set_transform": [_vp, _fp, _fp, _fp, _fp],
+    "gvdb2_get_transform": [_vp, _fp, _fp, _fp, _fp],
+    "gvdb2_save_vbx": [_vp, ctypes.c_char_p],
+    "gvdb2_load_vbx": [_vp, ctypes.c_char_p],
     "gvdb2_gather_level_set_fp16": [_vp, _i32, _i32, _f32, _fp, _ip, _i32, _i32],
     "gvdb2_scatter_density": [_vp, _i32, _f32, _f32, _fp, _i32, _i32],
     "gvdb2_gather_density": [_vp, _i32, _i32, _f32, _fp, _ip, _i32, _i32, _i32],

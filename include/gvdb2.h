@@ -93,6 +93,24 @@ GVDB2_API gvdb2_status gvdb2_set_option(gvdb2_volume *v, int option, int value);
 GVDB2_API gvdb2_status gvdb2_configure(gvdb2_volume *v, int q4, int q3, int q2, int q1, int q0);   /* Configure, VH:387 / V:2364-2377 */
 GVDB2_API gvdb2_status gvdb2_set_channel_default(gvdb2_volume *v, int cx, int cy, int cz);       /* SetChannelDefault, VH:390 */
 GVDB2_API gvdb2_status gvdb2_add_channel(gvdb2_volume *v, int chan, int dtype, int apron);       /* AddChannel, VH:392 / V:2437-2453 */
+/* Grid transform (SetTransform, V:5770; default pre-translation 0, scale 1,
+ * angles 0, translation 0, V:77): kept and stored in VBX files; the point
+ * path works in index space and does not apply it. */
+GVDB2_API gvdb2_status gvdb2_set_transform(gvdb2_volume *v, const float pretrans[3], const float scale[3],
+                                 const float angs[3], const float trans[3]);
+GVDB2_API gvdb2_status gvdb2_get_transform(gvdb2_volume *v, float pretrans[3], float scale[3], float angs[3],
+                                 float trans[3]);
+
+/* ---- VBX files (GVDB_FILESPEC.txt) ---- */
+/* SaveVBX (V:1626-1768): version 1.11, one grid of float channels in atlas
+ * layout with the GVDB topology, byte for byte as the reference writes it
+ * (the grid name is written as zeros). */
+GVDB2_API gvdb2_status gvdb2_save_vbx(gvdb2_volume *v, const char *path);
+/* LoadVBX (V:507-685): replaces the configuration, topology and channels
+ * with the file's, then assigns the atlas (UpdateAtlas) and fills it.
+ * Files with node bitmasks, other data types, compression, brick layout or
+ * other than 5 levels return GVDB2_ERR_UNSUPPORTED. */
+GVDB2_API gvdb2_status gvdb2_load_vbx(gvdb2_volume *v, const char *path);
 
 /* ---- points (SetPoints VH:541 / V:4900-4908) ---- */
 GVDB2_API gvdb2_status gvdb2_set_points(gvdb2_volume *v, gvdb2_points_view pos, gvdb2_points_view vel, gvdb2_points_view clr);

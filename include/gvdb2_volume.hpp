@@ -127,6 +127,16 @@ class VolumeGVDB {
         check(gvdb2_gather_level_set_fp16(v_, subcell_size, num_pnts, radius, t, &pSCPntsLength, chanLevelSet, chanClr),
               "GatherLevelSet_FP16");
     }
+    void SetTransform(Vec3F pretrans, Vec3F scal, Vec3F angs, Vec3F trans) {
+        const float p[3] = {pretrans.x, pretrans.y, pretrans.z}, s[3] = {scal.x, scal.y, scal.z},
+                    a[3] = {angs.x, angs.y, angs.z}, t[3] = {trans.x, trans.y, trans.z};
+        check(gvdb2_set_transform(v_, p, s, a, t), "SetTransform");
+    }
+    void SaveVBX(const std::string &fname) { check(gvdb2_save_vbx(v_, fname.c_str()), "SaveVBX"); }
+    bool LoadVBX(const std::string &fname) {
+        check(gvdb2_load_vbx(v_, fname.c_str()), "LoadVBX");
+        return true;
+    }
     void UpdateApron() { check(gvdb2_update_apron(v_, -1, 0.0f), "UpdateApron"); }
     void UpdateApron(unsigned char chan, float boundval = 0.0f) {
         check(gvdb2_update_apron(v_, chan, boundval), "UpdateApron");
