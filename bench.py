@@ -438,7 +438,7 @@ def run_ours(a):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": TRAFFIC_PER_BRICK[dom] * geo["B"] if dom in TRAFFIC_PER_BRICK else None,
                 "kernel": kernel_name, "peak_source": peak_kind,
-                "traffic_source": "ncu capture of a 2,097,152-point block, scaled by bricks"}
+                "traffic_source": "ncu capture of the 4,194,304-point block, scaled by bricks"}
 
     # end to end through the public API: every step copies its inputs from
     # pinned host memory and reads its gathered velocities back.  Two device
@@ -473,12 +473,12 @@ def run_ours(a):
 
 
 # DRAM bytes (read + write) per brick of each stage's kernels, from the ncu
-# capture of a 2,097,152-point block larger than L2 (11,016 bricks; summary in
-# profiles/k_scatter_own_merge_gather_dam2m.md).  Traffic grows with the brick
+# capture of the 4,194,304-point block (23,396 bricks; summary in
+# profiles/k_scatter_own_merge_gather_dam4m.md).  Traffic grows with the brick
 # count, so a launch moves about this many bytes x bricks.
 TRAFFIC_PER_BRICK = {
-    "scatter": (59.4e6 + 244.3e6 + 556.0e6 + 116.3e6) / 11016,
-    "gather": (159.9e6 + 21.2e6) / 11016,
+    "scatter": (192.7e6 + 407.5e6 + 754.4e6 + 220.1e6) / 23396,
+    "gather": (614.7e6 + 44.2e6 + 3.3e6 + 0.0) / 23396,
 }
 
 
