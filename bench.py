@@ -390,11 +390,8 @@ def run_ours(a):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        from gvdb2 import shard
+        return shard.max_over_ranks(x, device=f"cuda:{local}")
 
     # the sampler starts before the warm-up (its start-up stays out of the
     # timed region) and keeps sampling until the timed steps are done
@@ -502,17 +499,31 @@ def batched_step(v, K, n, chans_fwd, grad_chan, go):
 
 
 def run_batched(a):
+    """The 64 clouds in one batched pass against a per-cloud loop.  Under
+    torchrun the clouds are spread over the ranks (LPT by size, no data-path
+    collective); each rank batches its own share and the time is the max
+    over the ranks."""
     import numpy as np
     import torch
     import gvdb2
     import gvdb2.workloads as wl
-    clouds, _ = wl.batched_clouds()
+    from gvdb2 import shard
+    env = shard.RankEnv.from_env()
+    torch.cuda.set_device(env.local)
+    if env.world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    all_clouds, _ = wl.batched_clouds()
+    mine = shard.lpt_partition([len(c) for c in all_clouds], env.world)[env.rank]
+    clouds = [all_clouds[i] for i in mine]
     dev = [torch.from_numpy(c).cuda() for c in clouds]
     total = sum(len(c) for c in clouds)
+    job_total = sum(len(c) for c in all_clouds)
     K = gvdb2.KERNEL_CUBIC2
 
     def volume():
-        v = gvdb2.VolumeGVDB(0)
+        v = gvdb2.VolumeGVDB(env.local)
         v.Configure(3, 3, 3, 3, 3)
         for c in range(2):
             v.AddChannel(c, gvdb2.T_FLOAT, 1)
@@ -542,15 +553,19 @@ def run_batched(a):
         for _ in range(max(1, a.warmup)):
             f()
         torch.cuda.synchronize()
+        if env.world > 1:
+            dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(steps):
             f()
         e1.record()
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps
+        if env.world > 1:
+            dist.barrier()
+        return shard.max_over_ranks(e0.elapsed_time(e1) / steps, device=f"cuda:{env.local}")
 
-    clocks = Clocks(0)
+    clocks = Clocks(env.local)
     clocks.start()
     ms_b = timed(step_batched, a.steps)
     ms_l = timed(step_loop, max(1, a.steps // 4))
@@ -561,13 +576,20 @@ def run_batched(a):
     step_loop()
     same = all(bool(torch.equal(gob[0][first[c]:first[c + 1]], gol[c][0])) and
                bool(torch.equal(gob[2][first[c]:first[c + 1]], gol[c][2])) for c in range(len(clouds)))
-    line = {"metric": METRIC, "workload": f"batched: {len(clouds)} Gaussian clouds, {total} points, sizes log-uniform "
-            "in [1e4, 2e6], each in its own 1024^3 space; cubic B-spline r=2, density; forward + adjoint",
-            "value": total / (ms_b / 1e3), "unit": "points/s", "ms_per_step": ms_b,
-            "per_cloud_loop": {"value": total / (ms_l / 1e3), "ms_per_step": ms_l},
-            "speedup_vs_loop": ms_l / ms_b, "identical_to_loop": same, "n_gpus": 1, "steps": a.steps,
-            "data": "synthetic", "dtype": "f32", "clocks": clk}
-    print(json.dumps(line), flush=True)
+    same = shard.max_over_ranks(0.0 if same else 1.0, device=f"cuda:{env.local}") == 0.0
+    if env.rank == 0:
+        line = {"metric": METRIC, "workload": f"batched: {len(all_clouds)} Gaussian clouds, {job_total} points, sizes "
+                "log-uniform in [1e4, 2e6], each in its own 1024^3 space; cubic B-spline r=2, density; "
+                "forward + adjoint",
+                "value": job_total / (ms_b / 1e3), "unit": "points/s", "ms_per_step": ms_b,
+                "per_cloud_loop": {"value": job_total / (ms_l / 1e3), "ms_per_step": ms_l},
+                "speedup_vs_loop": ms_l / ms_b, "identical_to_loop": same, "n_gpus": env.world,
+                "scaling": "strong", "parallelism": f"clouds over {env.world} ranks (LPT by size)",
+                "steps": a.steps, "data": "synthetic", "dtype": "f32", "clocks": clk}
+        print(json.dumps(line), flush=True)
+    del vb, vl
+    if env.world > 1:
+        dist.destroy_process_group()
     return 0
 
 
