@@ -367,7 +367,7 @@ __device__ __forceinline__ void own_heavy(const SplatArgs &S, float *ext, int64_
         // a binned point lies in the brick, so its first taps are in [0, 8];
         // anything else (inconsistent input) is dropped, never written outside the tile
         const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
-        pb[r] = ok ? (fx | (fy << 8) | (fz << 16)) : 0;
+        pb[r] = ok ? fz * X::PS + fy * X::RS + fx : 0; // tile address of the point's first tap
 #pragma unroll
         for (int k = 0; k < N; k++) {
             pw[k][r] = wx[k];
@@ -439,9 +439,9 @@ __device__ __forceinline__ void own_heavy(const SplatArgs &S, float *ext, int64_
         if constexpr (N == 4) {
             // one point per warp step: lane = (tx, ty, z pair); two taps per lane
             const int tx = lane & 3, ty = (lane >> 2) & 3, tz0 = (lane >> 4) * 2;
+            const int loff = tz0 * X::PS + ty * X::RS + tx; // this lane's tap from the first tap
             for (int j = warp; j < cnt; j += kOwnThreads / 32) {
-                const int b = pb[j];
-                const int a0 = ((b >> 16) + tz0) * X::PS + (((b >> 8) & 255) + ty) * X::RS + (b & 255) + tx;
+                const int a0 = pb[j] + loff;
                 const float wxv = pw[tx][j], wyv = pw[N + ty][j];
                 const float w0 = wxv * (wyv * pw[2 * N + tz0][j]);
                 const float w1 = wxv * (wyv * pw[2 * N + tz0 + 1][j]);
@@ -455,11 +455,11 @@ __device__ __forceinline__ void own_heavy(const SplatArgs &S, float *ext, int64_
         } else {
             // four points per warp step, one tap per lane
             const int sub = lane >> 3, tx = lane & 1, ty = (lane >> 1) & 1, tz = (lane >> 2) & 1;
+            const int loff = tz * X::PS + ty * X::RS + tx;
             for (int j0 = warp * 4; j0 < cnt; j0 += kOwnThreads / 8) {
                 const int j = j0 + sub;
                 if (j >= cnt) continue;
-                const int b = pb[j];
-                const int a = ((b >> 16) + tz) * X::PS + (((b >> 8) & 255) + ty) * X::RS + (b & 255) + tx;
+                const int a = pb[j] + loff;
                 const float w = pw[tx][j] * (pw[N + ty][j] * pw[2 * N + tz][j]);
 #pragma unroll
                 for (int c = 0; c < NCH; c++)
@@ -512,7 +512,7 @@ __device__ __forceinline__ void own_light(const SplatArgs &S, float *ext, int64_
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float *tile = reinterpret_cast<float *>(light_smem) + warp * E3;
     float *stage = reinterpret_cast<float *>(light_smem) + kLightWarps * E3 + warp * 32 * (1 + 3 * N + NCH);
-    int32_t *pbase = reinterpret_cast<int32_t *>(stage); // packed first tap (x | y << 8 | z << 16)
+    int32_t *pbase = reinterpret_cast<int32_t *>(stage); // tile address of each point's first tap
     float *pw = stage + 32;                              // pw[k * 32 + j]: weight k (x taps, y taps, z taps)
     float *pa = pw + 3 * N * 32;                         // pa[c * 32 + j]: amount of channel c
     const int64_t w = block * kLightWarps + warp;
@@ -545,7 +545,7 @@ __device__ __forceinline__ void own_light(const SplatArgs &S, float *ext, int64_
         const int fz = T::eval(q.z + S.trans.z, wz) + o.z - oz;
         // a binned point's first taps lie in [0, 8]; anything else is dropped
         const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
-        pbase[lane] = ok ? (fx | (fy << 8) | (fz << 16)) : 0;
+        pbase[lane] = ok ? (fz * E + fy) * E + fx : 0; // tile address of the point's first tap
 #pragma unroll
         for (int k = 0; k < N; k++) {
             pw[k * 32 + lane] = wx[k];
@@ -571,8 +571,7 @@ __device__ __forceinline__ void own_light(const SplatArgs &S, float *ext, int64_
         __syncwarp();
         for (uint32_t j = 0; j < cnt; j++) {
             if (tap_lane) {
-                const int b = pbase[j];
-                const int a0 = (((b >> 16) + tz0) * E + ((b >> 8) & 255) + ty) * E + (b & 255) + tx;
+                const int a0 = pbase[j] + (tz0 * E + ty) * E + tx;
                 const float am = pa[c * 32 + j];
                 const float wxy = pw[tx * 32 + j], wyv = pw[(N + ty) * 32 + j];
                 tile[a0] += am * (wxy * (wyv * pw[(2 * N + tz0) * 32 + j]));
