@@ -750,6 +750,10 @@ def run_sparse(a):
     torch.cuda.synchronize()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / a.steps
+    if a.quick:  # timed steps only
+        print(json.dumps({"metric": METRIC, "workload": SPARSE_WORKLOAD, "value": n / (ms / 1e3),
+                          "unit": "points/s", "ms_per_step": ms, "n_points": n, "clocks": clk}), flush=True)
+        return 0
     # per-stage device time (event pairs), median over 3 steps
     per = {}
     for _ in range(3):

@@ -290,6 +290,37 @@ struct PartMap {
 template <int KERNEL>
 __device__ constexpr PartMap<KERNEL> kPartMap{};
 
+// The merge's sources per interior voxel v (x | y << 3 | z << 6) of a cell:
+// entry m of row v is the partial position (11 bits) and the neighbour
+// direction d (5 bits, z-major in {-1,0,1}^3) of source m, or 0xFFFF when
+// source m does not cover v.  Source m steps across the faces named by its
+// bits (x, y, z) toward the near face of v when v lies within H of one.
+template <int KERNEL>
+struct alignas(16) MergeMap {
+    uint16_t src[512][8];
+    constexpr MergeMap() : src() {
+        using X = ExtTile<KERNEL>;
+        for (int v = 0; v < 512; v++) {
+            const int vx = v & 7, vy = (v >> 3) & 7, vz = v >> 6;
+            const int ex = vx < X::H ? -1 : (vx >= 8 - X::H ? 1 : 0);
+            const int ey = vy < X::H ? -1 : (vy >= 8 - X::H ? 1 : 0);
+            const int ez = vz < X::H ? -1 : (vz >= 8 - X::H ? 1 : 0);
+            for (int m = 0; m < 8; m++) {
+                const bool used = (!(m & 1) || ex) && (!(m & 2) || ey) && (!(m & 4) || ez);
+                const int dx = (m & 1) ? ex : 0, dy = (m & 2) ? ey : 0, dz = (m & 4) ? ez : 0;
+                const int d = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+                src[v][m] = used ? (uint16_t)(X::part_index(vx - 8 * dx + X::H, vy - 8 * dy + X::H,
+                                                            vz - 8 * dz + X::H) | (d << 11))
+                                 : (uint16_t)0xFFFF;
+            }
+        }
+    }
+};
+template <int KERNEL>
+__device__ constexpr MergeMap<KERNEL> kMergeMap{};
+static_assert(ExtTile<GVDB2_KERNEL_CUBIC2>::E3 <= 2048 && ExtTile<GVDB2_KERNEL_TENT1>::E3 <= 2048,
+              "partial positions fit 11 bits");
+
 constexpr int kOwnThreads = 256;
 constexpr int kOwnChunk = 128; // points staged per pass
 
@@ -609,17 +640,14 @@ __device__ __forceinline__ void merge_voxel(const SplatArgs &S, const float *ext
                                             int v) {
     using X = ExtTile<KERNEL>;
     const int vx = v & 7, vy = (v >> 3) & 7, vz = v >> 6;
-    const int ex = vx < X::H ? -1 : (vx >= 8 - X::H ? 1 : 0);
-    const int ey = vy < X::H ? -1 : (vy >= 8 - X::H ? 1 : 0);
-    const int ez = vz < X::H ? -1 : (vz >= 8 - X::H ? 1 : 0);
+    const uint4 row = *reinterpret_cast<const uint4 *>(kMergeMap<KERNEL>.src[v]);
+    const uint32_t w[4] = {row.x, row.y, row.z, row.w};
     float part[8][NCH];
 #pragma unroll
     for (int m = 0; m < 8; m++) {
-        const int dx = (m & 1) ? ex : 0, dy = (m & 2) ? ey : 0, dz = (m & 4) ? ez : 0;
-        const bool used = (!(m & 1) || ex) && (!(m & 2) || ey) && (!(m & 4) || ez);
-        const int32_t e = used ? ne[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] : -1;
-        const int ux = vx - 8 * dx + X::H, uy = vy - 8 * dy + X::H, uz = vz - 8 * dz + X::H;
-        const float *src = ext + (int64_t)(e >= 0 ? e : 0) * NCH * X::E3 + X::part_index(ux, uy, uz);
+        const uint32_t ent = (w[m >> 1] >> (16 * (m & 1))) & 0xFFFFu;
+        const int32_t e = ent != 0xFFFFu ? ne[ent >> 11] : -1;
+        const float *src = ext + (int64_t)(e >= 0 ? e : 0) * NCH * X::E3 + (ent & 2047u);
 #pragma unroll
         for (int c = 0; c < NCH; c++) part[m][c] = e >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
     }
@@ -813,16 +841,21 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
     const int a = G.apron, tl = G.tile;
     if (threadIdx.x < 27) nbs[threadIdx.x] = G.nbr27[slot * 27 + threadIdx.x];
     __syncthreads();
-    // halo tile from the interiors of this brick and its neighbours
-    for (int i = threadIdx.x; i < ht3; i += blockDim.x) {
-        // brick-local voxel of tile element i
-        const int lx = i % ht - H + kCell * cx, ly = (i / ht) % ht - H + kCell * cy,
-                  lz = i / (ht * ht) - H + kCell * cz;
-        const int dx = lx < 0 ? -1 : (lx >= res ? 1 : 0), dy = ly < 0 ? -1 : (ly >= res ? 1 : 0),
-                  dz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
-        const int32_t nb = nbs[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
-        const int64_t off = (int64_t)nb * G.tvox +
-                            ((int64_t)(lz - dz * res + a) * tl + (ly - dy * res + a)) * tl + (lx - dx * res + a);
+    // halo tile from the interiors of this brick and its neighbours: one
+    // tile row (fixed y, z) per half-warp, lane l < ht loading x = l; the
+    // lane's x neighbour and x offset are fixed for the whole tile
+    static_assert(ht <= 16, "a tile row fits a half-warp");
+    const int hl = threadIdx.x & 15;
+    const int lx = hl - H + kCell * cx;
+    const int ex = lx < 0 ? -1 : (lx >= res ? 1 : 0);
+    const int xo = lx - ex * res + a;
+    for (int r = threadIdx.x >> 4; r < ht * ht; r += blockDim.x >> 4) {
+        if (hl >= ht) continue;
+        const int ly = r % ht - H + kCell * cy, lz = r / ht - H + kCell * cz;
+        const int dy = ly < 0 ? -1 : (ly >= res ? 1 : 0), dz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
+        const int32_t nb = nbs[(dz + 1) * 9 + (dy + 1) * 3 + (ex + 1)];
+        const int64_t off = (int64_t)nb * G.tvox + ((lz - dz * res + a) * tl + (ly - dy * res + a)) * tl + xo;
+        const int i = r * ht + hl;
 #pragma unroll
         for (int c = 0; c < NCH; c++) tile[c * ht3 + i] = nb >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
     }
