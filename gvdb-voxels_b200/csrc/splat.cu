@@ -273,22 +273,25 @@ struct ExtTile {
         return 512 + start - (r > 13 ? 512 : 0) + local;
     }
 };
-// The inverse of part_index: the extended-tile voxel (x | y << 4 | z << 8)
-// of each partial position, so that the own phase writes its partial in
-// order (coalesced) and looks the tile up.
-template <int KERNEL>
-struct PartMap {
-    uint16_t xyz[ExtTile<KERNEL>::E3];
-    constexpr PartMap() : xyz() {
+// The inverse of part_index: the tile address (plane stride PS, row stride
+// RS) of each partial position, so that phase 1 writes its partial in order
+// (coalesced) and looks each value up in its tile.
+template <int KERNEL, int PS, int RS>
+struct PartAddr {
+    uint16_t addr[ExtTile<KERNEL>::E3];
+    constexpr PartAddr() : addr() {
         constexpr int E = ExtTile<KERNEL>::E;
         for (int z = 0; z < E; z++)
             for (int y = 0; y < E; y++)
                 for (int x = 0; x < E; x++)
-                    xyz[ExtTile<KERNEL>::part_index(x, y, z)] = (uint16_t)(x | (y << 4) | (z << 8));
+                    addr[ExtTile<KERNEL>::part_index(x, y, z)] = (uint16_t)(z * PS + y * RS + x);
     }
 };
+// the CTA tile of a heavy cell (padded plane stride) and a light cell's warp tile
 template <int KERNEL>
-__device__ constexpr PartMap<KERNEL> kPartMap{};
+__device__ constexpr PartAddr<KERNEL, ExtTile<KERNEL>::PS, ExtTile<KERNEL>::RS> kHeavyAddr{};
+template <int KERNEL>
+__device__ constexpr PartAddr<KERNEL, ExtTile<KERNEL>::E * ExtTile<KERNEL>::E, ExtTile<KERNEL>::E> kLightAddr{};
 
 // The merge's sources per interior voxel v (x | y << 3 | z << 6) of a cell:
 // entry m of row v is the partial position (11 bits) and the neighbour
@@ -378,7 +381,9 @@ __device__ __forceinline__ void own_heavy(const SplatArgs &S, float *ext, int64_
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
-    for (int i = threadIdx.x; i < NCH * X::CS; i += kOwnThreads) acc_hi[i] = acc_lo[i] = 0;
+    static_assert(X::CS % 4 == 0, "16-byte zeroing");
+    for (int i = threadIdx.x; i < NCH * X::CS / 2; i += kOwnThreads) // acc_hi and acc_lo, adjacent
+        reinterpret_cast<int4 *>(acc_hi)[i] = make_int4(0, 0, 0, 0);
     if (threadIdx.x < NCH) amax_bits[threadIdx.x] = 0;
     const uint32_t beg = S.bin_off[cell], R = S.bin_off[cell + 1] - beg;
     const Node &nd = S.leaves[S.slot_leaf[slot]];
@@ -500,13 +505,12 @@ __device__ __forceinline__ void own_heavy(const SplatArgs &S, float *ext, int64_
     }
     __syncthreads();
     // thread t writes partial positions t, t+256, ... (coalesced) of
-    // channel c, looking their tile voxel up in kPartMap
+    // channel c, looking their tile voxel up in kHeavyAddr
     static_assert(kOwnThreads < X::E3, "one channel step per iteration");
     float *dst = ext + (int64_t)S.cell_ext[cell] * NCH * X::E3;
     int c = 0, j = threadIdx.x;
     for (int i = threadIdx.x; i < NCH * X::E3; i += kOwnThreads) {
-        const int q = kPartMap<KERNEL>.xyz[j];
-        const int k = c * X::CS + (q >> 8) * X::PS + ((q >> 4) & 15) * X::RS + (q & 15);
+        const int k = c * X::CS + kHeavyAddr<KERNEL>.addr[j];
         // |sum| < 2^53: exact in double; the power-of-two scaling is exact
         const long long sum = ((long long)acc_hi[k] << L) + (long long)acc_lo[k];
         dst[i] = (float)((double)sum * inv_s[c]);
@@ -611,10 +615,7 @@ __device__ __forceinline__ void own_light(const SplatArgs &S, float *ext, int64_
             __syncwarp();
         }
         float *dc = dst + c * E3;
-        for (int i = lane; i < E3; i += 32) {
-            const int q = kPartMap<KERNEL>.xyz[i];
-            dc[i] = tile[((q >> 8) * E + ((q >> 4) & 15)) * E + (q & 15)];
-        }
+        for (int i = lane; i < E3; i += 32) dc[i] = tile[kLightAddr<KERNEL>.addr[i]];
         __syncwarp();
     }
 }
@@ -822,6 +823,8 @@ __device__ __forceinline__ void gather_point(const GatherArgs &G, int32_t pidx, 
     }
 }
 
+constexpr int kGatherThreads = 256; // threads of a k_gather_tile CTA
+
 template <int KERNEL, int MODE, int NCH>
 __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t block) {
     constexpr int H = Taps<KERNEL>::N / 2;
@@ -845,19 +848,48 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
     // tile row (fixed y, z) per half-warp, lane l < ht loading x = l; the
     // lane's x neighbour and x offset are fixed for the whole tile
     static_assert(ht <= 16, "a tile row fits a half-warp");
+    constexpr int rows_per_pass = kGatherThreads / 16, passes = (ht * ht + rows_per_pass - 1) / rows_per_pass;
     const int hl = threadIdx.x & 15;
     const int lx = hl - H + kCell * cx;
     const int ex = lx < 0 ? -1 : (lx >= res ? 1 : 0);
     const int xo = lx - ex * res + a;
-    for (int r = threadIdx.x >> 4; r < ht * ht; r += blockDim.x >> 4) {
-        if (hl >= ht) continue;
+    // row r's brick (-1: outside the volume or no row) and offset of its voxel hl
+    auto row_src = [&](int r, int64_t &off) -> int32_t {
+        const bool in = hl < ht && r < ht * ht;
         const int ly = r % ht - H + kCell * cy, lz = r / ht - H + kCell * cz;
         const int dy = ly < 0 ? -1 : (ly >= res ? 1 : 0), dz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
-        const int32_t nb = nbs[(dz + 1) * 9 + (dy + 1) * 3 + (ex + 1)];
-        const int64_t off = (int64_t)nb * G.tvox + ((lz - dz * res + a) * tl + (ly - dy * res + a)) * tl + xo;
-        const int i = r * ht + hl;
+        const int32_t nb = in ? nbs[(dz + 1) * 9 + (dy + 1) * 3 + (ex + 1)] : -1;
+        off = (int64_t)nb * G.tvox + ((lz - dz * res + a) * tl + (ly - dy * res + a)) * tl + xo;
+        return nb;
+    };
+    if constexpr (MODE == kFwd) {
+        // row by row: the forward point phase needs few registers, and
+        // holding the whole staging in registers would cut the CTAs per SM
+        for (int r = threadIdx.x >> 4; r < ht * ht; r += rows_per_pass) {
+            int64_t off;
+            const int32_t nb = row_src(r, off);
+            if (hl < ht)
 #pragma unroll
-        for (int c = 0; c < NCH; c++) tile[c * ht3 + i] = nb >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
+                for (int c = 0; c < NCH; c++) tile[c * ht3 + r * ht + hl] = nb >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
+        }
+    } else {
+        // the adjoint point phases hold more registers than the staging
+        // needs: every load of the thread is issued before the first store
+        float val[passes][NCH];
+#pragma unroll
+        for (int k = 0; k < passes; k++) {
+            int64_t off;
+            const int32_t nb = row_src((int)(threadIdx.x >> 4) + k * rows_per_pass, off);
+#pragma unroll
+            for (int c = 0; c < NCH; c++) val[k][c] = nb >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < passes; k++) {
+            const int r = (int)(threadIdx.x >> 4) + k * rows_per_pass;
+            if (hl < ht && r < ht * ht)
+#pragma unroll
+                for (int c = 0; c < NCH; c++) tile[c * ht3 + r * ht + hl] = val[k][c];
+        }
     }
     __syncthreads();
     const Node &nd = G.leaves[G.slot_leaf[slot]];
@@ -867,7 +899,7 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
 #pragma unroll
         for (int c = 0; c < NCH; c++) g[c] = tile[c * ht3 + k];
     };
-    for (uint32_t j = beg + threadIdx.x; j < end; j += blockDim.x)
+    for (uint32_t j = beg + threadIdx.x; j < end; j += kGatherThreads)
         gather_point<KERNEL, MODE, NCH>(G, G.perm[j], ox, oy, oz, fetch);
 }
 
@@ -909,7 +941,7 @@ __device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t 
 // One fused launch measured slower: the light path's registers (66) halved
 // the tiles' occupancy.
 template <int KERNEL, int MODE, int NCH>
-__global__ void __launch_bounds__(256) k_gather_tile(GatherArgs G) {
+__global__ void __launch_bounds__(kGatherThreads) k_gather_tile(GatherArgs G) {
     gather_tile_cell<KERNEL, MODE, NCH>(G, blockIdx.x);
 }
 template <int KERNEL, int MODE, int NCH>
@@ -1042,7 +1074,7 @@ gvdb2_status launch_gather(Volume *v, const GatherArgs &G) {
     // tiles for the huge and heavy cells, then the light cells, a warp each
     // (every cell gets a tile when the caller supplied the binning)
     const int64_t heavy = G.cell_list ? v->heavy_grid : G.ncell;
-    if (heavy > 0) k<<<(unsigned)heavy, 256, smem, v->stream>>>(G);
+    if (heavy > 0) k<<<(unsigned)heavy, kGatherThreads, smem, v->stream>>>(G);
     if (G.cell_list && v->light_grid > 0)
         k_gather_light<KERNEL, MODE, NCH><<<(unsigned)((v->light_grid + 7) / 8), 256, 0, v->stream>>>(G);
     GV_CUDA(v, cudaGetLastError());
