@@ -474,8 +474,8 @@ def run_ours(a):
 # profiles/k_scatter_own_merge_gather_dam4m.md).  Traffic grows with the brick
 # count, so a launch moves about this many bytes x bricks.
 TRAFFIC_PER_BRICK = {
-    "scatter": (192.7e6 + 407.5e6 + 754.4e6 + 220.1e6) / 23396,
-    "gather": (614.7e6 + 44.2e6 + 3.3e6 + 0.0) / 23396,
+    "scatter": (199.4e6 + 406.3e6 + 752.9e6 + 220.4e6) / 23396,
+    "gather": (635.0e6 + 42.7e6 + 3.3e6 + 0.0) / 23396,
 }
 
 
