@@ -284,6 +284,12 @@ gvdb2_status gvdb2_update_atlas(gvdb2_volume *h) {
     return gvdb2::update_atlas(VOL(h));
 }
 
+gvdb2_status gvdb2_activate_space(gvdb2_volume *h, const float *xyz, int64_t n, uint64_t *out) {
+    CHECK_HANDLE(h);
+    if (n < 0 || (n > 0 && (!xyz || !out))) return gvdb2::fail(VOL(h), GVDB2_ERR_ARG, "ActivateSpace: bad arguments");
+    return gvdb2::activate_space(VOL(h), xyz, n, out);
+}
+
 gvdb2_status gvdb2_clear_channel(gvdb2_volume *h, int chan) {
     CHECK_HANDLE(h);
     return gvdb2::clear_channel(VOL(h), chan);

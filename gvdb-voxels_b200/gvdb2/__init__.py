@@ -22,8 +22,9 @@ NODE_DTYPE = np.dtype([
     ("mParent", np.uint64), ("mChildList", np.uint64), ("mMask", np.uint64),
 ])
 AMAP_DTYPE = np.dtype([("mPos", np.int32, 3), ("mLeafID", np.int32)])
+ID_UNDEFL = 0xFFFFFFFF  # gvdb_types.h:55: no node
 
-__all__ = ["VolumeGVDB", "GvdbError", "KERNEL_TENT1", "KERNEL_CUBIC2", "T_FLOAT", "NODE_DTYPE", "AMAP_DTYPE",
+__all__ = ["VolumeGVDB", "GvdbError", "KERNEL_TENT1", "KERNEL_CUBIC2", "T_FLOAT", "NODE_DTYPE", "AMAP_DTYPE", "ID_UNDEFL",
            "view_of", "declared_symbols"]
 
 
@@ -139,6 +140,20 @@ class VolumeGVDB:
 
     def UpdateAtlas(self):
         self._check(self._L.gvdb2_update_atlas(self._h), "UpdateAtlas")
+
+    def ActivateSpace(self, pos):
+        """ActivateSpace(Vector3DF) (V:2766-2856) for one (x, y, z) or an (N, 3)
+        host array of positions, in order: the leaf's pool reference where it
+        existed, ID_UNDEFL where the call created it (or could not activate
+        it).  Returns an int for one position, else a uint64 numpy array."""
+        import numpy as np
+        p = np.ascontiguousarray(pos, dtype=np.float32)
+        one = p.ndim == 1
+        p = p.reshape(-1, 3)
+        out = np.empty(len(p), np.uint64)
+        self._check(self._L.gvdb2_activate_space(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), len(p),
+                                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))), "ActivateSpace")
+        return int(out[0]) if one else out
 
     def ClearChannel(self, chan):
         self._check(self._L.gvdb2_clear_channel(self._h, chan), "ClearChannel")

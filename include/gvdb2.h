@@ -140,6 +140,15 @@ GVDB2_API gvdb2_status gvdb2_rebuild_topology(gvdb2_volume *v, int n, float radi
 GVDB2_API gvdb2_status gvdb2_accumulate_topology(gvdb2_volume *v, int n, float radius, const float orig[3], int min_depth); /* AccumulateTopology, V:1158-1178 */
 GVDB2_API gvdb2_status gvdb2_finish_topology(gvdb2_volume *v, int commit, int bounds);            /* FinishTopology, V:1579-1593 */
 GVDB2_API gvdb2_status gvdb2_update_atlas(gvdb2_volume *v);                                       /* UpdateAtlas, V:2630-2704 */
+/* ActivateSpace(Vector3DF), V:2766-2856 (with Reparent V:2726-2762): activates
+ * the brick holding each of the n HOST positions xyz[3i..3i+2] (truncated to
+ * int), in order, creating the root, the path and, for a position outside
+ * the tree, a new covering root.  out[i] (host) = the leaf's pool reference
+ * when it existed, GVDB2_ID_UNDEFL when the call created it or the position
+ * lies outside the top configured level.  Synchronises the stream; the next
+ * RebuildTopology starts from a full rebuild. */
+#define GVDB2_ID_UNDEFL 0xFFFFFFFFull
+GVDB2_API gvdb2_status gvdb2_activate_space(gvdb2_volume *v, const float *xyz, int64_t n, uint64_t *out);
 GVDB2_API gvdb2_status gvdb2_clear_channel(gvdb2_volume *v, int chan);                            /* ClearChannel, V:1596-1603 */
 GVDB2_API gvdb2_status gvdb2_update_neighbors(gvdb2_volume *v);                                   /* UpdateNeighbors, V:2527-2556 */
 

@@ -86,6 +86,13 @@ class VolumeGVDB {
         check(gvdb2_finish_topology(v_, commit ? 1 : 0, bounds ? 1 : 0), "FinishTopology");
     }
     void UpdateAtlas() { check(gvdb2_update_atlas(v_), "UpdateAtlas"); }
+    // ActivateSpace(Vector3DF): the leaf's pool reference if it existed, else ID_UNDEFL
+    uint64_t ActivateSpace(Vec3F pos) {
+        const float p[3] = {pos.x, pos.y, pos.z};
+        uint64_t out = GVDB2_ID_UNDEFL;
+        check(gvdb2_activate_space(v_, p, 1, &out), "ActivateSpace");
+        return out;
+    }
     void ClearChannel(unsigned char chan) { check(gvdb2_clear_channel(v_, chan), "ClearChannel"); }
     void UpdateNeighbors() { check(gvdb2_update_neighbors(v_), "UpdateNeighbors"); }
 

@@ -793,6 +793,152 @@ int orc_accumulate_topology(orc_volume *v, orc_view pos, int n, float radius, co
 }
 
 /* ------------------------------------------------------------------ */
+/* ActivateSpace: the host tree walk that activates the brick holding   */
+/* one position, creating the root, the path and, when the position is  */
+/* outside the tree, a new covering root (V:2707-2856, V:2980-3026).    */
+/* ------------------------------------------------------------------ */
+
+static orc_node *node_ref(orc_volume *v, uint64_t id) { return &v->pool[(id >> 8) & 0xFF][id >> 16]; }
+
+/* GetCoveringNode (V:2915-2931) of an integer position. */
+static void covering_node_i(const orc_volume *v, int lev, const int pos[3], int out[3]) {
+    int range = range_of(v, lev);
+    for (int a = 0; a < 3; a++) {
+        if (lev == ORC_MAXLEV - 1) {
+            out[a] = 0;
+        } else {
+            int np = pos[a] / range * range;
+            if (pos[a] < np) np -= range;
+            out[a] = np;
+        }
+    }
+}
+
+/* getPosInNode (V:2858-2875), the host form of the device test above:
+ * child bit of pos inside node id, 0 if outside. */
+static int node_bit(orc_volume *v, uint64_t id, const int pos[3], uint32_t *bit) {
+    const orc_node *nd = node_ref(v, id);
+    int64_t b = 0;
+    const int in = pos_in_node(v, nd->mLev, nd->mPos, pos, &b);
+    *bit = in ? (uint32_t)b : 0u;
+    return in;
+}
+
+/* getChildNode (V:3079-3091, no bitmasks). */
+static uint64_t child_at(orc_volume *v, uint64_t id, uint32_t b) {
+    const orc_node *nd = node_ref(v, id);
+    if (nd->mChildList == ID_UNDEFL) return ID_UNDEF64;
+    return v->clist[nd->mLev][(int64_t)(nd->mChildList >> 16) * res3_of(v, nd->mLev) + b];
+}
+
+/* InsertChild (V:2980-3026, no bitmasks): the child list is allocated,
+ * 0xFF-filled, with the node's first child. */
+static uint64_t insert_child(orc_volume *v, uint64_t id, uint64_t child, uint32_t b) {
+    node_ref(v, child)->mParent = id;
+    const int lev = node_ref(v, id)->mLev;
+    if (node_ref(v, id)->mChildList == ID_UNDEFL) {
+        int64_t c = pool_alloc_clist(v, lev);
+        if (c < 0) return ID_UNDEFL;
+        node_ref(v, id)->mChildList = elem(1, lev, (uint64_t)c);
+        memset(v->clist[lev] + c * res3_of(v, lev), 0xFF, (size_t)res3_of(v, lev) * sizeof(uint64_t));
+    }
+    v->clist[lev][(int64_t)(node_ref(v, id)->mChildList >> 16) * res3_of(v, lev) + b] = child;
+    return child;
+}
+
+/* AddChildNode (V:2707-2723): a node of level plev-1 at the child position
+ * of bit b (getPosFromBit, gvdb_volume_gvdb.h:602-609), linked under id. */
+static uint64_t add_child_node(orc_volume *v, uint64_t id, const int ppos[3], int plev, uint32_t b) {
+    const int lev = plev - 1;
+    int64_t idx = pool_alloc_node(v, lev);
+    if (idx < 0) return ID_UNDEFL;
+    const int logr = v->logdim[plev], mask = (1 << logr) - 1, rng = range_of(v, lev);
+    const int p[3] = {(int)(b & mask) * rng + ppos[0], (int)((b >> logr) & mask) * rng + ppos[1],
+                      (int)((b >> (2 * logr)) & mask) * rng + ppos[2]};
+    setup_node(v, lev, idx, p, 1);
+    return insert_child(v, id, elem(0, lev, (uint64_t)idx), b);
+}
+
+static uint64_t activate_space(orc_volume *v, uint64_t id, const int pos[3], int *bnew, uint64_t stop, int stoplev);
+
+/* Reparent (V:2726-2762): a root of the lowest level whose covering node
+ * holds both the old root and pos; the old root is linked in (stop node)
+ * and the path to pos created.  Returns the parent of pos's leaf. */
+static uint64_t reparent(orc_volume *v, int lev, uint64_t prev, const int pos[3], int *bnew) {
+    const int pp[3] = {node_ref(v, prev)->mPos[0], node_ref(v, prev)->mPos[1], node_ref(v, prev)->mPos[2]};
+    int p1[3] = {0, 0, 0}, p2[3];
+    int cover = 0;
+    while (!cover && lev < ORC_MAXLEV) {
+        lev++;
+        covering_node_i(v, lev, pos, p1);
+        covering_node_i(v, lev, pp, p2);
+        cover = p1[0] == p2[0] && p1[1] == p2[1] && p1[2] == p2[2];
+    }
+    if (lev >= ORC_MAXLEV || lev >= v->nlev) return ID_UNDEFL; /* PoolAlloc refuses unconfigured levels (A:165) */
+    int64_t idx = pool_alloc_node(v, lev);
+    if (idx < 0) return ID_UNDEFL;
+    setup_node(v, lev, idx, p1, 1);
+    const uint64_t root = elem(0, lev, (uint64_t)idx);
+    int bn = 0;
+    activate_space(v, root, pp, &bn, prev, 0);
+    const uint64_t leaf = activate_space(v, root, pos, bnew, ID_UNDEFL, 0);
+    v->root = root;
+    return leaf == ID_UNDEFL ? ID_UNDEFL : node_ref(v, leaf)->mParent;
+}
+
+/* ActivateSpace (V:2804-2856) with a stop node and a stop level. */
+static uint64_t activate_space(orc_volume *v, uint64_t id, const int pos[3], int *bnew, uint64_t stop, int stoplev) {
+    if (v->root == ID_UNDEFL && id == v->root) { /* first node: a root of the stop level */
+        int p[3];
+        covering_node_i(v, stoplev, pos, p);
+        int64_t idx = pool_alloc_node(v, stoplev);
+        if (idx < 0) return ID_UNDEFL;
+        setup_node(v, stoplev, idx, p, 1);
+        v->root = id = elem(0, stoplev, (uint64_t)idx);
+    }
+    uint32_t b;
+    if (node_bit(v, id, pos, &b)) {
+        const int lev = node_ref(v, id)->mLev;
+        if (stop != ID_UNDEFL) {
+            const orc_node *sn = node_ref(v, stop);
+            if (pos[0] == sn->mPos[0] && pos[1] == sn->mPos[1] && pos[2] == sn->mPos[2] &&
+                child_at(v, id, b) == ID_UNDEF64 && lev == sn->mLev + 1)
+                return insert_child(v, id, stop, b);
+        }
+        if (lev == stoplev) return id;
+        uint64_t child = child_at(v, id, b);
+        if (child == ID_UNDEF64) {
+            const int pp[3] = {node_ref(v, id)->mPos[0], node_ref(v, id)->mPos[1], node_ref(v, id)->mPos[2]};
+            child = add_child_node(v, id, pp, lev, b);
+            if (child == ID_UNDEFL) return ID_UNDEFL;
+            if (lev == 1) *bnew = 1;
+        }
+        if (((child >> 8) & 0xFF) == 0) return child; /* isLeaf */
+        return activate_space(v, child, pos, bnew, stop, stoplev);
+    }
+    uint64_t parent = node_ref(v, id)->mParent;
+    if (parent == ID_UNDEFL) {
+        parent = reparent(v, node_ref(v, id)->mLev, id, pos, bnew);
+        if (parent == ID_UNDEFL) return ID_UNDEFL;
+    }
+    return activate_space(v, parent, pos, bnew, stop, stoplev);
+}
+
+/* ActivateSpace(Vector3DF) (V:2766-2774): the position truncated to int;
+ * returns the leaf's pool reference when it existed already, ID_UNDEFL
+ * when it was created or nothing could be activated. */
+uint64_t orc_activate_space(orc_volume *v, float x, float y, float z) {
+    if (v->nlev == 0) return ID_UNDEFL;
+    const int pos[3] = {(int)x, (int)y, (int)z};
+    int bnew = 0;
+    uint64_t id = activate_space(v, v->root, pos, &bnew, ID_UNDEFL, 0);
+    if (id == ID_UNDEFL || bnew) return ID_UNDEFL;
+    return id;
+}
+
+uint64_t orc_root(const orc_volume *v) { return v->root; }
+
+/* ------------------------------------------------------------------ */
 /* atlas                                                                */
 /* ------------------------------------------------------------------ */
 

@@ -58,6 +58,8 @@ def lib():
             "orc_rebuild_topology": (i32, [vp, _View, i32, f32, fp]),
             "orc_accumulate_topology": (i32, [vp, _View, i32, f32, fp, i32]),
             "orc_update_atlas": (i32, [vp]),
+            "orc_activate_space": (ctypes.c_uint64, [vp, f32, f32, f32]),
+            "orc_root": (ctypes.c_uint64, [vp]),
             "orc_clear_channel": (i32, [vp, i32]),
             "orc_insert_points": (i32, [vp, _View, i32, fp, ip, ip, ip]),
             "orc_scatter_density": (i32, [vp, _View, i32, f32, f32, fp, i32, ip]),
@@ -174,6 +176,14 @@ class Oracle:
     def accumulate_topology(self, pos, radius, orig=(0, 0, 0), min_depth=0):
         pos = np.ascontiguousarray(pos, dtype=np.float32)
         return self.L.orc_accumulate_topology(self.h, view(pos), pos.shape[0], float(radius), _f3(orig), min_depth)
+
+    def activate_space(self, x, y, z):
+        """ActivateSpace(Vector3DF): the leaf's pool reference when it existed,
+        ID_UNDEFL (0xFFFFFFFF) when it was created or nothing was activated."""
+        return int(self.L.orc_activate_space(self.h, float(x), float(y), float(z)))
+
+    def root(self):
+        return int(self.L.orc_root(self.h))
 
     def update_atlas(self):
         _check(self.L.orc_update_atlas(self.h), "update_atlas")

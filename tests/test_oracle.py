@@ -320,3 +320,83 @@ def test_gather_adjoint_fd(oracle_mod):
     lhs = float(np.sum(gg * interior(o.atlas(0), o.apron())))
     rhs = float(np.sum(dout * o.gather_kernel(2, pts, [0])))
     assert abs(lhs - rhs) < 1e-9 * max(1.0, abs(rhs))
+
+
+ID_UNDEFL = 0xFFFFFFFF
+
+
+def activation_positions(seed=9):
+    """Positions for ActivateSpace: scattered ones, a repeat, one that needs a
+    new root above the old one, negative and far ones outside every level."""
+    rng = np.random.default_rng(seed)
+    near = rng.uniform(0.0, 300.0, (40, 3))
+    far = np.array([[5000.0, 20, 30], [5000.0, 20, 30], [-5.0, 2, 2], [3.0, 3, 3], [40000.0, 1, 1],
+                    [120.7, 64.2, 0.5]])
+    return np.concatenate([near[:20], far, near[20:]]).astype(np.float32)
+
+
+def descend(o, root, p):
+    """The leaf holding integer position p, found through the child lists
+    from `root`; None when p has no leaf."""
+    if root == ID_UNDEFL:
+        return None
+    r = root
+    while True:
+        lev, idx = (r >> 8) & 0xFF, r >> 16
+        nd = o.nodes(lev)[idx]
+        res, rng = o.res(lev), o.range(lev)
+        rel = p - nd["mPos"].astype(np.int64)
+        if np.any(rel < 0) or np.any(rel >= rng):
+            return None
+        if lev == 0:
+            return r
+        loc = rel * res // rng
+        c = int(o.childlists(lev)[int(nd["mChildList"]) >> 16, (loc[2] * res + loc[1]) * res + loc[0]])
+        if c == UNDEF64:
+            return None
+        r = c
+
+
+def test_activate_space_tree(oracle_mod):
+    """ActivateSpace from an empty volume: each result is the leaf's reference
+    when it existed (and, the reference's quirk, when the call created the
+    first root, a leaf), else ID_UNDEFL; afterwards the position's leaf is
+    reachable from the root unless it lies outside the top level; every link
+    is consistent both ways and every node sits on its level's grid."""
+    o = make_oracle(oracle_mod)
+    for x in activation_positions():
+        p = x.astype(np.int64)  # float -> int truncates toward zero, as Vector3DI(Vector3DF) does
+        root0 = o.root()
+        before = descend(o, root0, p)
+        got = o.activate_space(*x)
+        after = descend(o, o.root(), p)
+        if before is not None:
+            assert got == before and after == before
+        elif root0 == ID_UNDEFL:
+            assert got == after == o.root()
+        else:
+            assert got == ID_UNDEFL
+        outside = np.any(p < 0) or np.any(p >= o.range(4))
+        assert (after is None) == bool(outside), f"position {p}"
+    root = o.root()
+    assert (root >> 8) & 0xFF == 4 and int(o.nodes(4)[root >> 16]["mParent"]) == ID_UNDEFL
+    for lev in range(5):
+        nd = o.nodes(lev)
+        assert np.all(nd["mPos"] % o.range(lev) == 0)
+        assert np.all(nd["mFlags"] == 1) and np.all(nd["mValue"] == -1)
+        if lev == 0:
+            continue
+        cl = o.childlists(lev)
+        res, rng = o.res(lev), o.range(lev)
+        for i, n in enumerate(nd):
+            li = int(n["mChildList"]) >> 16
+            assert li == i  # lists allocated in node order
+            for bit in np.nonzero(cl[li] != UNDEF64)[0]:
+                c = int(cl[li, bit])
+                cn = o.nodes((c >> 8) & 0xFF)[c >> 16]
+                assert (c >> 8) & 0xFF == lev - 1 and int(cn["mParent"]) == (i << 16) | (lev << 8)
+                loc = (cn["mPos"] - n["mPos"]) * res // rng
+                assert (loc[2] * res + loc[1]) * res + loc[0] == bit
+        # every node below the root is listed by its parent
+        below = o.nodes(lev - 1)
+        assert np.count_nonzero(cl != UNDEF64) == len(below) - (1 if (root >> 8) & 0xFF == lev - 1 else 0)
