@@ -290,6 +290,11 @@ gvdb2_status gvdb2_activate_space(gvdb2_volume *h, const float *xyz, int64_t n, 
     return gvdb2::activate_space(VOL(h), xyz, n, out);
 }
 
+gvdb2_status gvdb2_compact_pools(gvdb2_volume *h) {
+    CHECK_HANDLE(h);
+    return gvdb2::compact_pools(VOL(h));
+}
+
 gvdb2_status gvdb2_clear_channel(gvdb2_volume *h, int chan) {
     CHECK_HANDLE(h);
     return gvdb2::clear_channel(VOL(h), chan);

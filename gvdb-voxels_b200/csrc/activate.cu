@@ -24,6 +24,7 @@
 #include "gvdb2_internal.h"
 
 #include <cmath>
+#include <string>
 #include <vector>
 
 namespace gvdb2 {
@@ -196,12 +197,12 @@ struct HostTree {
 
 } // namespace
 
-gvdb2_status activate_space(Volume *v, const float *xyz, int64_t n, uint64_t *out) {
-    if (v->nlev <= 0) return fail(v, GVDB2_ERR_STATE, "ActivateSpace before Configure");
-    if (n == 0) return GVDB2_OK;
-    cudaStream_t s = v->stream;
-    GV_CUDA(v, cudaStreamSynchronize(s));
-    HostTree t;
+namespace {
+
+// The device pools into t (levels 0 .. nlev-1); t.root = the node at the
+// volume's depth, when there are nodes.
+gvdb2_status read_pools(Volume *v, HostTree &t, const char *what) {
+    GV_CUDA(v, cudaStreamSynchronize(v->stream));
     t.v = v;
     int64_t total = 0;
     for (int l = 0; l < v->nlev; l++) {
@@ -221,9 +222,39 @@ gvdb2_status activate_space(Volume *v, const float *xyz, int64_t n, uint64_t *ou
     if (total > 0) {
         const int d = v->depth;
         if (d < 0 || d >= v->nlev || v->pool_cnt[d] < 1 || t.nodes[d][0].mParent != kUndefL)
-            return fail(v, GVDB2_ERR_STATE, "ActivateSpace: no root at the volume's depth");
+            return fail(v, GVDB2_ERR_STATE, std::string(what) + ": no root at the volume's depth");
         t.root = make_ref(0, d, 0);
     }
+    return GVDB2_OK;
+}
+
+// t's pools back to the device, whole, with their counts.
+gvdb2_status write_pools(Volume *v, HostTree &t) {
+    cudaStream_t s = v->stream;
+    for (int l = 0; l < v->nlev; l++) {
+        const int64_t cnt = (int64_t)t.nodes[l].size();
+        if (cnt == 0 && v->pool_cnt[l] == 0) continue;
+        GV_TRY(pool_reserve(v, l, cnt)); // contents are rewritten whole below
+        if (cnt > 0)
+            GV_CUDA(v, cudaMemcpyAsync(v->pool[l].p, t.nodes[l].data(), sizeof(Node) * cnt, cudaMemcpyHostToDevice, s));
+        if (l > 0 && cnt > 0) {
+            t.lists[l].resize((size_t)(cnt * v->res3(l)), kUndef64);
+            GV_CUDA(v, cudaMemcpyAsync(v->clist[l].p, t.lists[l].data(), sizeof(uint64_t) * t.lists[l].size(),
+                                       cudaMemcpyHostToDevice, s));
+        }
+        v->pool_cnt[l] = cnt;
+    }
+    GV_CUDA(v, cudaStreamSynchronize(s)); // the host mirror is released on return
+    return GVDB2_OK;
+}
+
+} // namespace
+
+gvdb2_status activate_space(Volume *v, const float *xyz, int64_t n, uint64_t *out) {
+    if (v->nlev <= 0) return fail(v, GVDB2_ERR_STATE, "ActivateSpace before Configure");
+    if (n == 0) return GVDB2_OK;
+    HostTree t;
+    GV_TRY(read_pools(v, t, "ActivateSpace"));
     for (int64_t i = 0; i < n; i++) {
         const float *x = xyz + 3 * i;
         if (!(fabsf(x[0]) < 2.0e9f && fabsf(x[1]) < 2.0e9f && fabsf(x[2]) < 2.0e9f)) {
@@ -243,21 +274,72 @@ gvdb2_status activate_space(Volume *v, const float *xyz, int64_t n, uint64_t *ou
     if (t.root == kUndefL) return GVDB2_OK; // nothing was activated
     if (ref_ndx(t.root) != 0)
         return fail(v, GVDB2_ERR_UNSUPPORTED, "ActivateSpace: new root is not the first node of its level");
-    for (int l = 0; l < v->nlev; l++) {
-        const int64_t cnt = (int64_t)t.nodes[l].size();
-        if (cnt == v->pool_cnt[l] && cnt == 0) continue;
-        GV_TRY(pool_reserve(v, l, cnt)); // contents are rewritten whole below
-        if (cnt > 0)
-            GV_CUDA(v, cudaMemcpyAsync(v->pool[l].p, t.nodes[l].data(), sizeof(Node) * cnt, cudaMemcpyHostToDevice, s));
-        if (l > 0 && cnt > 0) {
-            t.lists[l].resize((size_t)(cnt * v->res3(l)), kUndef64);
-            GV_CUDA(v, cudaMemcpyAsync(v->clist[l].p, t.lists[l].data(), sizeof(uint64_t) * t.lists[l].size(),
-                                       cudaMemcpyHostToDevice, s));
-        }
-        v->pool_cnt[l] = cnt;
-    }
-    GV_CUDA(v, cudaStreamSynchronize(s)); // the host mirror is released on return
+    GV_TRY(write_pools(v, t));
     return adopt_pools(v, ref_lev(t.root));
+}
+
+// Pool compaction (no reference counterpart; the reference keeps delinked
+// nodes for good).  An incremental rebuild delinks the nodes it no longer
+// needs (mParent = ID_UNDEF64, their parent's slot cleared, gvdbDelinkLeafBricks
+// / gvdbDelinkBricks, cuda_gvdb_nodes.cuh:401-467) but leaves them in the
+// pools, where every sweep over a level still visits them.  Compaction drops
+// them, keeps the order of the rest, and rewrites the references: parents,
+// child-list entries and child-list indices (list index = node index).  The
+// flagged leaves keep their order, so UpdateAtlas hands out the same slots
+// and the channel data stay valid.  The rebuild state (full or incremental,
+// depth, bounding box) is kept, so the next RebuildTopology continues as it
+// would have.
+gvdb2_status compact_pools(Volume *v) {
+    if (v->nlev <= 0) return fail(v, GVDB2_ERR_STATE, "CompactPools before Configure");
+    HostTree t;
+    GV_TRY(read_pools(v, t, "CompactPools"));
+    if (t.root == kUndefL) return GVDB2_OK;
+    std::vector<int64_t> remap[kMaxLev];
+    HostTree c;
+    c.v = v;
+    for (int l = 0; l < v->nlev; l++) {
+        remap[l].assign(t.nodes[l].size(), -1);
+        for (size_t i = 0; i < t.nodes[l].size(); i++)
+            if (t.nodes[l][i].mParent != kUndef64) remap[l][i] = (int64_t)c.nodes[l].size(), c.nodes[l].push_back(t.nodes[l][i]);
+    }
+    for (int l = 0; l < v->nlev; l++) {
+        const int64_t r3 = l > 0 ? v->res3(l) : 0;
+        if (l > 0) c.lists[l].assign((size_t)(c.nodes[l].size() * r3), kUndef64);
+        for (size_t i = 0; i < c.nodes[l].size(); i++) {
+            Node &nd = c.nodes[l][i];
+            if (nd.mParent != kUndefL) { // every kept node below the root has a live parent
+                const int pl = ref_lev(nd.mParent);
+                const int64_t pi = ref_ndx(nd.mParent);
+                if (pl != l + 1 || pi >= (int64_t)remap[pl].size() || remap[pl][pi] < 0)
+                    return fail(v, GVDB2_ERR_STATE, "CompactPools: a kept node's parent was delinked");
+                nd.mParent = make_ref(0, pl, (uint64_t)remap[pl][pi]);
+            }
+            if (l == 0 || nd.mChildList == kUndefL) continue;
+            const int64_t old = ref_ndx(nd.mChildList);
+            nd.mChildList = make_ref(1, l, (uint64_t)i);
+            for (int64_t b = 0; b < r3; b++) {
+                const uint64_t e = t.lists[l][(size_t)(old * r3 + b)];
+                if (e == kUndef64) continue;
+                const int64_t ci = ref_ndx(e);
+                if (ref_lev(e) != l - 1 || ci >= (int64_t)remap[l - 1].size() || remap[l - 1][ci] < 0)
+                    return fail(v, GVDB2_ERR_STATE, "CompactPools: a child list holds a delinked node");
+                c.lists[l][(size_t)(i * r3 + b)] = make_ref(0, l - 1, (uint64_t)remap[l - 1][ci]);
+            }
+        }
+    }
+    const int rl = ref_lev(t.root);
+    if (remap[rl][ref_ndx(t.root)] != 0) return fail(v, GVDB2_ERR_STATE, "CompactPools: the root is not first");
+    // the rebuild state survives the re-adoption
+    const bool rebuild = v->rebuild_topo;
+    const int cur = v->cur_depth;
+    float lo[3], hi[3];
+    for (int a = 0; a < 3; a++) lo[a] = v->posmin[a], hi[a] = v->posmax[a];
+    GV_TRY(write_pools(v, c));
+    GV_TRY(adopt_pools(v, rl));
+    v->rebuild_topo = rebuild;
+    v->cur_depth = cur;
+    for (int a = 0; a < 3; a++) v->posmin[a] = lo[a], v->posmax[a] = hi[a];
+    return GVDB2_OK;
 }
 
 } // namespace gvdb2

@@ -246,6 +246,7 @@ gvdb2_status alloc_channel_storage(Volume *v, int chan);
 gvdb2_status pool_reserve(Volume *v, int lev, int64_t cnt);
 gvdb2_status adopt_pools(Volume *v, int depth);
 gvdb2_status activate_space(Volume *v, const float *xyz, int64_t n, uint64_t *out);
+gvdb2_status compact_pools(Volume *v);
 gvdb2_status save_vbx(Volume *v, const char *path);
 gvdb2_status load_vbx(Volume *v, const char *path);
 gvdb2_status update_neighbors(Volume *v);

@@ -155,6 +155,11 @@ class VolumeGVDB:
                                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))), "ActivateSpace")
         return int(out[0]) if one else out
 
+    def CompactPools(self):
+        """Drop the nodes incremental rebuilds delinked and renumber the rest
+        (no reference counterpart); call UpdateAtlas before the next splat."""
+        self._check(self._L.gvdb2_compact_pools(self._h), "CompactPools")
+
     def ClearChannel(self, chan):
         self._check(self._L.gvdb2_clear_channel(self._h, chan), "ClearChannel")
 

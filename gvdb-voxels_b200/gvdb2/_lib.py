@@ -63,6 +63,7 @@ _SIGS = {
     "gvdb2_finish_topology": [_vp, _i32, _i32],
     "gvdb2_update_atlas": [_vp],
     "gvdb2_activate_space": [_vp, _fp, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64)],
+    "gvdb2_compact_pools": [_vp],
     "gvdb2_clear_channel": [_vp, _i32],
     "gvdb2_update_neighbors": [_vp],
     "gvdb2_insert_points": [_vp, _i32, _fp, _i32],

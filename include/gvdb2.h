@@ -149,6 +149,13 @@ GVDB2_API gvdb2_status gvdb2_update_atlas(gvdb2_volume *v);                     
  * RebuildTopology starts from a full rebuild. */
 #define GVDB2_ID_UNDEFL 0xFFFFFFFFull
 GVDB2_API gvdb2_status gvdb2_activate_space(gvdb2_volume *v, const float *xyz, int64_t n, uint64_t *out);
+/* Pool compaction (no reference counterpart; the reference keeps the nodes an
+ * incremental rebuild delinks, gvdbDelinkLeafBricks / gvdbDelinkBricks,
+ * kernels/cuda_gvdb_nodes.cuh:401-467, in its pools for good): drops them and
+ * renumbers the rest in order.  Live leaves keep their order, so UpdateAtlas
+ * gives them the same slots; call it before the next splat or gather.  The
+ * rebuild state is kept: the next RebuildTopology continues incrementally. */
+GVDB2_API gvdb2_status gvdb2_compact_pools(gvdb2_volume *v);
 GVDB2_API gvdb2_status gvdb2_clear_channel(gvdb2_volume *v, int chan);                            /* ClearChannel, V:1596-1603 */
 GVDB2_API gvdb2_status gvdb2_update_neighbors(gvdb2_volume *v);                                   /* UpdateNeighbors, V:2527-2556 */
 

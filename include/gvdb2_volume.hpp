@@ -86,6 +86,8 @@ class VolumeGVDB {
         check(gvdb2_finish_topology(v_, commit ? 1 : 0, bounds ? 1 : 0), "FinishTopology");
     }
     void UpdateAtlas() { check(gvdb2_update_atlas(v_), "UpdateAtlas"); }
+    // drops the nodes incremental rebuilds delinked (no reference counterpart)
+    void CompactPools() { check(gvdb2_compact_pools(v_), "CompactPools"); }
     // ActivateSpace(Vector3DF): the leaf's pool reference if it existed, else ID_UNDEFL
     uint64_t ActivateSpace(Vec3F pos) {
         const float p[3] = {pos.x, pos.y, pos.z};

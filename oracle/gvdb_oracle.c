@@ -938,6 +938,74 @@ uint64_t orc_activate_space(orc_volume *v, float x, float y, float z) {
 
 uint64_t orc_root(const orc_volume *v) { return v->root; }
 
+/* CompactPools (no reference counterpart): the nodes an incremental rebuild
+ * delinked (mParent = ID_UNDEF64, gvdbDelinkLeafBricks / gvdbDelinkBricks,
+ * N:401-467) are dropped; the rest keep their order and their references
+ * (parents, child-list entries, child-list index = node index) are
+ * renumbered.  Moves run toward lower indices in increasing order, so the
+ * compaction is done in place. */
+int orc_compact_pools(orc_volume *v) {
+    if (v->root == ID_UNDEFL) return ORC_OK;
+    int64_t *remap[ORC_MAXLEV] = {0};
+    int64_t kept[ORC_MAXLEV] = {0};
+    int st = ORC_OK;
+    for (int l = 0; l < v->nlev; l++) {
+        remap[l] = (int64_t *)malloc(sizeof(int64_t) * (size_t)(v->pool_cnt[l] + 1));
+        if (!remap[l]) {
+            st = ORC_ERR_STATE;
+            goto done;
+        }
+        for (int64_t i = 0; i < v->pool_cnt[l]; i++) remap[l][i] = v->pool[l][i].mParent == ID_UNDEF64 ? -1 : kept[l]++;
+    }
+    for (int l = 0; l < v->nlev; l++) {
+        const int64_t r3 = l > 0 ? res3_of(v, l) : 0;
+        for (int64_t i = 0; i < v->pool_cnt[l]; i++) {
+            const int64_t ni = remap[l][i];
+            if (ni < 0) continue;
+            orc_node nd = v->pool[l][i];
+            if (nd.mParent != ID_UNDEFL) {
+                const int pl = (int)((nd.mParent >> 8) & 0xFF);
+                const int64_t pi = (int64_t)(nd.mParent >> 16);
+                if (pl != l + 1 || pi >= v->pool_cnt[pl] || remap[pl][pi] < 0) {
+                    st = ORC_ERR_STATE;
+                    goto done;
+                }
+                nd.mParent = elem(0, pl, (uint64_t)remap[pl][pi]);
+            }
+            if (l > 0 && nd.mChildList != ID_UNDEFL) {
+                const uint64_t *src = v->clist[l] + (int64_t)(nd.mChildList >> 16) * r3;
+                uint64_t *dst = v->clist[l] + ni * r3;
+                for (int64_t b = 0; b < r3; b++) {
+                    const uint64_t e = src[b];
+                    uint64_t ne = ID_UNDEF64;
+                    if (e != ID_UNDEF64) {
+                        const int64_t ci = (int64_t)(e >> 16);
+                        if ((int)((e >> 8) & 0xFF) != l - 1 || ci >= v->pool_cnt[l - 1] || remap[l - 1][ci] < 0) {
+                            st = ORC_ERR_STATE;
+                            goto done;
+                        }
+                        ne = elem(0, l - 1, (uint64_t)remap[l - 1][ci]);
+                    }
+                    dst[b] = ne; /* dst <= src: an entry is read before it is overwritten */
+                }
+                nd.mChildList = elem(1, l, (uint64_t)ni);
+            }
+            v->pool[l][ni] = nd;
+        }
+    }
+    {
+        const int rl = (int)((v->root >> 8) & 0xFF);
+        v->root = elem(0, rl, (uint64_t)remap[rl][v->root >> 16]);
+    }
+    for (int l = 0; l < v->nlev; l++) {
+        v->pool_cnt[l] = kept[l];
+        if (l > 0) v->clist_cnt[l] = kept[l];
+    }
+done:
+    for (int l = 0; l < ORC_MAXLEV; l++) free(remap[l]);
+    return st;
+}
+
 /* ------------------------------------------------------------------ */
 /* atlas                                                                */
 /* ------------------------------------------------------------------ */

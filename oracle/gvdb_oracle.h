@@ -82,6 +82,7 @@ int orc_update_atlas(orc_volume *v);
 /* ActivateSpace (V:2766-2856): leaf reference if it existed, else ID_UNDEFL */
 uint64_t orc_activate_space(orc_volume *v, float x, float y, float z);
 uint64_t orc_root(const orc_volume *v); /* mRoot */
+int orc_compact_pools(orc_volume *v); /* drop delinked nodes, renumber the rest */
 int orc_clear_channel(orc_volume *v, int chan);
 
 int orc_insert_points(orc_volume *v, orc_view pos, int n, const float trans[3], int32_t *pnode, int32_t *poff, int32_t *gcnt);

@@ -60,6 +60,7 @@ def lib():
             "orc_update_atlas": (i32, [vp]),
             "orc_activate_space": (ctypes.c_uint64, [vp, f32, f32, f32]),
             "orc_root": (ctypes.c_uint64, [vp]),
+            "orc_compact_pools": (i32, [vp]),
             "orc_clear_channel": (i32, [vp, i32]),
             "orc_insert_points": (i32, [vp, _View, i32, fp, ip, ip, ip]),
             "orc_scatter_density": (i32, [vp, _View, i32, f32, f32, fp, i32, ip]),
@@ -184,6 +185,9 @@ class Oracle:
 
     def root(self):
         return int(self.L.orc_root(self.h))
+
+    def compact_pools(self):
+        _check(self.L.orc_compact_pools(self.h), "compact_pools")
 
     def update_atlas(self):
         _check(self.L.orc_update_atlas(self.h), "update_atlas")

@@ -254,3 +254,29 @@ def test_sparse_extent_takes_hash_path(gvdb2_mod, oracle_mod):
     v.UpdateAtlas()
     compare_topology(v, o)
     assert np.array_equal(v.atlas_map(), o.atlas_map())
+
+
+def test_compact_pools_bit_exact(gvdb2_mod, oracle_mod):
+    """CompactPools after incremental rebuilds left delinked nodes: pools,
+    child lists and atlas map match the oracle's compaction bit for bit, and
+    so do the incremental rebuilds and the scatter that follow."""
+    import torch
+    import gvdb2.workloads as wl
+    p, vel = wl.dam_block(sites=(48, 12, 48), origin=(40.0, 40.0, 40.0), seed=11)
+    o = make_oracle(oracle_mod)
+    v = gpu_volume(gvdb2_mod, p)
+    for step, q in enumerate(_drift_steps(p, vel, 6)):
+        assert o.rebuild_topology(q, 2.0) == 0
+        t = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+        v.SetPoints(t)
+        v._pts = t
+        v.RebuildTopology(len(q), 2.0)
+        if step == 3:
+            assert o.pool_count(0) > o.used_leaves()
+            o.compact_pools()
+            v.CompactPools()
+            assert o.pool_count(0) == o.used_leaves()
+        compare_topology(v, o)
+        o.update_atlas()
+        v.UpdateAtlas()
+        assert np.array_equal(v.atlas_map(), o.atlas_map())
