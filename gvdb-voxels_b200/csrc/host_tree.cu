@@ -1,3 +1,5 @@
+// Host-side operations on the node pools: ActivateSpace and CompactPools.
+//
 // ActivateSpace: activate the brick that holds a position, one position at
 // a time, by the reference's host tree walk (VolumeGVDB::ActivateSpace,
 // source/gvdb_library/src/gvdb_volume_gvdb.cpp:2766-2856, with Reparent
