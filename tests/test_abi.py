@@ -97,3 +97,18 @@ def test_cpp_facade_compiles_and_links(built_lib, tmp_path):
     r = subprocess.run([gxx, "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(out),
                         "-L", libdir, "-lgvdb2", f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_wrapper_argument_counts_match_header():
+    """Every ctypes binding passes as many arguments as the header declares:
+    a binding slip would otherwise show only on a GPU."""
+    import re
+    from gvdb2 import _lib
+    txt = re.sub(r"/\*.*?\*/", "", open(_lib.HEADER).read(), flags=re.S)
+    decls = dict(re.findall(r"GVDB2_API\s+[\w\s\*]*?\b(gvdb2_\w+)\s*\(([^)]*)\)\s*;", txt))
+    assert decls, "no declarations parsed"
+    for name, params in decls.items():
+        p = params.strip()
+        n = 0 if p in ("", "void") else p.count(",") + 1
+        if name in _lib._SIGS:
+            assert len(_lib._SIGS[name]) == n, f"{name}: header takes {n} arguments, binding {len(_lib._SIGS[name])}"
