@@ -261,6 +261,8 @@ gvdb2_status insert_points_subcell(Volume *v, int sc, int n, float radius, const
 gvdb2_status get_min_max_vel(Volume *v, int n);
 
 // ---- splat.cu ----
+// 1 to kMaxSplatChan channels, each one that the volume holds
+gvdb2_status check_chans(Volume *v, const int *chans, int nch);
 gvdb2_status scatter_density_ref(Volume *v, int n, float radius, float amp, const float trans[3], int expand);
 gvdb2_status gather_voxels(Volume *v, int sc, float radius, int chan, int accum, bool levelset, bool fp16 = false);
 gvdb2_status scatter_kernel(Volume *v, int kernel, int n, const float trans[3], gvdb2_points_view weight,

@@ -252,6 +252,15 @@ gvdb2_status write_pools(Volume *v, HostTree &t) {
 
 } // namespace
 
+namespace {
+// A refused batch leaves the device pools as they were; its results are all
+// ID_UNDEFL, so no entry refers to a node of the discarded host mirror.
+gvdb2_status refuse_batch(Volume *v, gvdb2_status st, const char *msg, uint64_t *out, int64_t n) {
+    for (int64_t i = 0; i < n; i++) out[i] = kUndefL;
+    return fail(v, st, msg);
+}
+} // namespace
+
 gvdb2_status activate_space(Volume *v, const float *xyz, int64_t n, uint64_t *out) {
     if (v->nlev <= 0) return fail(v, GVDB2_ERR_STATE, "ActivateSpace before Configure");
     if (n == 0) return GVDB2_OK;
@@ -265,17 +274,19 @@ gvdb2_status activate_space(Volume *v, const float *xyz, int64_t n, uint64_t *ou
         }
         const int p[3] = {(int)x[0], (int)x[1], (int)x[2]}; // Vector3DF -> Vector3DI truncates toward zero
         if (t.root == kUndefL && (p[0] < 0 || p[1] < 0 || p[2] < 0))
-            return fail(v, GVDB2_ERR_UNSUPPORTED,
-                        "ActivateSpace: a first position with a negative coordinate would root the tree at negative "
-                        "brick coordinates");
+            return refuse_batch(v, GVDB2_ERR_UNSUPPORTED,
+                                "ActivateSpace: a first position with a negative coordinate would root the tree at "
+                                "negative brick coordinates", out, n);
         bool fresh = false;
         const uint64_t r = t.walk(t.root, p, fresh, kUndefL, 0);
-        if (t.broken) return fail(v, GVDB2_ERR_UNSUPPORTED, "ActivateSpace: child lists out of node order");
+        if (t.broken)
+            return refuse_batch(v, GVDB2_ERR_UNSUPPORTED, "ActivateSpace: child lists out of node order", out, n);
         out[i] = (r == kUndefL || fresh) ? kUndefL : r;
     }
     if (t.root == kUndefL) return GVDB2_OK; // nothing was activated
     if (ref_ndx(t.root) != 0)
-        return fail(v, GVDB2_ERR_UNSUPPORTED, "ActivateSpace: new root is not the first node of its level");
+        return refuse_batch(v, GVDB2_ERR_UNSUPPORTED, "ActivateSpace: new root is not the first node of its level",
+                            out, n);
     GV_TRY(write_pools(v, t));
     return adopt_pools(v, ref_lev(t.root));
 }

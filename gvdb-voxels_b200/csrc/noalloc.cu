@@ -23,7 +23,9 @@
 // a stand-in symbol, not a device address.  The first call on each device
 // (with that device current) looks the address up with
 // cudaGetSymbolAddress and caches it; that first call should come before any
-// stream capture.
+// stream capture.  The cached address belongs to the device's current
+// context: a process that calls cudaDeviceReset must not call this entry
+// point on that device afterwards (the module is reloaded at a new address).
 #include <mutex>
 
 #include "dev_common.cuh"
@@ -153,6 +155,10 @@ extern "C" gvdb2_status gvdb2_gather_kernel_noalloc(gvdb2_volume *h, int kernel,
         return fail(v, GVDB2_ERR_CAPACITY,
                     "gvdb2_gather_kernel_noalloc takes at most 32,768 active 8^3 cells (bricks of 8^3 voxels)");
     if (!out || out_stride < nch) return fail(v, GVDB2_ERR_ARG, "bad output buffer");
+    // every argument is checked before the first memset or launch, so a
+    // refused call leaves `out` and the scratch array as they were
+    if (kernel != GVDB2_KERNEL_TENT1 && kernel != GVDB2_KERNEL_CUBIC2) return fail(v, GVDB2_ERR_ARG, "unknown kernel");
+    GV_TRY(check_chans(v, chans, nch));
     const float zero[3] = {0, 0, 0};
     if (!trans) trans = zero;
     uint32_t *base = nullptr;

@@ -967,13 +967,6 @@ AtlasGeom atlas_geom(const Volume *v) {
     return A;
 }
 
-gvdb2_status check_chans(Volume *v, const int *chans, int nch) {
-    if (!chans || nch < 1 || nch > kMaxSplatChan) return fail(v, GVDB2_ERR_ARG, "1 to 8 channels per splat call");
-    for (int c = 0; c < nch; c++)
-        if (chans[c] < 0 || chans[c] >= kMaxChan || !v->has_chan[chans[c]]) return fail(v, GVDB2_ERR_ARG, "bad channel");
-    return GVDB2_OK;
-}
-
 template <class Args>
 void fill_topology(Volume *v, Args &S) {
     S.slot_leaf = v->slot_leaf.as<int32_t>();
@@ -1136,6 +1129,13 @@ void set_attrs(uint32_t &mask, PointsView *dst, const gvdb2_points_view *attrs, 
 }
 
 } // namespace
+
+gvdb2_status check_chans(Volume *v, const int *chans, int nch) {
+    if (!chans || nch < 1 || nch > kMaxSplatChan) return fail(v, GVDB2_ERR_ARG, "1 to 8 channels per splat call");
+    for (int c = 0; c < nch; c++)
+        if (chans[c] < 0 || chans[c] >= kMaxChan || !v->has_chan[chans[c]]) return fail(v, GVDB2_ERR_ARG, "bad channel");
+    return GVDB2_OK;
+}
 
 gvdb2_status scatter_density_ref(Volume *v, int n, float radius, float amp, const float trans[3], int expand) {
     (void)amp; // unused by the reference kernel (P:525-573)

@@ -146,7 +146,9 @@ GVDB2_API gvdb2_status gvdb2_update_atlas(gvdb2_volume *v);                     
  * the tree, a new covering root.  out[i] (host) = the leaf's pool reference
  * when it existed, GVDB2_ID_UNDEFL when the call created it or the position
  * lies outside the top configured level.  Synchronises the stream; the next
- * RebuildTopology starts from a full rebuild. */
+ * RebuildTopology starts from a full rebuild.  A refused batch (status other
+ * than GVDB2_OK) leaves the pools unchanged and sets every out[i] to
+ * GVDB2_ID_UNDEFL. */
 #define GVDB2_ID_UNDEFL 0xFFFFFFFFull
 GVDB2_API gvdb2_status gvdb2_activate_space(gvdb2_volume *v, const float *xyz, int64_t n, uint64_t *out);
 /* Pool compaction (no reference counterpart; the reference keeps the nodes an
