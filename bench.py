@@ -1,15 +1,23 @@
 """Benchmark of the point -> sparse-volume step on B200.
 
-Workload (the dynamic SPH-like configuration): 4,194,304 points on a jittered
-lattice filling a 256x128x256-voxel block, velocity ~ N(0,1), Configure
-(3,3,3,3,3) (8^3 bricks, apron 1), channels density + 3 x velocity.  One step:
-advect p += 0.1 v -> RebuildTopology(N, 2.0) -> UpdateAtlas -> cubic B-spline
-scatter (r = 2) of mass and momentum -> UpdateApron -> cubic gather of the 3
-velocity channels back to the points.
+Default workload (the dynamic step the throughput target is stated on):
+16,777,216 points on a jittered lattice (256 x 256 x 256 sites at spacing
+(1, 0.5, 1)) filling a 256x128x256-voxel dam block, velocity ~ N(0,1),
+Configure(3,3,3,3,3) (8^3 bricks, apron 1), channels density + 3 x velocity.
+One step: advect p += 0.1 v -> RebuildTopology(N, 2.0) -> UpdateAtlas ->
+cubic B-spline scatter (r = 2) of mass and momentum -> UpdateApron -> cubic
+gather of the 3 velocity channels back to the points.
 
-`python bench.py [--gpus N --steps K --warmup W]` prints one JSON line.
-`--impl reference` times the CPU restatement of the reference's path on the
-host cores instead (the reference's host library does not build here).
+`python bench.py [--gpus N --steps K --warmup W]` prints one JSON line.  At
+N = 1 the line also carries the rest of the metric, each measured in the same
+run: the 4,194,304-point dynamic step, the incremental topology state
+machine, the adjoint step against the forward step, the 64 batched clouds
+against a per-cloud loop, and the reference's own CUDA kernels against this
+library on the reference's point path.
+`--impl reference` times the reference's host path (ActivateSpace topology,
+host atlas, CPU splat and gather) on all host cores instead: the reference's
+host library does not build here (it needs GL), so this is the CPU
+restatement of that path.
 """
 import argparse
 import json
@@ -23,12 +31,17 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "gvdb-voxels_b200"))
 
 METRIC = "points/s rebuild+scatter+gather at <=1e-5 err, % HBM peak; adjoint & batched vs plain"
-WORKLOAD = "dynamic SPH-like step: 4,194,304-pt jittered lattice, cubic B-spline r=2, density+3 vel channels"
-WORKLOAD_16M = "dynamic SPH-like step: 16,777,216-pt jittered lattice (spacing 1,0.5,1), cubic B-spline r=2, 4 channels"
-N_POINTS = 4_194_304
-SITES = (256, 64, 256)
 DT = 0.1
 RADIUS = 2.0
+
+WORKLOADS = {
+    "dam16m": dict(sites=(256, 256, 256), spacing=(1.0, 0.5, 1.0),
+                   desc="dynamic SPH-like step: 16,777,216-pt jittered lattice (256x256x256 sites, spacing 1,0.5,1) "
+                        "in a 256x128x256-voxel block, cubic B-spline r=2, density+3 vel channels"),
+    "dam": dict(sites=(256, 64, 256), spacing=(1.0, 2.0, 1.0),
+                desc="dynamic SPH-like step: 4,194,304-pt jittered lattice (256x64x256 sites, spacing 1,2,1) "
+                     "in a 256x128x256-voxel block, cubic B-spline r=2, density+3 vel channels"),
+}
 
 
 def parse():
@@ -38,12 +51,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="the main line only (no 4M, incremental, adjoint, "
+                                                              "batched or reference-kernel legs)")
     ap.add_argument("--incremental", action="store_true", help="reference state machine instead of full rebuilds")
     ap.add_argument("--quick", action="store_true", help="timed steps only (no baseline, e2e or launch count)")
-    ap.add_argument("--sites", default="256,64,256", help="lattice sites x,y,z (smaller cases for profiling)")
-    ap.add_argument("--workload", default="dam", choices=["dam", "dam16m", "batched", "adjoint", "sparse67m"],
-                    help="dam: the contract line (dynamic step, 4,194,304 points); dam16m: the same step on "
-                         "16,777,216 points; batched: 64 clouds, batch vs per-cloud loop; adjoint: the "
+    ap.add_argument("--sites", default=None, help="lattice sites x,y,z (smaller cases for profiling)")
+    ap.add_argument("--workload", default="dam16m", choices=["dam16m", "dam", "batched", "adjoint", "sparse67m"],
+                    help="dam16m: the contract line (dynamic step, 16,777,216 points); dam: the same step on "
+                         "4,194,304 points; batched: 64 clouds, batch vs per-cloud loop; adjoint: the "
                          "differentiable splat, adjoint vs forward; sparse67m: the large sparse scene "
                          "(67,108,864-point Gaussian mixture, 32^3 bricks, forward + adjoint)")
     ap.add_argument("--points", type=int, default=0, help="sparse67m: fewer points (smaller cases for profiling)")
@@ -105,6 +120,25 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def workload_points(a):
+    """(positions, velocities, description) of the dam-block workload."""
+    import gvdb2.workloads as wl
+    w = WORKLOADS[a.workload]
+    sites = tuple(int(x) for x in a.sites.split(",")) if a.sites else w["sites"]
+    pos, vel = wl.dam_block(sites=sites, spacing=w["spacing"])
+    desc = w["desc"] if not a.sites else f"{w['desc']} (reduced to {sites[0]}x{sites[1]}x{sites[2]} sites)"
+    return pos, vel, desc
+
+
+def static_config(a, n, ws):
+    """The workload as both arms name it (no measured quantities)."""
+    desc = WORKLOADS[a.workload]["desc"] if not a.sites else f"{a.workload} sites {a.sites}"
+    return {"workload": desc, "points_per_gpu": int(n),
+            "rebuild": "incremental state machine" if a.incremental else "full rebuild every step",
+            "l2": "inputs larger than L2 (positions + velocities alone exceed 126 MB)",
+            "parallelism": f"replicas x{ws}"}
+
+
 class Pipeline:
     """The benchmark step over libgvdb2 (through the VolumeGVDB mirror)."""
 
@@ -137,31 +171,17 @@ class Pipeline:
         self.attrs = [None, (vel, 0), (vel, 1), (vel, 2)]
         self.v.SetPoints(pos)
 
-    def step(self, events=None):
+    def step(self):
         v, n, K = self.v, self.n, self.gvdb2.KERNEL_CUBIC2
-        rec = (lambda name: events.append((name, self._ev()))) if events is not None else (lambda name: None)
-        rec("start")
         self.pos.add_(self.vel, alpha=DT)  # advect (the simulation's own update)
-        rec("advect")
+        v.SetPoints(self.pos)  # positions changed in place: the binning is redone
         if self.full:
             v.RequestFullRebuild(True)
         v.RebuildTopology(n, RADIUS)
         v.UpdateAtlas()
-        rec("topology")
-        if events is not None:  # bin first so the scatter interval is the scatter kernel alone
-            v.GatherKernel(K, n, [1, 2, 3], out=self.out)
-            rec("binning")
         v.ScatterKernel(K, n, [0, 1, 2, 3], weight=1.0, attrs=self.attrs)
-        rec("scatter")
         v.UpdateApron(-1, 0.0)
-        rec("apron")
         v.GatherKernel(K, n, [1, 2, 3], out=self.out)
-        rec("gather")
-
-    def _ev(self):
-        e = self.torch.cuda.Event(enable_timing=True)
-        e.record()
-        return e
 
     def geometry(self):
         inf = self.v.info()
@@ -171,11 +191,17 @@ class Pipeline:
 
 
 # ----------------------------------------------------------------------------
-# CPU restatement (oracle) timing: the reference arm and the cpu_baseline leg
+# The reference's host path on the CPU: the cpu_baseline leg and the
+# reference arm.  The reference's host library does not build here (GL), so
+# its path runs as the C restatement: ActivateSpace at every brick of each
+# point's activation box (the host topology build), the host atlas
+# assignment, then the splat, apron and gather loops.
 # ----------------------------------------------------------------------------
-def _oracle_step(args):
-    """One step of the workload on the CPU oracle over a sample of points."""
-    pos, vel = args
+_SHM = {}
+
+
+def _host_step(pos, vel):
+    """One step of the workload on the host path over (pos, vel); seconds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import oracle
@@ -185,9 +211,7 @@ def _oracle_step(args):
     for c in range(4):
         o.add_channel(c, 1)
     p = (pos + np.float32(DT) * vel).astype(np.float32)
-    st = o.rebuild_topology(p, RADIUS)
-    if st != 0:
-        raise RuntimeError(f"oracle rebuild failed: {st}")
+    o.activate_points(p, RADIUS)
     o.update_atlas()
     o.scatter_kernel(oracle.KERNEL_CUBIC2, p, [0, 1, 2, 3], attrs=[None, vel[:, 0], vel[:, 1], vel[:, 2]])
     for c in range(4):
@@ -197,46 +221,75 @@ def _oracle_step(args):
     return time.perf_counter() - t0
 
 
-def _sample(pos, vel, n, part=0):
-    """A contiguous run of lattice rows (a spatial sub-block of the dam)."""
-    start = (part * n) % max(1, len(pos) - n)
-    return pos[start:start + n].copy(), vel[start:start + n].copy()
+def _attach(name, n):
+    import numpy as np
+    from multiprocessing import shared_memory
+    if name not in _SHM:
+        shm = shared_memory.SharedMemory(name=name)
+        _SHM[name] = (shm, np.ndarray((n, 6), np.float32, buffer=shm.buf))
+    return _SHM[name][1]
 
 
-def cpu_baseline(pos, vel, n=N_POINTS):
-    dt = _oracle_step(_sample(pos, vel, n))
+def _host_task(args):
+    name, n, start, count = args
+    buf = _attach(name, n)
+    pv = buf[start:start + count]
+    return _host_step(pv[:, :3].copy(), pv[:, 3:].copy())
+
+
+def cpu_baseline(pos, vel, n):
+    """The host path single-threaded on a contiguous sub-block of n points."""
+    n = min(n, len(pos))
+    dt = _host_step(pos[:n].copy(), vel[:n].copy())
     return {"value": n / dt, "unit": "points/s", "cores": 1, "kind": "port",
-            "sample": f"one full step over {n} lattice points, single-threaded C restatement",
+            "sample": f"one step over the first {n} lattice points (a contiguous slab of the block): host "
+                      "ActivateSpace topology, host atlas, CPU cubic splat, apron and gather, single-threaded",
             "seconds": round(dt, 3)}
 
 
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
     import multiprocessing as mp
-    import gvdb2.workloads as wl
-    pos, vel = wl.dam_block(sites=SITES)
+    import numpy as np
+    from multiprocessing import shared_memory
+    pos, vel, _ = workload_points(a)
+    n = len(pos)
     cores = os.cpu_count() or 1
-    per = 262_144
-    samples = [_sample(pos, vel, per, k) for k in range(cores)]
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        for _ in range(a.warmup):
-            pool.map(_oracle_step, samples)
-        times = []
-        for _ in range(a.steps):
-            t0 = time.perf_counter()
-            pool.map(_oracle_step, samples)
-            times.append(time.perf_counter() - t0)
+    per = min(262_144, max(1, n // cores))
+    shm = shared_memory.SharedMemory(create=True, size=n * 24)
+    try:
+        buf = np.ndarray((n, 6), np.float32, buffer=shm.buf)
+        buf[:, :3] = pos
+        buf[:, 3:] = vel
+        del pos, vel
+        stride = max(per, (n - per) // max(1, cores - 1))
+        tasks = [(shm.name, n, min(k * stride, n - per), per) for k in range(cores)]
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(cores) as pool:
+            for _ in range(a.warmup):
+                pool.map(_host_task, tasks)
+            times = []
+            for _ in range(a.steps):
+                t0 = time.perf_counter()
+                pool.map(_host_task, tasks)
+                times.append(time.perf_counter() - t0)
+        del buf
+    finally:
+        shm.close()
+        shm.unlink()
     total = sum(times)
     value = per * cores * a.steps / total
+    sample = (f"{cores} processes, each one step over its own contiguous slab of {per} lattice points per "
+              f"timed step: host ActivateSpace topology (single-threaded per volume, as the reference), host "
+              f"atlas, CPU cubic splat, apron and gather")
     line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1e3 * total / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "sample_points_per_step": per * cores},
-            "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": "port",
-                             "sample": f"{cores} processes x {per} contiguous lattice points per step"},
+            "config": static_config(a, n, ws),
+            "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -247,7 +300,6 @@ def run_reference(a):
 # ----------------------------------------------------------------------------
 def stage_times(pipe, reps=7):
     """Median device time of each stage (one launch each for the splats)."""
-    import statistics as st
     import torch
     v, n, K = pipe.v, pipe.n, pipe.gvdb2.KERNEL_CUBIC2
 
@@ -263,7 +315,7 @@ def stage_times(pipe, reps=7):
             b.record()
             torch.cuda.synchronize()
             ts.append(a.elapsed_time(b))
-        return st.median(ts)
+        return statistics.median(ts)
 
     def topo():
         v.RequestFullRebuild(True)
@@ -358,11 +410,24 @@ def e2e_pipelined(pipe, pos, vel, steps, barrier):
     return e0.elapsed_time(e1)
 
 
+def timed_steps(pipe, steps, warmup):
+    """Device ms of `steps` pipeline steps after `warmup` untimed ones."""
+    import torch
+    for _ in range(warmup):
+        pipe.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        pipe.step()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
 def run_ours(a):
-    import numpy as np
     import torch
     import torch.distributed as dist
-    import gvdb2.workloads as wl
     from gvdb2 import metrics
 
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -372,14 +437,10 @@ def run_ours(a):
     if ws > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    if a.workload == "dam16m":  # 256x256x256 sites at spacing (1, 0.5, 1): the same block, 4x denser
-        pos, vel = wl.dam_block(sites=(256, 256, 256), spacing=(1.0, 0.5, 1.0))
-    else:
-        sites = tuple(int(x) for x in a.sites.split(","))
-        pos, vel = wl.dam_block(sites=sites)
+    pos, vel, desc = workload_points(a)
     cpu = None
     if rank == 0 and ws == 1 and not (a.no_cpu_baseline or a.quick):
-        cpu = cpu_baseline(pos, vel)
+        cpu = cpu_baseline(pos, vel, 4_194_304)
 
     pipe = Pipeline(local, pos, vel, full_rebuild=not a.incremental)
     n = pipe.n
@@ -414,7 +475,7 @@ def run_ours(a):
     if a.quick:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
-                              "ms_per_step": ms / a.steps, "quick": True}), flush=True)
+                              "ms_per_step": ms / a.steps, "quick": True, "workload": desc}), flush=True)
         return 0
 
     # per-stage device times: each stage repeated on the launching stream,
@@ -426,16 +487,17 @@ def run_ours(a):
     stages = {}
     for k in ("topology", "binning", "scatter", "apron", "gather"):
         gbs = sb[k] / (stage_ms[k] / 1e3) / 1e9 if stage_ms.get(k) else None
-        stages[k] = {"ms": round(stage_ms.get(k, 0.0), 4), "alg_bytes": sb[k], "GBps": gbs}
+        stages[k] = {"ms": round(stage_ms.get(k, 0.0), 4), "alg_bytes": sb[k], "GBps": gbs,
+                     "frac_of_peak": gbs / peak if gbs else None}
     dom = max(("scatter", "gather", "apron"), key=lambda k: stage_ms.get(k, 0.0))
     achieved = sb[dom] / (stage_ms[dom] / 1e3) / 1e9
-    kernel_name = {"scatter": "scatter stage: k_scatter_own<cubic,4> (heavy and light cells) + "
-                              "k_scatter_merge_cta<cubic,4>",
-                   "gather": "k_gather_tile<cubic,fwd,3> + k_gather_light<cubic,fwd,3>", "apron": "k_apron"}[dom]
+    step_alg = sum(sb.values())
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": TRAFFIC_PER_BRICK[dom] * geo["B"] if dom in TRAFFIC_PER_BRICK else None,
-                "kernel": kernel_name, "peak_source": peak_kind,
-                "traffic_source": "ncu capture of the 4,194,304-point block, scaled by bricks"}
+                "kernel": STAGE_KERNELS[dom], "stage": dom, "peak_source": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
+                "traffic_source": TRAFFIC_SOURCE,
+                "step": {"alg_bytes": step_alg, "achieved": step_alg / (ms / a.steps / 1e3) / 1e9,
+                         "frac": step_alg / (ms / a.steps / 1e3) / 1e9 / peak}}
 
     # end to end through the public API: every step copies its inputs from
     # pinned host memory and reads its gathered velocities back.  Two device
@@ -450,33 +512,208 @@ def run_ours(a):
     pipe.v.SetStream(0)
     barrier()
     launches = count_launches(pipe) * a.steps
+    extras = {}
+    if rank == 0 and ws == 1 and not a.no_extras and not a.sites:
+        del pipe
+        torch.cuda.empty_cache()
+        extras = run_extras(a, pos, vel)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
                 "warmup": max(3, a.warmup), "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD if a.workload == "dam" else WORKLOAD_16M,
-                           "points_per_gpu": n, "bricks": geo["B"], "nodes": geo["U"],
-                           "rebuild": "incremental state machine" if a.incremental else "full rebuild every step",
-                           "l2": "inputs larger than L2 (positions+velocities 100 MB, atlas "
-                                 f"{4 * 4 * geo['B'] * geo['T'] / 1e6:.0f} MB per step)",
-                           "parallelism": f"replicas x{ws}"},
+                "config": static_config(a, n, ws),
+                "geometry": {"bricks": geo["B"], "nodes": geo["U"],
+                             "atlas_mb_per_channel": round(4 * geo["B"] * geo["T"] / 1e6, 1)},
                 "roofline": roofline, "stages": stages, "clocks": clk, "e2e": e2e, "gpu_launches": launches,
                 "cpu_baseline": cpu}
+        line.update(extras)
         print(json.dumps(line), flush=True)
-    del pipe
     if ws > 1:
         dist.destroy_process_group()
     return 0
 
 
-# DRAM bytes (read + write) per brick of each stage's kernels, from the ncu
-# capture of the 4,194,304-point block (23,396 bricks; summary in
-# profiles/k_scatter_own_merge_gather_dam4m.md).  Traffic grows with the brick
-# count, so a launch moves about this many bytes x bricks.
+# DRAM bytes (read + write) per brick of each stage's kernels, from an ncu
+# capture of one launch of each kernel on the 4,194,304-point block,
+# divided by its bricks.  Traffic grows with the brick count, so a launch
+# moves about this many bytes x bricks.
 TRAFFIC_PER_BRICK = {
     "scatter": (199.4e6 + 406.3e6 + 752.9e6 + 220.4e6) / 23396,
     "gather": (635.0e6 + 42.7e6 + 3.3e6 + 0.0) / 23396,
 }
+TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4,194,304-point block, scaled by bricks"
+STAGE_KERNELS = {"scatter": "scatter stage: k_scatter_own<cubic,4> (heavy and light cells) + "
+                            "k_scatter_merge_cta<cubic,4>",
+                 "gather": "k_gather_tile<cubic,fwd,3> + k_gather_light<cubic,fwd,3>", "apron": "k_apron"}
+
+
+# ----------------------------------------------------------------------------
+# the rest of the metric, each measured in the same run (N = 1)
+# ----------------------------------------------------------------------------
+def run_extras(a, pos16, vel16):
+    import torch
+    out = {}
+
+    def guard(name, f):
+        try:
+            out[name] = f()
+        except Exception as e:  # an extra leg never takes the main line down
+            out[name] = {"error": f"{type(e).__name__}: {e}"[:300]}
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
+    guard("incremental", lambda: extra_incremental(pos16, vel16, a.warmup))
+    guard("config1_4m", lambda: extra_config1())
+    guard("adjoint", lambda: measure_adjoint(steps=20, warmup=3))
+    guard("batched", lambda: measure_batched(steps=3, warmup=1))
+    guard("vs_ref_kernels", lambda: extra_ref_kernels())
+    summary = {}
+    if isinstance(out.get("adjoint"), dict) and "adjoint_over_forward" in out["adjoint"]:
+        summary["adjoint_over_forward"] = out["adjoint"]["adjoint_over_forward"]
+    if isinstance(out.get("batched"), dict) and "speedup_vs_loop" in out["batched"]:
+        summary["batched_over_loop"] = out["batched"]["speedup_vs_loop"]
+    if isinstance(out.get("vs_ref_kernels"), dict) and "speedup_device" in out["vs_ref_kernels"]:
+        summary["vs_ref_kernels"] = out["vs_ref_kernels"]["speedup_device"]
+    out.update(summary)
+    return out
+
+
+def extra_incremental(pos, vel, warmup):
+    """The reference's state machine on the 16M-point step (the first two
+    RebuildTopology calls full, incremental from the third, V:1181-1218):
+    10 steps of the advect, timed after `warmup` steps, against the same
+    steps with a full rebuild every step."""
+    res = {}
+    for name, full in (("incremental", False), ("full", True)):
+        pipe = Pipeline(0, pos, vel, full_rebuild=full)
+        ms = timed_steps(pipe, 10, max(3, warmup))
+        inf = pipe.v.info()
+        res[name] = {"ms_per_step": ms / 10, "value": pipe.n * 10 / (ms / 1e3), "leaves": int(inf.pool_count[0]),
+                     "bricks": int(inf.atlas_slots)}
+        del pipe
+    res["incremental_over_full_speedup"] = res["full"]["ms_per_step"] / res["incremental"]["ms_per_step"]
+    res["workload"] = "16,777,216-pt dam block, 10 timed advect steps (dt 0.1), stale leaves kept by the state machine"
+    return res
+
+
+def extra_config1():
+    """The 4,194,304-point dynamic step (the configuration's own size)."""
+    import gvdb2.workloads as wl
+    pos, vel = wl.dam_block(sites=WORKLOADS["dam"]["sites"], spacing=WORKLOADS["dam"]["spacing"])
+    pipe = Pipeline(0, pos, vel, full_rebuild=True)
+    ms = timed_steps(pipe, 20, 3)
+    return {"workload": WORKLOADS["dam"]["desc"], "ms_per_step": ms / 20, "value": pipe.n * 20 / (ms / 1e3),
+            "unit": "points/s"}
+
+
+def extra_ref_kernels(steps=3, warmup=1):
+    """The reference's own CUDA kernels (the gvdb-voxels kernel module
+    compiled for sm_100a behind its host restatement, the prebuilt replay
+    library that also generated the golden vectors) against libgvdb2, both
+    on the reference's point path on the same advected 4,194,304 dam points:
+    RebuildTopology -> UpdateAtlas -> InsertPoints -> ScatterDensity ->
+    UpdateApron -> InsertPointsSubcell -> GatherDensity.  Per stage: device
+    time of the kernels, copies and fills (CUPTI), and host wall time
+    around the synchronised call (the reference's stages include host loops
+    and blocking copies)."""
+    import ctypes
+    import numpy as np
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    import gvdb2
+    import gvdb2.workloads as wl
+    lib = os.path.join(ROOT, "oracle", "_ref", "libgvdbref.so")
+    if not os.path.exists(lib):
+        return {"unavailable": "the replay library of the reference's kernels was not built"}
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden as mg
+    stages = ["rebuild", "atlas", "insert", "scatter", "apron", "subcell", "gather"]
+    pos, vel = wl.dam_block(sites=WORKLOADS["dam"]["sites"], spacing=WORKLOADS["dam"]["spacing"])
+    pts = []
+    p = pos
+    for _ in range(warmup + steps):
+        p = (p + np.float32(DT) * vel).astype(np.float32)
+        pts.append(np.ascontiguousarray(p))
+    mg.check_inputs(dict(cfg=(3, 3, 3, 3, 3), radius=RADIUS, pts=pts, ops=[]))  # every kernel box inside the root
+
+    def timed_stage(f):
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            t0 = time.perf_counter()
+            f()
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+        dev = sum(e.device_time for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA) / 1e3
+        return dev, wall * 1e3
+
+    def ref_side():
+        R = mg.Ref(0)
+        R("rd_configure", 3, 3, 3, 3, 3)
+        R("rd_add_channel", 0, 1)
+        zero = (ctypes.c_float * 3)(0, 0, 0)
+        ln = ctypes.c_int(0)
+        calls = {
+            "rebuild": lambda n: (R("rd_request_full_rebuild"), R("rd_rebuild_topology", n, RADIUS, zero)),
+            "atlas": lambda n: (R("rd_update_atlas"), R("rd_clear_channel", 0)),
+            "insert": lambda n: R("rd_insert_points", n, zero),
+            "scatter": lambda n: R("rd_scatter_density", n, 1.0, 1.0, zero, 0),
+            "apron": lambda n: R("rd_update_apron", 0, 0.0),
+            "subcell": lambda n: R("rd_insert_points_subcell", 4, n, RADIUS, zero, ctypes.byref(ln)),
+            "gather": lambda n: R("rd_gather_density", n, 1.0, 0, 0),
+        }
+        t = {k: [] for k in stages}
+        for q in pts:
+            R("rd_set_points", q.ctypes.data, len(q))
+            for k in stages:
+                t[k].append(timed_stage(lambda: calls[k](len(q))))
+        leaves = int(R.counts()[0])
+        R.close()
+        return t, leaves, ln.value
+
+    def our_side():
+        v = gvdb2.VolumeGVDB(0)
+        v.Configure(3, 3, 3, 3, 3)
+        v.AddChannel(0, gvdb2.T_FLOAT, 1)
+        box = {}
+        calls = {
+            "rebuild": lambda n: (v.RequestFullRebuild(True), v.RebuildTopology(n, RADIUS)),
+            "atlas": lambda n: (v.UpdateAtlas(), v.ClearChannel(0)),
+            "insert": lambda n: v.InsertPoints(n),
+            "scatter": lambda n: v.ScatterDensity(n, 1.0, 1.0, (0, 0, 0), False),
+            "apron": lambda n: v.UpdateApron(0, 0.0),
+            "subcell": lambda n: box.__setitem__("len", v.InsertPointsSubcell(4, n, RADIUS)),
+            "gather": lambda n: v.GatherDensity(4, n, 1.0, (0, 0, 0), box["len"], 0),
+        }
+        t = {k: [] for k in stages}
+        for q in pts:
+            tq = torch.from_numpy(q).cuda()
+            v.SetPoints(tq)
+            for k in stages:
+                t[k].append(timed_stage(lambda: calls[k](len(q))))
+        leaves = int(v.info().pool_count[0])
+        v.close()
+        return t, leaves, box["len"]
+
+    rt, rleaves, rlen = ref_side()
+    ot, oleaves, olen = our_side()
+    res = {"workload": "reference point path on the 4,194,304-pt dam block, advected 0.1 v per step; "
+                       f"{steps} timed steps after {warmup}",
+           "timing": "device: CUPTI kernel+copy+fill time per stage; host: wall time around the synchronised call",
+           "reference_ms": {}, "ours_ms": {}, "check": {"leaves": [rleaves, oleaves], "subcell_len": [rlen, olen]}}
+    dev_r = dev_o = wall_r = wall_o = 0.0
+    for k in stages:
+        dr = statistics.median(x[0] for x in rt[k][warmup:])
+        do = statistics.median(x[0] for x in ot[k][warmup:])
+        hr = statistics.median(x[1] for x in rt[k][warmup:])
+        ho = statistics.median(x[1] for x in ot[k][warmup:])
+        res["reference_ms"][k] = {"device": round(dr, 4), "host_wall": round(hr, 4)}
+        res["ours_ms"][k] = {"device": round(do, 4), "host_wall": round(ho, 4)}
+        dev_r, dev_o, wall_r, wall_o = dev_r + dr, dev_o + do, wall_r + hr, wall_o + ho
+    res["reference_ms"]["total"] = {"device": round(dev_r, 4), "host_wall": round(wall_r, 4)}
+    res["ours_ms"]["total"] = {"device": round(dev_o, 4), "host_wall": round(wall_o, 4)}
+    res["speedup_device"] = dev_r / dev_o if dev_o > 0 else None
+    res["speedup_host_wall"] = wall_r / wall_o if wall_o > 0 else None
+    return res
 
 
 # ----------------------------------------------------------------------------
@@ -498,22 +735,16 @@ def batched_step(v, K, n, chans_fwd, grad_chan, go):
     v.ScatterDensityBackward(K, n, [grad_chan], weight=1.0, grad_pos=go[2], grad_weight=go[3], grad_attr=go[4])
 
 
-def run_batched(a):
+def measure_batched(steps, warmup, env=None):
     """The 64 clouds in one batched pass against a per-cloud loop.  Under
     torchrun the clouds are spread over the ranks (LPT by size, no data-path
     collective); each rank batches its own share and the time is the max
     over the ranks."""
-    import numpy as np
     import torch
     import gvdb2
     import gvdb2.workloads as wl
     from gvdb2 import shard
-    env = shard.RankEnv.from_env()
-    torch.cuda.set_device(env.local)
-    if env.world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    env = env or shard.RankEnv()
     all_clouds, _ = wl.batched_clouds()
     mine = shard.lpt_partition([len(c) for c in all_clouds], env.world)[env.rank]
     clouds = [all_clouds[i] for i in mine]
@@ -549,26 +780,27 @@ def run_batched(a):
             vl.SetPoints(t)
             batched_step(vl, K, len(t), [0], 1, gol[c])
 
-    def timed(f, steps):
-        for _ in range(max(1, a.warmup)):
+    def timed(f, k):
+        import torch.distributed as dist
+        for _ in range(max(1, warmup)):
             f()
         torch.cuda.synchronize()
         if env.world > 1:
             dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(steps):
+        for _ in range(k):
             f()
         e1.record()
         torch.cuda.synchronize()
         if env.world > 1:
             dist.barrier()
-        return shard.max_over_ranks(e0.elapsed_time(e1) / steps, device=f"cuda:{env.local}")
+        return shard.max_over_ranks(e0.elapsed_time(e1) / k, device=f"cuda:{env.local}")
 
     clocks = Clocks(env.local)
     clocks.start()
-    ms_b = timed(step_batched, a.steps)
-    ms_l = timed(step_loop, max(1, a.steps // 4))
+    ms_b = timed(step_batched, steps)
+    ms_l = timed(step_loop, max(1, steps))
     clk = clocks.stop()
     # identical results, cloud by cloud
     first = vb.BatchPoints(dev, BATCH_SPACE_LOG2)
@@ -577,18 +809,33 @@ def run_batched(a):
     same = all(bool(torch.equal(gob[0][first[c]:first[c + 1]], gol[c][0])) and
                bool(torch.equal(gob[2][first[c]:first[c + 1]], gol[c][2])) for c in range(len(clouds)))
     same = shard.max_over_ranks(0.0 if same else 1.0, device=f"cuda:{env.local}") == 0.0
-    if env.rank == 0:
-        line = {"metric": METRIC, "workload": f"batched: {len(all_clouds)} Gaussian clouds, {job_total} points, sizes "
-                "log-uniform in [1e4, 2e6], each in its own 1024^3 space; cubic B-spline r=2, density; "
-                "forward + adjoint",
-                "value": job_total / (ms_b / 1e3), "unit": "points/s", "ms_per_step": ms_b,
-                "per_cloud_loop": {"value": job_total / (ms_l / 1e3), "ms_per_step": ms_l},
-                "speedup_vs_loop": ms_l / ms_b, "identical_to_loop": same, "n_gpus": env.world,
-                "scaling": "strong", "parallelism": f"clouds over {env.world} ranks (LPT by size)",
-                "steps": a.steps, "data": "synthetic", "dtype": "f32", "clocks": clk}
-        print(json.dumps(line), flush=True)
     del vb, vl
+    return {"workload": f"batched: {len(all_clouds)} Gaussian clouds, {job_total} points, sizes log-uniform in "
+                        "[1e4, 2e6], each in its own 1024^3 space; cubic B-spline r=2, density; forward + adjoint",
+            "value": job_total / (ms_b / 1e3), "unit": "points/s", "ms_per_step": ms_b,
+            "per_cloud_loop": {"value": job_total / (ms_l / 1e3), "ms_per_step": ms_l},
+            "speedup_vs_loop": ms_l / ms_b, "identical_to_loop": same, "n_gpus": env.world,
+            "scaling": "strong", "parallelism": f"clouds over {env.world} ranks (LPT by size)", "steps": steps,
+            "clocks": clk}
+
+
+def run_batched(a):
+    import torch
+    from gvdb2 import shard
+    env = shard.RankEnv.from_env()
+    torch.cuda.set_device(env.local)
     if env.world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = measure_batched(a.steps, a.warmup, env)
+    if env.rank == 0:
+        line = {"metric": METRIC}
+        line.update(res)
+        line.update({"data": "synthetic", "dtype": "f32"})
+        print(json.dumps(line), flush=True)
+    if env.world > 1:
+        import torch.distributed as dist
         dist.destroy_process_group()
     return 0
 
@@ -596,7 +843,7 @@ def run_batched(a):
 # ----------------------------------------------------------------------------
 # differentiable splat: adjoint step vs forward step
 # ----------------------------------------------------------------------------
-def run_adjoint(a):
+def measure_adjoint(steps, warmup):
     """1,000,000 shell points splatted with the tent kernel into their own
     topology; loss = sum over voxels of (rho - rho_target)^2 plus the sum of
     the density gathered back at the points.  Forward = splat + loss +
@@ -641,28 +888,35 @@ def run_adjoint(a):
         v.ScatterDensityBackward(K, n, [2], weight=1.0, grad_pos=gp_s, grad_weight=gw, grad_attr=ga)
 
     def timed(f):
-        for _ in range(max(3, a.warmup)):
+        for _ in range(max(3, warmup)):
             f()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(a.steps):
+        for _ in range(steps):
             f()
         e1.record()
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / a.steps
+        return e0.elapsed_time(e1) / steps
 
     clocks = Clocks(0)
     clocks.start()
     ms_f = timed(forward)
     ms_b = timed(adjoint)
     clk = clocks.stop()
-    line = {"metric": METRIC, "workload": "differentiable splat: 1,000,000 shell points (r 96-100) and a "
-            "1,000,000-point target (r 90-104), tent r=1, loss = sum (rho - rho_t)^2 + sum gathered",
-            "value": n / ((ms_f + ms_b) / 1e3), "unit": "points/s", "forward_ms": ms_f, "adjoint_ms": ms_b,
-            "adjoint_over_forward": ms_b / ms_f, "bricks": int(v.info().atlas_slots), "n_gpus": 1,
-            "steps": a.steps, "data": "synthetic", "dtype": "f32", "clocks": clk,
-            "loss": float(loss[0].item())}
+    res = {"workload": "differentiable splat: 1,000,000 shell points (r 96-100) and a 1,000,000-point target "
+                       "(r 90-104), tent r=1, loss = sum (rho - rho_t)^2 + sum gathered",
+           "value": n / ((ms_f + ms_b) / 1e3), "unit": "points/s", "forward_ms": ms_f, "adjoint_ms": ms_b,
+           "adjoint_over_forward": ms_b / ms_f, "bricks": int(v.info().atlas_slots), "steps": steps,
+           "clocks": clk, "loss": float(loss[0].item())}
+    v.close()
+    return res
+
+
+def run_adjoint(a):
+    line = {"metric": METRIC}
+    line.update(measure_adjoint(a.steps, a.warmup))
+    line.update({"n_gpus": 1, "data": "synthetic", "dtype": "f32"})
     print(json.dumps(line), flush=True)
     return 0
 
@@ -684,7 +938,6 @@ def run_sparse(a):
     (dL/dpos, dL/dweight, dL/dattr).  Per-kernel device times come from one
     profiled step after the timed region; GB/s per kernel is algorithmic
     bytes over that time."""
-    import numpy as np
     import torch
     import gvdb2
     import gvdb2.workloads as wl
@@ -707,7 +960,6 @@ def run_sparse(a):
         v.AddChannel(c, gvdb2.T_FLOAT, 1)
     v.SetPoints(pos)
     attrs = [None, (vel, 0), (vel, 1), (vel, 2)]
-    stage = {}
 
     def rec(events, name):
         if events is not None:
@@ -718,6 +970,7 @@ def run_sparse(a):
     def step(events=None):
         rec(events, "start")
         pos.add_(vel, alpha=DT)
+        v.SetPoints(pos)
         v.RequestFullRebuild(True)
         v.RebuildTopology(n, RADIUS)
         v.UpdateAtlas()
@@ -778,14 +1031,8 @@ def run_sparse(a):
     inf = v.info()
     slots = int(inf.atlas_slots)
     ncell = slots * 64
-    busy = int(inf.splat_cells) if int(inf.splat_cells) >= 0 else None
-    T3, R3, E3 = int(inf.tile_res) ** 3, 32 ** 3, 12 ** 3
-    # algorithmic bytes per launch (forward scatter 4 ch, gather 3 ch)
-    alg = {}
-    if busy is not None:
-        alg["k_scatter_own<2, 4>"] = n * 28 + busy * 4 * E3 * 4
-        alg["k_scatter_merge<2, 4>"] = busy * 4 * E3 * 4 + ncell * 512 * 4 * 4
-    alg["k_apron"] = slots * (T3 - R3) * 4 * 2
+    T3, R3 = int(inf.tile_res) ** 3, 32 ** 3
+    alg = {"k_apron": slots * (T3 - R3) * 4 * 2}
     total_ms = sum(d[1] for d in kt.values())
     kernels = []
     for nm, (cnt, t) in sorted(kt.items(), key=lambda x: -x[1][1]):
@@ -798,8 +1045,8 @@ def run_sparse(a):
         kernels.append(row)
     peak, src = peaks()
     line = {"metric": METRIC, "workload": SPARSE_WORKLOAD, "value": n / (ms / 1e3), "unit": "points/s",
-            "ms_per_step": ms, "stage_ms": stage, "bricks": slots, "cells": ncell, "cells_with_points": busy,
-            "n_points": n, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "data": "synthetic", "dtype": "f32",
+            "ms_per_step": ms, "stage_ms": stage, "bricks": slots, "cells": ncell, "n_points": n, "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "data": "synthetic", "dtype": "f32",
             "hbm_peak_gbs": peak, "peak_source": src, "kernels": kernels[:16], "clocks": clk,
             "device_mem_gb": round(torch.cuda.max_memory_allocated() / 1e9, 2)}
     print(json.dumps(line), flush=True)
@@ -809,6 +1056,9 @@ def run_sparse(a):
 def main():
     a = parse()
     if a.impl == "reference":
+        if a.workload not in WORKLOADS:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the dam-block step"}))
+            return 0
         return run_reference(a)
     if a.workload == "batched":
         return run_batched(a)

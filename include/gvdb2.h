@@ -113,6 +113,14 @@ GVDB2_API gvdb2_status gvdb2_save_vbx(gvdb2_volume *v, const char *path);
 GVDB2_API gvdb2_status gvdb2_load_vbx(gvdb2_volume *v, const char *path);
 
 /* ---- points (SetPoints VH:541 / V:4900-4908) ---- */
+/* Non-owning views, as the reference's DataPtr.  The kernel splats and
+ * gathers bin the points by cell once and reuse the bins while the topology,
+ * the point view (base, count, stride, offset) and the translation stay the
+ * same.  A caller that changes the positions in place (an advect step on the
+ * same buffer) calls gvdb2_set_points again, or rebuilds the topology, before
+ * the next splat or gather: either drops the bins.  Bins kept across moved
+ * positions drop the points that left their cells (they splat and gather
+ * nothing), as the reference's pnode from a stale InsertPoints would. */
 GVDB2_API gvdb2_status gvdb2_set_points(gvdb2_volume *v, gvdb2_points_view pos, gvdb2_points_view vel, gvdb2_points_view clr);
 
 /* Batched clouds (no counterpart in the reference, which holds one cloud

@@ -938,6 +938,36 @@ uint64_t orc_activate_space(orc_volume *v, float x, float y, float z) {
 
 uint64_t orc_root(const orc_volume *v) { return v->root; }
 
+/* The reference's host path of a topology build from points (the CPU-side
+ * equivalent of RebuildTopology, V:1181-1218): ActivateSpace (V:2766-2856)
+ * at every leaf-brick corner of each point's activation box [int(w) - r,
+ * int(w) + 2r] (the box of gvdbCalcExtraBrickId, P:467-512; it holds the
+ * point's own brick), one position at a time, in point order, so the leaves
+ * cover the same bricks as a full rebuild.  Used as the timed host baseline;
+ * returns the number of ActivateSpace calls, or -1 when a walk failed. */
+int64_t orc_activate_points(orc_volume *v, orc_view pos, int64_t n, float radius, const float orig[3]) {
+    if (v->nlev == 0) return -1;
+    const int rr = range_of(v, 0);
+    int64_t calls = 0;
+    for (int64_t i = 0; i < n; i++) {
+        const float *p = view_f3(pos, i);
+        const float w[3] = {p[0] + orig[0], p[1] + orig[1], p[2] + orig[2]};
+        if (w[0] < 0 || w[1] < 0 || w[2] < 0) continue;
+        int bmin[3], bmax[3];
+        box_bounds(w, radius, 2.0f, bmin, bmax);
+        int nd[3];
+        for (nd[0] = bmin[0] / rr * rr; nd[0] <= bmax[0] / rr * rr; nd[0] += rr)
+            for (nd[1] = bmin[1] / rr * rr; nd[1] <= bmax[1] / rr * rr; nd[1] += rr)
+                for (nd[2] = bmin[2] / rr * rr; nd[2] <= bmax[2] / rr * rr; nd[2] += rr) {
+                    if (nd[0] < 0 || nd[1] < 0 || nd[2] < 0) continue;
+                    int bnew = 0;
+                    if (activate_space(v, v->root, nd, &bnew, ID_UNDEFL, 0) == ID_UNDEFL && !bnew) return -1;
+                    calls++;
+                }
+    }
+    return calls;
+}
+
 /* CompactPools (no reference counterpart): the nodes an incremental rebuild
  * delinked (mParent = ID_UNDEF64, gvdbDelinkLeafBricks / gvdbDelinkBricks,
  * N:401-467) are dropped; the rest keep their order and their references

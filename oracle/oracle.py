@@ -59,6 +59,7 @@ def lib():
             "orc_accumulate_topology": (i32, [vp, _View, i32, f32, fp, i32]),
             "orc_update_atlas": (i32, [vp]),
             "orc_activate_space": (ctypes.c_uint64, [vp, f32, f32, f32]),
+            "orc_activate_points": (i64, [vp, _View, i64, f32, fp]),
             "orc_root": (ctypes.c_uint64, [vp]),
             "orc_compact_pools": (i32, [vp]),
             "orc_clear_channel": (i32, [vp, i32]),
@@ -182,6 +183,16 @@ class Oracle:
         """ActivateSpace(Vector3DF): the leaf's pool reference when it existed,
         ID_UNDEFL (0xFFFFFFFF) when it was created or nothing was activated."""
         return int(self.L.orc_activate_space(self.h, float(x), float(y), float(z)))
+
+    def activate_points(self, pos, radius, orig=(0, 0, 0)):
+        """The reference's host topology path: ActivateSpace at every leaf
+        brick of each point's activation box, in point order.  Returns the
+        number of ActivateSpace calls."""
+        pos = np.ascontiguousarray(pos, dtype=np.float32)
+        calls = int(self.L.orc_activate_points(self.h, view(pos), pos.shape[0], float(radius), _f3(orig)))
+        if calls < 0:
+            raise OracleError("activate_points: a tree walk failed")
+        return calls
 
     def root(self):
         return int(self.L.orc_root(self.h))
