@@ -802,7 +802,10 @@ def measure_batched(steps, warmup, env=None):
     ms_b = timed(step_batched, steps)
     ms_l = timed(step_loop, max(1, steps))
     clk = clocks.stop()
-    # identical results, cloud by cloud
+    # identical results, cloud by cloud, with stable binning on both sides
+    # (each cell then adds its points in the same order)
+    vb.SetDeterministic(True)
+    vl.SetDeterministic(True)
     first = vb.BatchPoints(dev, BATCH_SPACE_LOG2)
     batched_step(vb, K, total, [0], 1, gob)
     step_loop()

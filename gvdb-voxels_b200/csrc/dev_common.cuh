@@ -158,6 +158,8 @@ __device__ __forceinline__ int32_t leaf_at_o(const LeafLookup &L, float wx, floa
 // brick of res0 = 8m voxels holds m^3 cells; cell id = slot * m^3 +
 // (cz * m + cy) * m + cx.  For 8^3 bricks a cell is the brick.
 constexpr int kCell = 8;
+// Points of a cell are binned by region (see k_bin_count): 3 per axis.
+constexpr int kRegions = 27;
 __device__ __forceinline__ void cell_coords(int64_t cell, int m, int m3, int64_t &slot, int &cx, int &cy, int &cz) {
     if (m3 == 1) { // 8^3 bricks: the cell is the brick
         slot = cell;
@@ -178,12 +180,10 @@ __device__ __forceinline__ void cell_coords(int64_t cell, int m, int m3, int64_t
 // stored from the back (list[ncell - 1], list[ncell - 2], ..., cnt[1] of
 // them).  Light cells are listed apart (light[0 .. cnt[2])).  The gather
 // stages a halo tile per huge or heavy cell and reads the taps of light
-// cells' points straight from the atlas, one warp per light cell; the
-// splat's own phase likewise gives a huge or heavy cell a CTA and a light
-// cell a warp.  Every cell with points has a partial, indexed by its rank
-// among those cells in cell order (cell_ext).
+// cells' points straight from the atlas, one warp per light cell.
 constexpr uint32_t kHeavyCell = 1024;
 constexpr uint32_t kLightCell = 32;
+constexpr uint32_t kGiantCell = 4096; // the scatter gives such a cell a whole CTA
 // The i-th huge or heavy cell, or -1 past their end.
 __device__ __forceinline__ int64_t cell_at(int64_t i, const int32_t *list, const uint32_t *cnt, int64_t ncell) {
     const int64_t h = cnt[0];

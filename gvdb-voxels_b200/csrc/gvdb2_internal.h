@@ -157,15 +157,16 @@ struct Volume {
     DevBuf pnode, poff, gcnt, goff, psorted;
     int64_t pnode_n = 0;
 
-    // kernel-splat binning
-    DevBuf pbin, prank, bin_cnt, bin_off, perm;
+    // kernel-splat binning: per point its (cell, region) bin and rank, the
+    // points in bin order (perm), each (cell, region) bin's first entry
+    // (reg_off, 27 per cell) and each cell's (bin_off)
+    DevBuf pbin, prank, bin_cnt, bin_off, reg_off, perm;
     // cells that hold points: huge and heavy ones (order of cell_at), light
-    // ones, each cell's partial index (rank among the cells with points, in
-    // cell order; -1 if empty), the three counts, each cell's 27 neighbour
-    // partial indices (cell_nbr), scan scratch (cell_rank); heavy_grid,
-    // light_grid and cell_grid bound the huge+heavy, light and all lists
-    DevBuf cell_list, cell_light, cell_ext, cell_cnt, cell_nbr, cell_rank;
-    int64_t cell_grid = 0, heavy_grid = 0, light_grid = 0;
+    // ones, giant ones (the scatter's CTA cells) and the four counts;
+    // heavy_grid, light_grid and cell_grid bound the huge+heavy, light and
+    // all lists, giant_grid the giant list
+    DevBuf cell_list, cell_light, cell_giant, cell_cnt;
+    int64_t cell_grid = 0, heavy_grid = 0, light_grid = 0, giant_grid = 0;
     struct BinKey {
         bool valid = false;
         int kernel = 0;

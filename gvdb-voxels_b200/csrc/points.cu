@@ -51,9 +51,23 @@ __global__ void k_sort_points(PointsView pos, int64_t n, float3 trans, const int
     out[3 * k + 2] = p.z + trans.z;
 }
 
-// Bins every point by the 8^3 cell that contains it, cell = slot * m^3 +
-// cell in the brick (-1 when no active brick contains it); ranks come from
+// Bins every point by the 8^3 cell that contains it and by its region in
+// that cell: bin = cell * 27 + (rz * 3 + ry) * 3 + rx, cell = slot * m^3 +
+// cell in the brick (-1 when no active brick contains it).  Per axis the
+// region is 0 when the kernel's stencil reaches into the cell below (first
+// tap < 0), 2 when it reaches into the cell above (last tap >= 8), else 1 (a
+// stencil is narrower than a cell, so never both).  A cell's points so come
+// ordered by region, and the points of a neighbour whose stencils reach a
+// cell are a few contiguous runs of that neighbour's bin.  Ranks come from
 // warp-aggregated counters.
+template <int KERNEL>
+__device__ __forceinline__ int region_axis(float w, int cell_lo) {
+    // first tap of Taps<KERNEL>::eval, relative to the cell's first voxel
+    const int first = (int)floorf(w - 0.5f) - Taps<KERNEL>::LO - cell_lo;
+    return first < 0 ? 0 : (first + Taps<KERNEL>::N - 1 >= kCell ? 2 : 1);
+}
+
+template <int KERNEL>
 __global__ void k_bin_count(PointsView pos, int64_t n, float3 trans, LeafLookup L, const int32_t *leaf_slot, int m,
                             uint32_t *cnt, int32_t *pbin, int32_t *prank) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -67,8 +81,13 @@ __global__ void k_bin_count(PointsView pos, int64_t n, float3 trans, LeafLookup 
             const int32_t slot = leaf >= 0 ? leaf_slot[leaf] : -1;
             if (slot >= 0) {
                 const int rm = (1 << L.g.log2r0) - 1; // local voxel = voxel mod res0
-                bin = slot * m * m * m + cell_of_local(((int)w[0] + o.x) & rm, ((int)w[1] + o.y) & rm,
-                                                       ((int)w[2] + o.z) & rm, m);
+                const int vx = (int)w[0] + o.x, vy = (int)w[1] + o.y, vz = (int)w[2] + o.z;
+                const int lx = vx & rm, ly = vy & rm, lz = vz & rm;
+                // the cell's first voxel along each axis, in the point's grid coordinates
+                const int rx = region_axis<KERNEL>(w[0], (vx & ~(kCell - 1)) - o.x);
+                const int ry = region_axis<KERNEL>(w[1], (vy & ~(kCell - 1)) - o.y);
+                const int rz = region_axis<KERNEL>(w[2], (vz & ~(kCell - 1)) - o.z);
+                bin = (slot * m * m * m + cell_of_local(lx, ly, lz, m)) * kRegions + (rz * 3 + ry) * 3 + rx;
             }
         }
     }
@@ -80,6 +99,12 @@ __global__ void k_bin_count(PointsView pos, int64_t n, float3 trans, LeafLookup 
     } else if (i < n) {
         pbin[i] = -1;
     }
+}
+
+// bin_off[c] = reg_off[c * 27]: each cell's first point (c = ncell: the end)
+__global__ void k_cell_off(const uint32_t *reg_off, int64_t ncell, uint32_t *bin_off) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c <= ncell) bin_off[c] = reg_off[c * kRegions];
 }
 
 // keys for the stable (deterministic) binning: bin id, unbinned last
@@ -102,7 +127,10 @@ __global__ void k_bin_fill(const int32_t *pbin, const int32_t *prank, int64_t n,
 // heavy from its back, light in `light`; see cell_at).
 constexpr int64_t kCellCountReadback = 1 << 16; // cells
 
-__global__ void k_cell_list(const uint32_t *off, int64_t ncell, int32_t *list, int32_t *light, uint32_t *cnt) {
+// Cells of more than kGiantCell points are also listed in `giant` (count
+// cnt[3]): the scatter gives each of them a CTA.
+__global__ void k_cell_list(const uint32_t *off, int64_t ncell, int32_t *list, int32_t *light, int32_t *giant,
+                            uint32_t *cnt) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t k = c < ncell ? off[c + 1] - off[c] : 0u;
     const int cls = k == 0 ? -1 : (k > kHeavyCell ? 0 : (k > kLightCell ? 1 : 2));
@@ -112,38 +140,8 @@ __global__ void k_cell_list(const uint32_t *off, int64_t ncell, int32_t *list, i
         if (cls == 2) light[r] = (int32_t)c;
         else list[cls == 0 ? (int64_t)r : ncell - 1 - r] = (int32_t)c;
     }
-}
-
-// flag[cell] = 1 if the cell holds points
-__global__ void k_cell_flags(const uint32_t *off, int64_t ncell, uint32_t *flag) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < ncell) flag[c] = off[c + 1] > off[c] ? 1u : 0u;
-}
-
-// ext[cell] = the cell's partial index: its rank among the cells that hold
-// points, in cell order (so neighbouring cells' partials lie close together
-// whatever order the own phase runs them in); -1 if it holds none
-__global__ void k_cell_ext(const uint32_t *off, const uint32_t *rank, int64_t ncell, int32_t *ext) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < ncell) ext[c] = off[c + 1] > off[c] ? (int32_t)rank[c] : -1;
-}
-
-// nbr[cell * 27 + d] = the partial index of neighbour cell d = (dz+1)*9 +
-// (dy+1)*3 + (dx+1) of the cell (its partial in the splat), -1 if it holds
-// no points or lies outside the active bricks.
-__global__ void k_cell_nbrs(int64_t ncell, const int32_t *nbr27, const int32_t *ext, int m, int m3, int32_t *nbr) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ncell * 27) return;
-    const int64_t cell = t < (1ll << 32) ? (int64_t)((uint32_t)t / 27u) : t / 27;
-    const int d = (int)(t - cell * 27);
-    int64_t slot;
-    int cx, cy, cz;
-    cell_coords(cell, m, m3, slot, cx, cy, cz);
-    int ncx = cx + d % 3 - 1, ncy = cy + (d / 3) % 3 - 1, ncz = cz + d / 9 - 1;
-    const int bx = ncx < 0 ? -1 : (ncx >= m ? 1 : 0), by = ncy < 0 ? -1 : (ncy >= m ? 1 : 0),
-              bz = ncz < 0 ? -1 : (ncz >= m ? 1 : 0);
-    const int32_t ns = nbr27[slot * 27 + (bz + 1) * 9 + (by + 1) * 3 + (bx + 1)];
-    nbr[t] = ns >= 0 ? ext[(int64_t)ns * m3 + ((ncz - bz * m) * m + (ncy - by * m)) * m + (ncx - bx * m)] : -1;
+    const unsigned big = __ballot_sync(0xffffffffu, k > kGiantCell);
+    if (k > kGiantCell) giant[warp_agg_inc(cnt, 3u, big)] = (int32_t)c;
 }
 
 // gvdbSetFlagSubcell (P:109-118)
@@ -308,8 +306,8 @@ gvdb2_status insert_points(Volume *v, int n, const float trans[3], int prefix) {
 
 gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     Volume::BinKey &k = v->bin_key;
-    (void)kernel; // the bins (slot of each point) do not depend on the kernel
-    if (k.valid && k.n == n && k.topo == v->topo_version && k.det == (v->deterministic != 0) &&
+    // the regions depend on the kernel's stencil, so the bins do too
+    if (k.valid && k.n == n && k.kernel == kernel && k.topo == v->topo_version && k.det == (v->deterministic != 0) &&
         k.pos.base == v->pos.base &&
         k.pos.stride == v->pos.stride && k.pos.offset == v->pos.offset && k.trans[0] == trans[0] &&
         k.trans[1] == trans[1] && k.trans[2] == trans[2])
@@ -319,41 +317,48 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     cudaStream_t s = v->stream;
     const int m = v->res(0) / kCell; // cells per brick edge (bins are 8^3 cells)
     if (m < 1 || v->res(0) % kCell) return fail(v, GVDB2_ERR_UNSUPPORTED, "kernel splats need bricks of a multiple of 8 voxels");
-    int64_t nbins = v->atlas_last * m * m * m;
-    if (nbins >= INT32_MAX) return fail(v, GVDB2_ERR_CAPACITY, "more than 2^31 cells of 8^3 voxels");
+    const int64_t nbins = v->atlas_last * m * m * m; // cells
+    const int64_t nreg = nbins * kRegions;          // (cell, region) bins
+    if (nreg >= INT32_MAX) return fail(v, GVDB2_ERR_CAPACITY, "more than 2^31 / 27 cells of 8^3 voxels");
     GV_CUDA(v, v->pbin.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
     GV_CUDA(v, v->prank.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
     GV_CUDA(v, v->perm.ensure(sizeof(int32_t) * (size_t)std::max(n, 1), s));
-    GV_CUDA(v, v->bin_cnt.ensure(sizeof(uint32_t) * (size_t)(nbins + 1), s));
+    GV_CUDA(v, v->bin_cnt.ensure(sizeof(uint32_t) * (size_t)(nreg + 1), s));
+    GV_CUDA(v, v->reg_off.ensure(sizeof(uint32_t) * (size_t)(nreg + 1), s));
     GV_CUDA(v, v->bin_off.ensure(sizeof(uint32_t) * (size_t)(nbins + 1), s));
-    GV_CUDA(v, cudaMemsetAsync(v->bin_cnt.p, 0, sizeof(uint32_t) * (size_t)(nbins + 1), s));
+    GV_CUDA(v, cudaMemsetAsync(v->bin_cnt.p, 0, sizeof(uint32_t) * (size_t)(nreg + 1), s));
     float3 t = make_float3(trans[0], trans[1], trans[2]);
     LeafLookup L = make_lookup(v);
     if (n > 0) {
-        k_bin_count<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(), m,
-                                                                v->bin_cnt.as<uint32_t>(), v->pbin.as<int32_t>(),
-                                                                v->prank.as<int32_t>());
+        auto kc = kernel == GVDB2_KERNEL_TENT1 ? k_bin_count<GVDB2_KERNEL_TENT1> : k_bin_count<GVDB2_KERNEL_CUBIC2>;
+        kc<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t, L, v->leaf_slot.as<int32_t>(), m,
+                                                     v->bin_cnt.as<uint32_t>(), v->pbin.as<int32_t>(),
+                                                     v->prank.as<int32_t>());
         GV_CUDA(v, cudaGetLastError());
     }
-    GV_TRY(exclusive_scan_u32(v, v->bin_cnt.as<uint32_t>(), v->bin_off.as<uint32_t>(), nbins));
+    GV_TRY(exclusive_scan_u32(v, v->bin_cnt.as<uint32_t>(), v->reg_off.as<uint32_t>(), nreg));
+    k_cell_off<<<grid_for(nbins + 1, 256, 1ll << 31), 256, 0, s>>>(v->reg_off.as<uint32_t>(), nbins,
+                                                                   v->bin_off.as<uint32_t>());
+    GV_CUDA(v, cudaGetLastError());
     if (n > 0 && v->deterministic) {
         // stable counting sort: a radix sort of (bin, point index) keeps each
-        // bin's points in index order, independent of atomic timing
-        uint64_t *keys = nullptr;
-        GV_CUDA(v, cudaMallocAsync((void **)&keys, sizeof(uint64_t) * (size_t)n, s));
+        // bin's points in index order, independent of atomic timing; its key
+        // buffer is the volume's scratch (grown like every other buffer)
+        GV_CUDA(v, v->tmp_c.ensure(sizeof(uint64_t) * (size_t)n, s));
+        uint64_t *keys = v->tmp_c.as<uint64_t>();
         k_bin_keys<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pbin.as<int32_t>(), n, keys, v->perm.as<int32_t>());
-        gvdb2_status st = radix_sort_u64(v, keys, v->perm.as<int32_t>(), n, 0, 32);
-        cudaFreeAsync(keys, s);
-        GV_TRY(st);
+        GV_TRY(radix_sort_u64(v, keys, v->perm.as<int32_t>(), n, 0, 32));
     } else if (n > 0) {
         k_bin_fill<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pbin.as<int32_t>(), v->prank.as<int32_t>(), n,
-                                                               v->bin_off.as<uint32_t>(), v->perm.as<int32_t>());
+                                                               v->reg_off.as<uint32_t>(), v->perm.as<int32_t>());
         GV_CUDA(v, cudaGetLastError());
     }
-    // the cells that hold points, by class
+    // the cells that hold points, by class (the gathers' grids)
     GV_CUDA(v, v->cell_list.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
     GV_CUDA(v, v->cell_light.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
-    GV_CUDA(v, v->cell_ext.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
+    const int64_t giant_cap = std::min<int64_t>(std::max<int64_t>(nbins, 1), n / (int64_t)kGiantCell + 1);
+    GV_CUDA(v, v->cell_giant.ensure(sizeof(int32_t) * (size_t)giant_cap, s));
+    v->giant_grid = giant_cap;
     GV_CUDA(v, v->cell_cnt.ensure(sizeof(uint32_t) * 4, s));
     GV_CUDA(v, cudaMemsetAsync(v->cell_cnt.p, 0, sizeof(uint32_t) * 4, s));
 
@@ -361,23 +366,13 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     if (nbins > 0) {
         const int g = grid_for(nbins, 256, 1ll << 31);
         k_cell_list<<<g, 256, 0, s>>>(v->bin_off.as<uint32_t>(), nbins, v->cell_list.as<int32_t>(),
-                                      v->cell_light.as<int32_t>(), v->cell_cnt.as<uint32_t>());
-        GV_CUDA(v, v->cell_rank.ensure(sizeof(uint32_t) * 2 * (size_t)(nbins + 1), s));
-        uint32_t *flag = v->cell_rank.as<uint32_t>(), *rank = flag + nbins + 1;
-        k_cell_flags<<<g, 256, 0, s>>>(v->bin_off.as<uint32_t>(), nbins, flag);
-        GV_TRY(exclusive_scan_u32(v, flag, rank, nbins));
-        k_cell_ext<<<g, 256, 0, s>>>(v->bin_off.as<uint32_t>(), rank, nbins, v->cell_ext.as<int32_t>());
-        GV_CUDA(v, cudaGetLastError());
-        // each cell's 27 neighbour partials, for the merge
-        GV_CUDA(v, v->cell_nbr.ensure(sizeof(int32_t) * 27 * (size_t)nbins, s));
-        k_cell_nbrs<<<grid_for(nbins * 27, 256, 1ll << 31), 256, 0, s>>>(nbins, v->nbr27.as<int32_t>(),
-                                                                        v->cell_ext.as<int32_t>(), m, m * m * m,
-                                                                        v->cell_nbr.as<int32_t>());
+                                      v->cell_light.as<int32_t>(), v->cell_giant.as<int32_t>(),
+                                      v->cell_cnt.as<uint32_t>());
         GV_CUDA(v, cudaGetLastError());
         v->cell_grid = v->heavy_grid = v->light_grid = nbins;
         if (nbins > kCellCountReadback) {
-            // many cells: size the splat scratch and the grids by the cells
-            // of each class (one 12-byte read) rather than by all cells
+            // many cells: size the gathers' grids by the cells of each class
+            // (one 12-byte read) rather than by all cells
             uint32_t c3[3] = {0, 0, 0};
             GV_CUDA(v, cudaMemcpyAsync(c3, v->cell_cnt.p, sizeof(c3), cudaMemcpyDeviceToHost, s));
             GV_CUDA(v, cudaStreamSynchronize(s));

@@ -202,496 +202,320 @@ struct SplatArgs {
     const Node *leaves;
     const int32_t *nbr27;
     const uint32_t *bin_off;
+    const uint32_t *reg_off; // per (cell, region) bin its first entry of perm (k_bin_count)
     const int32_t *perm;
-    int res0, log2r0, apron, tile;
+    int res0, apron, tile;
     int m, m3; // cells per brick edge, per brick
-    // huge and heavy cells (order of cell_at), light cells, each cell's index
-    // in the splat's own order; cell_list == nullptr: every cell, in cell order
-    const int32_t *cell_list, *cell_light, *cell_ext;
+    // huge and heavy cells (order of cell_at), light cells; cell_list ==
+    // nullptr: every cell, in cell order
+    const int32_t *cell_list, *cell_light, *cell_giant;
     const uint32_t *cell_cnt;
     int64_t ncell;
-    const int32_t *cell_nbr;      // per cell, the own-order index of its 27 neighbours (-1: none)
     int64_t tvox;
 };
 
 
-// ---- two-phase scatter ---------------------------------------------------
+// ---- owner-computes scatter --------------------------------------------
 //
-// The kernels work on cells, 8^3 blocks of a brick (the brick itself for
-// 8^3 bricks).
-// Phase 1 (k_scatter_own): one CTA per cell of more than kLightCell points
-// (own_light, in the same launch: one warp per lighter cell) splats only the points
-// binned to it, with unclipped stencils, into an extended tile
-// that covers every tap of those points: [-H, 8+H)^3 with H = N/2 (12^3 for
-// the cubic B-spline, 10^3 for the tent).  The tile is then written out as
-// float partial sums.
-// Phase 2 (k_scatter_merge): one thread per interior voxel of every cell
-// adds, in a fixed neighbour order, the partials whose extended tile covers
-// the voxel, and writes the channel once.
+// One warp per cell (an 8^3 block of a brick; the brick itself for 8^3
+// bricks) computes the cell's interior voxels from every point whose stencil
+// reaches them and writes each voxel once: no atomics, no partial sums in
+// memory, no zero-fill pass.  Its sources are the cell's own points and,
+// from each of the 26 neighbour cells, the regions of that cell's bin whose
+// stencils cross the shared face, edge or corner (k_bin_count bins points by
+// cell and region), so every source is a point the cell needs.
 //
-// Accumulation in phase 1 is exact: each contribution x (in units of 2^-s)
-// is rounded to an integer and split as rint(x) = hi * 2^L + lo, both parts
-// obtained with the float "magic number" rounding (t = x*2^-L + 1.5*2^23
-// holds rint(x*2^-L) in its low mantissa bits; the remainder x - hi*2^L is
-// exact), and added with native int32 shared-memory atomics.  The integer
-// sums do not depend on the order of the atomics, and the merge sums a fixed
-// sequence of floats, so the result is bit-reproducible run to run.
-// Bounds (R = points of the brick, max|a| = largest |weighted amount| among
-// them, so a brick's result depends on its own points only):
-//   L = min(22, 31 - bits(R+1))      -> |sum lo| <= R * 2^(L-1) < 2^31
-//   max|a| * 2^s < 2^(21+L)          -> |x * 2^-L| < 2^22 (magic range)
-//   R * max|a| * 2^s < 2^(29+L)      -> |sum hi| < 2^29 + R/2
-template <int KERNEL>
-struct ExtTile {
-    static constexpr int N = Taps<KERNEL>::N;
-    static constexpr int H = N / 2;
-    static constexpr int E = 8 + N;                 // 12 (cubic) or 10 (tent)
-    static constexpr int RS = E;                    // row stride (words)
-    static constexpr int PS = N == 4 ? E * E + 8 : E * E; // plane stride: 152 puts a warp's 32 taps in 32 banks
-    static constexpr int CS = E * PS;               // channel stride
-    static constexpr int E3 = E * E * E;            // floats per channel in the global partial
-    // Position in the global partial of extended-tile voxel (ux, uy, uz) in
-    // [0, E)^3.  Per channel the partial holds 27 regions: the cell's 8^3
-    // interior first, then the halo beyond each face, edge and corner d in
-    // {-1,0,1}^3 (z-major order of d), each z-major with extent 8 along the
-    // axes where d is 0 and H where it is not.  The merge so reads whole
-    // 32-byte-aligned rows of the interior (8 floats) and packed rows of
-    // the halos, instead of 8 floats straddling two sectors of a 12-float
-    // row.  Region d starts, in the plain z-major order of the regions, at
-    // start_z E^2 + s_z start_y E + s_z s_y start_x, with start and s the
-    // region's first extended coordinate and extent along each axis.
-    __host__ __device__ static constexpr int part_index(int ux, int uy, int uz) {
-        const int dx = ux < H ? -1 : (ux >= 8 + H ? 1 : 0), dy = uy < H ? -1 : (uy >= 8 + H ? 1 : 0),
-                  dz = uz < H ? -1 : (uz >= 8 + H ? 1 : 0);
-        const int sx0 = dx < 0 ? 0 : (dx == 0 ? H : 8 + H), sy0 = dy < 0 ? 0 : (dy == 0 ? H : 8 + H),
-                  sz0 = dz < 0 ? 0 : (dz == 0 ? H : 8 + H);
-        const int ex = dx == 0 ? 8 : H, ey = dy == 0 ? 8 : H, ez = dz == 0 ? 8 : H;
-        const int local = ((uz - sz0) * ey + (uy - sy0)) * ex + (ux - sx0);
-        if ((dx | dy | dz) == 0) return local; // interior
-        const int r = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-        const int start = sz0 * E * E + ez * sy0 * E + ez * ey * sx0;
-        return 512 + start - (r > 13 ? 512 : 0) + local;
-    }
-};
-// The inverse of part_index: the tile address (plane stride PS, row stride
-// RS) of each partial position, so that phase 1 writes its partial in order
-// (coalesced) and looks each value up in its tile.
-template <int KERNEL, int PS, int RS>
-struct PartAddr {
-    uint16_t addr[ExtTile<KERNEL>::E3];
-    constexpr PartAddr() : addr() {
-        constexpr int E = ExtTile<KERNEL>::E;
-        for (int z = 0; z < E; z++)
-            for (int y = 0; y < E; y++)
-                for (int x = 0; x < E; x++)
-                    addr[ExtTile<KERNEL>::part_index(x, y, z)] = (uint16_t)(z * PS + y * RS + x);
-    }
-};
-// the CTA tile of a heavy cell (padded plane stride) and a light cell's warp tile
-template <int KERNEL>
-__device__ constexpr PartAddr<KERNEL, ExtTile<KERNEL>::PS, ExtTile<KERNEL>::RS> kHeavyAddr{};
-template <int KERNEL>
-__device__ constexpr PartAddr<KERNEL, ExtTile<KERNEL>::E * ExtTile<KERNEL>::E, ExtTile<KERNEL>::E> kLightAddr{};
+// The warp turns its sources into records in shared memory, a chunk of at
+// most kScCap at a time: per point the x weights on the cell's 8 voxel
+// columns and the y weights on its 8 rows (zero where the stencil does not
+// reach), the z weights of its N taps and the channel amounts.  A stable
+// counting sort orders the chunk by (first z tap, x group, first y tap);
+// the x group says which halves of the cell's x range the stencil reaches
+// (lower only, both, upper only).  Lane (y, q, h) owns the voxels x in
+// [4q, 4q+4), row y, z in [4h, 4h+4) of every channel in registers and walks
+// only the records that reach them: for each first z tap, two contiguous
+// runs of the sorted chunk (its x groups, first y taps y-N+1..y).  The loop
+// over first z taps is unrolled relative to 4h, so each record's adds go to
+// accumulator planes fixed at compile time: paired register FMAs.
+//
+// The adds happen in the order of the sources (the bins) and of the stable
+// sort, so with deterministic binning the result is bit-reproducible.
+constexpr int kScWarps = 4;                    // cells per CTA
+constexpr int kScCap = 128;                    // records per chunk
+constexpr int kScBins = 11 * 3 * 11;           // (first z tap + 3, x group, first y tap + 3)
 
-// The merge's sources per interior voxel v (x | y << 3 | z << 6) of a cell:
-// entry m of row v is the partial position (11 bits) and the neighbour
-// direction d (5 bits, z-major in {-1,0,1}^3) of source m, or 0xFFFF when
-// source m does not cover v.  Source m steps across the faces named by its
-// bits (x, y, z) toward the near face of v when v lies within H of one.
-template <int KERNEL>
-struct alignas(16) MergeMap {
-    uint16_t src[512][8];
-    constexpr MergeMap() : src() {
-        using X = ExtTile<KERNEL>;
-        for (int v = 0; v < 512; v++) {
-            const int vx = v & 7, vy = (v >> 3) & 7, vz = v >> 6;
-            const int ex = vx < X::H ? -1 : (vx >= 8 - X::H ? 1 : 0);
-            const int ey = vy < X::H ? -1 : (vy >= 8 - X::H ? 1 : 0);
-            const int ez = vz < X::H ? -1 : (vz >= 8 - X::H ? 1 : 0);
-            for (int m = 0; m < 8; m++) {
-                const bool used = (!(m & 1) || ex) && (!(m & 2) || ey) && (!(m & 4) || ez);
-                const int dx = (m & 1) ? ex : 0, dy = (m & 2) ? ey : 0, dz = (m & 4) ? ez : 0;
-                const int d = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-                src[v][m] = used ? (uint16_t)(X::part_index(vx - 8 * dx + X::H, vy - 8 * dy + X::H,
-                                                            vz - 8 * dz + X::H) | (d << 11))
-                                 : (uint16_t)0xFFFF;
+struct ScChunk {
+    float4 xw[kScCap][2]; // x weights on the cell's voxel columns 0..7
+    float wy[kScCap][8];  // y weights on the cell's rows 0..7
+    float4 wz[kScCap];    // z weights of the taps (zero past N)
+    float4 am[kScCap];    // channel amounts (zero past NCH)
+    uint16_t key[kScCap];
+    uint16_t rank[kScCap];
+    uint16_t order[kScCap];
+    uint16_t off[kScBins + 1];
+};
+
+// Sort the chunk's `fill` records by key (stable) into C.order.
+__device__ __forceinline__ void sc_sort_chunk(ScChunk &C, int fill, int lane) {
+    for (int i = lane; i <= kScBins; i += 32) C.off[i] = 0;
+    __syncwarp();
+    for (int base = 0; base < fill; base += 32) { // in record order: stable ranks
+        const int i = base + lane;
+        const bool ok = i < fill;
+        const unsigned act = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+            const uint32_t k = C.key[i];
+            const unsigned peers = __match_any_sync(act, k);
+            const uint32_t before = C.off[k];
+            C.rank[i] = (uint16_t)(before + __popc(peers & lanemask_lt()));
+            __syncwarp(act);
+            if (lane == __ffs(peers) - 1) C.off[k] = (uint16_t)(before + __popc(peers));
+        }
+        __syncwarp();
+    }
+    // exclusive scan of the counts in place; off[kScBins] becomes fill
+    constexpr int per = (kScBins + 1 + 31) / 32;
+    uint32_t local[per], sum = 0;
+#pragma unroll
+    for (int t = 0; t < per; t++) {
+        const int i = lane * per + t;
+        local[t] = i <= kScBins ? C.off[i] : 0u;
+        sum += local[t];
+    }
+    uint32_t inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    uint32_t run = inc - sum;
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < per; t++) {
+        const int i = lane * per + t;
+        if (i <= kScBins) C.off[i] = (uint16_t)run;
+        run += local[t];
+    }
+    __syncwarp();
+    for (int i = lane; i < fill; i += 32) C.order[C.off[C.key[i]] + C.rank[i]] = (uint16_t)i;
+    __syncwarp();
+}
+
+// Adds the chunk's records that reach lane (y, q, h)'s voxels.
+template <int KERNEL, int NCH>
+__device__ __forceinline__ void sc_accumulate(const ScChunk &C, float2 (&acc)[4][2][NCH], int y, int q, int h) {
+    constexpr int N = Taps<KERNEL>::N;
+#pragma unroll
+    for (int sp = -3; sp <= 3; sp++) { // first z tap relative to 4h
+        if (sp + N - 1 < 0) continue;
+        const int s = sp + 4 * h; // first z tap relative to the cell, in [-3, 7]
+#pragma unroll 1
+        for (int g = 0; g < 2; g++) {
+            const int kb = ((s + 3) * 3 + q + g) * 11;
+            const int lo = C.off[kb + max(y - N + 1, -3) + 3], hi = C.off[kb + y + 4];
+            for (int i = lo; i < hi; i++) {
+                const int r = C.order[i];
+                const float4 xv = C.xw[r][q];
+                const float wyv = C.wy[r][y];
+                const float4 zv = C.wz[r];
+                const float4 av = C.am[r];
+                const float zk[4] = {zv.x, zv.y, zv.z, zv.w};
+                const float ak[4] = {av.x, av.y, av.z, av.w};
+                const float2 x01 = make_float2(xv.x, xv.y), x23 = make_float2(xv.z, xv.w);
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    const float ay = ak[c] * wyv;
+#pragma unroll
+                    for (int k = 0; k < N; k++) {
+                        const int zz = sp + k;
+                        if (zz < 0 || zz >= 4) continue;
+                        const float t = ay * zk[k];
+                        const float2 tt = make_float2(t, t);
+                        acc[zz][0][c] = __ffma2_rn(tt, x01, acc[zz][0][c]);
+                        acc[zz][1][c] = __ffma2_rn(tt, x23, acc[zz][1][c]);
+                    }
+                }
             }
         }
     }
-};
-template <int KERNEL>
-__device__ constexpr MergeMap<KERNEL> kMergeMap{};
-static_assert(ExtTile<GVDB2_KERNEL_CUBIC2>::E3 <= 2048 && ExtTile<GVDB2_KERNEL_TENT1>::E3 <= 2048,
-              "partial positions fit 11 bits");
+}
 
-constexpr int kOwnThreads = 256;
-constexpr int kOwnChunk = 128; // points staged per pass
-
+// Blocks [0, single_blocks) take kScWarps cells each, a warp per cell;
+// the rest take one giant cell each (more than kGiantCell points of its
+// own), whose sources the CTA's warps share in turn, 32 at a time; their
+// accumulators are summed in a fixed order at the end.
 template <int KERNEL, int NCH>
-constexpr size_t own_smem_bytes() {
-    return sizeof(int32_t) * 2 * NCH * ExtTile<KERNEL>::CS +
-           sizeof(float) * (3 * Taps<KERNEL>::N + NCH) * kOwnChunk + sizeof(int32_t) * kOwnChunk;
-}
-
-// Split step 2^L of the fixed-point sums of R points.
-__device__ __forceinline__ int fixed_level(uint32_t R) {
-    const int L = 31 - (32 - __clz((int)R + 1));
-    return L > 22 ? 22 : L;
-}
-
-// Scale 2^sc applied to the contributions of R points whose largest
-// |weighted amount| is am (0 when there is nothing to add); inv = 2^-sc.
-__device__ __forceinline__ float fixed_scale(uint32_t R, int L, float am, double &inv) {
-    int e1 = 0, e2 = 0;
-    frexpf(am, &e1);             // am < 2^e1
-    frexpf((float)R * am, &e2);  // R*am < 2^e2
-    const int sc = min(21 + L - e1, 29 + L - e2);
-    const bool on = am > 0.0f && R > 0;
-    inv = on ? ldexp(1.0, -sc) : 0.0;
-    return on ? ldexpf(1.0f, sc) : 0.0f;
-}
-
-__device__ __forceinline__ void fixed_add(int32_t *hi_acc, int32_t *lo_acc, int idx, float x, float inv2L, float two2L) {
-    const float M = 12582912.0f; // 1.5 * 2^23
-    const float t = fmaf(x, inv2L, M);
-    const int hi = __float_as_int(t) - 0x4B400000;
-    const float r = fmaf(t - M, -two2L, x);
-    const int lo = __float_as_int(r + M) - 0x4B400000;
-    atomicAdd(hi_acc + idx, hi);
-    atomicAdd(lo_acc + idx, lo);
-}
-
-template <int KERNEL, int NCH>
-__device__ __forceinline__ void own_heavy(const SplatArgs &S, float *ext, int64_t block) {
+__global__ void __launch_bounds__(32 * kScWarps, 4) k_scatter_cells(SplatArgs S, int64_t single_blocks) {
     using T = Taps<KERNEL>;
-    using X = ExtTile<KERNEL>;
     constexpr int N = T::N;
-    extern __shared__ __align__(16) unsigned char own_smem[];
-    int32_t *acc_hi = reinterpret_cast<int32_t *>(own_smem);
-    int32_t *acc_lo = acc_hi + NCH * X::CS;
-    float(*pw)[kOwnChunk] = reinterpret_cast<float(*)[kOwnChunk]>(acc_lo + NCH * X::CS);
-    float(*pa)[kOwnChunk] = pw + 3 * N;
-    int32_t *pb = reinterpret_cast<int32_t *>(pa + NCH);
-    __shared__ double inv_s[NCH];
-    __shared__ int32_t amax_bits[NCH]; // max |weighted amount| of the cell's points, as float bits
-    // the block-th huge or heavy cell (light cells: own_light); its partial
-    // goes to ext[cell_ext[cell]]
-    const int64_t cell = cell_at(block, S.cell_list, S.cell_cnt, S.ncell);
-    if (cell < 0) return;
+    static_assert(kScWarps == 4, "a giant cell's warps reduce one accumulator plane each");
+    extern __shared__ __align__(16) unsigned char sc_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    ScChunk &C = reinterpret_cast<ScChunk *>(sc_smem)[warp];
+    int64_t cell;
+    int W; // warps sharing the cell
+    if ((int64_t)blockIdx.x < single_blocks) {
+        cell = (int64_t)blockIdx.x * kScWarps + warp;
+        if (cell >= S.ncell) return;
+        if (S.bin_off[cell + 1] - S.bin_off[cell] > kGiantCell) return; // a CTA of its own
+        W = 1;
+    } else {
+        const int64_t gi = (int64_t)blockIdx.x - single_blocks;
+        if (gi >= (int64_t)S.cell_cnt[3]) return; // every warp of the CTA
+        cell = S.cell_giant[gi];
+        W = kScWarps;
+    }
+    const int wturn = W == 1 ? 0 : warp;
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
-    static_assert(X::CS % 4 == 0, "16-byte zeroing");
-    for (int i = threadIdx.x; i < NCH * X::CS / 2; i += kOwnThreads) // acc_hi and acc_lo, adjacent
-        reinterpret_cast<int4 *>(acc_hi)[i] = make_int4(0, 0, 0, 0);
-    if (threadIdx.x < NCH) amax_bits[threadIdx.x] = 0;
-    const uint32_t beg = S.bin_off[cell], R = S.bin_off[cell + 1] - beg;
     const Node &nd = S.leaves[S.slot_leaf[slot]];
-    const int ox = nd.mPos[0] + kCell * cx - X::H, oy = nd.mPos[1] + kCell * cy - X::H,
-              oz = nd.mPos[2] + kCell * cz - X::H;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ox = nd.mPos[0] + kCell * cx, oy = nd.mPos[1] + kCell * cy, oz = nd.mPos[2] + kCell * cz;
+    // lane d < 27: the neighbour cell in direction d = (dz+1)*9 + (dy+1)*3 + (dx+1), or -1
+    int64_t nb = -1;
+    if (lane < 27) {
+        const int ncx = cx + lane % 3 - 1, ncy = cy + lane / 3 % 3 - 1, ncz = cz + lane / 9 - 1;
+        const int bx = ncx < 0 ? -1 : (ncx >= S.m ? 1 : 0), by = ncy < 0 ? -1 : (ncy >= S.m ? 1 : 0),
+                  bz = ncz < 0 ? -1 : (ncz >= S.m ? 1 : 0);
+        const int32_t ns = (bx | by | bz) == 0 ? (int32_t)slot
+                                               : S.nbr27[slot * 27 + (bz + 1) * 9 + (by + 1) * 3 + (bx + 1)];
+        if (ns >= 0) nb = (int64_t)ns * S.m3 + ((ncz - bz * S.m) * S.m + (ncy - by * S.m)) * S.m + (ncx - bx * S.m);
+    }
+    const int y = lane & 7, q = (lane >> 3) & 1, h = lane >> 4;
+    float2 acc[4][2][NCH];
+#pragma unroll
+    for (int z = 0; z < 4; z++)
+#pragma unroll
+        for (int x = 0; x < 2; x++)
+#pragma unroll
+            for (int c = 0; c < NCH; c++) acc[z][x][c] = make_float2(0.0f, 0.0f);
+    int fill = 0;
+    int step = 0; // 32-source steps so far (the warps of a giant cell take turns)
 
-    // Stage one point as record r of the current chunk (amounts times `scale`).
-    auto stage = [&](uint32_t j, int r, const float *scale, float *amt_out) {
-        const int32_t p = S.perm[beg + j];
-        const float3 q = load_f3(S.pos, p);
-        const int3 o = point_origin(S.pos, p);
-        float wx[N], wy[N], wz[N];
-        const int fx = T::eval(q.x + S.trans.x, wx) + o.x - ox;
-        const int fy = T::eval(q.y + S.trans.y, wy) + o.y - oy;
-        const int fz = T::eval(q.z + S.trans.z, wz) + o.z - oz;
-        // a binned point lies in the brick, so its first taps are in [0, 8];
-        // anything else (inconsistent input) is dropped, never written outside the tile
-        const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
-        pb[r] = ok ? fz * X::PS + fy * X::RS + fx : 0; // tile address of the point's first tap
+    // records of the sources [beg, end) of perm, 32 at a time
+    auto take = [&](uint32_t beg, uint32_t end) {
+        for (uint32_t base = beg; base < end; base += 32) {
+            if (step++ % W != wturn) continue;
+            if (fill > kScCap - 32) {
+                sc_sort_chunk(C, fill, lane);
+                sc_accumulate<KERNEL, NCH>(C, acc, y, q, h);
+                __syncwarp();
+                fill = 0;
+            }
+            const uint32_t j = base + lane;
+            bool ok = j < end;
+            int32_t p = 0;
+            float wx[N], wyt[N], wzt[N];
+            int fx = 0, fy = 0, fz = 0;
+            if (ok) {
+                p = S.perm[j];
+                const float3 pt = load_f3(S.pos, p);
+                const int3 o = point_origin(S.pos, p);
+                fx = T::eval(pt.x + S.trans.x, wx) + o.x - ox;
+                fy = T::eval(pt.y + S.trans.y, wyt) + o.y - oy;
+                fz = T::eval(pt.z + S.trans.z, wzt) + o.z - oz;
+                // the stencil reaches the cell on every axis (true of every
+                // source by construction of the regions)
+                ok = fx > -N && fx < kCell && fy > -N && fy < kCell && fz > -N && fz < kCell;
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const int r = fill + __popc(mask & lanemask_lt());
+                float *xr = reinterpret_cast<float *>(C.xw[r]);
+                float *yr = C.wy[r];
+                reinterpret_cast<float4 *>(xr)[0] = reinterpret_cast<float4 *>(xr)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                reinterpret_cast<float4 *>(yr)[0] = reinterpret_cast<float4 *>(yr)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int k = 0; k < N; k++) {
-            pw[k][r] = wx[k];
-            pw[N + k][r] = wy[k];
-            pw[2 * N + k][r] = wz[k];
-        }
-        const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
+                for (int t = 0; t < N; t++) {
+                    if ((unsigned)(fx + t) < (unsigned)kCell) xr[fx + t] = wx[t];
+                    if ((unsigned)(fy + t) < (unsigned)kCell) yr[fy + t] = wyt[t];
+                }
+                float zz4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int c = 0; c < NCH; c++) {
-            const float am = ok ? (((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt) : 0.0f;
-            amt_out[c] = am;
-            pa[c][r] = am * scale[c];
+                for (int t = 0; t < N; t++) zz4[t] = wzt[t];
+                C.wz[r] = make_float4(zz4[0], zz4[1], zz4[2], zz4[3]);
+                const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
+                float a4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int c = 0; c < NCH; c++) a4[c] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt;
+                C.am[r] = make_float4(a4[0], a4[1], a4[2], a4[3]);
+                const int xg = fx < 5 - N ? 0 : (fx <= 3 ? 1 : 2); // lower half only, both, upper only
+                C.key[r] = (uint16_t)(((fz + 3) * 3 + xg) * 11 + fy + 3);
+            }
+            fill += __popc(mask);
         }
     };
 
-    // Pass over all the brick's points: the first chunk is staged unscaled
-    // and every amount enters the brick's max, which sets the scale (so the
-    // result depends only on this brick's points).
-    float one[NCH], mx[NCH];
-#pragma unroll
-    for (int c = 0; c < NCH; c++) {
-        one[c] = 1.0f;
-        mx[c] = 0.0f;
-    }
-    __syncthreads(); // amax_bits cleared
-    for (uint32_t j = threadIdx.x; j < R; j += kOwnThreads) {
-        float am[NCH];
-        if (j < (uint32_t)kOwnChunk) {
-            stage(j, (int)j, one, am);
+    for (int d = 0; d < 27; d++) {
+        const int64_t nc = __shfl_sync(0xffffffffu, nb, d);
+        if (nc < 0) continue;
+        // the neighbour's regions whose stencils reach this cell, per axis:
+        // across the lower face its upper band (2), across the upper face
+        // its lower band (0), along the axis all three
+        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
+        const int rx0 = dx < 0 ? 2 : 0, rx1 = dx > 0 ? 0 : 2, ry0 = dy < 0 ? 2 : 0, ry1 = dy > 0 ? 0 : 2;
+        const int rz0 = dz < 0 ? 2 : 0, rz1 = dz > 0 ? 0 : 2;
+        const uint32_t *ro = S.reg_off + nc * kRegions;
+        if (dx == 0 && dy == 0) { // whole planes of regions: one run per z band (one run for the cell itself)
+            if (dz == 0) take(ro[0], ro[kRegions]);
+            else take(ro[rz0 * 9], ro[rz0 * 9 + 9]);
+        } else if (dx == 0) {
+            for (int rz = rz0; rz <= rz1; rz++) take(ro[(rz * 3 + ry0) * 3], ro[(rz * 3 + ry0) * 3 + 3]);
         } else {
-            const int32_t p = S.perm[beg + j];
-            const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
-#pragma unroll
-            for (int c = 0; c < NCH; c++) am[c] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt;
+            for (int rz = rz0; rz <= rz1; rz++)
+                for (int ry = ry0; ry <= ry1; ry++) take(ro[(rz * 3 + ry) * 3 + rx0], ro[(rz * 3 + ry) * 3 + rx0 + 1]);
         }
-#pragma unroll
-        for (int c = 0; c < NCH; c++) mx[c] = fmaxf(mx[c], fabsf(am[c]));
+        (void)rx1;
     }
-#pragma unroll
-    for (int c = 0; c < NCH; c++) {
-        float x = mx[c];
-        for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, o));
-        if (lane == 0 && x > 0.0f) atomicMax(&amax_bits[c], __float_as_int(x));
+    if (fill > 0) {
+        sc_sort_chunk(C, fill, lane);
+        sc_accumulate<KERNEL, NCH>(C, acc, y, q, h);
     }
-    __syncthreads();
-    const int L = fixed_level(R);
-    const float inv2L = ldexpf(1.0f, -L), two2L = ldexpf(1.0f, L);
-    float scale[NCH];
-#pragma unroll
-    for (int c = 0; c < NCH; c++) {
-        double inv;
-        scale[c] = fixed_scale(R, L, __int_as_float(amax_bits[c]), inv);
-        if (threadIdx.x == 0) inv_s[c] = inv;
-    }
-    { // scale the staged first chunk
-        const int cnt0 = (int)min((uint32_t)kOwnChunk, R);
-        for (int r = threadIdx.x; r < cnt0; r += kOwnThreads)
-#pragma unroll
-            for (int c = 0; c < NCH; c++) pa[c][r] *= scale[c];
-    }
-    for (uint32_t base = 0; base < R; base += kOwnChunk) {
-        const int cnt = (int)min((uint32_t)kOwnChunk, R - base);
-        if (base > 0) {
-            __syncthreads(); // previous chunk consumed
-            float am[NCH];
-            if ((int)threadIdx.x < cnt) stage(base + threadIdx.x, (int)threadIdx.x, scale, am);
-        }
-        __syncthreads();
-        if constexpr (N == 4) {
-            // one point per warp step: lane = (tx, ty, z pair); two taps per lane
-            const int tx = lane & 3, ty = (lane >> 2) & 3, tz0 = (lane >> 4) * 2;
-            const int loff = tz0 * X::PS + ty * X::RS + tx; // this lane's tap from the first tap
-            for (int j = warp; j < cnt; j += kOwnThreads / 32) {
-                const int a0 = pb[j] + loff;
-                const float wxv = pw[tx][j], wyv = pw[N + ty][j];
-                const float w0 = wxv * (wyv * pw[2 * N + tz0][j]);
-                const float w1 = wxv * (wyv * pw[2 * N + tz0 + 1][j]);
-#pragma unroll
-                for (int c = 0; c < NCH; c++) {
-                    const float am = pa[c][j];
-                    fixed_add(acc_hi + c * X::CS, acc_lo + c * X::CS, a0, am * w0, inv2L, two2L);
-                    fixed_add(acc_hi + c * X::CS, acc_lo + c * X::CS, a0 + X::PS, am * w1, inv2L, two2L);
-                }
-            }
-        } else {
-            // four points per warp step, one tap per lane
-            const int sub = lane >> 3, tx = lane & 1, ty = (lane >> 1) & 1, tz = (lane >> 2) & 1;
-            const int loff = tz * X::PS + ty * X::RS + tx;
-            for (int j0 = warp * 4; j0 < cnt; j0 += kOwnThreads / 8) {
-                const int j = j0 + sub;
-                if (j >= cnt) continue;
-                const int a = pb[j] + loff;
-                const float w = pw[tx][j] * (pw[N + ty][j] * pw[2 * N + tz][j]);
-#pragma unroll
-                for (int c = 0; c < NCH; c++)
-                    fixed_add(acc_hi + c * X::CS, acc_lo + c * X::CS, a, pa[c][j] * w, inv2L, two2L);
-            }
-        }
-    }
-    __syncthreads();
-    // thread t writes partial positions t, t+256, ... (coalesced) of
-    // channel c, looking their tile voxel up in kHeavyAddr
-    static_assert(kOwnThreads < X::E3, "one channel step per iteration");
-    float *dst = ext + (int64_t)S.cell_ext[cell] * NCH * X::E3;
-    int c = 0, j = threadIdx.x;
-    for (int i = threadIdx.x; i < NCH * X::E3; i += kOwnThreads) {
-        const int k = c * X::CS + kHeavyAddr<KERNEL>.addr[j];
-        // |sum| < 2^53: exact in double; the power-of-two scaling is exact
-        const long long sum = ((long long)acc_hi[k] << L) + (long long)acc_lo[k];
-        dst[i] = (float)((double)sum * inv_s[c]);
-        j += kOwnThreads;
-        if (j >= X::E3) {
-            j -= X::E3;
-            c++;
-        }
-    }
-}
-
-// Phase 1 for light cells (at most kLightCell = 32 points): one warp per
-// cell, so that a CTA-sized tile and its barriers are not spent on a few
-// points.  The warp sorts its points by index, stages their taps in shared
-// memory (one lane per point), then per channel accumulates them into a
-// warp-private float tile in that order -- each point's taps are distinct
-// voxels, handled by distinct lanes, so plain adds suffice and every voxel
-// sums its contributions in index order: the partial is bit-reproducible --
-// and writes the tile out in the partial layout of phase 1.  A partial of
-// at most 32 points is accurate to float rounding.
-constexpr int kLightWarps = 8;
-
-template <int KERNEL, int NCH>
-constexpr size_t own_light_smem_bytes() {
-    return sizeof(float) * kLightWarps * (ExtTile<KERNEL>::E3 + 32 * (1 + 3 * Taps<KERNEL>::N + NCH));
-}
-
-template <int KERNEL, int NCH>
-__device__ __forceinline__ void own_light(const SplatArgs &S, float *ext, int64_t block) {
-    using T = Taps<KERNEL>;
-    using X = ExtTile<KERNEL>;
-    constexpr int N = T::N, E = X::E, E3 = X::E3;
-    extern __shared__ __align__(16) unsigned char light_smem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float *tile = reinterpret_cast<float *>(light_smem) + warp * E3;
-    float *stage = reinterpret_cast<float *>(light_smem) + kLightWarps * E3 + warp * 32 * (1 + 3 * N + NCH);
-    int32_t *pbase = reinterpret_cast<int32_t *>(stage); // tile address of each point's first tap
-    float *pw = stage + 32;                              // pw[k * 32 + j]: weight k (x taps, y taps, z taps)
-    float *pa = pw + 3 * N * 32;                         // pa[c * 32 + j]: amount of channel c
-    const int64_t w = block * kLightWarps + warp;
-    if (w >= (int64_t)S.cell_cnt[2]) return;
-    const int64_t cell = S.cell_light[w];
-    const uint32_t beg = S.bin_off[cell], cnt = min(S.bin_off[cell + 1] - beg, 32u); // light: <= 32
-    // the cell's points in ascending index order (bitonic sort over the warp)
-    int32_t key = (uint32_t)lane < cnt ? S.perm[beg + lane] : INT32_MAX;
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1)
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            const int32_t other = __shfl_xor_sync(0xffffffffu, key, j);
-            const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
-            key = keep_min ? min(key, other) : max(key, other);
-        }
-    int64_t slot;
-    int cx, cy, cz;
-    cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
-    const Node &nd = S.leaves[S.slot_leaf[slot]];
-    const int ox = nd.mPos[0] + kCell * cx - X::H, oy = nd.mPos[1] + kCell * cy - X::H,
-              oz = nd.mPos[2] + kCell * cz - X::H;
-    if ((uint32_t)lane < cnt) {
-        const int32_t p = key;
-        const float3 q = load_f3(S.pos, p);
-        const int3 o = point_origin(S.pos, p);
-        float wx[N], wy[N], wz[N];
-        const int fx = T::eval(q.x + S.trans.x, wx) + o.x - ox;
-        const int fy = T::eval(q.y + S.trans.y, wy) + o.y - oy;
-        const int fz = T::eval(q.z + S.trans.z, wz) + o.z - oz;
-        // a binned point's first taps lie in [0, 8]; anything else is dropped
-        const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
-        pbase[lane] = ok ? (fz * E + fy) * E + fx : 0; // tile address of the point's first tap
-#pragma unroll
-        for (int k = 0; k < N; k++) {
-            pw[k * 32 + lane] = wx[k];
-            pw[(N + k) * 32 + lane] = wy[k];
-            pw[(2 * N + k) * 32 + lane] = wz[k];
-        }
-        const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
-#pragma unroll
-        for (int c = 0; c < NCH; c++)
-            pa[c * 32 + lane] = ok ? (((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt) : 0.0f;
-    }
-    __syncwarp();
-    float *dst = ext + (int64_t)S.cell_ext[cell] * NCH * E3;
-    // taps of a point per lane: cubic, lane = (tx, ty, z pair) with two taps;
-    // tent, lanes 0-7 = (tx, ty, tz)
-    const int tx = N == 4 ? (lane & 3) : (lane & 1), ty = N == 4 ? ((lane >> 2) & 3) : ((lane >> 1) & 1);
-    const int tz0 = N == 4 ? (lane >> 4) * 2 : ((lane >> 2) & 1);
-    const bool tap_lane = N == 4 || lane < 8;
-#pragma unroll 1
-    for (int c = 0; c < NCH; c++) {
-        float4 *t4 = reinterpret_cast<float4 *>(tile);
-        for (int i = lane; i < E3 / 4; i += 32) t4[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        __syncwarp();
-        for (uint32_t j = 0; j < cnt; j++) {
-            if (tap_lane) {
-                const int a0 = pbase[j] + (tz0 * E + ty) * E + tx;
-                const float am = pa[c * 32 + j];
-                const float wxy = pw[tx * 32 + j], wyv = pw[(N + ty) * 32 + j];
-                tile[a0] += am * (wxy * (wyv * pw[(2 * N + tz0) * 32 + j]));
-                if (N == 4) tile[a0 + E * E] += am * (wxy * (wyv * pw[(2 * N + tz0 + 1) * 32 + j]));
-            }
-            __syncwarp();
-        }
-        float *dc = dst + c * E3;
-        for (int i = lane; i < E3; i += 32) dc[i] = tile[kLightAddr<KERNEL>.addr[i]];
-        __syncwarp();
-    }
-}
-
-// Phase 1 in one launch: blocks [0, heavy_blocks) take a huge or heavy cell
-// each, the rest kLightWarps light cells each (kOwnThreads = 32 *
-// kLightWarps), so the light cells run beside the heavy ones.
-static_assert(kOwnThreads == 32 * kLightWarps, "one block size for both kinds of cell");
-template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(kOwnThreads) k_scatter_own(SplatArgs S, float *ext, int64_t heavy_blocks) {
-    if ((int64_t)blockIdx.x < heavy_blocks) own_heavy<KERNEL, NCH>(S, ext, blockIdx.x);
-    else own_light<KERNEL, NCH>(S, ext, blockIdx.x - heavy_blocks);
-}
-
-// Phase 2 (k_scatter_merge / k_scatter_merge_cta): voxel v of a cell sums,
-// in a fixed order, the partials of the cells whose extended tile covers
-// it: its own cell and, within H of a face, the neighbours across it (per
-// axis d = 0 and e = -1 or +1, never both, H <= 4), looked up in the cell's
-// 27-entry neighbour table.  The up to 8 partials are read first
-// (predicated), then summed, and the channel is written once.
-template <int KERNEL, int NCH>
-__device__ __forceinline__ void merge_voxel(const SplatArgs &S, const float *ext, const int32_t *ne, int64_t cell,
-                                            int v) {
-    using X = ExtTile<KERNEL>;
-    const int vx = v & 7, vy = (v >> 3) & 7, vz = v >> 6;
-    const uint4 row = *reinterpret_cast<const uint4 *>(kMergeMap<KERNEL>.src[v]);
-    const uint32_t w[4] = {row.x, row.y, row.z, row.w};
-    float part[8][NCH];
-#pragma unroll
-    for (int m = 0; m < 8; m++) {
-        const uint32_t ent = (w[m >> 1] >> (16 * (m & 1))) & 0xFFFFu;
-        const int32_t e = ent != 0xFFFFu ? ne[ent >> 11] : -1;
-        const float *src = ext + (int64_t)(e >= 0 ? e : 0) * NCH * X::E3 + (ent & 2047u);
-#pragma unroll
-        for (int c = 0; c < NCH; c++) part[m][c] = e >= 0 ? __ldcs(src + c * X::E3) : 0.0f;
-    }
-    float acc[NCH];
-#pragma unroll
-    for (int c = 0; c < NCH; c++) acc[c] = 0.0f;
-#pragma unroll
-    for (int m = 0; m < 8; m++)
-#pragma unroll
-        for (int c = 0; c < NCH; c++) acc[c] += part[m][c];
-    int64_t slot;
-    int cx, cy, cz;
-    cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
+    // each lane writes its 4 x 4 voxels of every channel once
     const int a = S.apron, tl = S.tile;
-    const int Lx = kCell * cx + vx, Ly = kCell * cy + vy, Lz = kCell * cz + vz; // voxel in the brick
-    const int64_t at = slot * S.tvox + ((int64_t)(Lz + a) * tl + (Ly + a)) * tl + (Lx + a);
+    const int64_t base = slot * S.tvox + (int64_t)(kCell * cx + 4 * q + a);
+    auto store = [&](int zz, int c, float2 v01, float2 v23) {
+        float *dst = S.chan[c] + base + ((int64_t)(kCell * cz + 4 * h + zz + a) * tl + (kCell * cy + y + a)) * tl;
+        dst[0] = v01.x;
+        dst[1] = v01.y;
+        dst[2] = v23.x;
+        dst[3] = v23.y;
+    };
+    if (W == 1) {
 #pragma unroll
-    for (int c = 0; c < NCH; c++)
-        if (c < S.nch) S.chan[c][at] = acc[c];
-}
-
-// Thread per voxel (sparse volumes): no shared memory or barrier, as many
-// voxels in flight as the registers allow; the neighbour row is read
-// through L1.
-template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(256) k_scatter_merge(SplatArgs S, const float *ext) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t cell = i >> 9;
-    if (cell >= S.ncell) return;
-    merge_voxel<KERNEL, NCH>(S, ext, S.cell_nbr + cell * 27, cell, (int)(i & 511));
-}
-
-// CTA per cell (dense volumes, where nearly every cell has partials): the
-// neighbour row staged once in shared memory.
-template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(512) k_scatter_merge_cta(SplatArgs S, const float *ext) {
-    __shared__ int32_t ne[27];
-    const int64_t cell = blockIdx.x;
-    if (threadIdx.x < 27) ne[threadIdx.x] = S.cell_nbr[cell * 27 + threadIdx.x];
+        for (int zz = 0; zz < 4; zz++)
+#pragma unroll
+            for (int c = 0; c < NCH; c++) store(zz, c, acc[zz][0][c], acc[zz][1][c]);
+        return;
+    }
+    // giant cell: the warps' accumulators through shared memory, summed in
+    // warp order; warp w sums and writes accumulator plane w of every lane
+    __syncthreads(); // every warp is done with its chunks
+    float2 *red = reinterpret_cast<float2 *>(sc_smem);
+    auto at = [&](int w, int zz, int xp, int c) { return (((w * 4 + zz) * 2 + xp) * NCH + c) * 32 + lane; };
+#pragma unroll
+    for (int zz = 0; zz < 4; zz++)
+#pragma unroll
+        for (int xp = 0; xp < 2; xp++)
+#pragma unroll
+            for (int c = 0; c < NCH; c++) red[at(warp, zz, xp, c)] = acc[zz][xp][c];
     __syncthreads();
-    merge_voxel<KERNEL, NCH>(S, ext, ne, cell, threadIdx.x);
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        float2 v[2];
+#pragma unroll
+        for (int xp = 0; xp < 2; xp++) {
+            v[xp] = red[at(0, warp, xp, c)];
+#pragma unroll
+            for (int w = 1; w < kScWarps; w++) {
+                const float2 u = red[at(w, warp, xp, c)];
+                v[xp].x += u.x;
+                v[xp].y += u.y;
+            }
+        }
+        store(warp, c, v[0], v[1]);
+    }
 }
-
 
 // ---------------------------------------------------------------------
 // tiled gathers: forward, scatter adjoint, gather adjoint
@@ -719,12 +543,11 @@ struct GatherArgs {
     const int32_t *perm;
     int res0, apron, tile;
     int m, m3; // cells per brick edge, per brick
-    // huge and heavy cells (order of cell_at), light cells, each cell's index
-    // in the splat's own order; cell_list == nullptr: every cell, in cell order
-    const int32_t *cell_list, *cell_light, *cell_ext;
+    // huge and heavy cells (order of cell_at), light cells; cell_list ==
+    // nullptr: every cell, in cell order
+    const int32_t *cell_list, *cell_light;
     const uint32_t *cell_cnt;
     int64_t ncell;
-    const int32_t *cell_nbr; // (not used by the gathers)
     int64_t tvox;
 };
 
@@ -824,15 +647,59 @@ __device__ __forceinline__ void gather_point(const GatherArgs &G, int32_t pidx, 
 }
 
 constexpr int kGatherThreads = 256; // threads of a k_gather_tile CTA
+constexpr int kGatherChunk = 1024;  // points ordered per pass
 
+// A voxel's channels side by side in the staged tile: one shared-memory
+// load per tap serves every channel.
+template <int NCH> struct GVec { using T = float4; };
+template <> struct GVec<1> { using T = float; };
+template <> struct GVec<2> { using T = float2; };
+template <int NCH>
+__device__ __forceinline__ void gvec_put(typename GVec<NCH>::T &v, const float (&g)[NCH]) {
+    if constexpr (NCH == 1) v = g[0];
+    else if constexpr (NCH == 2) v = make_float2(g[0], g[1]);
+    else if constexpr (NCH == 3) v = make_float4(g[0], g[1], g[2], 0.0f);
+    else v = make_float4(g[0], g[1], g[2], g[3]);
+}
+template <int NCH>
+__device__ __forceinline__ void gvec_get(const typename GVec<NCH>::T &v, float *g) {
+    if constexpr (NCH == 1) g[0] = v;
+    else if constexpr (NCH == 2) g[0] = v.x, g[1] = v.y;
+    else {
+        g[0] = v.x, g[1] = v.y, g[2] = v.z;
+        if constexpr (NCH == 4) g[3] = v.w;
+    }
+}
+
+template <int KERNEL, int NCH>
+constexpr size_t gather_tile_smem() {
+    constexpr int ht = kCell + Taps<KERNEL>::N;
+    return sizeof(typename GVec<NCH>::T) * ht * ht * ht + sizeof(uint16_t) * 3 * kGatherChunk +
+           sizeof(uint32_t) * 1024;
+}
+
+// One CTA per huge or heavy cell (every cell when the binning came from the
+// caller): stages the cell plus a halo of N/2 voxels (12^3 for the cubic
+// B-spline) from the interiors of its brick and the neighbours, the
+// channels of a voxel side by side, then serves the cell's points from
+// shared memory.  The points are visited in the order of their first tap
+// (a counting sort in shared memory, kGatherChunk at a time), so the lanes
+// of a warp read neighbouring voxels: few bank conflicts, and lanes on the
+// same voxel share one load.
 template <int KERNEL, int MODE, int NCH>
 __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t block) {
-    constexpr int H = Taps<KERNEL>::N / 2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float *tile = reinterpret_cast<float *>(smem_raw);
-    __shared__ int32_t nbs[27];
-    // one CTA per 8^3 cell of a brick: the cell plus its halo is staged
+    constexpr int N = Taps<KERNEL>::N, H = N / 2;
     constexpr int ht = kCell + 2 * H, ht3 = ht * ht * ht;
+    constexpr int nkeys = (kCell + 1) * (kCell + 1) * (kCell + 1); // first taps in [0, 8]^3 of the frame
+    using V = typename GVec<NCH>::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tile = reinterpret_cast<V *>(smem_raw);
+    uint16_t *key = reinterpret_cast<uint16_t *>(tile + ht3);
+    uint16_t *rank = key + kGatherChunk;
+    uint16_t *order = rank + kGatherChunk;
+    uint32_t *hist = reinterpret_cast<uint32_t *>(order + kGatherChunk); // nkeys + 1 (+ scan scratch)
+    __shared__ int32_t nbs[27];
+    __shared__ uint32_t wsum[kGatherThreads / 32];
     const int res = G.res0;
     const int64_t cell = G.cell_list ? cell_at(block, G.cell_list, G.cell_cnt, G.ncell) : block;
     if (cell < 0) return;
@@ -844,63 +711,84 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
     const int a = G.apron, tl = G.tile;
     if (threadIdx.x < 27) nbs[threadIdx.x] = G.nbr27[slot * 27 + threadIdx.x];
     __syncthreads();
-    // halo tile from the interiors of this brick and its neighbours: one
-    // tile row (fixed y, z) per half-warp, lane l < ht loading x = l; the
-    // lane's x neighbour and x offset are fixed for the whole tile
-    static_assert(ht <= 16, "a tile row fits a half-warp");
-    constexpr int rows_per_pass = kGatherThreads / 16, passes = (ht * ht + rows_per_pass - 1) / rows_per_pass;
-    const int hl = threadIdx.x & 15;
-    const int lx = hl - H + kCell * cx;
-    const int ex = lx < 0 ? -1 : (lx >= res ? 1 : 0);
-    const int xo = lx - ex * res + a;
-    // row r's brick (-1: outside the volume or no row) and offset of its voxel hl
-    auto row_src = [&](int r, int64_t &off) -> int32_t {
-        const bool in = hl < ht && r < ht * ht;
-        const int ly = r % ht - H + kCell * cy, lz = r / ht - H + kCell * cz;
-        const int dy = ly < 0 ? -1 : (ly >= res ? 1 : 0), dz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
-        const int32_t nb = in ? nbs[(dz + 1) * 9 + (dy + 1) * 3 + (ex + 1)] : -1;
-        off = (int64_t)nb * G.tvox + ((lz - dz * res + a) * tl + (ly - dy * res + a)) * tl + xo;
-        return nb;
-    };
-    if constexpr (MODE == kFwd) {
-        // row by row: the forward point phase needs few registers, and
-        // holding the whole staging in registers would cut the CTAs per SM
-        for (int r = threadIdx.x >> 4; r < ht * ht; r += rows_per_pass) {
-            int64_t off;
-            const int32_t nb = row_src(r, off);
-            if (hl < ht)
+    // halo tile from the interiors of this brick and its neighbours; all of a
+    // thread's loads are issued before its stores
+    constexpr int per = (ht3 + kGatherThreads - 1) / kGatherThreads;
+    float val[per][NCH];
 #pragma unroll
-                for (int c = 0; c < NCH; c++) tile[c * ht3 + r * ht + hl] = nb >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
-        }
-    } else {
-        // the adjoint point phases hold more registers than the staging
-        // needs: every load of the thread is issued before the first store
-        float val[passes][NCH];
+    for (int k = 0; k < per; k++) {
+        const int t = (int)threadIdx.x + k * kGatherThreads;
+        const int tx = t % ht, ty = t / ht % ht, tz = t / (ht * ht);
+        const int lx = kCell * cx + tx - H, ly = kCell * cy + ty - H, lz = kCell * cz + tz - H;
+        const int dx = lx < 0 ? -1 : (lx >= res ? 1 : 0), dy = ly < 0 ? -1 : (ly >= res ? 1 : 0),
+                  dz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
+        const int32_t nb = t < ht3 ? nbs[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] : -1;
+        const int64_t off = (int64_t)nb * G.tvox +
+                            ((int64_t)(lz - dz * res + a) * tl + (ly - dy * res + a)) * tl + (lx - dx * res + a);
 #pragma unroll
-        for (int k = 0; k < passes; k++) {
-            int64_t off;
-            const int32_t nb = row_src((int)(threadIdx.x >> 4) + k * rows_per_pass, off);
-#pragma unroll
-            for (int c = 0; c < NCH; c++) val[k][c] = nb >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
-        }
-#pragma unroll
-        for (int k = 0; k < passes; k++) {
-            const int r = (int)(threadIdx.x >> 4) + k * rows_per_pass;
-            if (hl < ht && r < ht * ht)
-#pragma unroll
-                for (int c = 0; c < NCH; c++) tile[c * ht3 + r * ht + hl] = val[k][c];
-        }
+        for (int c = 0; c < NCH; c++) val[k][c] = nb >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
     }
-    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < per; k++) {
+        const int t = (int)threadIdx.x + k * kGatherThreads;
+        if (t < ht3) gvec_put<NCH>(tile[t], val[k]);
+    }
     const Node &nd = G.leaves[G.slot_leaf[slot]];
     const int ox = nd.mPos[0] + kCell * cx - H, oy = nd.mPos[1] + kCell * cy - H, oz = nd.mPos[2] + kCell * cz - H;
-    auto fetch = [&](int x, int y, int z, float g[NCH]) {
-        const int k = (z * ht + y) * ht + x;
+    auto fetch = [&](int x, int y, int z, float g[NCH]) { gvec_get<NCH>(tile[(z * ht + y) * ht + x], g); };
+    for (uint32_t cb = beg; cb < end; cb += kGatherChunk) {
+        const int cnt = (int)min((uint32_t)kGatherChunk, end - cb);
+        for (int i = threadIdx.x; i <= nkeys; i += kGatherThreads) hist[i] = 0;
+        __syncthreads(); // (also: the tile is staged)
+        // key = the point's first tap in the frame (clamped; a point moved
+        // since the binning gathers zero whatever its key)
+        for (int j = threadIdx.x; j < cnt; j += kGatherThreads) {
+            const int32_t p = G.perm[cb + j];
+            const float3 q = load_f3(G.pos, p);
+            const int3 o = point_origin(G.pos, p);
+            const int fx = (int)floorf(q.x + G.trans.x - 0.5f) - Taps<KERNEL>::LO + o.x - ox;
+            const int fy = (int)floorf(q.y + G.trans.y - 0.5f) - Taps<KERNEL>::LO + o.y - oy;
+            const int fz = (int)floorf(q.z + G.trans.z - 0.5f) - Taps<KERNEL>::LO + o.z - oz;
+            const int kx = min(max(fx, 0), kCell), ky = min(max(fy, 0), kCell), kz = min(max(fz, 0), kCell);
+            const int k = (kz * (kCell + 1) + ky) * (kCell + 1) + kx;
+            key[j] = (uint16_t)k;
+            rank[j] = (uint16_t)atomicAdd(&hist[k], 1u);
+        }
+        __syncthreads();
+        { // exclusive scan of hist[0 .. nkeys) in place
+            constexpr int hp = (nkeys + kGatherThreads - 1) / kGatherThreads;
+            uint32_t loc[hp], sum = 0;
 #pragma unroll
-        for (int c = 0; c < NCH; c++) g[c] = tile[c * ht3 + k];
-    };
-    for (uint32_t j = beg + threadIdx.x; j < end; j += kGatherThreads)
-        gather_point<KERNEL, MODE, NCH>(G, G.perm[j], ox, oy, oz, fetch);
+            for (int t = 0; t < hp; t++) {
+                const int i = (int)threadIdx.x * hp + t;
+                loc[t] = i < nkeys ? hist[i] : 0u;
+                sum += loc[t];
+            }
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            uint32_t inc = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            if (lane == 31) wsum[warp] = inc;
+            __syncthreads();
+            uint32_t run = inc - sum;
+            for (int w = 0; w < warp; w++) run += wsum[w];
+#pragma unroll
+            for (int t = 0; t < hp; t++) {
+                const int i = (int)threadIdx.x * hp + t;
+                if (i < nkeys) hist[i] = run;
+                run += loc[t];
+            }
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < cnt; j += kGatherThreads) order[hist[key[j]] + rank[j]] = (uint16_t)j;
+        __syncthreads();
+        for (int j = threadIdx.x; j < cnt; j += kGatherThreads)
+            gather_point<KERNEL, MODE, NCH>(G, G.perm[cb + order[j]], ox, oy, oz, fetch);
+        __syncthreads(); // the order arrays are reused by the next chunk
+    }
 }
 
 // The points of light cells: one warp per cell, one lane per point (a light
@@ -978,9 +866,7 @@ void fill_topology(Volume *v, Args &S) {
     S.m = v->res(0) / kCell;
     S.m3 = S.m * S.m * S.m;
     S.cell_list = v->cell_list.as<int32_t>();
-    S.cell_nbr = v->cell_nbr.as<int32_t>();
     S.cell_light = v->cell_light.as<int32_t>();
-    S.cell_ext = v->cell_ext.as<int32_t>();
     S.cell_cnt = v->cell_cnt.as<uint32_t>();
     S.ncell = v->atlas_last * S.m3;
     S.apron = v->apron;
@@ -999,24 +885,16 @@ gvdb2_status launch_smem(Volume *v, K kernel, size_t smem, const char *what) {
     return GVDB2_OK;
 }
 
-// Two-phase scatter of up to 4 channels (one group).
+// Owner-computes scatter of up to 4 channels (one group): a warp per cell,
+// every cell of the active bricks (cells no stencil reaches get zeros).
 template <int KERNEL, int NCH>
 gvdb2_status scatter_group(Volume *v, const SplatArgs &S) {
-    using X = ExtTile<KERNEL>;
-    cudaStream_t s = v->stream;
-    // one partial per cell that holds points (at most cell_grid of them)
-    const int64_t nown = v->cell_grid;
-    GV_CUDA(v, v->scratch.ensure(sizeof(float) * (size_t)nown * NCH * X::E3 + 256, s));
-    float *ext = v->scratch.as<float>();
-    constexpr size_t smem = std::max(own_smem_bytes<KERNEL, NCH>(), own_light_smem_bytes<KERNEL, NCH>());
-    auto k1 = k_scatter_own<KERNEL, NCH>;
-    GV_TRY(launch_smem(v, k1, smem, "scatter"));
-    const int64_t own_blocks = v->heavy_grid + (v->light_grid + kLightWarps - 1) / kLightWarps;
-    if (own_blocks > 0) k1<<<(unsigned)own_blocks, kOwnThreads, smem, s>>>(S, ext, v->heavy_grid);
-    if (4 * nown >= 3 * S.ncell) // dense: most cells hold points
-        k_scatter_merge_cta<KERNEL, NCH><<<(unsigned)S.ncell, 512, 0, s>>>(S, ext);
-    else
-        k_scatter_merge<KERNEL, NCH><<<(unsigned)(S.ncell * 2), 256, 0, s>>>(S, ext);
+    constexpr size_t smem = sizeof(ScChunk) * kScWarps;
+    auto k = k_scatter_cells<KERNEL, NCH>;
+    GV_TRY(launch_smem(v, k, smem, "scatter"));
+    const int64_t single = (S.ncell + kScWarps - 1) / kScWarps;
+    const int64_t blocks = single + v->giant_grid; // giant cells: at most n / kGiantCell of them
+    if (blocks > 0) k<<<(unsigned)blocks, 32 * kScWarps, smem, v->stream>>>(S, single);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
@@ -1035,7 +913,7 @@ SplatArgs channel_group(const SplatArgs &S, int first, int count) {
 }
 
 template <int KERNEL>
-gvdb2_status scatter_two_phase(Volume *v, const SplatArgs &S) {
+gvdb2_status scatter_groups(Volume *v, const SplatArgs &S) {
     for (int first = 0; first < S.nch; first += 4) {
         const int cnt = std::min(4, S.nch - first);
         const SplatArgs G = channel_group(S, first, cnt);
@@ -1053,15 +931,13 @@ gvdb2_status run_scatter(Volume *v, int kernel, const SplatArgs &S) {
     if (v->atlas_last == 0) return GVDB2_OK;
     if (v->res(0) % kCell)
         return fail(v, GVDB2_ERR_UNSUPPORTED, "kernel splats need bricks of a multiple of 8 voxels");
-    return kernel == GVDB2_KERNEL_TENT1 ? scatter_two_phase<GVDB2_KERNEL_TENT1>(v, S)
-                                        : scatter_two_phase<GVDB2_KERNEL_CUBIC2>(v, S);
+    return kernel == GVDB2_KERNEL_TENT1 ? scatter_groups<GVDB2_KERNEL_TENT1>(v, S)
+                                        : scatter_groups<GVDB2_KERNEL_CUBIC2>(v, S);
 }
 
 template <int KERNEL, int MODE, int NCH>
 gvdb2_status launch_gather(Volume *v, const GatherArgs &G) {
-    constexpr int H = Taps<KERNEL>::N / 2;
-    constexpr int ht = kCell + 2 * H;
-    const size_t smem = sizeof(float) * (size_t)NCH * ht * ht * ht;
+    constexpr size_t smem = gather_tile_smem<KERNEL, NCH>();
     auto k = k_gather_tile<KERNEL, MODE, NCH>;
     GV_TRY(launch_smem(v, k, smem, "gather"));
     // tiles for the huge and heavy cells, then the light cells, a warp each
@@ -1204,7 +1080,8 @@ gvdb2_status scatter_kernel(Volume *v, int kernel, int n, const float trans[3], 
     S.nch = nch;
     for (int c = 0; c < kMaxSplatChan; c++) S.chan[c] = c < nch ? v->atlas[chans[c]].as<float>() : nullptr;
     fill_topology(v, S);
-    S.log2r0 = v->logdim[0];
+    S.reg_off = v->reg_off.as<uint32_t>();
+    S.cell_giant = v->cell_giant.as<int32_t>();
     return run_scatter(v, kernel, S);
 }
 
@@ -1300,7 +1177,8 @@ gvdb2_status gather_kernel_backward(Volume *v, int kernel, int n, const float tr
         }
         S.nch = nch;
         fill_topology(v, S);
-        S.log2r0 = v->logdim[0];
+        S.reg_off = v->reg_off.as<uint32_t>();
+        S.cell_giant = v->cell_giant.as<int32_t>();
         GV_TRY(run_scatter(v, kernel, S));
     }
     if (!grad_pos || n == 0) return GVDB2_OK;

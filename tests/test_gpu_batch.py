@@ -1,6 +1,7 @@
 """Batched clouds: several point clouds packed into one volume must give,
-cloud by cloud, exactly what a volume of their own gives. The checks are
-bit for bit, forward and adjoint:
+cloud by cloud, exactly what a volume of their own gives.  With stable
+(deterministic) binning a cell adds its points in the same order either way,
+so the checks are bit for bit, forward and adjoint:
   - the same bricks and atlas tiles (apron included);
   - the same gathered values;
   - the same dL/dG grids;
@@ -36,6 +37,7 @@ def run(gvdb2_mod, pts_list, kernel, batched):
     vols = []
     if batched:
         v = gvdb2_mod.VolumeGVDB(0)
+        v.SetDeterministic(True)
         v.Configure(*CFG)
         for c in range(4):
             v.AddChannel(c, gvdb2_mod.T_FLOAT, 1)
@@ -46,6 +48,7 @@ def run(gvdb2_mod, pts_list, kernel, batched):
         groups = []
         for p in pts_list:
             v = gvdb2_mod.VolumeGVDB(0)
+            v.SetDeterministic(True)
             v.Configure(*CFG)
             for c in range(4):
                 v.AddChannel(c, gvdb2_mod.T_FLOAT, 1)

@@ -5,15 +5,16 @@ FP64 oracle would take minutes per call.  Each property holds exactly in the
 oracle on a smaller lattice of the same layout:
 
 * power-of-two homogeneity: amounts times 2 give channel values times 2, bit
-  for bit (the split fixed point rescales by a power of two; light cells add
-  floats whose doubling is exact);
+  for bit (every product and sum of the splat scales exactly by a power of
+  two, and both channels of one call add their records in the same order);
 * the adjoint identity <scatter(a), g> = <a, gather(g)> over the interior
   voxels: the gather is the transpose of the scatter, taps outside the active
   bricks being dropped by one and read as 0 by the other;
 * partition of unity: the taps of every point lie in active bricks (radius-2
   activation covers the cubic stencil) and their weights sum to 1, so the
   scattered mass is the number of points and a field of ones gathers to 1;
-* run-to-run reproducibility of the default scatter.
+* run-to-run reproducibility of the default scatter over the same bins, and
+  of a full re-binning in deterministic mode.
 """
 import numpy as np
 import pytest
@@ -98,3 +99,14 @@ def test_full_size_scatter_reproducible(dam):
         v.ScatterKernel(2, n, [0, 2], weight=a, attrs=[None, (vx, 0)])
         runs.append((inner(v.atlas_tensor(0)).clone(), inner(v.atlas_tensor(2)).clone()))
     assert torch.equal(runs[0][0], runs[1][0]) and torch.equal(runs[0][1], runs[1][1])
+    # deterministic mode: every call re-bins the points (SetPoints drops the
+    # bins) and still gives the same bits
+    v.SetDeterministic(True)
+    det = []
+    for _ in range(2):
+        v.SetPoints(v._pts)
+        v.ScatterKernel(2, n, [0, 2], weight=a, attrs=[None, (vx, 0)])
+        det.append((inner(v.atlas_tensor(0)).clone(), inner(v.atlas_tensor(2)).clone()))
+    v.SetDeterministic(False)
+    assert torch.equal(det[0][0], det[1][0]) and torch.equal(det[0][1], det[1][1])
+    assert float((det[0][0] - runs[0][0]).abs().max()) <= REL_TOL * float(runs[0][0].abs().max())
