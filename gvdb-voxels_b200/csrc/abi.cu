@@ -274,9 +274,9 @@ gvdb2_status gvdb2_accumulate_topology(gvdb2_volume *h, int n, float radius, con
 
 gvdb2_status gvdb2_finish_topology(gvdb2_volume *h, int commit, int bounds) {
     CHECK_HANDLE(h);
-    (void)commit;
-    (void)bounds;
-    return GVDB2_OK; // pools already live on the device; no host mirror to commit
+    (void)commit; // pools already live on the device; no host mirror to commit
+    if (bounds) return gvdb2::compute_bounds(VOL(h));
+    return GVDB2_OK;
 }
 
 gvdb2_status gvdb2_update_atlas(gvdb2_volume *h) {
@@ -445,6 +445,12 @@ gvdb2_status gvdb2_get_info(gvdb2_volume *h, gvdb2_info *out) {
         out->root_pos[a] = v->root_pos[a];
     }
     out->tile_res = v->tile_res();
+    for (int a = 0; a < 3; a++) {
+        out->vol_min[a] = v->vox_min[a];
+        out->vol_max[a] = v->vox_max[a];
+        out->vox_res[a] = v->vox_res[a];
+        out->vox_res_max[a] = v->vox_res_max[a];
+    }
     out->splat_cells = -1;
     if (v->bin_key.valid && v->cell_cnt.p) {
         uint32_t c3[3] = {0, 0, 0};

@@ -128,6 +128,9 @@ struct Volume {
     int depth = 0;
     int root_pos[3] = {0, 0, 0};
     float posmin[3] = {0, 0, 0}, posmax[3] = {0, 0, 0};
+    // ComputeBounds (V:1792-1816): mVoxMin/mVoxMax (= mObjMin/mObjMax, what
+    // getVolMin/getVolMax return), mVoxRes and the largest mVoxRes so far
+    float vox_min[3] = {0, 0, 0}, vox_max[3] = {0, 0, 0}, vox_res[3] = {0, 0, 0}, vox_res_max[3] = {0, 0, 0};
     int64_t pool_cnt[kMaxLev] = {0};
     int64_t used_leaves = 0;
     DevBuf pool[kMaxLev];     // Node arrays
@@ -252,6 +255,7 @@ gvdb2_status save_vbx(Volume *v, const char *path);
 gvdb2_status load_vbx(Volume *v, const char *path);
 gvdb2_status update_neighbors(Volume *v);
 gvdb2_status clear_channel(Volume *v, int chan);
+gvdb2_status compute_bounds(Volume *v);
 gvdb2_status sync_counts(Volume *v);
 
 // ---- points.cu ----

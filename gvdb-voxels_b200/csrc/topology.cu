@@ -295,6 +295,35 @@ __global__ void k_leaf_flags(const Node *leaves, int64_t n, uint32_t *flags) {
     flags[i] = leaves[i].mFlags ? 1u : 0u;
 }
 
+// ComputeBounds (V:1792-1816): min of the flagged leaves' corners and max of
+// their far corners (corner + range(0)), both seeded with leaf 0's corner
+// whatever its flag, as the reference seeds them.  out[0..3) min, out[3..6)
+// max; a block reduces its leaves before one atomic per word.
+__global__ void k_leaf_bounds(const Node *leaves, int64_t n, int range0, int32_t *out) {
+    __shared__ int32_t red[6];
+    if (threadIdx.x < 6) red[threadIdx.x] = threadIdx.x < 3 ? INT32_MAX : INT32_MIN;
+    __syncthreads();
+    int32_t lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const Node &nd = leaves[i];
+        if (i == 0)
+            for (int a = 0; a < 3; a++) lo[a] = min(lo[a], nd.mPos[a]), hi[a] = max(hi[a], nd.mPos[a]);
+        if (!nd.mFlags) continue;
+        for (int a = 0; a < 3; a++) lo[a] = min(lo[a], nd.mPos[a]), hi[a] = max(hi[a], nd.mPos[a] + range0);
+    }
+    for (int a = 0; a < 3; a++) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = min(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0)
+        for (int a = 0; a < 3; a++) atomicMin(&red[a], lo[a]), atomicMax(&red[3 + a], hi[a]);
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&out[threadIdx.x], red[threadIdx.x]);
+    else if (threadIdx.x < 6) atomicMax(&out[threadIdx.x], red[threadIdx.x]);
+}
+
 // AtlasAlloc + getAtlasPos (A:692-715) and AssignMapping (V:2681-2689).
 __global__ void k_atlas_assign(Node *leaves, int64_t n, const uint32_t *flags, const uint32_t *slot, int sx, int sy,
                                int tile, int apron, AtlasNode *amap, int32_t *slot_leaf, int32_t *leaf_slot) {
@@ -1204,6 +1233,31 @@ gvdb2_status update_neighbors(Volume *v) {
                                                                     v->nbr6.as<int32_t>());
     GV_CUDA(v, cudaGetLastError());
     v->nbr6_valid = true;
+    return GVDB2_OK;
+}
+
+// ComputeBounds (V:1792-1816) for FinishTopology: mVoxMin/mVoxMax (and the
+// equal world-space mObjMin/mObjMax), mVoxRes and its running maximum.
+gvdb2_status compute_bounds(Volume *v) {
+    const int64_t n = v->pool_cnt[0];
+    if (n == 0) return GVDB2_OK; // the reference reads leaf 0, which does not exist: bounds unchanged
+    cudaStream_t s = v->stream;
+    if (!v->dev_small.p) {
+        GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), s));
+        GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
+    }
+    const int32_t init[6] = {INT32_MAX, INT32_MAX, INT32_MAX, INT32_MIN, INT32_MIN, INT32_MIN};
+    GV_CUDA(v, cudaMemcpyAsync(dev_words(v)->bbox, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    k_leaf_bounds<<<std::min(grid_for(n, 256), 4 * kSmCount), 256, 0, s>>>(v->pool_ptr(0), n, (int)v->range(0),
+                                                                           dev_words(v)->bbox);
+    GV_CUDA(v, cudaGetLastError());
+    GV_TRY(read_words(v));
+    for (int a = 0; a < 3; a++) {
+        v->vox_min[a] = (float)host_words(v)->bbox[a];
+        v->vox_max[a] = (float)host_words(v)->bbox[3 + a];
+        v->vox_res[a] = v->vox_max[a] - v->vox_min[a];
+        if (v->vox_res[a] > v->vox_res_max[a]) v->vox_res_max[a] = v->vox_res[a];
+    }
     return GVDB2_OK;
 }
 

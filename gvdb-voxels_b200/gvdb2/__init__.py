@@ -138,6 +138,13 @@ class VolumeGVDB:
     def FinishTopology(self, commit=True, bounds=True):
         self._check(self._L.gvdb2_finish_topology(self._h, int(commit), int(bounds)), "FinishTopology")
 
+    def getVolMin(self):
+        """gvdb_volume_base.h:57: the bounds of the last FinishTopology(bounds=True)."""
+        return tuple(self.info().vol_min)
+
+    def getVolMax(self):
+        return tuple(self.info().vol_max)
+
     def UpdateAtlas(self):
         self._check(self._L.gvdb2_update_atlas(self._h), "UpdateAtlas")
 

@@ -31,7 +31,9 @@ class Info(ctypes.Structure):
                 ("atlas_slots", ctypes.c_int64), ("atlas_capacity", ctypes.c_int64),
                 ("atlas_subdim", ctypes.c_int32 * 3), ("res", ctypes.c_int32 * 10), ("range", ctypes.c_int64 * 10),
                 ("posmin", ctypes.c_float * 3), ("posmax", ctypes.c_float * 3), ("root_pos", ctypes.c_int32 * 3),
-                ("tile_res", ctypes.c_int32), ("splat_cells", ctypes.c_int64)]
+                ("tile_res", ctypes.c_int32), ("splat_cells", ctypes.c_int64),
+                ("vol_min", ctypes.c_float * 3), ("vol_max", ctypes.c_float * 3), ("vox_res", ctypes.c_float * 3),
+                ("vox_res_max", ctypes.c_float * 3)]
 
 
 class GvdbError(RuntimeError):

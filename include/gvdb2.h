@@ -79,6 +79,11 @@ typedef struct gvdb2_info {
     int32_t tile_res;         /* res0 + 2*apron */
     int64_t splat_cells;      /* 8^3 brick cells holding points at the last kernel-splat
                                  binning, -1 before one (no counterpart in the reference) */
+    /* ComputeBounds (V:1792-1816), set by FinishTopology(bounds): */
+    float vol_min[3];         /* getVolMin (gvdb_volume_base.h:57): mObjMin = mVoxMin */
+    float vol_max[3];         /* getVolMax (gvdb_volume_base.h:59): mObjMax = mVoxMax */
+    float vox_res[3];         /* mVoxRes = mVoxMax - mVoxMin */
+    float vox_res_max[3];     /* mVoxResMax, the largest mVoxRes so far */
 } gvdb2_info;
 
 /* ---- lifetime (SetCudaDevice VH:325 / V:240-334, Initialize VH:326 / V:2320-2361) ---- */
@@ -146,7 +151,10 @@ GVDB2_API gvdb2_status gvdb2_batch_origin(gvdb2_volume *v, int cloud, int32_t ou
 GVDB2_API gvdb2_status gvdb2_request_full_rebuild(gvdb2_volume *v, int flag);                     /* RequestFullRebuild, VH:432 */
 GVDB2_API gvdb2_status gvdb2_rebuild_topology(gvdb2_volume *v, int n, float radius, const float orig[3]);  /* RebuildTopology, V:1181-1218 */
 GVDB2_API gvdb2_status gvdb2_accumulate_topology(gvdb2_volume *v, int n, float radius, const float orig[3], int min_depth); /* AccumulateTopology, V:1158-1178 */
-GVDB2_API gvdb2_status gvdb2_finish_topology(gvdb2_volume *v, int commit, int bounds);            /* FinishTopology, V:1579-1593 */
+/* FinishTopology, V:1579-1593: with `bounds`, ComputeBounds (V:1792-1816) over
+ * the leaves (read back into gvdb2_info vol_min/vol_max; synchronises the
+ * stream); `commit` has nothing to do (the pools live on the device). */
+GVDB2_API gvdb2_status gvdb2_finish_topology(gvdb2_volume *v, int commit, int bounds);
 GVDB2_API gvdb2_status gvdb2_update_atlas(gvdb2_volume *v);                                       /* UpdateAtlas, V:2630-2704 */
 /* ActivateSpace(Vector3DF), V:2766-2856 (with Reparent V:2726-2762): activates
  * the brick holding each of the n HOST positions xyz[3i..3i+2] (truncated to

@@ -185,6 +185,16 @@ class VolumeGVDB {
         return i;
     }
     long long getNumTotalNodes(int lev) { return Info().pool_count[lev]; }
+    // getVolMin / getVolMax (gvdb_volume_base.h:57-59): the bounds of the
+    // last FinishTopology(commit, true), i.e. ComputeBounds (V:1792-1816)
+    Vec3F getVolMin() {
+        gvdb2_info i = Info();
+        return Vec3F{i.vol_min[0], i.vol_min[1], i.vol_min[2]};
+    }
+    Vec3F getVolMax() {
+        gvdb2_info i = Info();
+        return Vec3F{i.vol_max[0], i.vol_max[1], i.vol_max[2]};
+    }
     long long getNumUsedNodes(int lev) {
         gvdb2_info i = Info();
         return lev == 0 ? i.used_leaves : i.pool_count[lev];

@@ -938,6 +938,27 @@ uint64_t orc_activate_space(orc_volume *v, float x, float y, float z) {
 
 uint64_t orc_root(const orc_volume *v) { return v->root; }
 
+/* ComputeBounds (V:1792-1816): mVoxMin = mVoxMax = leaf 0's corner (its flag
+ * not consulted), then over the flagged leaves the min of the corners and
+ * the max of corner + range(0), compared as floats against the int corners
+ * as the reference does; mObjMin/mObjMax equal them.  Returns -1 with no
+ * leaf (the reference would read a leaf that does not exist). */
+int orc_compute_bounds(const orc_volume *v, float vmin[3], float vmax[3]) {
+    if (v->nlev == 0 || v->pool_cnt[0] == 0) return -1;
+    const int range = range_of(v, 0);
+    const orc_node *n0 = &v->pool[0][0];
+    for (int a = 0; a < 3; a++) vmin[a] = vmax[a] = (float)n0->mPos[a];
+    for (int64_t i = 0; i < v->pool_cnt[0]; i++) {
+        const orc_node *nd = &v->pool[0][i];
+        if (!nd->mFlags) continue;
+        for (int a = 0; a < 3; a++) {
+            if ((float)nd->mPos[a] < vmin[a]) vmin[a] = (float)nd->mPos[a];
+            if ((float)(nd->mPos[a] + range) > vmax[a]) vmax[a] = (float)(nd->mPos[a] + range);
+        }
+    }
+    return 0;
+}
+
 /* The reference's host path of a topology build from points (the CPU-side
  * equivalent of RebuildTopology, V:1181-1218): ActivateSpace (V:2766-2856)
  * at every leaf-brick corner of each point's activation box [int(w) - r,

@@ -82,6 +82,7 @@ int orc_update_atlas(orc_volume *v);
 /* ActivateSpace (V:2766-2856): leaf reference if it existed, else ID_UNDEFL */
 uint64_t orc_activate_space(orc_volume *v, float x, float y, float z);
 int64_t orc_activate_points(orc_volume *v, orc_view pos, int64_t n, float radius, const float orig[3]);
+int orc_compute_bounds(const orc_volume *v, float vmin[3], float vmax[3]);
 uint64_t orc_root(const orc_volume *v); /* mRoot */
 int orc_compact_pools(orc_volume *v); /* drop delinked nodes, renumber the rest */
 int orc_clear_channel(orc_volume *v, int chan);

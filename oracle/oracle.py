@@ -60,6 +60,7 @@ def lib():
             "orc_update_atlas": (i32, [vp]),
             "orc_activate_space": (ctypes.c_uint64, [vp, f32, f32, f32]),
             "orc_activate_points": (i64, [vp, _View, i64, f32, fp]),
+            "orc_compute_bounds": (i32, [vp, fp, fp]),
             "orc_root": (ctypes.c_uint64, [vp]),
             "orc_compact_pools": (i32, [vp]),
             "orc_clear_channel": (i32, [vp, i32]),
@@ -193,6 +194,15 @@ class Oracle:
         if calls < 0:
             raise OracleError("activate_points: a tree walk failed")
         return calls
+
+    def compute_bounds(self):
+        """ComputeBounds: (mVoxMin, mVoxMax) as float32 arrays."""
+        lo = np.zeros(3, np.float32)
+        hi = np.zeros(3, np.float32)
+        fpp = ctypes.POINTER(ctypes.c_float)
+        if self.L.orc_compute_bounds(self.h, lo.ctypes.data_as(fpp), hi.ctypes.data_as(fpp)) != 0:
+            raise OracleError("compute_bounds: no leaf")
+        return lo, hi
 
     def root(self):
         return int(self.L.orc_root(self.h))

@@ -280,3 +280,31 @@ def test_compact_pools_bit_exact(gvdb2_mod, oracle_mod):
         o.update_atlas()
         v.UpdateAtlas()
         assert np.array_equal(v.atlas_map(), o.atlas_map())
+
+
+def test_compute_bounds_bit_exact(gvdb2_mod, oracle_mod):
+    """FinishTopology(bounds) = ComputeBounds (V:1792-1816): the box of the
+    flagged leaves seeded with leaf 0's corner, after a full rebuild and
+    after incremental rebuilds that leave stale (unflagged) leaves in the
+    pool; getVolMin/getVolMax return it, and mVoxResMax only grows."""
+    import torch
+    import gvdb2.workloads as wl
+    p, vel = wl.dam_block(sites=(48, 12, 48), origin=(40.0, 40.0, 40.0), seed=12)
+    o = make_oracle(oracle_mod)
+    v = gpu_volume(gvdb2_mod, p)
+    res_max = np.zeros(3, np.float32)
+    stale_seen = False
+    for q in _drift_steps(p, vel, 5):
+        assert o.rebuild_topology(q, 2.0) == 0
+        t = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+        v.SetPoints(t)
+        v._pts = t
+        v.RebuildTopology(len(q), 2.0)
+        v.FinishTopology(True, True)
+        lo, hi = o.compute_bounds()
+        assert np.array_equal(np.array(v.getVolMin(), np.float32), lo)
+        assert np.array_equal(np.array(v.getVolMax(), np.float32), hi)
+        res_max = np.maximum(res_max, hi - lo)
+        assert np.array_equal(np.array(v.info().vox_res_max[:], np.float32), res_max)
+        stale_seen |= o.pool_count(0) > o.used_leaves()
+    assert stale_seen

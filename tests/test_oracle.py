@@ -457,3 +457,22 @@ def test_compact_pools(oracle_mod):
         assert np.array_equal(a.atlas(0), b.atlas(0))
         check_links(b)
         p = p + np.array([6.0, 0.0, 0.0], np.float32) + np.float32(0.2) * vel
+
+
+def test_compute_bounds(oracle_mod):
+    """ComputeBounds (V:1792-1816) against a numpy restatement over the leaf
+    pool: the flagged leaves' corners and far corners, seeded with leaf 0."""
+    import gvdb2.workloads as wl
+    p, vel = wl.dam_block(sites=(32, 8, 32), origin=(40.0, 40.0, 40.0), seed=13)
+    o = make_oracle(oracle_mod)
+    q = p
+    for step in range(4):  # the third and fourth rebuilds are incremental
+        assert o.rebuild_topology(q, 2.0) == 0
+        nodes = o.nodes(0)
+        flagged = nodes["mFlags"] != 0
+        pos = nodes["mPos"].astype(np.float32)
+        want_lo = np.minimum(pos[0], pos[flagged].min(0))
+        want_hi = np.maximum(pos[0], (pos[flagged] + o.range(0)).max(0))
+        lo, hi = o.compute_bounds()
+        assert np.array_equal(lo, want_lo) and np.array_equal(hi, want_hi), step
+        q = (q + np.float32(3.0) * vel).astype(np.float32)
