@@ -130,7 +130,7 @@ gvdb2_status gvdb2_synchronize(gvdb2_volume *h) {
     CHECK_HANDLE(h);
     cudaError_t e = cudaStreamSynchronize(h->v.stream);
     if (e != cudaSuccess) return gvdb2::cuda_fail(VOL(h), e, "synchronize");
-    return GVDB2_OK;
+    return gvdb2::flush_status(VOL(h));
 }
 
 gvdb2_status gvdb2_set_option(gvdb2_volume *h, int option, int value) {
@@ -153,6 +153,7 @@ gvdb2_status gvdb2_configure(gvdb2_volume *h, int q4, int q3, int q2, int q1, in
     for (int n = 0; n < 5; n++) v->logdim[n] = r[n] == 0 ? 1 : r[n];
     for (int l = 0; l < gvdb2::kMaxLev; l++) v->pool_cnt[l] = 0;
     v->used_leaves = 0;
+    v->all_leaves_flagged = false;
     v->atlas_last = 0;
     v->atlas_valid = false;
     v->rebuild_topo = true;
@@ -425,6 +426,7 @@ gvdb2_status gvdb2_get_info(gvdb2_volume *h, gvdb2_info *out) {
     Volume *v = VOL(h);
     cudaError_t e = cudaStreamSynchronize(v->stream);
     if (e != cudaSuccess) return gvdb2::cuda_fail(v, e, "get_info");
+    GV_TRY(gvdb2::flush_status(v));
     std::memset(out, 0, sizeof(*out));
     out->depth = v->depth;
     out->top_level = v->top_level();

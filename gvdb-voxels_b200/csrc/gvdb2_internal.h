@@ -133,6 +133,12 @@ struct Volume {
     float vox_min[3] = {0, 0, 0}, vox_max[3] = {0, 0, 0}, vox_res[3] = {0, 0, 0}, vox_res_max[3] = {0, 0, 0};
     int64_t pool_cnt[kMaxLev] = {0};
     int64_t used_leaves = 0;
+    // every pool leaf is flagged (true right after a full rebuild): UpdateAtlas
+    // then knows its slot count without reading it back
+    bool all_leaves_flagged = false;
+    // the device status word of the last full rebuild is checked at the
+    // next read-back of the small device words instead of by a read of its own
+    bool status_pending = false;
     DevBuf pool[kMaxLev];     // Node arrays
     DevBuf clist[kMaxLev];    // uint64 child lists (lev >= 1)
     uint64_t topo_version = 0;
@@ -257,6 +263,9 @@ gvdb2_status update_neighbors(Volume *v);
 gvdb2_status clear_channel(Volume *v, int chan);
 gvdb2_status compute_bounds(Volume *v);
 gvdb2_status sync_counts(Volume *v);
+// reads back the small device words when a full rebuild's status check is
+// pending and reports its error, if any
+gvdb2_status flush_status(Volume *v);
 
 // ---- points.cu ----
 gvdb2_status insert_points(Volume *v, int n, const float trans[3], int prefix);

@@ -240,12 +240,22 @@ struct SplatArgs {
 //
 // The adds happen in the order of the sources (the bins) and of the stable
 // sort, so with deterministic binning the result is bit-reproducible.
+#ifndef GVDB2_SC_CAP
+#define GVDB2_SC_CAP 128
+#endif
+#ifndef GVDB2_SC_MIN_BLOCKS
+#define GVDB2_SC_MIN_BLOCKS 4
+#endif
 constexpr int kScWarps = 4;                    // cells per CTA
-constexpr int kScCap = 128;                    // records per chunk
+constexpr int kScCap = GVDB2_SC_CAP;           // records per chunk
 constexpr int kScBins = 11 * 3 * 11;           // (first z tap + 3, x group, first y tap + 3)
 
 struct ScChunk {
-    float4 xw[kScCap][2]; // x weights on the cell's voxel columns 0..7
+    // x weights on the cell's voxel columns 0..7: half q (columns 4q..4q+3)
+    // of record r sits at xw[r][q ^ (r & 1)], so that the lanes of one
+    // quarter-warp reading the same half of different records spread over
+    // all eight 16-byte bank groups
+    float4 xw[kScCap][2];
     float wy[kScCap][8];  // y weights on the cell's rows 0..7
     float4 wz[kScCap];    // z weights of the taps (zero past N)
     float4 am[kScCap];    // channel amounts (zero past NCH)
@@ -315,7 +325,7 @@ __device__ __forceinline__ void sc_accumulate(const ScChunk &C, float2 (&acc)[4]
             const int lo = C.off[kb + max(y - N + 1, -3) + 3], hi = C.off[kb + y + 4];
             for (int i = lo; i < hi; i++) {
                 const int r = C.order[i];
-                const float4 xv = C.xw[r][q];
+                const float4 xv = C.xw[r][q ^ (r & 1)];
                 const float wyv = C.wy[r][y];
                 const float4 zv = C.wz[r];
                 const float4 av = C.am[r];
@@ -345,7 +355,7 @@ __device__ __forceinline__ void sc_accumulate(const ScChunk &C, float2 (&acc)[4]
 // own), whose sources the CTA's warps share in turn, 32 at a time; their
 // accumulators are summed in a fixed order at the end.
 template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(32 * kScWarps, 4) k_scatter_cells(SplatArgs S, int64_t single_blocks) {
+__global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_cells(SplatArgs S, int64_t single_blocks) {
     using T = Taps<KERNEL>;
     constexpr int N = T::N;
     static_assert(kScWarps == 4, "a giant cell's warps reduce one accumulator plane each");
@@ -425,9 +435,10 @@ __global__ void __launch_bounds__(32 * kScWarps, 4) k_scatter_cells(SplatArgs S,
                 float *yr = C.wy[r];
                 reinterpret_cast<float4 *>(xr)[0] = reinterpret_cast<float4 *>(xr)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
                 reinterpret_cast<float4 *>(yr)[0] = reinterpret_cast<float4 *>(yr)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                const int sw = (r & 1) * 4; // the halves of odd records are swapped
 #pragma unroll
                 for (int t = 0; t < N; t++) {
-                    if ((unsigned)(fx + t) < (unsigned)kCell) xr[fx + t] = wx[t];
+                    if ((unsigned)(fx + t) < (unsigned)kCell) xr[(fx + t) ^ sw] = wx[t];
                     if ((unsigned)(fy + t) < (unsigned)kCell) yr[fy + t] = wyt[t];
                 }
                 float zz4[4] = {0.f, 0.f, 0.f, 0.f};

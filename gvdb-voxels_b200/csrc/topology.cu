@@ -400,10 +400,21 @@ inline uint32_t next_pow2(uint64_t x) {
 SmallWords *host_words(Volume *v) { return reinterpret_cast<SmallWords *>(v->host_small); }
 SmallWords *dev_words(Volume *v) { return v->dev_small.as<SmallWords>(); }
 
+// The status a full rebuild left in the small words, once they are back on
+// the host (build_from_keys defers its check to the next read-back).
+gvdb2_status check_pending_status(Volume *v) {
+    if (!v->status_pending) return GVDB2_OK;
+    v->status_pending = false;
+    const int32_t st = host_words(v)->status;
+    if (st & kDevHashFull) return fail(v, GVDB2_ERR_CAPACITY, "leaf map overflow in the last full rebuild");
+    if (st & kDevBadIndex) return fail(v, GVDB2_ERR_STATE, "node without parent in the last full rebuild");
+    return GVDB2_OK;
+}
+
 gvdb2_status read_words(Volume *v) {
     GV_CUDA(v, cudaMemcpyAsync(v->host_small, v->dev_small.p, sizeof(SmallWords), cudaMemcpyDeviceToHost, v->stream));
     GV_CUDA(v, cudaStreamSynchronize(v->stream));
-    return GVDB2_OK;
+    return check_pending_status(v);
 }
 
 
@@ -464,6 +475,7 @@ gvdb2_status set_difference(Volume *v, const uint64_t *keys, int64_t n, const ui
 gvdb2_status clear_pools(Volume *v) { // Clear (V:2487-2503)
     for (int l = 0; l < kMaxLev; l++) v->pool_cnt[l] = 0;
     v->used_leaves = 0;
+    v->all_leaves_flagged = false;
     v->atlas_last = 0;
     v->atlas_valid = false;
     v->rebuild_topo = true;
@@ -639,10 +651,12 @@ gvdb2_status build_from_keys(Volume *v, const int64_t nB[], const int64_t nE[], 
         if (cnt > 0) k_build_link<<<grid_for(cnt, 256, 1ll << 31), 256, 0, s>>>(L);
         GV_CUDA(v, cudaGetLastError());
     }
-    GV_TRY(read_words(v));
-    if (host_words(v)->status & kDevHashFull) return fail(v, GVDB2_ERR_CAPACITY, "leaf map overflow");
-    if (host_words(v)->status & kDevBadIndex) return fail(v, GVDB2_ERR_STATE, "node without parent in full rebuild");
+    // the status word is checked at the next read-back of the small words
+    // (the next rebuild's bounding box, Synchronize or GetInfo), not by a
+    // stall here
+    v->status_pending = true;
     v->used_leaves = v->pool_cnt[0];
+    v->all_leaves_flagged = true;
     return GVDB2_OK;
 }
 
@@ -1028,6 +1042,11 @@ KeyGeom key_geom(const Volume *v) {
 
 gvdb2_status incremental_rebuild(Volume *v, int n, float radius, const float orig[3], bool accum);
 
+gvdb2_status flush_status(Volume *v) {
+    if (!v->status_pending || !v->dev_small.p) return GVDB2_OK;
+    return read_words(v);
+}
+
 gvdb2_status sync_counts(Volume *v) {
     GV_CUDA(v, cudaStreamSynchronize(v->stream));
     return GVDB2_OK;
@@ -1104,6 +1123,7 @@ gvdb2_status rebuild_topology(Volume *v, int n, float radius, const float orig[3
                                                                         dev_words(v)->bbox);
     GV_CUDA(v, cudaGetLastError());
     GV_TRY(read_words(v));
+    v->all_leaves_flagged = false;
     for (int a = 0; a < 3; a++) {
         float lo = ord2f(host_words(v)->bbox[a]) - 1.0f, hi = ord2f(host_words(v)->bbox[3 + a]) + 2.0f;
         v->posmin[a] = 0 > lo ? 0 : lo;
@@ -1185,7 +1205,9 @@ gvdb2_status update_atlas(Volume *v) {
     if (total > 0) k_leaf_flags<<<grid_for(total, 256, 1ll << 31), 256, 0, s>>>(v->pool_ptr(0), total, flags);
     gvdb2_status st = exclusive_scan_u32(v, flags, scan, total);
     uint32_t nflag = 0;
-    if (st == GVDB2_OK) {
+    if (st == GVDB2_OK && v->all_leaves_flagged) {
+        nflag = (uint32_t)total; // a full rebuild flags every leaf: no read-back
+    } else if (st == GVDB2_OK) {
         cudaError_t e = cudaMemcpyAsync(&nflag, scan + total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) st = cuda_fail(v, e, "update_atlas count");
@@ -1697,6 +1719,8 @@ gvdb2_status adopt_pools(Volume *v, int depth) {
         GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), s));
         GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
     }
+    if (v->status_pending) GV_TRY(read_words(v)); // before the status word is cleared below
+    v->all_leaves_flagged = false;
     Node root;
     GV_CUDA(v, cudaMemcpy(&root, v->pool[depth].p, sizeof(Node), cudaMemcpyDeviceToHost));
     v->depth = depth;
