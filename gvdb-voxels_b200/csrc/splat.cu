@@ -229,14 +229,17 @@ struct SplatArgs {
 // most kScCap at a time: per point the x weights on the cell's 8 voxel
 // columns and the y weights on its 8 rows (zero where the stencil does not
 // reach), the z weights of its N taps and the channel amounts.  A stable
-// counting sort orders the chunk by (first z tap, x group, first y tap);
-// the x group says which halves of the cell's x range the stencil reaches
-// (lower only, both, upper only).  Lane (y, q, h) owns the voxels x in
-// [4q, 4q+4), row y, z in [4h, 4h+4) of every channel in registers and walks
-// only the records that reach them: for each first z tap, two contiguous
-// runs of the sorted chunk (its x groups, first y taps y-N+1..y).  The loop
-// over first z taps is unrolled relative to 4h, so each record's adds go to
-// accumulator planes fixed at compile time: paired register FMAs.
+// counting sort orders the chunk by (first z tap, x group); the x group says
+// which halves of the cell's x range the stencil reaches (lower only, both,
+// upper only).  Lane (y, q, h) owns the voxels x in [4q, 4q+4), row y, z in
+// [4h, 4h+4) of every channel in registers.  The 8 lanes of one (q, h) walk
+// the same records together -- for each first z tap one contiguous run of
+// the sorted chunk, its two x groups that reach half q -- so each record is
+// read once per group (a shared-memory broadcast) and the group's loop has
+// no divergence; a record adds to the 4 of the group's 8 rows that its
+// stencil covers (the other lanes add its zero y weight).  The loop over
+// first z taps is unrolled relative to 4h, so every add goes to an
+// accumulator plane fixed at compile time: paired register FMAs.
 //
 // The adds happen in the order of the sources (the bins) and of the stable
 // sort, so with deterministic binning the result is bit-reproducible.
@@ -248,7 +251,7 @@ struct SplatArgs {
 #endif
 constexpr int kScWarps = 4;                    // cells per CTA
 constexpr int kScCap = GVDB2_SC_CAP;           // records per chunk
-constexpr int kScBins = 11 * 3 * 11;           // (first z tap + 3, x group, first y tap + 3)
+constexpr int kScBins = 11 * 3;                // (first z tap + 3, x group)
 
 struct ScChunk {
     // x weights on the cell's voxel columns 0..7: half q (columns 4q..4q+3)
@@ -263,6 +266,8 @@ struct ScChunk {
     uint16_t rank[kScCap];
     uint16_t order[kScCap];
     uint16_t off[kScBins + 1];
+    uint2 run[64]; // the cell's sources: runs [x, y) of perm (at most 1 + 2 + 6 + 18 + 4 + 12 + 12 + 8 = 63)
+    uint32_t run_first[64]; // sources before run k (the runs read as one sequence)
 };
 
 // Sort the chunk's `fill` records by key (stable) into C.order.
@@ -311,7 +316,7 @@ __device__ __forceinline__ void sc_sort_chunk(ScChunk &C, int fill, int lane) {
     __syncwarp();
 }
 
-// Adds the chunk's records that reach lane (y, q, h)'s voxels.
+// Adds the chunk's records that reach the voxels of lane (y, q, h)'s group.
 template <int KERNEL, int NCH>
 __device__ __forceinline__ void sc_accumulate(const ScChunk &C, float2 (&acc)[4][2][NCH], int y, int q, int h) {
     constexpr int N = Taps<KERNEL>::N;
@@ -319,10 +324,9 @@ __device__ __forceinline__ void sc_accumulate(const ScChunk &C, float2 (&acc)[4]
     for (int sp = -3; sp <= 3; sp++) { // first z tap relative to 4h
         if (sp + N - 1 < 0) continue;
         const int s = sp + 4 * h; // first z tap relative to the cell, in [-3, 7]
-#pragma unroll 1
-        for (int g = 0; g < 2; g++) {
-            const int kb = ((s + 3) * 3 + q + g) * 11;
-            const int lo = C.off[kb + max(y - N + 1, -3) + 3], hi = C.off[kb + y + 4];
+        {
+            const int kb = (s + 3) * 3 + q; // x groups q and q + 1 reach half q
+            const int lo = C.off[kb], hi = C.off[kb + 2];
             for (int i = lo; i < hi; i++) {
                 const int r = C.order[i];
                 const float4 xv = C.xw[r][q ^ (r & 1)];
@@ -381,16 +385,69 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
     cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
     const Node &nd = S.leaves[S.slot_leaf[slot]];
     const int ox = nd.mPos[0] + kCell * cx, oy = nd.mPos[1] + kCell * cy, oz = nd.mPos[2] + kCell * cz;
-    // lane d < 27: the neighbour cell in direction d = (dz+1)*9 + (dy+1)*3 + (dx+1), or -1
-    int64_t nb = -1;
+    // The sources, as runs of perm in a fixed order: lane d < 27 lists those of
+    // the neighbour cell in direction d = (dz+1)*9 + (dy+1)*3 + (dx+1): its
+    // regions whose stencils reach this cell -- per axis, across the lower
+    // face its upper band (2), across the upper face its lower band (0),
+    // along the axis all three -- merged into as few runs as the region
+    // order allows.
+    int nrun = 0;
+    uint2 runs[9];
     if (lane < 27) {
-        const int ncx = cx + lane % 3 - 1, ncy = cy + lane / 3 % 3 - 1, ncz = cz + lane / 9 - 1;
+        const int dx = lane % 3 - 1, dy = lane / 3 % 3 - 1, dz = lane / 9 - 1;
+        const int ncx = cx + dx, ncy = cy + dy, ncz = cz + dz;
         const int bx = ncx < 0 ? -1 : (ncx >= S.m ? 1 : 0), by = ncy < 0 ? -1 : (ncy >= S.m ? 1 : 0),
                   bz = ncz < 0 ? -1 : (ncz >= S.m ? 1 : 0);
         const int32_t ns = (bx | by | bz) == 0 ? (int32_t)slot
                                                : S.nbr27[slot * 27 + (bz + 1) * 9 + (by + 1) * 3 + (bx + 1)];
-        if (ns >= 0) nb = (int64_t)ns * S.m3 + ((ncz - bz * S.m) * S.m + (ncy - by * S.m)) * S.m + (ncx - bx * S.m);
+        if (ns >= 0) {
+            const int64_t nc =
+                (int64_t)ns * S.m3 + ((ncz - bz * S.m) * S.m + (ncy - by * S.m)) * S.m + (ncx - bx * S.m);
+            const uint32_t *ro = S.reg_off + nc * kRegions;
+            const int rx0 = dx < 0 ? 2 : 0, ry0 = dy < 0 ? 2 : 0, ry1 = dy > 0 ? 0 : 2;
+            const int rz0 = dz < 0 ? 2 : 0, rz1 = dz > 0 ? 0 : 2;
+            auto add = [&](int r0, int r1) { // regions [r0, r1)
+                const uint2 u = make_uint2(ro[r0], ro[r1]);
+                if (u.y > u.x) runs[nrun++] = u;
+            };
+            if (dx == 0 && dy == 0) {
+                if (dz == 0) add(0, kRegions);
+                else add(rz0 * 9, rz0 * 9 + 9);
+            } else if (dx == 0) {
+                for (int rz = rz0; rz <= rz1; rz++) add((rz * 3 + ry0) * 3, (rz * 3 + ry0) * 3 + 3);
+            } else {
+                for (int rz = rz0; rz <= rz1; rz++)
+                    for (int ry = ry0; ry <= ry1; ry++) add((rz * 3 + ry) * 3 + rx0, (rz * 3 + ry) * 3 + rx0 + 1);
+            }
+        }
     }
+    // the lanes' runs one after the other, each with the number of sources
+    // before it, so that the warp reads them as one sequence, 32 at a time
+    uint32_t len = 0;
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+        if (k < nrun) len += runs[k].y - runs[k].x;
+    int first = nrun;
+    uint32_t before = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) { // inclusive prefixes over the lanes
+        const int t = __shfl_up_sync(0xffffffffu, first, o);
+        const uint32_t u = __shfl_up_sync(0xffffffffu, before, o);
+        if (lane >= o) first += t, before += u;
+    }
+    const int total_runs = __shfl_sync(0xffffffffu, first, 31);
+    const uint32_t total_src = __shfl_sync(0xffffffffu, before, 31);
+    first -= nrun;
+    before -= len;
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+        if (k < nrun) {
+            C.run[first + k] = runs[k];
+            C.run_first[first + k] = before;
+            before += runs[k].y - runs[k].x;
+        }
+    __syncwarp();
+
     const int y = lane & 7, q = (lane >> 3) & 1, h = lane >> 4;
     float2 acc[4][2][NCH];
 #pragma unroll
@@ -401,10 +458,8 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
             for (int c = 0; c < NCH; c++) acc[z][x][c] = make_float2(0.0f, 0.0f);
     int fill = 0;
     int step = 0; // 32-source steps so far (the warps of a giant cell take turns)
-
-    // records of the sources [beg, end) of perm, 32 at a time
-    auto take = [&](uint32_t beg, uint32_t end) {
-        for (uint32_t base = beg; base < end; base += 32) {
+    for (uint32_t vbase = 0; vbase < total_src; vbase += 32) {
+        {
             if (step++ % W != wturn) continue;
             if (fill > kScCap - 32) {
                 sc_sort_chunk(C, fill, lane);
@@ -412,8 +467,20 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
                 __syncwarp();
                 fill = 0;
             }
-            const uint32_t j = base + lane;
-            bool ok = j < end;
+            // this lane's source: the run holding sequence index vi (binary
+            // search of the run starts) and the perm entry inside it
+            const uint32_t vi = vbase + lane;
+            bool ok = vi < total_src;
+            uint32_t j = 0;
+            if (ok) {
+                int lo = 0, hi = total_runs - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (C.run_first[mid] <= vi) lo = mid;
+                    else hi = mid - 1;
+                }
+                j = C.run[lo].x + (vi - C.run_first[lo]);
+            }
             int32_t p = 0;
             float wx[N], wyt[N], wzt[N];
             int fx = 0, fy = 0, fz = 0;
@@ -451,32 +518,10 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
                 for (int c = 0; c < NCH; c++) a4[c] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt;
                 C.am[r] = make_float4(a4[0], a4[1], a4[2], a4[3]);
                 const int xg = fx < 5 - N ? 0 : (fx <= 3 ? 1 : 2); // lower half only, both, upper only
-                C.key[r] = (uint16_t)(((fz + 3) * 3 + xg) * 11 + fy + 3);
+                C.key[r] = (uint16_t)((fz + 3) * 3 + xg);
             }
             fill += __popc(mask);
         }
-    };
-
-    for (int d = 0; d < 27; d++) {
-        const int64_t nc = __shfl_sync(0xffffffffu, nb, d);
-        if (nc < 0) continue;
-        // the neighbour's regions whose stencils reach this cell, per axis:
-        // across the lower face its upper band (2), across the upper face
-        // its lower band (0), along the axis all three
-        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
-        const int rx0 = dx < 0 ? 2 : 0, rx1 = dx > 0 ? 0 : 2, ry0 = dy < 0 ? 2 : 0, ry1 = dy > 0 ? 0 : 2;
-        const int rz0 = dz < 0 ? 2 : 0, rz1 = dz > 0 ? 0 : 2;
-        const uint32_t *ro = S.reg_off + nc * kRegions;
-        if (dx == 0 && dy == 0) { // whole planes of regions: one run per z band (one run for the cell itself)
-            if (dz == 0) take(ro[0], ro[kRegions]);
-            else take(ro[rz0 * 9], ro[rz0 * 9 + 9]);
-        } else if (dx == 0) {
-            for (int rz = rz0; rz <= rz1; rz++) take(ro[(rz * 3 + ry0) * 3], ro[(rz * 3 + ry0) * 3 + 3]);
-        } else {
-            for (int rz = rz0; rz <= rz1; rz++)
-                for (int ry = ry0; ry <= ry1; ry++) take(ro[(rz * 3 + ry) * 3 + rx0], ro[(rz * 3 + ry) * 3 + rx0 + 1]);
-        }
-        (void)rx1;
     }
     if (fill > 0) {
         sc_sort_chunk(C, fill, lane);
