@@ -316,7 +316,8 @@ __device__ __forceinline__ void sc_sort_chunk(ScChunk &C, int fill, int lane) {
     __syncwarp();
 }
 
-// Adds the chunk's records that reach the voxels of lane (y, q, h)'s group.
+// Adds the chunk's records that reach the voxels of lane (y, q, h)'s group:
+// for each first z tap, the run of x groups q and q + 1.
 template <int KERNEL, int NCH>
 __device__ __forceinline__ void sc_accumulate(const ScChunk &C, float2 (&acc)[4][2][NCH], int y, int q, int h) {
     constexpr int N = Taps<KERNEL>::N;
@@ -324,35 +325,80 @@ __device__ __forceinline__ void sc_accumulate(const ScChunk &C, float2 (&acc)[4]
     for (int sp = -3; sp <= 3; sp++) { // first z tap relative to 4h
         if (sp + N - 1 < 0) continue;
         const int s = sp + 4 * h; // first z tap relative to the cell, in [-3, 7]
-        {
-            const int kb = (s + 3) * 3 + q; // x groups q and q + 1 reach half q
-            const int lo = C.off[kb], hi = C.off[kb + 2];
-            for (int i = lo; i < hi; i++) {
-                const int r = C.order[i];
-                const float4 xv = C.xw[r][q ^ (r & 1)];
-                const float wyv = C.wy[r][y];
-                const float4 zv = C.wz[r];
-                const float4 av = C.am[r];
-                const float zk[4] = {zv.x, zv.y, zv.z, zv.w};
-                const float ak[4] = {av.x, av.y, av.z, av.w};
-                const float2 x01 = make_float2(xv.x, xv.y), x23 = make_float2(xv.z, xv.w);
+        auto visit = [&](int r) {
+            const float4 xv = C.xw[r][q ^ (r & 1)];
+            const float wyv = C.wy[r][y];
+            const float4 zv = C.wz[r];
+            const float4 av = C.am[r];
+            const float zk[4] = {zv.x, zv.y, zv.z, zv.w};
+            const float ak[4] = {av.x, av.y, av.z, av.w};
+            const float2 x01 = make_float2(xv.x, xv.y), x23 = make_float2(xv.z, xv.w);
 #pragma unroll
-                for (int c = 0; c < NCH; c++) {
-                    const float ay = ak[c] * wyv;
+            for (int c = 0; c < NCH; c++) {
+                const float ay = ak[c] * wyv;
 #pragma unroll
-                    for (int k = 0; k < N; k++) {
-                        const int zz = sp + k;
-                        if (zz < 0 || zz >= 4) continue;
-                        const float t = ay * zk[k];
-                        const float2 tt = make_float2(t, t);
-                        acc[zz][0][c] = __ffma2_rn(tt, x01, acc[zz][0][c]);
-                        acc[zz][1][c] = __ffma2_rn(tt, x23, acc[zz][1][c]);
-                    }
+                for (int k = 0; k < N; k++) {
+                    const int zz = sp + k;
+                    if (zz < 0 || zz >= 4) continue;
+                    const float t = ay * zk[k];
+                    const float2 tt = make_float2(t, t);
+                    acc[zz][0][c] = __ffma2_rn(tt, x01, acc[zz][0][c]);
+                    acc[zz][1][c] = __ffma2_rn(tt, x23, acc[zz][1][c]);
                 }
             }
-        }
+        };
+        const int kb = (s + 3) * 3 + q; // x groups q and q + 1 reach half q
+        const int hi = C.off[kb + 2];
+        for (int i = C.off[kb]; i < hi; i++) visit(C.order[i]);
     }
 }
+
+// The same adds with the accumulators paired along channels ({c, c+1} of
+// one voxel in a float2) instead of along x: a record's amounts times its
+// y and z weights form the channel pairs directly, and each x weight is used
+// as the other factor of every pair (NCH > 1; an odd last channel is paired
+// with a zero amount).
+template <int KERNEL, int NP>
+__device__ __forceinline__ void sc_accumulate_cp(const ScChunk &C, float2 (&acc)[4][4][NP], int y, int q, int h) {
+    constexpr int N = Taps<KERNEL>::N;
+#pragma unroll
+    for (int sp = -3; sp <= 3; sp++) { // first z tap relative to 4h
+        if (sp + N - 1 < 0) continue;
+        const int s = sp + 4 * h; // first z tap relative to the cell, in [-3, 7]
+        auto visit = [&](int r) {
+            const float4 xv = C.xw[r][q ^ (r & 1)];
+            const float wyv = C.wy[r][y];
+            const float4 zv = C.wz[r];
+            const float4 av = C.am[r];
+            const float zk[4] = {zv.x, zv.y, zv.z, zv.w};
+            const float2 ap[2] = {make_float2(av.x, av.y), make_float2(av.z, av.w)};
+            const float xs[4] = {xv.x, xv.y, xv.z, xv.w};
+            float2 ay[NP];
+#pragma unroll
+            for (int cp = 0; cp < NP; cp++) ay[cp] = __fmul2_rn(ap[cp], make_float2(wyv, wyv));
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                const int zz = sp + k;
+                if (zz < 0 || zz >= 4) continue;
+#pragma unroll
+                for (int cp = 0; cp < NP; cp++) {
+                    const float2 t = __fmul2_rn(ay[cp], make_float2(zk[k], zk[k]));
+#pragma unroll
+                    for (int x = 0; x < 4; x++) acc[zz][x][cp] = __ffma2_rn(t, make_float2(xs[x], xs[x]), acc[zz][x][cp]);
+                }
+            }
+        };
+        const int kb = (s + 3) * 3 + q; // x groups q and q + 1 reach half q
+        const int hi = C.off[kb + 2];
+        for (int i = C.off[kb]; i < hi; i++) visit(C.order[i]);
+    }
+}
+
+#ifndef GVDB2_SC_CHPAIR
+#define GVDB2_SC_CHPAIR 1
+#endif
+// Channel pairs for 2 to 4 channels, x pairs for one channel.
+template <int NCH> struct ScLayout { static constexpr bool kChPairs = GVDB2_SC_CHPAIR && NCH > 1; };
 
 // Blocks [0, single_blocks) take kScWarps cells each, a warp per cell;
 // the rest take one giant cell each (more than kGiantCell points of its
@@ -449,13 +495,25 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
     __syncwarp();
 
     const int y = lane & 7, q = (lane >> 3) & 1, h = lane >> 4;
-    float2 acc[4][2][NCH];
+    constexpr bool kCp = ScLayout<NCH>::kChPairs;
+    constexpr int NP = (NCH + 1) / 2;
+    float2 acc[4][2][NCH];   // x pairs
+    float2 accp[4][4][NP];   // channel pairs
 #pragma unroll
-    for (int z = 0; z < 4; z++)
+    for (int z = 0; z < 4; z++) {
 #pragma unroll
         for (int x = 0; x < 2; x++)
 #pragma unroll
             for (int c = 0; c < NCH; c++) acc[z][x][c] = make_float2(0.0f, 0.0f);
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int c = 0; c < NP; c++) accp[z][x][c] = make_float2(0.0f, 0.0f);
+    }
+    auto accumulate = [&]() {
+        if constexpr (kCp) sc_accumulate_cp<KERNEL, NP>(C, accp, y, q, h);
+        else sc_accumulate<KERNEL, NCH>(C, acc, y, q, h);
+    };
     int fill = 0;
     int step = 0; // 32-source steps so far (the warps of a giant cell take turns)
     for (uint32_t vbase = 0; vbase < total_src; vbase += 32) {
@@ -463,7 +521,7 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
             if (step++ % W != wturn) continue;
             if (fill > kScCap - 32) {
                 sc_sort_chunk(C, fill, lane);
-                sc_accumulate<KERNEL, NCH>(C, acc, y, q, h);
+                accumulate();
                 __syncwarp();
                 fill = 0;
             }
@@ -525,7 +583,18 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
     }
     if (fill > 0) {
         sc_sort_chunk(C, fill, lane);
-        sc_accumulate<KERNEL, NCH>(C, acc, y, q, h);
+        accumulate();
+    }
+    if constexpr (kCp) { // to x pairs for the write-out (register renaming)
+#pragma unroll
+        for (int z = 0; z < 4; z++)
+#pragma unroll
+            for (int c = 0; c < NCH; c++)
+#pragma unroll
+                for (int xp = 0; xp < 2; xp++) {
+                    const float2 a0 = accp[z][2 * xp][c / 2], a1 = accp[z][2 * xp + 1][c / 2];
+                    acc[z][xp][c] = (c & 1) ? make_float2(a0.y, a1.y) : make_float2(a0.x, a1.x);
+                }
     }
     // each lane writes its 4 x 4 voxels of every channel once
     const int a = S.apron, tl = S.tile;
