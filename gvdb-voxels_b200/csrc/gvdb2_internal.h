@@ -170,6 +170,12 @@ struct Volume {
     // points in bin order (perm), each (cell, region) bin's first entry
     // (reg_off, 27 per cell) and each cell's (bin_off)
     DevBuf pbin, prank, bin_cnt, bin_off, reg_off, perm;
+    // the binned points' data in bin order, so that the splat kernels read
+    // a cell's points contiguously: per entry of perm the translated
+    // position and the cloud index (float4, w = int bits, -1 outside a
+    // batch), made with the bins; and the splat's channel amounts (float4),
+    // made by each scatter call
+    DevBuf bin_pos, bin_amt;
     // cells that hold points: huge and heavy ones (order of cell_at), light
     // ones, giant ones (the scatter's CTA cells) and the four counts;
     // heavy_grid, light_grid and cell_grid bound the huge+heavy, light and

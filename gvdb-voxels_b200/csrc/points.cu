@@ -123,6 +123,19 @@ __global__ void k_bin_fill(const int32_t *pbin, const int32_t *prank, int64_t n,
     if (b >= 0) perm[off[b] + prank[i]] = (int32_t)i;
 }
 
+// bin_pos[j] = the translated position of the point at bin-order entry j
+// (perm[j]) and its cloud index (-1 outside a batch), for the j below the
+// number of binned points, reg_off[nreg].
+__global__ void k_bin_pack_pos(const int32_t *perm, const uint32_t *reg_off, int64_t nreg, PointsView pos,
+                               float3 trans, float4 *bin_pos) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= (int64_t)reg_off[nreg]) return;
+    const int32_t p = perm[j];
+    const float3 q = load_f3(pos, p);
+    const int32_t cloud = pos.cloud ? pos.cloud[p] : -1;
+    bin_pos[j] = make_float4(q.x + trans.x, q.y + trans.y, q.z + trans.z, __int_as_float(cloud));
+}
+
 // List the cells that hold points by class (huge from the front of `list`,
 // heavy from its back, light in `light`; see cell_at).
 constexpr int64_t kCellCountReadback = 1 << 16; // cells
@@ -351,6 +364,13 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     } else if (n > 0) {
         k_bin_fill<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pbin.as<int32_t>(), v->prank.as<int32_t>(), n,
                                                                v->reg_off.as<uint32_t>(), v->perm.as<int32_t>());
+        GV_CUDA(v, cudaGetLastError());
+    }
+    // the points' positions in bin order
+    GV_CUDA(v, v->bin_pos.ensure(sizeof(float4) * (size_t)std::max(n, 1), s));
+    if (n > 0) {
+        k_bin_pack_pos<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->perm.as<int32_t>(), v->reg_off.as<uint32_t>(), nreg,
+                                                                  v->pos, t, v->bin_pos.as<float4>());
         GV_CUDA(v, cudaGetLastError());
     }
     // the cells that hold points, by class (the gathers' grids)

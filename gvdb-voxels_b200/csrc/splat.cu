@@ -204,6 +204,8 @@ struct SplatArgs {
     const uint32_t *bin_off;
     const uint32_t *reg_off; // per (cell, region) bin its first entry of perm (k_bin_count)
     const int32_t *perm;
+    const float4 *bin_pos;   // per entry of perm: translated position, cloud index bits
+    float4 *bin_amt;         // per entry of perm: the channel amounts of this call
     int res0, apron, tile;
     int m, m3; // cells per brick edge, per brick
     // huge and heavy cells (order of cell_at), light cells; cell_list ==
@@ -316,6 +318,41 @@ __device__ __forceinline__ void sc_sort_chunk(ScChunk &C, int fill, int lane) {
     __syncwarp();
 }
 
+#ifndef GVDB2_SC_PIPE
+#define GVDB2_SC_PIPE 0
+#endif
+#ifndef GVDB2_SC_PREFETCH
+#define GVDB2_SC_PREFETCH 0
+#endif
+// A record's values that lane (y, q) reads.
+struct ScRec {
+    float4 xv; // x weights on columns 4q..4q+3
+    float wy;  // y weight on row y
+    float4 zv; // z weights of the taps
+    float4 av; // channel amounts
+};
+__device__ __forceinline__ ScRec sc_load(const ScChunk &C, int r, int y, int q) {
+    return ScRec{C.xw[r][q ^ (r & 1)], C.wy[r][y], C.wz[r], C.am[r]};
+}
+// Visits the sorted chunk's records i in [lo, hi) in order; with
+// GVDB2_SC_PIPE the next record's values are read while the current one is
+// added.
+template <class Visit>
+__device__ __forceinline__ void sc_walk(const ScChunk &C, int lo, int hi, int y, int q, const Visit &visit) {
+    if (GVDB2_SC_PIPE) {
+        if (lo >= hi) return;
+        ScRec cur = sc_load(C, C.order[lo], y, q);
+        for (int i = lo; i < hi; i++) {
+            ScRec nxt = cur;
+            if (i + 1 < hi) nxt = sc_load(C, C.order[i + 1], y, q);
+            visit(cur);
+            cur = nxt;
+        }
+    } else {
+        for (int i = lo; i < hi; i++) visit(sc_load(C, C.order[i], y, q));
+    }
+}
+
 // Adds the chunk's records that reach the voxels of lane (y, q, h)'s group:
 // for each first z tap, the run of x groups q and q + 1.
 template <int KERNEL, int NCH>
@@ -325,11 +362,11 @@ __device__ __forceinline__ void sc_accumulate(const ScChunk &C, float2 (&acc)[4]
     for (int sp = -3; sp <= 3; sp++) { // first z tap relative to 4h
         if (sp + N - 1 < 0) continue;
         const int s = sp + 4 * h; // first z tap relative to the cell, in [-3, 7]
-        auto visit = [&](int r) {
-            const float4 xv = C.xw[r][q ^ (r & 1)];
-            const float wyv = C.wy[r][y];
-            const float4 zv = C.wz[r];
-            const float4 av = C.am[r];
+        auto visit = [&](const ScRec &d) {
+            const float4 xv = d.xv;
+            const float wyv = d.wy;
+            const float4 zv = d.zv;
+            const float4 av = d.av;
             const float zk[4] = {zv.x, zv.y, zv.z, zv.w};
             const float ak[4] = {av.x, av.y, av.z, av.w};
             const float2 x01 = make_float2(xv.x, xv.y), x23 = make_float2(xv.z, xv.w);
@@ -349,7 +386,7 @@ __device__ __forceinline__ void sc_accumulate(const ScChunk &C, float2 (&acc)[4]
         };
         const int kb = (s + 3) * 3 + q; // x groups q and q + 1 reach half q
         const int hi = C.off[kb + 2];
-        for (int i = C.off[kb]; i < hi; i++) visit(C.order[i]);
+        sc_walk(C, C.off[kb], hi, y, q, visit);
     }
 }
 
@@ -365,11 +402,11 @@ __device__ __forceinline__ void sc_accumulate_cp(const ScChunk &C, float2 (&acc)
     for (int sp = -3; sp <= 3; sp++) { // first z tap relative to 4h
         if (sp + N - 1 < 0) continue;
         const int s = sp + 4 * h; // first z tap relative to the cell, in [-3, 7]
-        auto visit = [&](int r) {
-            const float4 xv = C.xw[r][q ^ (r & 1)];
-            const float wyv = C.wy[r][y];
-            const float4 zv = C.wz[r];
-            const float4 av = C.am[r];
+        auto visit = [&](const ScRec &d) {
+            const float4 xv = d.xv;
+            const float wyv = d.wy;
+            const float4 zv = d.zv;
+            const float4 av = d.av;
             const float zk[4] = {zv.x, zv.y, zv.z, zv.w};
             const float2 ap[2] = {make_float2(av.x, av.y), make_float2(av.z, av.w)};
             const float xs[4] = {xv.x, xv.y, xv.z, xv.w};
@@ -390,7 +427,7 @@ __device__ __forceinline__ void sc_accumulate_cp(const ScChunk &C, float2 (&acc)
         };
         const int kb = (s + 3) * 3 + q; // x groups q and q + 1 reach half q
         const int hi = C.off[kb + 2];
-        for (int i = C.off[kb]; i < hi; i++) visit(C.order[i]);
+        sc_walk(C, C.off[kb], hi, y, q, visit);
     }
 }
 
@@ -515,70 +552,103 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
         else sc_accumulate<KERNEL, NCH>(C, acc, y, q, h);
     };
     int fill = 0;
-    int step = 0; // 32-source steps so far (the warps of a giant cell take turns)
-    for (uint32_t vbase = 0; vbase < total_src; vbase += 32) {
-        {
-            if (step++ % W != wturn) continue;
-            if (fill > kScCap - 32) {
-                sc_sort_chunk(C, fill, lane);
-                accumulate();
-                __syncwarp();
-                fill = 0;
-            }
-            // this lane's source: the run holding sequence index vi (binary
-            // search of the run starts) and the perm entry inside it
-            const uint32_t vi = vbase + lane;
-            bool ok = vi < total_src;
-            uint32_t j = 0;
-            if (ok) {
-                int lo = 0, hi = total_runs - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (C.run_first[mid] <= vi) lo = mid;
-                    else hi = mid - 1;
-                }
-                j = C.run[lo].x + (vi - C.run_first[lo]);
-            }
-            int32_t p = 0;
-            float wx[N], wyt[N], wzt[N];
-            int fx = 0, fy = 0, fz = 0;
-            if (ok) {
-                p = S.perm[j];
-                const float3 pt = load_f3(S.pos, p);
-                const int3 o = point_origin(S.pos, p);
-                fx = T::eval(pt.x + S.trans.x, wx) + o.x - ox;
-                fy = T::eval(pt.y + S.trans.y, wyt) + o.y - oy;
-                fz = T::eval(pt.z + S.trans.z, wzt) + o.z - oz;
-                // the stencil reaches the cell on every axis (true of every
-                // source by construction of the regions)
-                ok = fx > -N && fx < kCell && fy > -N && fy < kCell && fz > -N && fz < kCell;
-            }
-            const unsigned mask = __ballot_sync(0xffffffffu, ok);
-            if (ok) {
-                const int r = fill + __popc(mask & lanemask_lt());
-                float *xr = reinterpret_cast<float *>(C.xw[r]);
-                float *yr = C.wy[r];
-                reinterpret_cast<float4 *>(xr)[0] = reinterpret_cast<float4 *>(xr)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-                reinterpret_cast<float4 *>(yr)[0] = reinterpret_cast<float4 *>(yr)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-                const int sw = (r & 1) * 4; // the halves of odd records are swapped
+    // One lane's source of a step: its point, the cloud origin and the
+    // channel amounts (all the global reads of a record).
+    struct Src {
+        bool ok;
+        float3 pt;
+        int3 o;
+        float a4[4];
+    };
+    auto fetch = [&](uint32_t vb) {
+        Src d;
+        d.ok = false;
+        d.pt = make_float3(0.f, 0.f, 0.f);
+        d.o = make_int3(0, 0, 0);
 #pragma unroll
-                for (int t = 0; t < N; t++) {
-                    if ((unsigned)(fx + t) < (unsigned)kCell) xr[(fx + t) ^ sw] = wx[t];
-                    if ((unsigned)(fy + t) < (unsigned)kCell) yr[fy + t] = wyt[t];
-                }
-                float zz4[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                for (int t = 0; t < N; t++) zz4[t] = wzt[t];
-                C.wz[r] = make_float4(zz4[0], zz4[1], zz4[2], zz4[3]);
-                const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
-                float a4[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                for (int c = 0; c < NCH; c++) a4[c] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt;
-                C.am[r] = make_float4(a4[0], a4[1], a4[2], a4[3]);
-                const int xg = fx < 5 - N ? 0 : (fx <= 3 ? 1 : 2); // lower half only, both, upper only
-                C.key[r] = (uint16_t)((fz + 3) * 3 + xg);
+        for (int c = 0; c < 4; c++) d.a4[c] = 0.0f;
+        // the run holding sequence index vi (binary search of the run
+        // starts) and the perm entry inside it
+        const uint32_t vi = vb + lane;
+        if (vi < total_src) {
+            int lo = 0, hi = total_runs - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (C.run_first[mid] <= vi) lo = mid;
+                else hi = mid - 1;
             }
-            fill += __popc(mask);
+            const uint32_t j = C.run[lo].x + (vi - C.run_first[lo]);
+            const float4 q = S.bin_pos[j];
+            d.pt = make_float3(q.x, q.y, q.z);
+            const int32_t cloud = __float_as_int(q.w);
+            if (cloud >= 0) d.o = make_int3(S.pos.origin[3 * cloud], S.pos.origin[3 * cloud + 1], S.pos.origin[3 * cloud + 2]);
+            const float4 am = S.bin_amt[j];
+            d.a4[0] = am.x, d.a4[1] = am.y, d.a4[2] = am.z, d.a4[3] = am.w;
+            d.ok = true;
+        }
+        return d;
+    };
+    // The record of each lane's source, appended to the chunk.
+    auto build = [&](const Src &d) {
+        float wx[N], wyt[N], wzt[N];
+        int fx = 0, fy = 0, fz = 0;
+        bool ok = d.ok;
+        if (ok) {
+            fx = T::eval(d.pt.x, wx) + d.o.x - ox; // bin_pos holds the translated position
+            fy = T::eval(d.pt.y, wyt) + d.o.y - oy;
+            fz = T::eval(d.pt.z, wzt) + d.o.z - oz;
+            // the stencil reaches the cell on every axis (true of every
+            // source by construction of the regions)
+            ok = fx > -N && fx < kCell && fy > -N && fy < kCell && fz > -N && fz < kCell;
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+            const int r = fill + __popc(mask & lanemask_lt());
+            float *xr = reinterpret_cast<float *>(C.xw[r]);
+            float *yr = C.wy[r];
+            reinterpret_cast<float4 *>(xr)[0] = reinterpret_cast<float4 *>(xr)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            reinterpret_cast<float4 *>(yr)[0] = reinterpret_cast<float4 *>(yr)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            const int sw = (r & 1) * 4; // the halves of odd records are swapped
+#pragma unroll
+            for (int t = 0; t < N; t++) {
+                if ((unsigned)(fx + t) < (unsigned)kCell) xr[(fx + t) ^ sw] = wx[t];
+                if ((unsigned)(fy + t) < (unsigned)kCell) yr[fy + t] = wyt[t];
+            }
+            float zz4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int t = 0; t < N; t++) zz4[t] = wzt[t];
+            C.wz[r] = make_float4(zz4[0], zz4[1], zz4[2], zz4[3]);
+            C.am[r] = make_float4(d.a4[0], d.a4[1], d.a4[2], d.a4[3]);
+            const int xg = fx < 5 - N ? 0 : (fx <= 3 ? 1 : 2); // lower half only, both, upper only
+            C.key[r] = (uint16_t)((fz + 3) * 3 + xg);
+        }
+        fill += __popc(mask);
+    };
+    auto flush_if_full = [&]() {
+        if (fill > kScCap - 32) {
+            sc_sort_chunk(C, fill, lane);
+            accumulate();
+            __syncwarp();
+            fill = 0;
+        }
+    };
+    // the steps of 32 sources this warp takes (the warps of a giant cell take turns)
+    const uint32_t stride = 32u * W;
+    uint32_t vb = 32u * wturn;
+    if (GVDB2_SC_PREFETCH) {
+        // the next step's reads are in flight while this step's records are
+        // built and a full chunk is added
+        Src nxt = fetch(vb);
+        for (; vb < total_src; vb += stride) {
+            const Src cur = nxt;
+            if (vb + stride < total_src) nxt = fetch(vb + stride);
+            flush_if_full();
+            build(cur);
+        }
+    } else {
+        for (; vb < total_src; vb += stride) {
+            flush_if_full();
+            build(fetch(vb));
         }
     }
     if (fill > 0) {
@@ -674,28 +744,47 @@ struct GatherArgs {
     const uint32_t *cell_cnt;
     int64_t ncell;
     int64_t tvox;
+    const float4 *bin_pos; // per entry of perm: translated position, cloud bits (nullptr: read via perm)
 };
+
+// The translated position and cloud origin of point pidx, entry j of the
+// bin order: from the bin-ordered copy when there is one (contiguous reads
+// for a cell's points), else from the caller's view.
+__device__ __forceinline__ void gather_point_at(const GatherArgs &G, int32_t pidx, int64_t j, float3 &w, int3 &o) {
+    if (G.bin_pos) {
+        const float4 q = G.bin_pos[j];
+        w = make_float3(q.x, q.y, q.z);
+        const int32_t cloud = __float_as_int(q.w);
+        o = cloud >= 0 ? make_int3(G.pos.origin[3 * cloud], G.pos.origin[3 * cloud + 1], G.pos.origin[3 * cloud + 2])
+                       : make_int3(0, 0, 0);
+    } else {
+        const float3 p = load_f3(G.pos, pidx);
+        w = make_float3(p.x + G.trans.x, p.y + G.trans.y, p.z + G.trans.z);
+        o = point_origin(G.pos, pidx);
+    }
+}
 
 // One point of a gather, in any mode.  fetch(x, y, z, g) gives g[c], the
 // value of channel c at tap (x, y, z) of the cell's extended frame, whose
 // origin (ox, oy, oz) is the cell's first voxel minus H.
 template <int KERNEL, int MODE, int NCH, class Fetch>
-__device__ __forceinline__ void gather_point(const GatherArgs &G, int32_t pidx, int ox, int oy, int oz,
+__device__ __forceinline__ void gather_point(const GatherArgs &G, int32_t pidx, int64_t j, int ox, int oy, int oz,
                                              const Fetch &fetch) {
     using T = Taps<KERNEL>;
     constexpr int N = T::N;
-    const float3 p = load_f3(G.pos, pidx);
-    const int3 o = point_origin(G.pos, pidx);
+    float3 p;
+    int3 o;
+    gather_point_at(G, pidx, j, p, o);
     float wx[N], wy[N], wz[N], dx[N], dy[N], dz[N];
     int fx, fy, fz;
     if (MODE == kFwd) {
-        fx = T::eval(p.x + G.trans.x, wx) + o.x - ox;
-        fy = T::eval(p.y + G.trans.y, wy) + o.y - oy;
-        fz = T::eval(p.z + G.trans.z, wz) + o.z - oz;
+        fx = T::eval(p.x, wx) + o.x - ox;
+        fy = T::eval(p.y, wy) + o.y - oy;
+        fz = T::eval(p.z, wz) + o.z - oz;
     } else {
-        fx = T::eval_d(p.x + G.trans.x, wx, dx) + o.x - ox;
-        fy = T::eval_d(p.y + G.trans.y, wy, dy) + o.y - oy;
-        fz = T::eval_d(p.z + G.trans.z, wz, dz) + o.z - oz;
+        fx = T::eval_d(p.x, wx, dx) + o.x - ox;
+        fy = T::eval_d(p.y, wy, dy) + o.y - oy;
+        fz = T::eval_d(p.z, wz, dz) + o.z - oz;
     }
     // a binned point's first taps lie in [0, 8]; a point moved since the
     // binning (positions changed in place) gathers 0 and reads nothing outside
@@ -868,12 +957,12 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
         // key = the point's first tap in the frame (clamped; a point moved
         // since the binning gathers zero whatever its key)
         for (int j = threadIdx.x; j < cnt; j += kGatherThreads) {
-            const int32_t p = G.perm[cb + j];
-            const float3 q = load_f3(G.pos, p);
-            const int3 o = point_origin(G.pos, p);
-            const int fx = (int)floorf(q.x + G.trans.x - 0.5f) - Taps<KERNEL>::LO + o.x - ox;
-            const int fy = (int)floorf(q.y + G.trans.y - 0.5f) - Taps<KERNEL>::LO + o.y - oy;
-            const int fz = (int)floorf(q.z + G.trans.z - 0.5f) - Taps<KERNEL>::LO + o.z - oz;
+            float3 q;
+            int3 o;
+            gather_point_at(G, G.bin_pos ? 0 : G.perm[cb + j], (int64_t)cb + j, q, o);
+            const int fx = (int)floorf(q.x - 0.5f) - Taps<KERNEL>::LO + o.x - ox;
+            const int fy = (int)floorf(q.y - 0.5f) - Taps<KERNEL>::LO + o.y - oy;
+            const int fz = (int)floorf(q.z - 0.5f) - Taps<KERNEL>::LO + o.z - oz;
             const int kx = min(max(fx, 0), kCell), ky = min(max(fy, 0), kCell), kz = min(max(fz, 0), kCell);
             const int k = (kz * (kCell + 1) + ky) * (kCell + 1) + kx;
             key[j] = (uint16_t)k;
@@ -911,7 +1000,7 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
         for (int j = threadIdx.x; j < cnt; j += kGatherThreads) order[hist[key[j]] + rank[j]] = (uint16_t)j;
         __syncthreads();
         for (int j = threadIdx.x; j < cnt; j += kGatherThreads)
-            gather_point<KERNEL, MODE, NCH>(G, G.perm[cb + order[j]], ox, oy, oz, fetch);
+            gather_point<KERNEL, MODE, NCH>(G, G.perm[cb + order[j]], (int64_t)cb + order[j], ox, oy, oz, fetch);
         __syncthreads(); // the order arrays are reused by the next chunk
     }
 }
@@ -945,7 +1034,7 @@ __device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t 
 #pragma unroll
         for (int c = 0; c < NCH; c++) g[c] = ns >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
     };
-    gather_point<KERNEL, MODE, NCH>(G, G.perm[beg + lane], nd.mPos[0] + fx0, nd.mPos[1] + fy0, nd.mPos[2] + fz0,
+    gather_point<KERNEL, MODE, NCH>(G, G.perm[beg + lane], (int64_t)beg + lane, nd.mPos[0] + fx0, nd.mPos[1] + fy0, nd.mPos[2] + fz0,
                                     fetch);
 }
 
@@ -1010,15 +1099,34 @@ gvdb2_status launch_smem(Volume *v, K kernel, size_t smem, const char *what) {
     return GVDB2_OK;
 }
 
+// The channel amounts of the group in bin order: bin_amt[j] for the point
+// perm[j], j below the number of binned points (reg_off[ncell * 27]).
+template <int NCH>
+__global__ void k_pack_amounts(SplatArgs S) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= (int64_t)S.reg_off[S.ncell * kRegions]) return;
+    const int32_t p = S.perm[j];
+    const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
+    float a4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int c = 0; c < NCH; c++) a4[c] = ((S.attr_mask >> c) & 1) ? wt * load_f1(S.attr[c], p) : wt;
+    S.bin_amt[j] = make_float4(a4[0], a4[1], a4[2], a4[3]);
+}
+
 // Owner-computes scatter of up to 4 channels (one group): a warp per cell,
 // every cell of the active bricks (cells no stencil reaches get zeros).
 template <int KERNEL, int NCH>
-gvdb2_status scatter_group(Volume *v, const SplatArgs &S) {
+gvdb2_status scatter_group(Volume *v, const SplatArgs &S0) {
     constexpr size_t smem = sizeof(ScChunk) * kScWarps;
     auto k = k_scatter_cells<KERNEL, NCH>;
     GV_TRY(launch_smem(v, k, smem, "scatter"));
+    GV_CUDA(v, v->bin_amt.ensure(sizeof(float4) * (size_t)std::max<int64_t>(v->bin_key.n, 1), v->stream));
+    SplatArgs S = S0;
+    S.bin_amt = v->bin_amt.as<float4>();
     const int64_t single = (S.ncell + kScWarps - 1) / kScWarps;
     const int64_t blocks = single + v->giant_grid; // giant cells: at most n / kGiantCell of them
+    if (v->bin_key.n > 0)
+        k_pack_amounts<NCH><<<grid_for(v->bin_key.n, 256, 1ll << 31), 256, 0, v->stream>>>(S);
     if (blocks > 0) k<<<(unsigned)blocks, 32 * kScWarps, smem, v->stream>>>(S, single);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
@@ -1207,6 +1315,7 @@ gvdb2_status scatter_kernel(Volume *v, int kernel, int n, const float trans[3], 
     fill_topology(v, S);
     S.reg_off = v->reg_off.as<uint32_t>();
     S.cell_giant = v->cell_giant.as<int32_t>();
+    S.bin_pos = v->bin_pos.as<float4>();
     return run_scatter(v, kernel, S);
 }
 
@@ -1225,6 +1334,7 @@ gvdb2_status gather_kernel(Volume *v, int kernel, int n, const float trans[3], c
     G.out = out;
     G.out_stride = out_stride;
     fill_topology(v, G);
+    G.bin_pos = v->bin_pos.as<float4>(); // bins made by bin_points
     return run_gather<kFwd>(v, kernel, G);
 }
 
@@ -1272,6 +1382,7 @@ gvdb2_status scatter_kernel_backward(Volume *v, int kernel, int n, const float t
     G.grad_weight = grad_weight;
     G.grad_attr = grad_attr;
     fill_topology(v, G);
+    G.bin_pos = v->bin_pos.as<float4>(); // bins made by bin_points
     return run_gather<kScatterBwd>(v, kernel, G);
 }
 
@@ -1304,6 +1415,7 @@ gvdb2_status gather_kernel_backward(Volume *v, int kernel, int n, const float tr
         fill_topology(v, S);
         S.reg_off = v->reg_off.as<uint32_t>();
         S.cell_giant = v->cell_giant.as<int32_t>();
+        S.bin_pos = v->bin_pos.as<float4>();
         GV_TRY(run_scatter(v, kernel, S));
     }
     if (!grad_pos || n == 0) return GVDB2_OK;
@@ -1316,6 +1428,7 @@ gvdb2_status gather_kernel_backward(Volume *v, int kernel, int n, const float tr
     G.grad_out = grad_out;
     G.grad_pos = grad_pos;
     fill_topology(v, G);
+    G.bin_pos = v->bin_pos.as<float4>(); // bins made by bin_points
     return run_gather<kGatherBwd>(v, kernel, G);
 }
 
