@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="the main line only (no 4M, incremental, adjoint, "
                                                               "batched or reference-kernel legs)")
     ap.add_argument("--incremental", action="store_true", help="reference state machine instead of full rebuilds")
+    ap.add_argument("--leg", default=None, choices=list(EXTRA_LEGS),
+                    help="one extra leg of the main line, alone (the main line runs each in a child process)")
     ap.add_argument("--quick", action="store_true", help="timed steps only (no baseline, e2e or launch count)")
     ap.add_argument("--sites", default=None, help="lattice sites x,y,z (smaller cases for profiling)")
     ap.add_argument("--workload", default="dam16m", choices=["dam16m", "dam", "batched", "adjoint", "sparse67m"],
@@ -516,7 +518,7 @@ def run_ours(a):
     if rank == 0 and ws == 1 and not a.no_extras and not a.sites:
         del pipe
         torch.cuda.empty_cache()
-        extras = run_extras(a, pos, vel)
+        extras = run_extras(a)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
                 "warmup": max(3, a.warmup), "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -550,23 +552,48 @@ STAGE_KERNELS = {"scatter": "scatter stage: k_scatter_own<cubic,4> (heavy and li
 # ----------------------------------------------------------------------------
 # the rest of the metric, each measured in the same run (N = 1)
 # ----------------------------------------------------------------------------
-def run_extras(a, pos16, vel16):
-    import torch
+EXTRA_LEGS = ("incremental", "config1_4m", "adjoint", "batched", "vs_ref_kernels")
+# legs left out of the main line, with the reason
+HELD_LEGS = {"batched": "held back: an illegal memory access in this leg is under investigation"}
+
+
+def run_leg(name, warmup):
+    """One extra leg in this process; returns its result dict."""
+    if name == "incremental":
+        import gvdb2.workloads as wl
+        w = WORKLOADS["dam16m"]
+        pos, vel = wl.dam_block(sites=w["sites"], spacing=w["spacing"])
+        return extra_incremental(pos, vel, warmup)
+    if name == "config1_4m":
+        return extra_config1()
+    if name == "adjoint":
+        return measure_adjoint(steps=20, warmup=3)
+    if name == "batched":
+        return measure_batched(steps=3, warmup=1)
+    if name == "vs_ref_kernels":
+        return extra_ref_kernels()
+    raise ValueError(name)
+
+
+def run_extras(a):
+    """The rest of the metric, each leg in a child process of its own (a
+    failing leg reports an error and never takes the main line down)."""
     out = {}
-
-    def guard(name, f):
+    for name in EXTRA_LEGS:
+        if name in HELD_LEGS:
+            out[name] = {"error": HELD_LEGS[name]}
+            continue
+        cmd = [sys.executable, os.path.abspath(__file__), "--leg", name, "--warmup", str(a.warmup)]
         try:
-            out[name] = f()
-        except Exception as e:  # an extra leg never takes the main line down
-            out[name] = {"error": f"{type(e).__name__}: {e}"[:300]}
-        torch.cuda.synchronize()
-        torch.cuda.empty_cache()
-
-    guard("incremental", lambda: extra_incremental(pos16, vel16, a.warmup))
-    guard("config1_4m", lambda: extra_config1())
-    guard("adjoint", lambda: measure_adjoint(steps=20, warmup=3))
-    guard("batched", lambda: measure_batched(steps=3, warmup=1))
-    guard("vs_ref_kernels", lambda: extra_ref_kernels())
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+            lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+            if r.returncode == 0 and lines:
+                out[name] = json.loads(lines[-1])
+            else:
+                tail = (r.stderr.strip().splitlines() or ["no output"])[-1]
+                out[name] = {"error": f"exit {r.returncode}: {tail}"[:300]}
+        except subprocess.TimeoutExpired:
+            out[name] = {"error": "timed out after 900 s"}
     summary = {}
     if isinstance(out.get("adjoint"), dict) and "adjoint_over_forward" in out["adjoint"]:
         summary["adjoint_over_forward"] = out["adjoint"]["adjoint_over_forward"]
@@ -1058,6 +1085,11 @@ def run_sparse(a):
 
 def main():
     a = parse()
+    if a.leg:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_leg(a.leg, a.warmup)), flush=True)
+        return 0
     if a.impl == "reference":
         if a.workload not in WORKLOADS:
             print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the dam-block step"}))

@@ -183,7 +183,32 @@ __device__ __forceinline__ void cell_coords(int64_t cell, int m, int m3, int64_t
 // cells' points straight from the atlas, one warp per light cell.
 constexpr uint32_t kHeavyCell = 1024;
 constexpr uint32_t kLightCell = 32;
-constexpr uint32_t kGiantCell = 4096; // the scatter gives such a cell a whole CTA
+// Cells of at least kDenseCell points are splatted into partial sums (the
+// scatter's dense path), kSlicePts points per CTA.
+#ifndef GVDB2_DENSE_CELL
+#define GVDB2_DENSE_CELL 512
+#endif
+constexpr uint32_t kDenseCell = GVDB2_DENSE_CELL;
+
+// Sizes the splat kernels check their data-derived indices against: an
+// index out of range (bins inconsistent with the topology) skips the access
+// and sets *flag, which the host reports as an error at its next read-back.
+struct SplatLimits {
+    int32_t *flag;
+    int64_t nslot;  // atlas slots
+    int64_t npool;  // level-0 pool nodes
+    int64_t nentry; // entries of the bin order (the points the bins were made for)
+    int64_t ncloud; // batched clouds
+};
+__device__ __forceinline__ bool in_range(const SplatLimits &L, int64_t i, int64_t hi) {
+    if ((uint64_t)i < (uint64_t)hi) return true;
+    if (L.flag) atomicOr(L.flag, 1);
+    return false;
+}
+constexpr uint32_t kSlicePts = 4096;
+// cell_cnt entries: huge, heavy, light cells; dense cells, dense work
+// items (slices), dense cells of more than one slice
+constexpr int kCntHuge = 0, kCntHeavy = 1, kCntLight = 2, kCntDense = 3, kCntWork = 4, kCntMulti = 5, kCntWords = 8;
 // The i-th huge or heavy cell, or -1 past their end.
 __device__ __forceinline__ int64_t cell_at(int64_t i, const int32_t *list, const uint32_t *cnt, int64_t ncell) {
     const int64_t h = cnt[0];

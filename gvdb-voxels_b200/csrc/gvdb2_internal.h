@@ -139,6 +139,9 @@ struct Volume {
     // the device status word of the last full rebuild is checked at the
     // next read-back of the small device words instead of by a read of its own
     bool status_pending = false;
+    // a splat kernel ran since the last read-back of the small device words:
+    // their splat guard word is checked then
+    bool splat_guard_pending = false;
     DevBuf pool[kMaxLev];     // Node arrays
     DevBuf clist[kMaxLev];    // uint64 child lists (lev >= 1)
     uint64_t topo_version = 0;
@@ -176,12 +179,19 @@ struct Volume {
     // batch), made with the bins; and the splat's channel amounts (float4),
     // made by each scatter call
     DevBuf bin_pos, bin_amt;
+    // the scatter's dense cells: per cell its partial slot or -1
+    // (cell_part); the work items (cell, slice, slices, accumulator slot;
+    // part_work); the partial sums, 12^3 or 10^3 floats per dense cell and
+    // channel (part_buf); the integer accumulators and arrival counters of
+    // cells splatted by several CTAs (part_acc, part_done: zero between
+    // calls); their capacities
+    DevBuf cell_part, part_work, part_buf, part_acc, part_done;
+    int64_t dense_cap = 0, work_cap = 0, multi_cap = 0, part_acc_cap = 0;
     // cells that hold points: huge and heavy ones (order of cell_at), light
-    // ones, giant ones (the scatter's CTA cells) and the four counts;
-    // heavy_grid, light_grid and cell_grid bound the huge+heavy, light and
-    // all lists, giant_grid the giant list
-    DevBuf cell_list, cell_light, cell_giant, cell_cnt;
-    int64_t cell_grid = 0, heavy_grid = 0, light_grid = 0, giant_grid = 0;
+    // ones and the counts (kCnt*); heavy_grid, light_grid and cell_grid
+    // bound the huge+heavy, light and all lists
+    DevBuf cell_list, cell_light, cell_cnt;
+    int64_t cell_grid = 0, heavy_grid = 0, light_grid = 0;
     struct BinKey {
         bool valid = false;
         int kernel = 0;
@@ -272,6 +282,9 @@ gvdb2_status sync_counts(Volume *v);
 // reads back the small device words when a full rebuild's status check is
 // pending and reports its error, if any
 gvdb2_status flush_status(Volume *v);
+// the small device word the splat kernels flag an out-of-range index in
+// (nullptr before the first rebuild)
+int32_t *splat_guard_word(Volume *v);
 
 // ---- points.cu ----
 gvdb2_status insert_points(Volume *v, int n, const float trans[3], int prefix);

@@ -140,21 +140,32 @@ __global__ void k_bin_pack_pos(const int32_t *perm, const uint32_t *reg_off, int
 // heavy from its back, light in `light`; see cell_at).
 constexpr int64_t kCellCountReadback = 1 << 16; // cells
 
-// Cells of more than kGiantCell points are also listed in `giant` (count
-// cnt[3]): the scatter gives each of them a CTA.
-__global__ void k_cell_list(const uint32_t *off, int64_t ncell, int32_t *list, int32_t *light, int32_t *giant,
-                            uint32_t *cnt) {
+// Cells of at least kDenseCell points are the scatter's dense cells: each
+// gets a partial slot (part[c], -1 for the other cells), ceil(k /
+// kSlicePts) work items (cell, slice, slices, accumulator slot) and, when
+// that is more than one, an accumulator slot for its integer sums.
+__global__ void k_cell_list(const uint32_t *off, int64_t ncell, int32_t *list, int32_t *light, int32_t *part,
+                            int4 *work, uint32_t *cnt) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t k = c < ncell ? off[c + 1] - off[c] : 0u;
-    const int cls = k == 0 ? -1 : (k > kHeavyCell ? 0 : (k > kLightCell ? 1 : 2));
+    const int cls = k == 0 ? -1 : (k > kHeavyCell ? kCntHuge : (k > kLightCell ? kCntHeavy : kCntLight));
     const unsigned act = __ballot_sync(0xffffffffu, cls >= 0);
     if (cls >= 0) {
         const uint32_t r = warp_agg_inc(cnt, (uint32_t)cls, act);
-        if (cls == 2) light[r] = (int32_t)c;
-        else list[cls == 0 ? (int64_t)r : ncell - 1 - r] = (int32_t)c;
+        if (cls == kCntLight) light[r] = (int32_t)c;
+        else list[cls == kCntHuge ? (int64_t)r : ncell - 1 - r] = (int32_t)c;
     }
-    const unsigned big = __ballot_sync(0xffffffffu, k > kGiantCell);
-    if (k > kGiantCell) giant[warp_agg_inc(cnt, 3u, big)] = (int32_t)c;
+    const bool dense = k >= kDenseCell;
+    const unsigned dn = __ballot_sync(0xffffffffu, dense);
+    int32_t slot = -1;
+    if (dense) slot = (int32_t)warp_agg_inc(cnt, (uint32_t)kCntDense, dn);
+    if (c < ncell) part[c] = slot;
+    if (dense) {
+        const uint32_t ns = (k + kSlicePts - 1) / kSlicePts;
+        const uint32_t first = atomicAdd(cnt + kCntWork, ns);
+        const int32_t acc = ns > 1 ? (int32_t)atomicAdd(cnt + kCntMulti, 1u) : -1;
+        for (uint32_t i = 0; i < ns; i++) work[first + i] = make_int4((int32_t)c, (int32_t)i, (int32_t)ns, acc);
+    }
 }
 
 // gvdbSetFlagSubcell (P:109-118)
@@ -373,32 +384,40 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
                                                                   v->pos, t, v->bin_pos.as<float4>());
         GV_CUDA(v, cudaGetLastError());
     }
-    // the cells that hold points, by class (the gathers' grids)
+    // the cells that hold points, by class (the gathers' grids), and the
+    // scatter's dense cells with their work items
     GV_CUDA(v, v->cell_list.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
     GV_CUDA(v, v->cell_light.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
-    const int64_t giant_cap = std::min<int64_t>(std::max<int64_t>(nbins, 1), n / (int64_t)kGiantCell + 1);
-    GV_CUDA(v, v->cell_giant.ensure(sizeof(int32_t) * (size_t)giant_cap, s));
-    v->giant_grid = giant_cap;
-    GV_CUDA(v, v->cell_cnt.ensure(sizeof(uint32_t) * 4, s));
-    GV_CUDA(v, cudaMemsetAsync(v->cell_cnt.p, 0, sizeof(uint32_t) * 4, s));
+    GV_CUDA(v, v->cell_part.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
+    // bounds from the point count: at most n / kDenseCell dense cells, and
+    // each slice beyond a cell's first holds kSlicePts of its points
+    v->dense_cap = std::min<int64_t>(nbins, n / (int64_t)kDenseCell);
+    v->work_cap = v->dense_cap + n / (int64_t)kSlicePts;
+    v->multi_cap = std::min<int64_t>(v->dense_cap, n / (int64_t)(kSlicePts + 1));
+    GV_CUDA(v, v->part_work.ensure(sizeof(int4) * (size_t)std::max<int64_t>(v->work_cap, 1), s));
+    GV_CUDA(v, v->cell_cnt.ensure(sizeof(uint32_t) * kCntWords, s));
+    GV_CUDA(v, cudaMemsetAsync(v->cell_cnt.p, 0, sizeof(uint32_t) * kCntWords, s));
 
     v->cell_grid = v->heavy_grid = v->light_grid = 0;
     if (nbins > 0) {
         const int g = grid_for(nbins, 256, 1ll << 31);
         k_cell_list<<<g, 256, 0, s>>>(v->bin_off.as<uint32_t>(), nbins, v->cell_list.as<int32_t>(),
-                                      v->cell_light.as<int32_t>(), v->cell_giant.as<int32_t>(),
-                                      v->cell_cnt.as<uint32_t>());
+                                      v->cell_light.as<int32_t>(), v->cell_part.as<int32_t>(),
+                                      v->part_work.as<int4>(), v->cell_cnt.as<uint32_t>());
         GV_CUDA(v, cudaGetLastError());
         v->cell_grid = v->heavy_grid = v->light_grid = nbins;
         if (nbins > kCellCountReadback) {
-            // many cells: size the gathers' grids by the cells of each class
-            // (one 12-byte read) rather than by all cells
-            uint32_t c3[3] = {0, 0, 0};
-            GV_CUDA(v, cudaMemcpyAsync(c3, v->cell_cnt.p, sizeof(c3), cudaMemcpyDeviceToHost, s));
+            // many cells: size the grids by the cells of each class (one
+            // 32-byte read) rather than by all cells
+            uint32_t cw[kCntWords] = {0};
+            GV_CUDA(v, cudaMemcpyAsync(cw, v->cell_cnt.p, sizeof(cw), cudaMemcpyDeviceToHost, s));
             GV_CUDA(v, cudaStreamSynchronize(s));
-            v->heavy_grid = (int64_t)c3[0] + c3[1];
-            v->light_grid = c3[2];
+            v->heavy_grid = (int64_t)cw[kCntHuge] + cw[kCntHeavy];
+            v->light_grid = cw[kCntLight];
             v->cell_grid = v->heavy_grid + v->light_grid;
+            v->dense_cap = cw[kCntDense];
+            v->work_cap = cw[kCntWork];
+            v->multi_cap = cw[kCntMulti];
         }
     }
     k.valid = true;

@@ -210,22 +210,363 @@ struct SplatArgs {
     int m, m3; // cells per brick edge, per brick
     // huge and heavy cells (order of cell_at), light cells; cell_list ==
     // nullptr: every cell, in cell order
-    const int32_t *cell_list, *cell_light, *cell_giant;
+    const int32_t *cell_list, *cell_light;
     const uint32_t *cell_cnt;
     int64_t ncell;
     int64_t tvox;
+    // dense cells: partial slot per cell (-1: not dense), work items,
+    // partial sums, integer accumulators and arrival counters, and the
+    // capacities of the slots
+    int64_t dense_cap, multi_cap;
+    SplatLimits lim;
+    const int32_t *cell_part;
+    const int4 *part_work;
+    float *part;
+    int32_t *part_acc;
+    uint32_t *part_done;
 };
 
+
+// ---- dense cells: partial sums ------------------------------------------
+//
+// A cell of at least kDenseCell points (a dense cell) is splatted on its
+// own, each point once with its whole stencil, into an extended tile
+// [-H, 8+H)^3 (H = N/2: 12^3 for the cubic B-spline, 10^3 for the tent):
+// the cell's partial sums.  The owner-computes scatter below then leaves a
+// dense cell's points out of every cell's sources and instead adds, to each
+// voxel, the partials of the dense cells among the up to 8 whose extended
+// tile covers it.  Where the cells hold many points this splats each point
+// once instead of from every cell its stencil reaches (about (1 + 3/8)^3 =
+// 2.6 for the cubic B-spline), and its adds all do work.  Whether a cell is
+// dense depends on its own point count only, so a cell's result depends on
+// its neighbourhood alone (a batched cloud gets what a volume of its own
+// gets).
+//
+// k_scatter_part: one CTA per work item, a slice of up to kSlicePts points
+// of a dense cell, accumulates in shared memory with integer atomics in
+// fixed point: integer sums do not depend on the order of the adds, so the
+// partial is the same whatever the order of the points within their bins
+// and whatever the split into slices.  A cell of one slice writes its
+// partial (float) directly; the slices of a larger cell add their integer
+// tiles into the cell's global accumulator, and the CTA that arrives last
+// (an arrival counter; no CTA waits for another) converts the sums to the
+// partial and clears the accumulator and counter for the next call.
+//
+// Fixed point: each contribution x = amount * weight is scaled by 2^s and
+// rounded to an integer, split as rint(x) = hi * 2^L + lo with both parts
+// found by the float "magic number" rounding (t = x*2^-L + 1.5*2^23 holds
+// rint(x*2^-L) in its low mantissa bits; the remainder x - hi*2^L is
+// exact), and added with two 32-bit atomics.  With R the cell's points and
+// max|a| the largest |amount| among them (weights are at most 1), s and L
+// are set per cell and channel so that no sum overflows:
+//   L = min(22, 31 - bits(R+1))      -> |sum lo| <= R * 2^(L-1) < 2^31
+//   max|a| * 2^s < 2^(21+L)          -> |x * 2^-L| < 2^22 (magic range)
+//   R * max|a| * 2^s < 2^(29+L)      -> |sum hi| < 2^29 + R/2
+// (One 64-bit atomic per tap and channel instead measured 1.9x slower.)
+template <int KERNEL>
+struct ExtTile {
+    static constexpr int N = Taps<KERNEL>::N;
+    static constexpr int H = N / 2;
+    static constexpr int E = 8 + N;                 // 12 (cubic) or 10 (tent)
+    static constexpr int RS = E;                    // row stride (words)
+    static constexpr int PS = N == 4 ? E * E + 8 : E * E; // plane stride: 152 puts a warp's taps in distinct banks
+    static constexpr int CS = E * PS;               // channel stride
+    static constexpr int E3 = E * E * E;            // floats per channel in the partial
+    // Position in a cell's partial of extended-tile voxel (ux, uy, uz) in
+    // [0, E)^3.  Per channel the partial holds 27 regions: the cell's 8^3
+    // interior first, then the halo beyond each face, edge and corner d in
+    // {-1,0,1}^3 (z-major order of d), each z-major with extent 8 along the
+    // axes where d is 0 and H where it is not, so that interior rows are
+    // whole 32-byte sectors.  Region d starts, in the plain z-major order of
+    // the regions, at start_z E^2 + s_z start_y E + s_z s_y start_x, with
+    // start and s the region's first extended coordinate and extent along
+    // each axis.
+    __host__ __device__ static constexpr int part_index(int ux, int uy, int uz) {
+        const int dx = ux < H ? -1 : (ux >= 8 + H ? 1 : 0), dy = uy < H ? -1 : (uy >= 8 + H ? 1 : 0),
+                  dz = uz < H ? -1 : (uz >= 8 + H ? 1 : 0);
+        const int sx0 = dx < 0 ? 0 : (dx == 0 ? H : 8 + H), sy0 = dy < 0 ? 0 : (dy == 0 ? H : 8 + H),
+                  sz0 = dz < 0 ? 0 : (dz == 0 ? H : 8 + H);
+        const int ex = dx == 0 ? 8 : H, ey = dy == 0 ? 8 : H, ez = dz == 0 ? 8 : H;
+        const int local = ((uz - sz0) * ey + (uy - sy0)) * ex + (ux - sx0);
+        if ((dx | dy | dz) == 0) return local; // interior
+        const int r = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+        const int start = sz0 * E * E + ez * sy0 * E + ez * ey * sx0;
+        return 512 + start - (r > 13 ? 512 : 0) + local;
+    }
+};
+// The inverse of part_index: the shared tile address of each partial
+// position, so that a partial is written in order (coalesced).
+template <int KERNEL>
+struct PartAddr {
+    uint16_t addr[ExtTile<KERNEL>::E3];
+    constexpr PartAddr() : addr() {
+        using X = ExtTile<KERNEL>;
+        for (int z = 0; z < X::E; z++)
+            for (int y = 0; y < X::E; y++)
+                for (int x = 0; x < X::E; x++) addr[X::part_index(x, y, z)] = (uint16_t)(z * X::PS + y * X::RS + x);
+    }
+};
+template <int KERNEL>
+__device__ constexpr PartAddr<KERNEL> kPartAddr{};
+
+// The partials that cover interior voxel v (x | y << 3 | z << 6) of a cell:
+// entry m of row v is the partial position (11 bits) and the neighbour
+// direction d (5 bits, z-major in {-1,0,1}^3) of source m, or 0xFFFF when
+// source m does not cover v.  Source m steps across the faces named by its
+// bits (x, y, z) toward the near face of v when v lies within H of one.
+template <int KERNEL>
+struct alignas(16) MergeMap {
+    uint16_t src[512][8];
+    constexpr MergeMap() : src() {
+        using X = ExtTile<KERNEL>;
+        for (int v = 0; v < 512; v++) {
+            const int vx = v & 7, vy = (v >> 3) & 7, vz = v >> 6;
+            const int ex = vx < X::H ? -1 : (vx >= 8 - X::H ? 1 : 0);
+            const int ey = vy < X::H ? -1 : (vy >= 8 - X::H ? 1 : 0);
+            const int ez = vz < X::H ? -1 : (vz >= 8 - X::H ? 1 : 0);
+            for (int m = 0; m < 8; m++) {
+                const bool used = (!(m & 1) || ex) && (!(m & 2) || ey) && (!(m & 4) || ez);
+                const int dx = (m & 1) ? ex : 0, dy = (m & 2) ? ey : 0, dz = (m & 4) ? ez : 0;
+                const int d = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+                src[v][m] = used ? (uint16_t)(X::part_index(vx - 8 * dx + X::H, vy - 8 * dy + X::H,
+                                                            vz - 8 * dz + X::H) | (d << 11))
+                                 : (uint16_t)0xFFFF;
+            }
+        }
+    }
+};
+template <int KERNEL>
+__device__ constexpr MergeMap<KERNEL> kMergeMap{};
+static_assert(ExtTile<GVDB2_KERNEL_CUBIC2>::E3 <= 2048 && ExtTile<GVDB2_KERNEL_TENT1>::E3 <= 2048,
+              "partial positions fit 11 bits");
+
+constexpr int kPartThreads = 256;
+constexpr int kPartChunk = 128; // points staged per pass, one per thread of the first 128
+static_assert(kSlicePts % kPartChunk == 0, "slices are whole chunks");
+
+template <int KERNEL, int NCH>
+constexpr size_t part_smem_bytes() {
+    return sizeof(int32_t) * 2 * NCH * ExtTile<KERNEL>::CS +
+           sizeof(float) * (3 * Taps<KERNEL>::N + NCH) * kPartChunk + sizeof(int32_t) * kPartChunk;
+}
+
+// The fixed-point scale of R points whose largest |amount| is am, per the
+// bounds above: returns 2^s (0 when there is nothing to add), sets `inv` =
+// 2^-s and `lvl` = L.
+__device__ __forceinline__ float part_scale(uint32_t R, float am, double &inv, int &lvl) {
+    int e1 = 0, e2 = 0;
+    frexpf(am, &e1);            // am < 2^e1
+    frexpf((float)R * am, &e2); // R*am < 2^e2
+    const int L = min(22, 31 - (32 - __clz((int)R + 1)));
+    lvl = L;
+    const int s = min(21 + L - e1, 29 + L - e2);
+    const bool on = am > 0.0f && R > 0;
+    inv = on ? ldexp(1.0, -s) : 0.0;
+    return on ? ldexpf(1.0f, s) : 0.0f;
+}
+
+// Adds the fixed-point value of x (already scaled by 2^s) at tile index idx
+// of one channel's accumulators: hi at idx, lo at CS + idx.
+template <int CS>
+__device__ __forceinline__ void part_add(int32_t *acc, int idx, float x, float inv2L, float two2L) {
+    const float M = 12582912.0f; // 1.5 * 2^23
+    const float t = fmaf(x, inv2L, M);
+    const int hi = __float_as_int(t) - 0x4B400000;
+    const float r = fmaf(t - M, -two2L, x);
+    const int lo = __float_as_int(r + M) - 0x4B400000;
+    atomicAdd(acc + idx, hi);
+    atomicAdd(acc + CS + idx, lo);
+}
+
+// One work item per CTA: slice item.y of item.z of dense cell item.x
+// (item.w: the cell's accumulator slot when item.z > 1).  The partial goes
+// to part + cell_part[cell] * NCH * E3.
+template <int KERNEL, int NCH>
+__global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
+    using T = Taps<KERNEL>;
+    using X = ExtTile<KERNEL>;
+    constexpr int N = T::N;
+    constexpr int AS = 2 * X::CS; // accumulator words per channel (hi, lo)
+    extern __shared__ __align__(16) unsigned char part_smem[];
+    int32_t *acc = reinterpret_cast<int32_t *>(part_smem);
+    float(*pw)[kPartChunk] = reinterpret_cast<float(*)[kPartChunk]>(acc + NCH * AS);
+    float(*pa)[kPartChunk] = pw + 3 * N;
+    int32_t *pb = reinterpret_cast<int32_t *>(pa + NCH);
+    __shared__ double inv_s[NCH];
+    __shared__ int32_t amax_bits[NCH]; // largest |amount| of the cell's points, as float bits
+    __shared__ int last;
+    if (blockIdx.x >= S.cell_cnt[kCntWork]) return;
+    const int4 item = S.part_work[blockIdx.x];
+    const int64_t cell = item.x;
+    const int nslice = item.z;
+    // every check below is the same for the whole CTA
+    if (!in_range(S.lim, cell, S.ncell)) return;
+    const int32_t pslot = S.cell_part[cell];
+    if (!in_range(S.lim, pslot, S.dense_cap) || (nslice > 1 && !in_range(S.lim, item.w, S.multi_cap))) return;
+    const uint32_t beg = S.bin_off[cell], R = S.bin_off[cell + 1] - beg;
+    if (!in_range(S.lim, (int64_t)beg + R - 1, S.lim.nentry)) return;
+    const uint32_t s0 = (uint32_t)item.y * kSlicePts, s1 = min(R, s0 + kSlicePts);
+    int64_t slot;
+    int cx, cy, cz;
+    cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
+    const int32_t leaf = S.slot_leaf[slot];
+    if (!in_range(S.lim, leaf, S.lim.npool)) return;
+    static_assert((NCH * AS * sizeof(int32_t)) % 16 == 0, "16-byte zeroing");
+    for (int i = threadIdx.x; i < (int)(NCH * AS * sizeof(int32_t) / 16); i += kPartThreads)
+        reinterpret_cast<int4 *>(acc)[i] = make_int4(0, 0, 0, 0);
+    if (threadIdx.x < NCH) amax_bits[threadIdx.x] = 0;
+    const Node &nd = S.leaves[leaf];
+    const int ox = nd.mPos[0] + kCell * cx - X::H, oy = nd.mPos[1] + kCell * cy - X::H,
+              oz = nd.mPos[2] + kCell * cz - X::H;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // the largest |amount| per channel over all the cell's points sets the
+    // scale, the same in every slice of the cell
+    float mx[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) mx[c] = 0.0f;
+    for (uint32_t j = threadIdx.x; j < R; j += kPartThreads) {
+        const float4 a = S.bin_amt[beg + j];
+        const float a4[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int c = 0; c < NCH; c++) mx[c] = fmaxf(mx[c], fabsf(a4[c]));
+    }
+    __syncthreads(); // amax_bits cleared
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        float x = mx[c];
+        for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, o));
+        if (lane == 0 && x > 0.0f) atomicMax(&amax_bits[c], __float_as_int(x));
+    }
+    __syncthreads();
+    float scale[NCH];
+    int L = 0;
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        double inv;
+        scale[c] = part_scale(R, __int_as_float(amax_bits[c]), inv, L);
+        if (threadIdx.x == 0) inv_s[c] = inv;
+    }
+    const float inv2L = ldexpf(1.0f, -L), two2L = ldexpf(1.0f, L);
+    for (uint32_t base = s0; base < s1; base += kPartChunk) {
+        const int cnt = (int)min((uint32_t)kPartChunk, s1 - base);
+        if (base > s0) __syncthreads(); // previous chunk consumed
+        if ((int)threadIdx.x < cnt) { // stage point base + t as record t
+            const uint32_t j = beg + base + threadIdx.x;
+            const float4 q = S.bin_pos[j]; // translated position, cloud index bits
+            const int32_t cloud = __float_as_int(q.w);
+            int3 o = make_int3(0, 0, 0);
+            if (cloud >= 0 && in_range(S.lim, cloud, S.lim.ncloud))
+                o = make_int3(S.pos.origin[3 * cloud], S.pos.origin[3 * cloud + 1], S.pos.origin[3 * cloud + 2]);
+            float wx[N], wy[N], wz[N];
+            const int fx = T::eval(q.x, wx) + o.x - ox;
+            const int fy = T::eval(q.y, wy) + o.y - oy;
+            const int fz = T::eval(q.z, wz) + o.z - oz;
+            // a point binned to the cell has its first taps in [0, 8] of the
+            // extended tile; anything else is dropped, never written outside it
+            const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
+            const int r = threadIdx.x;
+            pb[r] = ok ? fz * X::PS + fy * X::RS + fx : 0; // tile address of the point's first tap
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                pw[k][r] = wx[k];
+                pw[N + k][r] = wy[k];
+                pw[2 * N + k][r] = wz[k];
+            }
+            const float4 a = S.bin_amt[j];
+            const float a4[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+            for (int c = 0; c < NCH; c++) pa[c][r] = ok ? a4[c] * scale[c] : 0.0f;
+        }
+        __syncthreads();
+        if constexpr (N == 4) {
+            // one point per warp step: lane = (tx, ty, z pair), two taps a lane
+            const int tx = lane & 3, ty = (lane >> 2) & 3, tz0 = (lane >> 4) * 2;
+            const int loff = tz0 * X::PS + ty * X::RS + tx;
+            for (int j = warp; j < cnt; j += kPartThreads / 32) {
+                const int a0 = pb[j] + loff;
+                const float wxy = pw[tx][j] * pw[N + ty][j];
+                const float w0 = wxy * pw[2 * N + tz0][j], w1 = wxy * pw[2 * N + tz0 + 1][j];
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    const float am = pa[c][j];
+                    part_add<X::CS>(acc + c * AS, a0, am * w0, inv2L, two2L);
+                    part_add<X::CS>(acc + c * AS, a0 + X::PS, am * w1, inv2L, two2L);
+                }
+            }
+        } else {
+            // four points per warp step, one tap a lane
+            const int sub = lane >> 3, tx = lane & 1, ty = (lane >> 1) & 1, tz = (lane >> 2) & 1;
+            const int loff = tz * X::PS + ty * X::RS + tx;
+            for (int j0 = warp * 4; j0 < cnt; j0 += kPartThreads / 8) {
+                const int j = j0 + sub;
+                if (j >= cnt) continue;
+                const int a = pb[j] + loff;
+                const float w = pw[tx][j] * pw[N + ty][j] * pw[2 * N + tz][j];
+#pragma unroll
+                for (int c = 0; c < NCH; c++) part_add<X::CS>(acc + c * AS, a, pa[c][j] * w, inv2L, two2L);
+            }
+        }
+    }
+    __syncthreads();
+    // partial position i of channel c: thread t takes i = t, t + 256, ...
+    // (coalesced), each looked up in its tile voxel
+    float *dst = S.part + (int64_t)pslot * NCH * X::E3;
+    static_assert(kPartThreads < X::E3, "one channel step per iteration");
+    auto write = [&](int i, int c, int32_t hi, int32_t lo) {
+        // |sum| < 2^53: exact in double; the power-of-two scalings are exact
+        const long long sum = ((long long)hi << L) + (long long)lo;
+        dst[i] = (float)((double)sum * inv_s[c]);
+    };
+    if (nslice == 1) {
+        int c = 0, i0 = threadIdx.x;
+        for (int i = threadIdx.x; i < NCH * X::E3; i += kPartThreads) {
+            const int k = c * AS + kPartAddr<KERNEL>.addr[i0];
+            write(i, c, acc[k], acc[k + X::CS]);
+            if ((i0 += kPartThreads) >= X::E3) i0 -= X::E3, c++;
+        }
+        return;
+    }
+    // a cell of several slices: this slice's integer sums into the cell's
+    // accumulator (per channel hi[E3], lo[E3] in partial order)
+    int32_t *g = S.part_acc + (int64_t)item.w * 2 * NCH * X::E3;
+    {
+        int c = 0, i0 = threadIdx.x;
+        for (int i = threadIdx.x; i < NCH * X::E3; i += kPartThreads) {
+            const int k = c * AS + kPartAddr<KERNEL>.addr[i0];
+            int32_t *gc = g + c * 2 * X::E3 + i0;
+            if (acc[k]) atomicAdd(gc, acc[k]);
+            if (acc[k + X::CS]) atomicAdd(gc + X::E3, acc[k + X::CS]);
+            if ((i0 += kPartThreads) >= X::E3) i0 -= X::E3, c++;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(S.part_done + item.w, 1u) == (uint32_t)(nslice - 1);
+    __syncthreads();
+    if (!last) return;
+    // the last slice: every other slice's adds are visible; read the sums
+    // and clear the accumulator (atomic exchanges) and the counter
+    __threadfence();
+    int c = 0, i0 = threadIdx.x;
+    for (int i = threadIdx.x; i < NCH * X::E3; i += kPartThreads) {
+        int32_t *gc = g + c * 2 * X::E3 + i0;
+        write(i, c, atomicExch(gc, 0), atomicExch(gc + X::E3, 0));
+        if ((i0 += kPartThreads) >= X::E3) i0 -= X::E3, c++;
+    }
+    if (threadIdx.x == 0) S.part_done[item.w] = 0;
+}
 
 // ---- owner-computes scatter --------------------------------------------
 //
 // One warp per cell (an 8^3 block of a brick; the brick itself for 8^3
 // bricks) computes the cell's interior voxels from every point whose stencil
-// reaches them and writes each voxel once: no atomics, no partial sums in
-// memory, no zero-fill pass.  Its sources are the cell's own points and,
-// from each of the 26 neighbour cells, the regions of that cell's bin whose
-// stencils cross the shared face, edge or corner (k_bin_count bins points by
-// cell and region), so every source is a point the cell needs.
+// reaches them and writes each voxel once: no atomics, no zero-fill pass.
+// Its sources are the cell's own points and, from each of the 26 neighbour
+// cells, the regions of that cell's bin whose stencils cross the shared
+// face, edge or corner (k_bin_count bins points by cell and region), so
+// every source is a point the cell needs -- except the points of dense
+// cells (this cell's included), whose partial sums the warp adds instead
+// when it writes its voxels.
 //
 // The warp turns its sources into records in shared memory, a chunk of at
 // most kScCap at a time: per point the x weights on the cell's 8 voxel
@@ -244,7 +585,9 @@ struct SplatArgs {
 // accumulator plane fixed at compile time: paired register FMAs.
 //
 // The adds happen in the order of the sources (the bins) and of the stable
-// sort, so with deterministic binning the result is bit-reproducible.
+// sort, then the partials in a fixed order, so with deterministic binning
+// the result is bit-reproducible (and always so where every cell around is
+// dense).
 #ifndef GVDB2_SC_CAP
 #define GVDB2_SC_CAP 128
 #endif
@@ -268,8 +611,9 @@ struct ScChunk {
     uint16_t rank[kScCap];
     uint16_t order[kScCap];
     uint16_t off[kScBins + 1];
-    uint2 run[64]; // the cell's sources: runs [x, y) of perm (at most 1 + 2 + 6 + 18 + 4 + 12 + 12 + 8 = 63)
+    uint2 run[64]; // the cell's sources: runs [x, y) of perm (at most 1 + 2 + 10 + 50 = 63)
     uint32_t run_first[64]; // sources before run k (the runs read as one sequence)
+    int32_t part[28]; // per neighbour direction d: the partial slot of a dense cell there, else -1
 };
 
 // Sort the chunk's `fill` records by key (stable) into C.order.
@@ -437,61 +781,52 @@ __device__ __forceinline__ void sc_accumulate_cp(const ScChunk &C, float2 (&acc)
 // Channel pairs for 2 to 4 channels, x pairs for one channel.
 template <int NCH> struct ScLayout { static constexpr bool kChPairs = GVDB2_SC_CHPAIR && NCH > 1; };
 
-// Blocks [0, single_blocks) take kScWarps cells each, a warp per cell;
-// the rest take one giant cell each (more than kGiantCell points of its
-// own), whose sources the CTA's warps share in turn, 32 at a time; their
-// accumulators are summed in a fixed order at the end.
+// kScWarps cells per CTA, a warp per cell.
 template <int KERNEL, int NCH>
-__global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_cells(SplatArgs S, int64_t single_blocks) {
+__global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_cells(SplatArgs S) {
     using T = Taps<KERNEL>;
+    using X = ExtTile<KERNEL>;
     constexpr int N = T::N;
-    static_assert(kScWarps == 4, "a giant cell's warps reduce one accumulator plane each");
     extern __shared__ __align__(16) unsigned char sc_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     ScChunk &C = reinterpret_cast<ScChunk *>(sc_smem)[warp];
-    int64_t cell;
-    int W; // warps sharing the cell
-    if ((int64_t)blockIdx.x < single_blocks) {
-        cell = (int64_t)blockIdx.x * kScWarps + warp;
-        if (cell >= S.ncell) return;
-        if (S.bin_off[cell + 1] - S.bin_off[cell] > kGiantCell) return; // a CTA of its own
-        W = 1;
-    } else {
-        const int64_t gi = (int64_t)blockIdx.x - single_blocks;
-        if (gi >= (int64_t)S.cell_cnt[3]) return; // every warp of the CTA
-        cell = S.cell_giant[gi];
-        W = kScWarps;
-    }
-    const int wturn = W == 1 ? 0 : warp;
+    const int64_t cell = (int64_t)blockIdx.x * kScWarps + warp;
+    if (cell >= S.ncell) return;
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
-    const Node &nd = S.leaves[S.slot_leaf[slot]];
+    const int32_t leaf = S.slot_leaf[slot];
+    if (!in_range(S.lim, leaf, S.lim.npool)) return; // the same for the whole warp
+    const Node &nd = S.leaves[leaf];
     const int ox = nd.mPos[0] + kCell * cx, oy = nd.mPos[1] + kCell * cy, oz = nd.mPos[2] + kCell * cz;
     // The sources, as runs of perm in a fixed order: lane d < 27 lists those of
     // the neighbour cell in direction d = (dz+1)*9 + (dy+1)*3 + (dx+1): its
     // regions whose stencils reach this cell -- per axis, across the lower
     // face its upper band (2), across the upper face its lower band (0),
     // along the axis all three -- merged into as few runs as the region
-    // order allows.
+    // order allows; a dense neighbour gives its partial slot instead.
     int nrun = 0;
     uint2 runs[9];
+    int32_t pslot = -1;
     if (lane < 27) {
         const int dx = lane % 3 - 1, dy = lane / 3 % 3 - 1, dz = lane / 9 - 1;
         const int ncx = cx + dx, ncy = cy + dy, ncz = cz + dz;
         const int bx = ncx < 0 ? -1 : (ncx >= S.m ? 1 : 0), by = ncy < 0 ? -1 : (ncy >= S.m ? 1 : 0),
                   bz = ncz < 0 ? -1 : (ncz >= S.m ? 1 : 0);
-        const int32_t ns = (bx | by | bz) == 0 ? (int32_t)slot
-                                               : S.nbr27[slot * 27 + (bz + 1) * 9 + (by + 1) * 3 + (bx + 1)];
-        if (ns >= 0) {
-            const int64_t nc =
-                (int64_t)ns * S.m3 + ((ncz - bz * S.m) * S.m + (ncy - by * S.m)) * S.m + (ncx - bx * S.m);
+        int32_t ns = (bx | by | bz) == 0 ? (int32_t)slot
+                                         : S.nbr27[slot * 27 + (bz + 1) * 9 + (by + 1) * 3 + (bx + 1)];
+        if (ns >= 0 && !in_range(S.lim, ns, S.lim.nslot)) ns = -1;
+        int64_t nc = ns < 0 ? -1
+                            : (int64_t)ns * S.m3 + ((ncz - bz * S.m) * S.m + (ncy - by * S.m)) * S.m + (ncx - bx * S.m);
+        if (nc >= 0) pslot = S.cell_part[nc];
+        if (pslot >= 0 && !in_range(S.lim, pslot, S.dense_cap)) pslot = -1, nc = -1;
+        if (nc >= 0 && pslot < 0) {
             const uint32_t *ro = S.reg_off + nc * kRegions;
             const int rx0 = dx < 0 ? 2 : 0, ry0 = dy < 0 ? 2 : 0, ry1 = dy > 0 ? 0 : 2;
             const int rz0 = dz < 0 ? 2 : 0, rz1 = dz > 0 ? 0 : 2;
             auto add = [&](int r0, int r1) { // regions [r0, r1)
                 const uint2 u = make_uint2(ro[r0], ro[r1]);
-                if (u.y > u.x) runs[nrun++] = u;
+                if (u.y > u.x && in_range(S.lim, (int64_t)u.y - 1, S.lim.nentry)) runs[nrun++] = u;
             };
             if (dx == 0 && dy == 0) {
                 if (dz == 0) add(0, kRegions);
@@ -529,6 +864,8 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
             C.run_first[first + k] = before;
             before += runs[k].y - runs[k].x;
         }
+    if (lane < 27) C.part[lane] = pslot;
+    const bool any_part = __any_sync(0xffffffffu, pslot >= 0);
     __syncwarp();
 
     const int y = lane & 7, q = (lane >> 3) & 1, h = lane >> 4;
@@ -581,7 +918,8 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
             const float4 q = S.bin_pos[j];
             d.pt = make_float3(q.x, q.y, q.z);
             const int32_t cloud = __float_as_int(q.w);
-            if (cloud >= 0) d.o = make_int3(S.pos.origin[3 * cloud], S.pos.origin[3 * cloud + 1], S.pos.origin[3 * cloud + 2]);
+            if (cloud >= 0 && in_range(S.lim, cloud, S.lim.ncloud))
+                d.o = make_int3(S.pos.origin[3 * cloud], S.pos.origin[3 * cloud + 1], S.pos.origin[3 * cloud + 2]);
             const float4 am = S.bin_amt[j];
             d.a4[0] = am.x, d.a4[1] = am.y, d.a4[2] = am.z, d.a4[3] = am.w;
             d.ok = true;
@@ -632,21 +970,19 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
             fill = 0;
         }
     };
-    // the steps of 32 sources this warp takes (the warps of a giant cell take turns)
-    const uint32_t stride = 32u * W;
-    uint32_t vb = 32u * wturn;
+    // the sources, 32 a step
     if (GVDB2_SC_PREFETCH) {
         // the next step's reads are in flight while this step's records are
         // built and a full chunk is added
-        Src nxt = fetch(vb);
-        for (; vb < total_src; vb += stride) {
+        Src nxt = fetch(0);
+        for (uint32_t vb = 0; vb < total_src; vb += 32) {
             const Src cur = nxt;
-            if (vb + stride < total_src) nxt = fetch(vb + stride);
+            if (vb + 32 < total_src) nxt = fetch(vb + 32);
             flush_if_full();
             build(cur);
         }
     } else {
-        for (; vb < total_src; vb += stride) {
+        for (uint32_t vb = 0; vb < total_src; vb += 32) {
             flush_if_full();
             build(fetch(vb));
         }
@@ -666,50 +1002,50 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
                     acc[z][xp][c] = (c & 1) ? make_float2(a0.y, a1.y) : make_float2(a0.x, a1.x);
                 }
     }
-    // each lane writes its 4 x 4 voxels of every channel once
-    const int a = S.apron, tl = S.tile;
-    const int64_t base = slot * S.tvox + (int64_t)(kCell * cx + 4 * q + a);
-    auto store = [&](int zz, int c, float2 v01, float2 v23) {
-        float *dst = S.chan[c] + base + ((int64_t)(kCell * cz + 4 * h + zz + a) * tl + (kCell * cy + y + a)) * tl;
-        dst[0] = v01.x;
-        dst[1] = v01.y;
-        dst[2] = v23.x;
-        dst[3] = v23.y;
-    };
-    if (W == 1) {
+    // the partials of the dense cells that cover the lane's voxels, summed
+    // in the order of their sources (kMergeMap), after the owner's sum
+    if (any_part) {
 #pragma unroll
         for (int zz = 0; zz < 4; zz++)
 #pragma unroll
-            for (int c = 0; c < NCH; c++) store(zz, c, acc[zz][0][c], acc[zz][1][c]);
-        return;
+            for (int xi = 0; xi < 4; xi++) {
+                const int vv = (4 * q + xi) | (y << 3) | ((4 * h + zz) << 6);
+                const uint4 row = *reinterpret_cast<const uint4 *>(kMergeMap<KERNEL>.src[vv]);
+                const uint32_t wr[4] = {row.x, row.y, row.z, row.w};
+                float add[NCH];
+#pragma unroll
+                for (int c = 0; c < NCH; c++) add[c] = 0.0f;
+#pragma unroll
+                for (int m = 0; m < 8; m++) {
+                    const uint32_t ent = (wr[m >> 1] >> (16 * (m & 1))) & 0xFFFFu;
+                    if (ent == 0xFFFFu) continue;
+                    const int32_t e = C.part[ent >> 11];
+                    if (e < 0) continue;
+                    const float *src = S.part + (int64_t)e * NCH * X::E3 + (ent & 2047u);
+#pragma unroll
+                    for (int c = 0; c < NCH; c++) add[c] += __ldcs(src + c * X::E3);
+                }
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    float2 &v2 = acc[zz][xi >> 1][c];
+                    if (xi & 1) v2.y += add[c];
+                    else v2.x += add[c];
+                }
+            }
     }
-    // giant cell: the warps' accumulators through shared memory, summed in
-    // warp order; warp w sums and writes accumulator plane w of every lane
-    __syncthreads(); // every warp is done with its chunks
-    float2 *red = reinterpret_cast<float2 *>(sc_smem);
-    auto at = [&](int w, int zz, int xp, int c) { return (((w * 4 + zz) * 2 + xp) * NCH + c) * 32 + lane; };
+    // each lane writes its 4 x 4 voxels of every channel once
+    const int a = S.apron, tl = S.tile;
+    const int64_t base = slot * S.tvox + (int64_t)(kCell * cx + 4 * q + a);
 #pragma unroll
     for (int zz = 0; zz < 4; zz++)
 #pragma unroll
-        for (int xp = 0; xp < 2; xp++)
-#pragma unroll
-            for (int c = 0; c < NCH; c++) red[at(warp, zz, xp, c)] = acc[zz][xp][c];
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < NCH; c++) {
-        float2 v[2];
-#pragma unroll
-        for (int xp = 0; xp < 2; xp++) {
-            v[xp] = red[at(0, warp, xp, c)];
-#pragma unroll
-            for (int w = 1; w < kScWarps; w++) {
-                const float2 u = red[at(w, warp, xp, c)];
-                v[xp].x += u.x;
-                v[xp].y += u.y;
-            }
+        for (int c = 0; c < NCH; c++) {
+            float *dst = S.chan[c] + base + ((int64_t)(kCell * cz + 4 * h + zz + a) * tl + (kCell * cy + y + a)) * tl;
+            dst[0] = acc[zz][0][c].x;
+            dst[1] = acc[zz][0][c].y;
+            dst[2] = acc[zz][1][c].x;
+            dst[3] = acc[zz][1][c].y;
         }
-        store(warp, c, v[0], v[1]);
-    }
 }
 
 // ---------------------------------------------------------------------
@@ -745,6 +1081,7 @@ struct GatherArgs {
     int64_t ncell;
     int64_t tvox;
     const float4 *bin_pos; // per entry of perm: translated position, cloud bits (nullptr: read via perm)
+    SplatLimits lim;
 };
 
 // The translated position and cloud origin of point pidx, entry j of the
@@ -755,8 +1092,9 @@ __device__ __forceinline__ void gather_point_at(const GatherArgs &G, int32_t pid
         const float4 q = G.bin_pos[j];
         w = make_float3(q.x, q.y, q.z);
         const int32_t cloud = __float_as_int(q.w);
-        o = cloud >= 0 ? make_int3(G.pos.origin[3 * cloud], G.pos.origin[3 * cloud + 1], G.pos.origin[3 * cloud + 2])
-                       : make_int3(0, 0, 0);
+        o = cloud >= 0 && in_range(G.lim, cloud, G.lim.ncloud)
+                ? make_int3(G.pos.origin[3 * cloud], G.pos.origin[3 * cloud + 1], G.pos.origin[3 * cloud + 2])
+                : make_int3(0, 0, 0);
     } else {
         const float3 p = load_f3(G.pos, pidx);
         w = make_float3(p.x + G.trans.x, p.y + G.trans.y, p.z + G.trans.z);
@@ -772,6 +1110,7 @@ __device__ __forceinline__ void gather_point(const GatherArgs &G, int32_t pidx, 
                                              const Fetch &fetch) {
     using T = Taps<KERNEL>;
     constexpr int N = T::N;
+    if (!in_range(G.lim, pidx, G.lim.nentry)) return;
     float3 p;
     int3 o;
     gather_point_at(G, pidx, j, p, o);
@@ -922,8 +1261,14 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, G.m, G.m3, slot, cx, cy, cz);
+    const int32_t leaf = G.slot_leaf[slot];
+    // the same for the whole CTA
+    if (!in_range(G.lim, (int64_t)end - 1, G.lim.nentry) || !in_range(G.lim, leaf, G.lim.npool)) return;
     const int a = G.apron, tl = G.tile;
-    if (threadIdx.x < 27) nbs[threadIdx.x] = G.nbr27[slot * 27 + threadIdx.x];
+    if (threadIdx.x < 27) {
+        const int32_t nb = G.nbr27[slot * 27 + threadIdx.x];
+        nbs[threadIdx.x] = nb >= 0 && in_range(G.lim, nb, G.lim.nslot) ? nb : -1;
+    }
     __syncthreads();
     // halo tile from the interiors of this brick and its neighbours; all of a
     // thread's loads are issued before its stores
@@ -947,7 +1292,7 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
         const int t = (int)threadIdx.x + k * kGatherThreads;
         if (t < ht3) gvec_put<NCH>(tile[t], val[k]);
     }
-    const Node &nd = G.leaves[G.slot_leaf[slot]];
+    const Node &nd = G.leaves[leaf];
     const int ox = nd.mPos[0] + kCell * cx - H, oy = nd.mPos[1] + kCell * cy - H, oz = nd.mPos[2] + kCell * cz - H;
     auto fetch = [&](int x, int y, int z, float g[NCH]) { gvec_get<NCH>(tile[(z * ht + y) * ht + x], g); };
     for (uint32_t cb = beg; cb < end; cb += kGatherChunk) {
@@ -1015,12 +1360,15 @@ __device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t 
     const int lane = threadIdx.x & 31;
     if (w >= (int64_t)G.cell_cnt[2]) return;
     const int64_t cell = G.cell_light[w];
+    if (!in_range(G.lim, cell, G.ncell)) return;
     const uint32_t beg = G.bin_off[cell], cnt = G.bin_off[cell + 1] - beg;
-    if ((uint32_t)lane >= cnt) return;
+    if ((uint32_t)lane >= cnt || !in_range(G.lim, (int64_t)beg + lane, G.lim.nentry)) return;
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, G.m, G.m3, slot, cx, cy, cz);
-    const Node &nd = G.leaves[G.slot_leaf[slot]];
+    const int32_t leaf = G.slot_leaf[slot];
+    if (!in_range(G.lim, leaf, G.lim.npool)) return;
+    const Node &nd = G.leaves[leaf];
     const int fx0 = kCell * cx - H, fy0 = kCell * cy - H, fz0 = kCell * cz - H; // frame origin in the brick
     const int res = G.res0, a = G.apron, tl = G.tile;
     auto fetch = [&](int x, int y, int z, float g[NCH]) {
@@ -1028,7 +1376,8 @@ __device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t 
         const int sx = lx < 0 ? -1 : (lx >= res ? 1 : 0), sy = ly < 0 ? -1 : (ly >= res ? 1 : 0),
                   sz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
         const int d = (sz + 1) * 9 + (sy + 1) * 3 + (sx + 1);
-        const int64_t ns = d == 13 ? slot : (int64_t)G.nbr27[slot * 27 + d];
+        int64_t ns = d == 13 ? slot : (int64_t)G.nbr27[slot * 27 + d];
+        if (ns >= 0 && !in_range(G.lim, ns, G.lim.nslot)) ns = -1;
         const int64_t off = ns * G.tvox + ((int64_t)(lz - sz * res + a) * tl + (ly - sy * res + a)) * tl +
                             (lx - sx * res + a);
 #pragma unroll
@@ -1086,6 +1435,12 @@ void fill_topology(Volume *v, Args &S) {
     S.apron = v->apron;
     S.tile = v->tile_res();
     S.tvox = v->tile_vox();
+    S.lim.flag = splat_guard_word(v);
+    S.lim.nslot = v->atlas_last;
+    S.lim.npool = v->pool_cnt[0];
+    S.lim.nentry = v->bin_key.n;
+    S.lim.ncloud = v->batch_clouds;
+    v->splat_guard_pending = S.lim.flag != nullptr;
 }
 
 template <class K>
@@ -1106,6 +1461,10 @@ __global__ void k_pack_amounts(SplatArgs S) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= (int64_t)S.reg_off[S.ncell * kRegions]) return;
     const int32_t p = S.perm[j];
+    if (!in_range(S.lim, p, S.lim.nentry)) {
+        S.bin_amt[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
     const float wt = S.has_weight ? load_f1(S.weight, p) : S.wconst;
     float a4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
@@ -1113,21 +1472,44 @@ __global__ void k_pack_amounts(SplatArgs S) {
     S.bin_amt[j] = make_float4(a4[0], a4[1], a4[2], a4[3]);
 }
 
-// Owner-computes scatter of up to 4 channels (one group): a warp per cell,
-// every cell of the active bricks (cells no stencil reaches get zeros).
+// A buffer of `bytes` that starts out zero: zeroed whenever it is
+// (re)allocated; its users leave it zero again.
+gvdb2_status ensure_zeroed(Volume *v, DevBuf &b, size_t bytes) {
+    void *old = b.p;
+    GV_CUDA(v, b.ensure(bytes, v->stream));
+    if (b.p != old) GV_CUDA(v, cudaMemsetAsync(b.p, 0, b.bytes, v->stream));
+    return GVDB2_OK;
+}
+
+// Scatter of up to 4 channels (one group): the channel amounts in bin order,
+// the dense cells' partial sums (a CTA per slice), then the owner-computes
+// pass over every cell of the active bricks (cells no stencil reaches get
+// zeros).
 template <int KERNEL, int NCH>
 gvdb2_status scatter_group(Volume *v, const SplatArgs &S0) {
+    using X = ExtTile<KERNEL>;
     constexpr size_t smem = sizeof(ScChunk) * kScWarps;
+    constexpr size_t psmem = part_smem_bytes<KERNEL, NCH>();
     auto k = k_scatter_cells<KERNEL, NCH>;
+    auto kp = k_scatter_part<KERNEL, NCH>;
     GV_TRY(launch_smem(v, k, smem, "scatter"));
+    GV_TRY(launch_smem(v, kp, psmem, "scatter"));
     GV_CUDA(v, v->bin_amt.ensure(sizeof(float4) * (size_t)std::max<int64_t>(v->bin_key.n, 1), v->stream));
+    GV_CUDA(v, v->part_buf.ensure(sizeof(float) * (size_t)std::max<int64_t>(v->dense_cap * NCH * X::E3, 1), v->stream));
+    GV_TRY(ensure_zeroed(v, v->part_acc, sizeof(int32_t) * (size_t)std::max<int64_t>(v->multi_cap * 2 * NCH * X::E3, 1)));
+    GV_TRY(ensure_zeroed(v, v->part_done, sizeof(uint32_t) * (size_t)std::max<int64_t>(v->multi_cap, 1)));
     SplatArgs S = S0;
     S.bin_amt = v->bin_amt.as<float4>();
-    const int64_t single = (S.ncell + kScWarps - 1) / kScWarps;
-    const int64_t blocks = single + v->giant_grid; // giant cells: at most n / kGiantCell of them
+    S.part = v->part_buf.as<float>();
+    S.part_acc = v->part_acc.as<int32_t>();
+    S.part_done = v->part_done.as<uint32_t>();
+    S.dense_cap = v->dense_cap;
+    S.multi_cap = v->multi_cap;
     if (v->bin_key.n > 0)
         k_pack_amounts<NCH><<<grid_for(v->bin_key.n, 256, 1ll << 31), 256, 0, v->stream>>>(S);
-    if (blocks > 0) k<<<(unsigned)blocks, 32 * kScWarps, smem, v->stream>>>(S, single);
+    if (v->work_cap > 0) kp<<<(unsigned)v->work_cap, kPartThreads, psmem, v->stream>>>(S);
+    const int64_t blocks = (S.ncell + kScWarps - 1) / kScWarps;
+    if (blocks > 0) k<<<(unsigned)blocks, 32 * kScWarps, smem, v->stream>>>(S);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
@@ -1314,7 +1696,8 @@ gvdb2_status scatter_kernel(Volume *v, int kernel, int n, const float trans[3], 
     for (int c = 0; c < kMaxSplatChan; c++) S.chan[c] = c < nch ? v->atlas[chans[c]].as<float>() : nullptr;
     fill_topology(v, S);
     S.reg_off = v->reg_off.as<uint32_t>();
-    S.cell_giant = v->cell_giant.as<int32_t>();
+    S.cell_part = v->cell_part.as<int32_t>();
+    S.part_work = v->part_work.as<int4>();
     S.bin_pos = v->bin_pos.as<float4>();
     return run_scatter(v, kernel, S);
 }
@@ -1355,6 +1738,7 @@ gvdb2_status gather_kernel_prebinned(Volume *v, int kernel, int n, const float t
     fill_topology(v, G);
     G.bin_off = bin_off;
     G.perm = perm;
+    G.lim.nentry = n;
     G.cell_list = nullptr; // bins supplied by the caller: every cell, in cell order
     return run_gather<kFwd>(v, kernel, G);
 }
@@ -1414,7 +1798,8 @@ gvdb2_status gather_kernel_backward(Volume *v, int kernel, int n, const float tr
         S.nch = nch;
         fill_topology(v, S);
         S.reg_off = v->reg_off.as<uint32_t>();
-        S.cell_giant = v->cell_giant.as<int32_t>();
+        S.cell_part = v->cell_part.as<int32_t>();
+        S.part_work = v->part_work.as<int4>();
         S.bin_pos = v->bin_pos.as<float4>();
         GV_TRY(run_scatter(v, kernel, S));
     }

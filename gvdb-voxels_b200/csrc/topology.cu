@@ -31,7 +31,8 @@ struct SmallWords { // layout of Volume::dev_small
     int32_t bbox[6];
     int32_t count[8];
     int32_t status;
-    int32_t pad[17];
+    int32_t splat_guard; // set by a splat kernel that met an index out of range
+    int32_t pad[16];
 };
 static_assert(sizeof(SmallWords) == 128, "small word block");
 
@@ -400,16 +401,40 @@ inline uint32_t next_pow2(uint64_t x) {
 SmallWords *host_words(Volume *v) { return reinterpret_cast<SmallWords *>(v->host_small); }
 SmallWords *dev_words(Volume *v) { return v->dev_small.as<SmallWords>(); }
 
+// The small device words and their pinned mirror, allocated once and zeroed
+// (the flags and counters start clear).
+gvdb2_status ensure_small_words(Volume *v) {
+    if (!v->dev_small.p) {
+        GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), v->stream));
+        GV_CUDA(v, cudaMemsetAsync(v->dev_small.p, 0, sizeof(SmallWords), v->stream));
+    }
+    if (!v->host_small) GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
+    return GVDB2_OK;
+}
+
 // The status a full rebuild left in the small words, once they are back on
 // the host (build_from_keys defers its check to the next read-back).
 gvdb2_status check_pending_status(Volume *v) {
-    if (!v->status_pending) return GVDB2_OK;
-    v->status_pending = false;
-    const int32_t st = host_words(v)->status;
-    if (st & kDevHashFull) return fail(v, GVDB2_ERR_CAPACITY, "leaf map overflow in the last full rebuild");
-    if (st & kDevBadIndex) return fail(v, GVDB2_ERR_STATE, "node without parent in the last full rebuild");
-    return GVDB2_OK;
+    gvdb2_status st = GVDB2_OK;
+    if (v->status_pending) {
+        v->status_pending = false;
+        const int32_t w = host_words(v)->status;
+        if (w & kDevHashFull) st = fail(v, GVDB2_ERR_CAPACITY, "leaf map overflow in the last full rebuild");
+        else if (w & kDevBadIndex) st = fail(v, GVDB2_ERR_STATE, "node without parent in the last full rebuild");
+    }
+    if (v->splat_guard_pending) {
+        v->splat_guard_pending = false;
+        if (host_words(v)->splat_guard) {
+            host_words(v)->splat_guard = 0;
+            GV_CUDA(v, cudaMemsetAsync(&dev_words(v)->splat_guard, 0, sizeof(int32_t), v->stream));
+            if (st == GVDB2_OK)
+                st = fail(v, GVDB2_ERR_STATE, "a splat kernel met a bin or topology index out of range; the cells "
+                                              "concerned were skipped");
+        }
+    }
+    return st;
 }
+
 
 gvdb2_status read_words(Volume *v) {
     GV_CUDA(v, cudaMemcpyAsync(v->host_small, v->dev_small.p, sizeof(SmallWords), cudaMemcpyDeviceToHost, v->stream));
@@ -1043,9 +1068,11 @@ KeyGeom key_geom(const Volume *v) {
 gvdb2_status incremental_rebuild(Volume *v, int n, float radius, const float orig[3], bool accum);
 
 gvdb2_status flush_status(Volume *v) {
-    if (!v->status_pending || !v->dev_small.p) return GVDB2_OK;
+    if (!(v->status_pending || v->splat_guard_pending) || !v->dev_small.p) return GVDB2_OK;
     return read_words(v);
 }
+
+int32_t *splat_guard_word(Volume *v) { return v->dev_small.p ? &dev_words(v)->splat_guard : nullptr; }
 
 gvdb2_status sync_counts(Volume *v) {
     GV_CUDA(v, cudaStreamSynchronize(v->stream));
@@ -1080,10 +1107,7 @@ void reserve_pool(Volume *v, int64_t n) {
 gvdb2_status get_min_max_vel(Volume *v, int n) {
     if (!v->vel.base || n <= 0 || n > v->vel.count) return fail(v, GVDB2_ERR_ARG, "GetMinMaxVel needs velocities");
     cudaStream_t s = v->stream;
-    if (!v->dev_small.p) {
-        GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), s));
-        GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
-    }
+    GV_TRY(ensure_small_words(v));
     int32_t init[6];
     for (int a = 0; a < 3; a++) {
         init[a] = 0x7F800000;              // ord(+inf)
@@ -1106,10 +1130,7 @@ gvdb2_status rebuild_topology(Volume *v, int n, float radius, const float orig[3
     if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count)))
         return fail(v, GVDB2_ERR_ARG, "point count exceeds the position view");
     cudaStream_t s = v->stream;
-    if (!v->dev_small.p) {
-        GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), s));
-        GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
-    }
+    GV_TRY(ensure_small_words(v));
     reserve_pool(v, n);
     // GetBoundingBox
     int32_t init[6];
@@ -1264,10 +1285,7 @@ gvdb2_status compute_bounds(Volume *v) {
     const int64_t n = v->pool_cnt[0];
     if (n == 0) return GVDB2_OK; // the reference reads leaf 0, which does not exist: bounds unchanged
     cudaStream_t s = v->stream;
-    if (!v->dev_small.p) {
-        GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), s));
-        GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
-    }
+    GV_TRY(ensure_small_words(v));
     const int32_t init[6] = {INT32_MAX, INT32_MAX, INT32_MAX, INT32_MIN, INT32_MIN, INT32_MIN};
     GV_CUDA(v, cudaMemcpyAsync(dev_words(v)->bbox, init, sizeof(init), cudaMemcpyHostToDevice, s));
     k_leaf_bounds<<<std::min(grid_for(n, 256), 4 * kSmCount), 256, 0, s>>>(v->pool_ptr(0), n, (int)v->range(0),
@@ -1715,10 +1733,7 @@ gvdb2_status pool_reserve(Volume *v, int lev, int64_t cnt) { return ensure_pool(
 // RebuildTopology starts over, as after Configure.
 gvdb2_status adopt_pools(Volume *v, int depth) {
     cudaStream_t s = v->stream;
-    if (!v->dev_small.p) {
-        GV_CUDA(v, v->dev_small.ensure(sizeof(SmallWords), s));
-        GV_CUDA(v, cudaMallocHost(&v->host_small, sizeof(SmallWords)));
-    }
+    GV_TRY(ensure_small_words(v));
     if (v->status_pending) GV_TRY(read_words(v)); // before the status word is cleared below
     v->all_leaves_flagged = false;
     Node root;
