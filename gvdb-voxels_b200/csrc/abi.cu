@@ -98,7 +98,9 @@ gvdb2_status gvdb2_create(gvdb2_volume **out, int device) {
         delete h;
         return GVDB2_ERR_NOMEM;
     }
-    if (h->v.dev_small.ensure(128, nullptr) != cudaSuccess) {
+    // the small device words start clear (their flags and counters are read
+    // back before some kernels write them)
+    if (h->v.dev_small.ensure(128, nullptr) != cudaSuccess || cudaMemset(h->v.dev_small.p, 0, 128) != cudaSuccess) {
         cudaFreeHost(h->v.host_small);
         delete h;
         return GVDB2_ERR_NOMEM;

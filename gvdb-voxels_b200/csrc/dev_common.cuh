@@ -200,9 +200,14 @@ struct SplatLimits {
     int64_t nentry; // entries of the bin order (the points the bins were made for)
     int64_t ncloud; // batched clouds
 };
-__device__ __forceinline__ bool in_range(const SplatLimits &L, int64_t i, int64_t hi) {
+// The first failing check of a call leaves its code in flag[0] and the
+// index and bound in flag[1..4].
+__device__ __forceinline__ bool in_range(const SplatLimits &L, int64_t i, int64_t hi, int code) {
     if ((uint64_t)i < (uint64_t)hi) return true;
-    if (L.flag) atomicOr(L.flag, 1);
+    if (L.flag && atomicCAS(L.flag, 0, code) == 0) {
+        L.flag[1] = (int32_t)(i >> 32), L.flag[2] = (int32_t)i;
+        L.flag[3] = (int32_t)(hi >> 32), L.flag[4] = (int32_t)hi;
+    }
     return false;
 }
 constexpr uint32_t kSlicePts = 4096;

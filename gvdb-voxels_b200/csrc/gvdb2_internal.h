@@ -186,6 +186,9 @@ struct Volume {
     // cells splatted by several CTAs (part_acc, part_done: zero between
     // calls); their capacities
     DevBuf cell_part, part_work, part_buf, part_acc, part_done;
+    // cells whose voxels k_scatter_merge adds partials to (count in the
+    // last 16 bytes)
+    DevBuf merge_list;
     int64_t dense_cap = 0, work_cap = 0, multi_cap = 0, part_acc_cap = 0;
     // cells that hold points: huge and heavy ones (order of cell_at), light
     // ones and the counts (kCnt*); heavy_grid, light_grid and cell_grid

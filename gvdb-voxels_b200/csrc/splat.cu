@@ -224,6 +224,9 @@ struct SplatArgs {
     float *part;
     int32_t *part_acc;
     uint32_t *part_done;
+    // cells with a dense cell among their 27 (k_scatter_cells lists them)
+    int32_t *merge_list;
+    uint32_t *merge_cnt;
 };
 
 
@@ -243,14 +246,18 @@ struct SplatArgs {
 // gets).
 //
 // k_scatter_part: one CTA per work item, a slice of up to kSlicePts points
-// of a dense cell, accumulates in shared memory with integer atomics in
-// fixed point: integer sums do not depend on the order of the adds, so the
-// partial is the same whatever the order of the points within their bins
-// and whatever the split into slices.  A cell of one slice writes its
-// partial (float) directly; the slices of a larger cell add their integer
-// tiles into the cell's global accumulator, and the CTA that arrives last
-// (an arrival counter; no CTA waits for another) converts the sums to the
-// partial and clears the accumulator and counter for the next call.
+// of a dense cell, accumulates its points' stencils in shared memory with
+// atomics.  A cell of one slice writes its partial directly; the slices of
+// a larger cell add their tiles into the cell's global accumulator, and the
+// CTA that arrives last (an arrival counter; no CTA waits for another)
+// writes the partial and clears the accumulator and counter for the next
+// call.  k_scatter_merge then adds the partials to the voxels they cover,
+// after the owner-computes pass has written its sums.
+//
+// The accumulators are fixed-point integers: integer sums do not depend on
+// the order of the adds, so the partial is the same whatever the order of
+// the points within their bins and whatever the split into slices.  (Float
+// shared-memory atomics, half as many, measured 16% slower.)
 //
 // Fixed point: each contribution x = amount * weight is scaled by 2^s and
 // rounded to an integer, split as rint(x) = hi * 2^L + lo with both parts
@@ -400,27 +407,27 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
     const int64_t cell = item.x;
     const int nslice = item.z;
     // every check below is the same for the whole CTA
-    if (!in_range(S.lim, cell, S.ncell)) return;
+    if (!in_range(S.lim, cell, S.ncell, 6)) return;
     const int32_t pslot = S.cell_part[cell];
-    if (!in_range(S.lim, pslot, S.dense_cap) || (nslice > 1 && !in_range(S.lim, item.w, S.multi_cap))) return;
+    if (!in_range(S.lim, pslot, S.dense_cap, 7) || (nslice > 1 && !in_range(S.lim, item.w, S.multi_cap, 8))) return;
     const uint32_t beg = S.bin_off[cell], R = S.bin_off[cell + 1] - beg;
-    if (!in_range(S.lim, (int64_t)beg + R - 1, S.lim.nentry)) return;
+    if (!in_range(S.lim, (int64_t)beg + R - 1, S.lim.nentry, 9)) return;
     const uint32_t s0 = (uint32_t)item.y * kSlicePts, s1 = min(R, s0 + kSlicePts);
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
     const int32_t leaf = S.slot_leaf[slot];
-    if (!in_range(S.lim, leaf, S.lim.npool)) return;
+    if (!in_range(S.lim, leaf, S.lim.npool, 10)) return;
     static_assert((NCH * AS * sizeof(int32_t)) % 16 == 0, "16-byte zeroing");
     for (int i = threadIdx.x; i < (int)(NCH * AS * sizeof(int32_t) / 16); i += kPartThreads)
         reinterpret_cast<int4 *>(acc)[i] = make_int4(0, 0, 0, 0);
-    if (threadIdx.x < NCH) amax_bits[threadIdx.x] = 0;
     const Node &nd = S.leaves[leaf];
     const int ox = nd.mPos[0] + kCell * cx - X::H, oy = nd.mPos[1] + kCell * cy - X::H,
               oz = nd.mPos[2] + kCell * cz - X::H;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // the largest |amount| per channel over all the cell's points sets the
     // scale, the same in every slice of the cell
+    if (threadIdx.x < NCH) amax_bits[threadIdx.x] = 0;
     float mx[NCH];
 #pragma unroll
     for (int c = 0; c < NCH; c++) mx[c] = 0.0f;
@@ -455,7 +462,7 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
             const float4 q = S.bin_pos[j]; // translated position, cloud index bits
             const int32_t cloud = __float_as_int(q.w);
             int3 o = make_int3(0, 0, 0);
-            if (cloud >= 0 && in_range(S.lim, cloud, S.lim.ncloud))
+            if (cloud >= 0 && in_range(S.lim, cloud, S.lim.ncloud, 5))
                 o = make_int3(S.pos.origin[3 * cloud], S.pos.origin[3 * cloud + 1], S.pos.origin[3 * cloud + 2]);
             float wx[N], wy[N], wz[N];
             const int fx = T::eval(q.x, wx) + o.x - ox;
@@ -512,28 +519,28 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
     // (coalesced), each looked up in its tile voxel
     float *dst = S.part + (int64_t)pslot * NCH * X::E3;
     static_assert(kPartThreads < X::E3, "one channel step per iteration");
-    auto write = [&](int i, int c, int32_t hi, int32_t lo) {
+    auto value = [&](int c, int32_t hi, int32_t lo) {
         // |sum| < 2^53: exact in double; the power-of-two scalings are exact
-        const long long sum = ((long long)hi << L) + (long long)lo;
-        dst[i] = (float)((double)sum * inv_s[c]);
+        return (float)((double)(((long long)hi << L) + (long long)lo) * inv_s[c]);
     };
     if (nslice == 1) {
         int c = 0, i0 = threadIdx.x;
         for (int i = threadIdx.x; i < NCH * X::E3; i += kPartThreads) {
             const int k = c * AS + kPartAddr<KERNEL>.addr[i0];
-            write(i, c, acc[k], acc[k + X::CS]);
+            dst[i] = value(c, acc[k], acc[k + X::CS]);
             if ((i0 += kPartThreads) >= X::E3) i0 -= X::E3, c++;
         }
         return;
     }
     // a cell of several slices: this slice's integer sums into the cell's
-    // accumulator (per channel hi[E3], lo[E3] in partial order)
-    int32_t *g = S.part_acc + (int64_t)item.w * 2 * NCH * X::E3;
+    // accumulator (per channel hi[E3], lo[E3], in partial order)
+    constexpr int GW = 2 * X::E3; // accumulator words per channel
+    int32_t *g = S.part_acc + (int64_t)item.w * NCH * GW;
     {
         int c = 0, i0 = threadIdx.x;
         for (int i = threadIdx.x; i < NCH * X::E3; i += kPartThreads) {
             const int k = c * AS + kPartAddr<KERNEL>.addr[i0];
-            int32_t *gc = g + c * 2 * X::E3 + i0;
+            int32_t *gc = g + c * GW + i0;
             if (acc[k]) atomicAdd(gc, acc[k]);
             if (acc[k + X::CS]) atomicAdd(gc + X::E3, acc[k + X::CS]);
             if ((i0 += kPartThreads) >= X::E3) i0 -= X::E3, c++;
@@ -549,8 +556,8 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
     __threadfence();
     int c = 0, i0 = threadIdx.x;
     for (int i = threadIdx.x; i < NCH * X::E3; i += kPartThreads) {
-        int32_t *gc = g + c * 2 * X::E3 + i0;
-        write(i, c, atomicExch(gc, 0), atomicExch(gc + X::E3, 0));
+        int32_t *gc = g + c * GW + i0;
+        dst[i] = value(c, atomicExch(gc, 0), atomicExch(gc + X::E3, 0));
         if ((i0 += kPartThreads) >= X::E3) i0 -= X::E3, c++;
     }
     if (threadIdx.x == 0) S.part_done[item.w] = 0;
@@ -565,8 +572,8 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
 // cells, the regions of that cell's bin whose stencils cross the shared
 // face, edge or corner (k_bin_count bins points by cell and region), so
 // every source is a point the cell needs -- except the points of dense
-// cells (this cell's included), whose partial sums the warp adds instead
-// when it writes its voxels.
+// cells (this cell's included), whose partial sums k_scatter_merge adds to
+// the voxels afterwards.
 //
 // The warp turns its sources into records in shared memory, a chunk of at
 // most kScCap at a time: per point the x weights on the cell's 8 voxel
@@ -585,9 +592,8 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
 // accumulator plane fixed at compile time: paired register FMAs.
 //
 // The adds happen in the order of the sources (the bins) and of the stable
-// sort, then the partials in a fixed order, so with deterministic binning
-// the result is bit-reproducible (and always so where every cell around is
-// dense).
+// sort, then k_scatter_merge adds the partials in a fixed order, so with
+// deterministic binning the result is bit-reproducible.
 #ifndef GVDB2_SC_CAP
 #define GVDB2_SC_CAP 128
 #endif
@@ -613,7 +619,6 @@ struct ScChunk {
     uint16_t off[kScBins + 1];
     uint2 run[64]; // the cell's sources: runs [x, y) of perm (at most 1 + 2 + 10 + 50 = 63)
     uint32_t run_first[64]; // sources before run k (the runs read as one sequence)
-    int32_t part[28]; // per neighbour direction d: the partial slot of a dense cell there, else -1
 };
 
 // Sort the chunk's `fill` records by key (stable) into C.order.
@@ -796,7 +801,7 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
     int cx, cy, cz;
     cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
     const int32_t leaf = S.slot_leaf[slot];
-    if (!in_range(S.lim, leaf, S.lim.npool)) return; // the same for the whole warp
+    if (!in_range(S.lim, leaf, S.lim.npool, 1)) return; // the same for the whole warp
     const Node &nd = S.leaves[leaf];
     const int ox = nd.mPos[0] + kCell * cx, oy = nd.mPos[1] + kCell * cy, oz = nd.mPos[2] + kCell * cz;
     // The sources, as runs of perm in a fixed order: lane d < 27 lists those of
@@ -815,18 +820,18 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
                   bz = ncz < 0 ? -1 : (ncz >= S.m ? 1 : 0);
         int32_t ns = (bx | by | bz) == 0 ? (int32_t)slot
                                          : S.nbr27[slot * 27 + (bz + 1) * 9 + (by + 1) * 3 + (bx + 1)];
-        if (ns >= 0 && !in_range(S.lim, ns, S.lim.nslot)) ns = -1;
+        if (ns >= 0 && !in_range(S.lim, ns, S.lim.nslot, 2)) ns = -1;
         int64_t nc = ns < 0 ? -1
                             : (int64_t)ns * S.m3 + ((ncz - bz * S.m) * S.m + (ncy - by * S.m)) * S.m + (ncx - bx * S.m);
         if (nc >= 0) pslot = S.cell_part[nc];
-        if (pslot >= 0 && !in_range(S.lim, pslot, S.dense_cap)) pslot = -1, nc = -1;
+        if (pslot >= 0 && !in_range(S.lim, pslot, S.dense_cap, 3)) pslot = -1, nc = -1;
         if (nc >= 0 && pslot < 0) {
             const uint32_t *ro = S.reg_off + nc * kRegions;
             const int rx0 = dx < 0 ? 2 : 0, ry0 = dy < 0 ? 2 : 0, ry1 = dy > 0 ? 0 : 2;
             const int rz0 = dz < 0 ? 2 : 0, rz1 = dz > 0 ? 0 : 2;
             auto add = [&](int r0, int r1) { // regions [r0, r1)
                 const uint2 u = make_uint2(ro[r0], ro[r1]);
-                if (u.y > u.x && in_range(S.lim, (int64_t)u.y - 1, S.lim.nentry)) runs[nrun++] = u;
+                if (u.y > u.x && in_range(S.lim, (int64_t)u.y - 1, S.lim.nentry, 4)) runs[nrun++] = u;
             };
             if (dx == 0 && dy == 0) {
                 if (dz == 0) add(0, kRegions);
@@ -864,7 +869,6 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
             C.run_first[first + k] = before;
             before += runs[k].y - runs[k].x;
         }
-    if (lane < 27) C.part[lane] = pslot;
     const bool any_part = __any_sync(0xffffffffu, pslot >= 0);
     __syncwarp();
 
@@ -918,7 +922,7 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
             const float4 q = S.bin_pos[j];
             d.pt = make_float3(q.x, q.y, q.z);
             const int32_t cloud = __float_as_int(q.w);
-            if (cloud >= 0 && in_range(S.lim, cloud, S.lim.ncloud))
+            if (cloud >= 0 && in_range(S.lim, cloud, S.lim.ncloud, 5))
                 d.o = make_int3(S.pos.origin[3 * cloud], S.pos.origin[3 * cloud + 1], S.pos.origin[3 * cloud + 2]);
             const float4 am = S.bin_amt[j];
             d.a4[0] = am.x, d.a4[1] = am.y, d.a4[2] = am.z, d.a4[3] = am.w;
@@ -1002,37 +1006,8 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
                     acc[z][xp][c] = (c & 1) ? make_float2(a0.y, a1.y) : make_float2(a0.x, a1.x);
                 }
     }
-    // the partials of the dense cells that cover the lane's voxels, summed
-    // in the order of their sources (kMergeMap), after the owner's sum
-    if (any_part) {
-#pragma unroll
-        for (int zz = 0; zz < 4; zz++)
-#pragma unroll
-            for (int xi = 0; xi < 4; xi++) {
-                const int vv = (4 * q + xi) | (y << 3) | ((4 * h + zz) << 6);
-                const uint4 row = *reinterpret_cast<const uint4 *>(kMergeMap<KERNEL>.src[vv]);
-                const uint32_t wr[4] = {row.x, row.y, row.z, row.w};
-                float add[NCH];
-#pragma unroll
-                for (int c = 0; c < NCH; c++) add[c] = 0.0f;
-#pragma unroll
-                for (int m = 0; m < 8; m++) {
-                    const uint32_t ent = (wr[m >> 1] >> (16 * (m & 1))) & 0xFFFFu;
-                    if (ent == 0xFFFFu) continue;
-                    const int32_t e = C.part[ent >> 11];
-                    if (e < 0) continue;
-                    const float *src = S.part + (int64_t)e * NCH * X::E3 + (ent & 2047u);
-#pragma unroll
-                    for (int c = 0; c < NCH; c++) add[c] += __ldcs(src + c * X::E3);
-                }
-#pragma unroll
-                for (int c = 0; c < NCH; c++) {
-                    float2 &v2 = acc[zz][xi >> 1][c];
-                    if (xi & 1) v2.y += add[c];
-                    else v2.x += add[c];
-                }
-            }
-    }
+    // cells with a dense cell around get its partials from k_scatter_merge
+    if (any_part && lane == 0) S.merge_list[atomicAdd(S.merge_cnt, 1u)] = (int32_t)cell;
     // each lane writes its 4 x 4 voxels of every channel once
     const int a = S.apron, tl = S.tile;
     const int64_t base = slot * S.tvox + (int64_t)(kCell * cx + 4 * q + a);
@@ -1046,6 +1021,62 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
             dst[2] = acc[zz][1][c].x;
             dst[3] = acc[zz][1][c].y;
         }
+}
+
+// Adds the dense cells' partials to the cells listed by k_scatter_cells
+// (those with a dense cell among their 27): a CTA per cell at a time, a
+// thread per interior voxel, which adds, in the order of kMergeMap, the
+// partials that cover the voxel to the sum the owner-computes pass wrote.
+constexpr int kMergeCtas = 8 * 148; // resident CTAs that loop over the list
+template <int KERNEL, int NCH>
+__global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S) {
+    using X = ExtTile<KERNEL>;
+    __shared__ int32_t ne[27]; // partial slot of the dense cell in each direction, or -1
+    const uint32_t count = *S.merge_cnt;
+    for (uint32_t li = blockIdx.x; li < count; li += gridDim.x) {
+        const int64_t cell = S.merge_list[li];
+        int64_t slot;
+        int cx, cy, cz;
+        cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
+        __syncthreads(); // the previous cell's table is no longer read
+        if (threadIdx.x < 27) {
+            const int d = threadIdx.x;
+            const int ncx = cx + d % 3 - 1, ncy = cy + d / 3 % 3 - 1, ncz = cz + d / 9 - 1;
+            const int bx = ncx < 0 ? -1 : (ncx >= S.m ? 1 : 0), by = ncy < 0 ? -1 : (ncy >= S.m ? 1 : 0),
+                      bz = ncz < 0 ? -1 : (ncz >= S.m ? 1 : 0);
+            int32_t ns = (bx | by | bz) == 0 ? (int32_t)slot
+                                             : S.nbr27[slot * 27 + (bz + 1) * 9 + (by + 1) * 3 + (bx + 1)];
+            int32_t e = -1;
+            if (ns >= 0 && in_range(S.lim, ns, S.lim.nslot, 21)) {
+                e = S.cell_part[(int64_t)ns * S.m3 + ((ncz - bz * S.m) * S.m + (ncy - by * S.m)) * S.m +
+                                (ncx - bx * S.m)];
+                if (e >= 0 && !in_range(S.lim, e, S.dense_cap, 22)) e = -1;
+            }
+            ne[d] = e;
+        }
+        __syncthreads();
+        const int v = threadIdx.x;
+        const uint4 row = *reinterpret_cast<const uint4 *>(kMergeMap<KERNEL>.src[v]);
+        const uint32_t wr[4] = {row.x, row.y, row.z, row.w};
+        float add[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; c++) add[c] = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const uint32_t ent = (wr[m >> 1] >> (16 * (m & 1))) & 0xFFFFu;
+            const int32_t e = ent != 0xFFFFu ? ne[ent >> 11] : -1;
+            if (e < 0) continue;
+            const float *src = S.part + (int64_t)e * NCH * X::E3 + (ent & 2047u);
+#pragma unroll
+            for (int c = 0; c < NCH; c++) add[c] += __ldcs(src + c * X::E3);
+        }
+        const int vx = v & 7, vy = (v >> 3) & 7, vz = v >> 6;
+        const int a = S.apron, tl = S.tile;
+        const int64_t at = slot * S.tvox + ((int64_t)(kCell * cz + vz + a) * tl + (kCell * cy + vy + a)) * tl +
+                           (kCell * cx + vx + a);
+#pragma unroll
+        for (int c = 0; c < NCH; c++) S.chan[c][at] += add[c];
+    }
 }
 
 // ---------------------------------------------------------------------
@@ -1092,7 +1123,7 @@ __device__ __forceinline__ void gather_point_at(const GatherArgs &G, int32_t pid
         const float4 q = G.bin_pos[j];
         w = make_float3(q.x, q.y, q.z);
         const int32_t cloud = __float_as_int(q.w);
-        o = cloud >= 0 && in_range(G.lim, cloud, G.lim.ncloud)
+        o = cloud >= 0 && in_range(G.lim, cloud, G.lim.ncloud, 12)
                 ? make_int3(G.pos.origin[3 * cloud], G.pos.origin[3 * cloud + 1], G.pos.origin[3 * cloud + 2])
                 : make_int3(0, 0, 0);
     } else {
@@ -1110,7 +1141,7 @@ __device__ __forceinline__ void gather_point(const GatherArgs &G, int32_t pidx, 
                                              const Fetch &fetch) {
     using T = Taps<KERNEL>;
     constexpr int N = T::N;
-    if (!in_range(G.lim, pidx, G.lim.nentry)) return;
+    if (!in_range(G.lim, pidx, G.lim.nentry, 13)) return;
     float3 p;
     int3 o;
     gather_point_at(G, pidx, j, p, o);
@@ -1263,11 +1294,11 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
     cell_coords(cell, G.m, G.m3, slot, cx, cy, cz);
     const int32_t leaf = G.slot_leaf[slot];
     // the same for the whole CTA
-    if (!in_range(G.lim, (int64_t)end - 1, G.lim.nentry) || !in_range(G.lim, leaf, G.lim.npool)) return;
+    if (!in_range(G.lim, (int64_t)end - 1, G.lim.nentry, 14) || !in_range(G.lim, leaf, G.lim.npool, 15)) return;
     const int a = G.apron, tl = G.tile;
     if (threadIdx.x < 27) {
         const int32_t nb = G.nbr27[slot * 27 + threadIdx.x];
-        nbs[threadIdx.x] = nb >= 0 && in_range(G.lim, nb, G.lim.nslot) ? nb : -1;
+        nbs[threadIdx.x] = nb >= 0 && in_range(G.lim, nb, G.lim.nslot, 16) ? nb : -1;
     }
     __syncthreads();
     // halo tile from the interiors of this brick and its neighbours; all of a
@@ -1360,14 +1391,14 @@ __device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t 
     const int lane = threadIdx.x & 31;
     if (w >= (int64_t)G.cell_cnt[2]) return;
     const int64_t cell = G.cell_light[w];
-    if (!in_range(G.lim, cell, G.ncell)) return;
+    if (!in_range(G.lim, cell, G.ncell, 17)) return;
     const uint32_t beg = G.bin_off[cell], cnt = G.bin_off[cell + 1] - beg;
-    if ((uint32_t)lane >= cnt || !in_range(G.lim, (int64_t)beg + lane, G.lim.nentry)) return;
+    if ((uint32_t)lane >= cnt || !in_range(G.lim, (int64_t)beg + lane, G.lim.nentry, 18)) return;
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, G.m, G.m3, slot, cx, cy, cz);
     const int32_t leaf = G.slot_leaf[slot];
-    if (!in_range(G.lim, leaf, G.lim.npool)) return;
+    if (!in_range(G.lim, leaf, G.lim.npool, 19)) return;
     const Node &nd = G.leaves[leaf];
     const int fx0 = kCell * cx - H, fy0 = kCell * cy - H, fz0 = kCell * cz - H; // frame origin in the brick
     const int res = G.res0, a = G.apron, tl = G.tile;
@@ -1377,7 +1408,7 @@ __device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t 
                   sz = lz < 0 ? -1 : (lz >= res ? 1 : 0);
         const int d = (sz + 1) * 9 + (sy + 1) * 3 + (sx + 1);
         int64_t ns = d == 13 ? slot : (int64_t)G.nbr27[slot * 27 + d];
-        if (ns >= 0 && !in_range(G.lim, ns, G.lim.nslot)) ns = -1;
+        if (ns >= 0 && !in_range(G.lim, ns, G.lim.nslot, 20)) ns = -1;
         const int64_t off = ns * G.tvox + ((int64_t)(lz - sz * res + a) * tl + (ly - sy * res + a)) * tl +
                             (lx - sx * res + a);
 #pragma unroll
@@ -1461,7 +1492,7 @@ __global__ void k_pack_amounts(SplatArgs S) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= (int64_t)S.reg_off[S.ncell * kRegions]) return;
     const int32_t p = S.perm[j];
-    if (!in_range(S.lim, p, S.lim.nentry)) {
+    if (!in_range(S.lim, p, S.lim.nentry, 11)) {
         S.bin_amt[j] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
@@ -1489,15 +1520,13 @@ template <int KERNEL, int NCH>
 gvdb2_status scatter_group(Volume *v, const SplatArgs &S0) {
     using X = ExtTile<KERNEL>;
     constexpr size_t smem = sizeof(ScChunk) * kScWarps;
-    constexpr size_t psmem = part_smem_bytes<KERNEL, NCH>();
     auto k = k_scatter_cells<KERNEL, NCH>;
-    auto kp = k_scatter_part<KERNEL, NCH>;
     GV_TRY(launch_smem(v, k, smem, "scatter"));
-    GV_TRY(launch_smem(v, kp, psmem, "scatter"));
     GV_CUDA(v, v->bin_amt.ensure(sizeof(float4) * (size_t)std::max<int64_t>(v->bin_key.n, 1), v->stream));
     GV_CUDA(v, v->part_buf.ensure(sizeof(float) * (size_t)std::max<int64_t>(v->dense_cap * NCH * X::E3, 1), v->stream));
     GV_TRY(ensure_zeroed(v, v->part_acc, sizeof(int32_t) * (size_t)std::max<int64_t>(v->multi_cap * 2 * NCH * X::E3, 1)));
     GV_TRY(ensure_zeroed(v, v->part_done, sizeof(uint32_t) * (size_t)std::max<int64_t>(v->multi_cap, 1)));
+    GV_CUDA(v, v->merge_list.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(S0.ncell, 1) + 16, v->stream));
     SplatArgs S = S0;
     S.bin_amt = v->bin_amt.as<float4>();
     S.part = v->part_buf.as<float>();
@@ -1505,11 +1534,22 @@ gvdb2_status scatter_group(Volume *v, const SplatArgs &S0) {
     S.part_done = v->part_done.as<uint32_t>();
     S.dense_cap = v->dense_cap;
     S.multi_cap = v->multi_cap;
+    // the list's count sits in its last 16 bytes
+    S.merge_cnt = reinterpret_cast<uint32_t *>(v->merge_list.as<char>() + v->merge_list.bytes - 16);
+    S.merge_list = v->merge_list.as<int32_t>();
+    GV_CUDA(v, cudaMemsetAsync(S.merge_cnt, 0, sizeof(uint32_t), v->stream));
     if (v->bin_key.n > 0)
         k_pack_amounts<NCH><<<grid_for(v->bin_key.n, 256, 1ll << 31), 256, 0, v->stream>>>(S);
-    if (v->work_cap > 0) kp<<<(unsigned)v->work_cap, kPartThreads, psmem, v->stream>>>(S);
+    if (v->work_cap > 0) {
+        constexpr size_t ps = part_smem_bytes<KERNEL, NCH>();
+        auto kp = k_scatter_part<KERNEL, NCH>;
+        GV_TRY(launch_smem(v, kp, ps, "scatter"));
+        kp<<<(unsigned)v->work_cap, kPartThreads, ps, v->stream>>>(S);
+    }
     const int64_t blocks = (S.ncell + kScWarps - 1) / kScWarps;
     if (blocks > 0) k<<<(unsigned)blocks, 32 * kScWarps, smem, v->stream>>>(S);
+    if (v->dense_cap > 0)
+        k_scatter_merge<KERNEL, NCH><<<(unsigned)std::min<int64_t>(S.ncell, kMergeCtas), 512, 0, v->stream>>>(S);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }

