@@ -349,12 +349,15 @@ static_assert(ExtTile<GVDB2_KERNEL_CUBIC2>::E3 <= 2048 && ExtTile<GVDB2_KERNEL_T
 
 constexpr int kPartThreads = 256;
 constexpr int kPartChunk = 128; // points staged per pass, one per thread of the first 128
+// row stride of the staged weights: a point's taps (one row each) fall in
+// different banks
+constexpr int kPartRow = kPartChunk + 1;
 static_assert(kSlicePts % kPartChunk == 0, "slices are whole chunks");
 
 template <int KERNEL, int NCH>
 constexpr size_t part_smem_bytes() {
     return sizeof(int32_t) * 2 * NCH * ExtTile<KERNEL>::CS +
-           sizeof(float) * (3 * Taps<KERNEL>::N + NCH) * kPartChunk + sizeof(int32_t) * kPartChunk;
+           sizeof(float) * (3 * Taps<KERNEL>::N + NCH) * kPartRow + sizeof(int32_t) * kPartChunk;
 }
 
 // The fixed-point scale of R points whose largest |amount| is am, per the
@@ -396,8 +399,8 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
     constexpr int AS = 2 * X::CS; // accumulator words per channel (hi, lo)
     extern __shared__ __align__(16) unsigned char part_smem[];
     int32_t *acc = reinterpret_cast<int32_t *>(part_smem);
-    float(*pw)[kPartChunk] = reinterpret_cast<float(*)[kPartChunk]>(acc + NCH * AS);
-    float(*pa)[kPartChunk] = pw + 3 * N;
+    float(*pw)[kPartRow] = reinterpret_cast<float(*)[kPartRow]>(acc + NCH * AS);
+    float(*pa)[kPartRow] = pw + 3 * N;
     int32_t *pb = reinterpret_cast<int32_t *>(pa + NCH);
     __shared__ double inv_s[NCH];
     __shared__ int32_t amax_bits[NCH]; // largest |amount| of the cell's points, as float bits
