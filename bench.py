@@ -477,7 +477,8 @@ def run_ours(a):
     if a.quick:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
-                              "ms_per_step": ms / a.steps, "quick": True, "workload": desc}), flush=True)
+                              "ms_per_step": ms / a.steps, "quick": True, "workload": desc,
+                              "bricks": pipe.geometry()["B"]}), flush=True)
         return 0
 
     # per-stage device times: each stage repeated on the launching stream,
@@ -536,16 +537,21 @@ def run_ours(a):
 
 
 # DRAM bytes (read + write) per brick of each stage's kernels, from an ncu
-# capture of one launch of each kernel on the 4,194,304-point block,
-# divided by its bricks.  Traffic grows with the brick count, so a launch
-# moves about this many bytes x bricks.
+# capture of one launch of each kernel on the 2,097,152-point block at the
+# default workload's density (128 x 128 x 128 lattice sites at spacing
+# (1, 0.5, 1): 1,024 points per 8^3 cell, 3,240 bricks), divided by its
+# bricks.  Traffic grows with the brick count at a fixed density, so a
+# launch moves about this many bytes x bricks.
 TRAFFIC_PER_BRICK = {
-    "scatter": (199.4e6 + 406.3e6 + 752.9e6 + 220.4e6) / 23396,
-    "gather": (635.0e6 + 42.7e6 + 3.3e6 + 0.0) / 23396,
+    # k_pack_amounts, k_scatter_part, k_scatter_cells, k_scatter_merge
+    "scatter": ((33.6 + 0.9) + (66.8 + 12.7) + (20.7 + 18.9) + (99.4 + 1.3)) * 1e6 / 3240,
+    # k_gather_tile, k_gather_light
+    "gather": ((70.5 + 3.1) + (12.4 + 0.0)) * 1e6 / 3240,
 }
-TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4,194,304-point block, scaled by bricks"
-STAGE_KERNELS = {"scatter": "scatter stage: k_scatter_own<cubic,4> (heavy and light cells) + "
-                            "k_scatter_merge_cta<cubic,4>",
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 2,097,152-point block at the "
+                  "16,777,216-point step's density, scaled by bricks")
+STAGE_KERNELS = {"scatter": "scatter stage: k_pack_amounts<4> + k_scatter_part<cubic,4> (dense cells' partials) + "
+                            "k_scatter_cells<cubic,4> (owner-computes) + k_scatter_merge<cubic,4>",
                  "gather": "k_gather_tile<cubic,fwd,3> + k_gather_light<cubic,fwd,3>", "apron": "k_apron"}
 
 
@@ -553,8 +559,8 @@ STAGE_KERNELS = {"scatter": "scatter stage: k_scatter_own<cubic,4> (heavy and li
 # the rest of the metric, each measured in the same run (N = 1)
 # ----------------------------------------------------------------------------
 EXTRA_LEGS = ("incremental", "config1_4m", "adjoint", "batched", "vs_ref_kernels")
-# legs left out of the main line, with the reason
-HELD_LEGS = {"batched": "held back: an illegal memory access in this leg is under investigation"}
+# legs left out of the main line, with the reason (none)
+HELD_LEGS = {}
 
 
 def run_leg(name, warmup):

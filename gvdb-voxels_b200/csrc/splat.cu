@@ -1027,21 +1027,21 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
 }
 
 // Adds the dense cells' partials to the cells listed by k_scatter_cells
-// (those with a dense cell among their 27): a CTA per cell at a time, a
-// thread per interior voxel, which adds, in the order of kMergeMap, the
-// partials that cover the voxel to the sum the owner-computes pass wrote.
-constexpr int kMergeCtas = 8 * 148; // resident CTAs that loop over the list
+// (those with a dense cell among their 27): a CTA per listed cell (CTAs
+// past the list's end return), a thread per interior voxel, which adds, in
+// the order of kMergeMap, the partials that cover the voxel to the sum the
+// owner-computes pass wrote.
 template <int KERNEL, int NCH>
 __global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S) {
     using X = ExtTile<KERNEL>;
     __shared__ int32_t ne[27]; // partial slot of the dense cell in each direction, or -1
-    const uint32_t count = *S.merge_cnt;
-    for (uint32_t li = blockIdx.x; li < count; li += gridDim.x) {
+    const uint32_t li = blockIdx.x;
+    if (li >= *S.merge_cnt) return;
+    {
         const int64_t cell = S.merge_list[li];
         int64_t slot;
         int cx, cy, cz;
         cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
-        __syncthreads(); // the previous cell's table is no longer read
         if (threadIdx.x < 27) {
             const int d = threadIdx.x;
             const int ncx = cx + d % 3 - 1, ncy = cy + d / 3 % 3 - 1, ncz = cz + d / 9 - 1;
@@ -1551,8 +1551,9 @@ gvdb2_status scatter_group(Volume *v, const SplatArgs &S0) {
     }
     const int64_t blocks = (S.ncell + kScWarps - 1) / kScWarps;
     if (blocks > 0) k<<<(unsigned)blocks, 32 * kScWarps, smem, v->stream>>>(S);
-    if (v->dense_cap > 0)
-        k_scatter_merge<KERNEL, NCH><<<(unsigned)std::min<int64_t>(S.ncell, kMergeCtas), 512, 0, v->stream>>>(S);
+    // a cell with a dense cell among its 27 neighbours: at most 27 per dense cell
+    const int64_t merge_grid = std::min<int64_t>(S.ncell, 27 * v->dense_cap);
+    if (merge_grid > 0) k_scatter_merge<KERNEL, NCH><<<(unsigned)merge_grid, 512, 0, v->stream>>>(S);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }

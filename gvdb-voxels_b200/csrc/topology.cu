@@ -958,8 +958,12 @@ gvdb2_status key_sets_bitmap(Volume *v, int n, float radius, const float orig[3]
         const size_t smem = sizeof(uint32_t) * 2 * (size_t)G[0].words;
         auto k = k_mark_bits<true>;
         if (smem > 48 * 1024) GV_CUDA(v, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k<<<std::min(grid_for(n, 256), 2 * kSmCount), 256, smem, s>>>(v->pos, n, t3, radius, 2.0f, do_box ? 1 : 0, g,
-                                                                       G[0], &dev_words(v)->status);
+        // as many CTAs as fit on an SM (each keeps its own copy of the bitmaps,
+        // flushed once), so that the points' loads overlap
+        const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / std::max<size_t>(smem, 1)));
+        k<<<std::min(grid_for(n, 256), per_sm * kSmCount), 256, smem, s>>>(v->pos, n, t3, radius, 2.0f,
+                                                                            do_box ? 1 : 0, g, G[0],
+                                                                            &dev_words(v)->status);
     } else if (n > 0) {
         k_mark_bits<false><<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t3, radius, 2.0f, do_box ? 1 : 0, g,
                                                                         G[0], &dev_words(v)->status);
