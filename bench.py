@@ -606,7 +606,7 @@ def run_extras(a):
     if isinstance(out.get("batched"), dict) and "speedup_vs_loop" in out["batched"]:
         summary["batched_over_loop"] = out["batched"]["speedup_vs_loop"]
     if isinstance(out.get("vs_ref_kernels"), dict) and "speedup_device" in out["vs_ref_kernels"]:
-        summary["vs_ref_kernels"] = out["vs_ref_kernels"]["speedup_device"]
+        summary["vs_ref_kernels_speedup"] = out["vs_ref_kernels"]["speedup_device"]
     out.update(summary)
     return out
 

@@ -37,7 +37,7 @@ namespace {
 constexpr int64_t kNoAllocMaxPoints = 1 << 20; // 1,048,576 points
 constexpr int64_t kNoAllocMaxBins = 1 << 15;   // 32,768 cells: active bricks of 8^3 (1/8 as many of 16^3)
 constexpr int64_t kOffWords = kNoAllocMaxBins + 1;
-constexpr int64_t kScratchWords = 3 * kNoAllocMaxPoints + kNoAllocMaxBins + kOffWords; // 12.25 MB
+constexpr int64_t kScratchWords = 3 * kNoAllocMaxPoints + kNoAllocMaxBins + kOffWords; // 12.25 MiB
 
 // [0, P) point bins, [P, 2P) ranks, [2P, 3P) bin-ordered point list,
 // [3P, 3P+S) per-bin counts, then S+1 per-bin offsets.

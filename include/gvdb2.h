@@ -240,11 +240,12 @@ GVDB2_API gvdb2_status gvdb2_gather_kernel_backward(gvdb2_volume *v, int kernel,
  * budget at start-up, a real-time loop that forbids allocation, a process
  * whose allocator belongs to another framework).  No counterpart in the
  * reference.  It performs no device allocation: its binning scratch is one
- * file-scope device array per GPU (12.25 MB, held until the process exits),
+ * file-scope device array per GPU (12.25 MiB, held until the process exits),
  * which limits a call to 1,048,576 points and 32,768 active bricks of 8^3
  * voxels (4,096 of 16^3, 512 of 32^3: 32,768 8^3 cells); larger
  * calls return GVDB2_ERR_CAPACITY.  The first call on a device looks up the
- * array's address (make it before any stream capture).  All calls share the
+ * array's address (make it before any stream capture) and keeps it, so the
+ * entry point must not be used after a cudaDeviceReset.  All calls share the
  * array, so calls whose GPU work overlaps race and must be ordered by the
  * caller.  Points outside every active brick gather 0. */
 GVDB2_API gvdb2_status gvdb2_gather_kernel_noalloc(gvdb2_volume *v, int kernel, int n, const float trans[3],
