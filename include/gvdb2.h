@@ -50,7 +50,7 @@ typedef int gvdb2_status;
 #define GVDB2_KERNEL_TENT1 1     /* trilinear tent, radius 1 voxel, voxel centres at i+0.5 */
 #define GVDB2_KERNEL_CUBIC2 2    /* cubic B-spline, radius 2 voxels */
 
-#define GVDB2_OPT_DETERMINISTIC 1 /* 1: kernel splats accumulate in 64-bit fixed point (bit-reproducible) */
+#define GVDB2_OPT_DETERMINISTIC 1 /* 1: stable binning, so kernel splats and gathers are bit-reproducible */
 
 typedef struct gvdb2_volume gvdb2_volume;
 
