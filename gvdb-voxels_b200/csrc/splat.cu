@@ -1159,8 +1159,9 @@ __device__ __forceinline__ void gather_point(const GatherArgs &G, int32_t pidx, 
         fy = T::eval_d(p.y, wy, dy) + o.y - oy;
         fz = T::eval_d(p.z, wz, dz) + o.z - oz;
     }
-    // a binned point's first taps lie in [0, 8]; a point moved since the
-    // binning (positions changed in place) gathers 0 and reads nothing outside
+    // a binned point's first taps lie in [0, 8]; a point read through the
+    // caller's view (bins made by the caller) that has moved since its binning
+    // gathers 0 and reads nothing outside
     if (!((unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u)) {
         fx = fy = fz = 0;
 #pragma unroll

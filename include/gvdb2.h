@@ -123,9 +123,10 @@ GVDB2_API gvdb2_status gvdb2_load_vbx(gvdb2_volume *v, const char *path);
  * the point view (base, count, stride, offset) and the translation stay the
  * same.  A caller that changes the positions in place (an advect step on the
  * same buffer) calls gvdb2_set_points again, or rebuilds the topology, before
- * the next splat or gather: either drops the bins.  Bins kept across moved
- * positions drop the points that left their cells (they splat and gather
- * nothing), as the reference's pnode from a stale InsertPoints would. */
+ * the next splat or gather: either drops the bins.  The bins hold a copy of
+ * the positions they were made from, so splats and gathers that reuse bins
+ * across positions moved in place see the positions of the binning, as the
+ * reference's kernels see its sorted point copy from a stale InsertPoints. */
 GVDB2_API gvdb2_status gvdb2_set_points(gvdb2_volume *v, gvdb2_points_view pos, gvdb2_points_view vel, gvdb2_points_view clr);
 
 /* Batched clouds (no counterpart in the reference, which holds one cloud
