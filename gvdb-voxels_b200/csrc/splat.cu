@@ -349,15 +349,16 @@ static_assert(ExtTile<GVDB2_KERNEL_CUBIC2>::E3 <= 2048 && ExtTile<GVDB2_KERNEL_T
 
 constexpr int kPartThreads = 256;
 constexpr int kPartChunk = 128; // points staged per pass, one per thread of the first 128
-// row stride of the staged weights: a point's taps (one row each) fall in
-// different banks
+// row stride of the staged x and y weights: a point's taps (one row each)
+// fall in different banks
 constexpr int kPartRow = kPartChunk + 1;
 static_assert(kSlicePts % kPartChunk == 0, "slices are whole chunks");
 
 template <int KERNEL, int NCH>
 constexpr size_t part_smem_bytes() {
     return sizeof(int32_t) * 2 * NCH * ExtTile<KERNEL>::CS +
-           sizeof(float) * (3 * Taps<KERNEL>::N + NCH) * kPartRow + sizeof(int32_t) * kPartChunk;
+           sizeof(float4) * 2 * kPartChunk + sizeof(float) * 2 * Taps<KERNEL>::N * kPartRow +
+           sizeof(int32_t) * kPartChunk;
 }
 
 // The fixed-point scale of R points whose largest |amount| is am, per the
@@ -399,9 +400,13 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
     constexpr int AS = 2 * X::CS; // accumulator words per channel (hi, lo)
     extern __shared__ __align__(16) unsigned char part_smem[];
     int32_t *acc = reinterpret_cast<int32_t *>(part_smem);
-    float(*pw)[kPartRow] = reinterpret_cast<float(*)[kPartRow]>(acc + NCH * AS);
-    float(*pa)[kPartRow] = pw + 3 * N;
-    int32_t *pb = reinterpret_cast<int32_t *>(pa + NCH);
+    // staged points: z weights and scaled amounts as float4 (a lane reads its
+    // two z weights in one load, the amounts in one broadcast), x and y
+    // weights in padded rows, the first tap's tile address
+    float4 *pz = reinterpret_cast<float4 *>(acc + NCH * AS);
+    float4 *pa = pz + kPartChunk;
+    float(*pw)[kPartRow] = reinterpret_cast<float(*)[kPartRow]>(pa + kPartChunk);
+    int32_t *pb = reinterpret_cast<int32_t *>(pw + 2 * N);
     __shared__ double inv_s[NCH];
     __shared__ int32_t amax_bits[NCH]; // largest |amount| of the cell's points, as float bits
     __shared__ int last;
@@ -476,16 +481,20 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
             const bool ok = (unsigned)fx <= 8u && (unsigned)fy <= 8u && (unsigned)fz <= 8u;
             const int r = threadIdx.x;
             pb[r] = ok ? fz * X::PS + fy * X::RS + fx : 0; // tile address of the point's first tap
+            float z4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int k = 0; k < N; k++) {
                 pw[k][r] = wx[k];
                 pw[N + k][r] = wy[k];
-                pw[2 * N + k][r] = wz[k];
+                z4[k] = wz[k];
             }
+            pz[r] = make_float4(z4[0], z4[1], z4[2], z4[3]);
             const float4 a = S.bin_amt[j];
             const float a4[4] = {a.x, a.y, a.z, a.w};
+            float s4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-            for (int c = 0; c < NCH; c++) pa[c][r] = ok ? a4[c] * scale[c] : 0.0f;
+            for (int c = 0; c < NCH; c++) s4[c] = ok ? a4[c] * scale[c] : 0.0f;
+            pa[r] = make_float4(s4[0], s4[1], s4[2], s4[3]);
         }
         __syncthreads();
         if constexpr (N == 4) {
@@ -495,10 +504,13 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
             for (int j = warp; j < cnt; j += kPartThreads / 32) {
                 const int a0 = pb[j] + loff;
                 const float wxy = pw[tx][j] * pw[N + ty][j];
-                const float w0 = wxy * pw[2 * N + tz0][j], w1 = wxy * pw[2 * N + tz0 + 1][j];
+                const float2 z2 = reinterpret_cast<const float2 *>(pz + j)[tz0 >> 1];
+                const float w0 = wxy * z2.x, w1 = wxy * z2.y;
+                const float4 a4 = pa[j];
+                const float am4[4] = {a4.x, a4.y, a4.z, a4.w};
 #pragma unroll
                 for (int c = 0; c < NCH; c++) {
-                    const float am = pa[c][j];
+                    const float am = am4[c];
                     part_add<X::CS>(acc + c * AS, a0, am * w0, inv2L, two2L);
                     part_add<X::CS>(acc + c * AS, a0 + X::PS, am * w1, inv2L, two2L);
                 }
@@ -511,9 +523,11 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
                 const int j = j0 + sub;
                 if (j >= cnt) continue;
                 const int a = pb[j] + loff;
-                const float w = pw[tx][j] * pw[N + ty][j] * pw[2 * N + tz][j];
+                const float4 z4 = pz[j], a4 = pa[j];
+                const float w = pw[tx][j] * pw[N + ty][j] * (tz ? z4.y : z4.x);
+                const float am4[4] = {a4.x, a4.y, a4.z, a4.w};
 #pragma unroll
-                for (int c = 0; c < NCH; c++) part_add<X::CS>(acc + c * AS, a, pa[c][j] * w, inv2L, two2L);
+                for (int c = 0; c < NCH; c++) part_add<X::CS>(acc + c * AS, a, am4[c] * w, inv2L, two2L);
             }
         }
     }
