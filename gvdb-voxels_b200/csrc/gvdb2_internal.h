@@ -150,6 +150,11 @@ struct Volume {
     // leaf lookup: level-0 key -> leaf pool index (flagged, i.e. linked, leaves only)
     DevBuf leafmap_keys, leafmap_vals;
     uint32_t leafmap_mask = 0;
+    // the leaf map holds exactly the leaves linked in the tree (true after a
+    // rebuild; pools adopted from a file or the host tree may hold linked
+    // leaves that are not flagged), so the incremental marking may look
+    // leaves up there instead of walking from the root
+    bool leafmap_is_tree = false;
 
     // scratch for the rebuild
     DevBuf hs_keys[2];        // hash sets (base, box)

@@ -649,6 +649,7 @@ gvdb2_status build_from_keys(Volume *v, const int64_t nB[], const int64_t nE[], 
     GV_CUDA(v, v->leafmap_vals.ensure(sizeof(int32_t) * lcap, s));
     GV_CUDA(v, cudaMemsetAsync(v->leafmap_keys.p, 0xFF, sizeof(uint64_t) * lcap, s));
     v->leafmap_mask = lcap - 1;
+    v->leafmap_is_tree = true;
     GV_CUDA(v, cudaMemsetAsync(&dev_words(v)->status, 0, sizeof(int32_t), s));
 
     for (int l = 0; l < depth; l++) {
@@ -1434,57 +1435,84 @@ __device__ bool tv_slot(const TreeView &T, int plev, const Node *pn, const int32
 
 // Step 1: marks and new keys.  A new key is lev<<3b | x<<2b | y<<b | z in
 // units of the level's range, which sorts like the reference's keys.
-__global__ void k_incre_mark(PointsView pos, int64_t n, float3 orig, float radius, TreeView T, int b, uint64_t *hs,
-                             uint32_t mask, int32_t *marker, int64_t total, int32_t *count, int32_t *status) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float3 p = load_f3(pos, i);
-    float w[3] = {p.x + orig.x, p.y + orig.y, p.z + orig.z};
-    if (w[0] < 0 || w[1] < 0 || w[2] < 0) return;
-    if (T.cnt[T.depth] < 1) return;
-    const int3 o3 = point_origin(pos, i);
-    const int o[3] = {o3.x, o3.y, o3.z};
+// Warps share their points' nodes: in round t each lane offers its box's
+// t-th node, and of the lanes offering the same node the lowest looks it up.
+__global__ void k_incre_mark(PointsView pos, int64_t n, float3 orig, float radius, TreeView T, KeyGeom g,
+                             uint64_t *hs, uint32_t mask, int32_t *marker, int64_t total, int32_t *count,
+                             int32_t *status, const uint64_t *lk, const int32_t *lv, uint32_t lmask, int use_map) {
+    // every lane of a warp takes part in the rounds (match_any): a thread
+    // without a point offers no nodes
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    bool valid = i < n && T.cnt[T.depth] >= 1;
+    float w[3] = {0, 0, 0};
+    int o[3] = {0, 0, 0};
+    if (valid) {
+        const float3 p = load_f3(pos, i);
+        w[0] = p.x + orig.x;
+        w[1] = p.y + orig.y;
+        w[2] = p.z + orig.z;
+        if (w[0] < 0 || w[1] < 0 || w[2] < 0) valid = false;
+        const int3 o3 = point_origin(pos, i);
+        o[0] = o3.x;
+        o[1] = o3.y;
+        o[2] = o3.z;
+    }
     const Node *root = &T.nodes[T.depth][0];
     const int64_t rr_root = T.range[T.depth];
     int bmin[3], bmax[3];
     for (int a = 0; a < 3; a++) {
-        int iw = (int)w[a];
+        const int iw = (int)w[a];
         bmin[a] = (int)((float)iw - radius);
         bmax[a] = (int)((float)iw + radius);
     }
     for (int lev = 0; lev < T.depth; lev++) {
         const int rr = (int)T.range[lev];
-        // node corners in absolute coordinates; for a batched cloud whose
-        // origin is a multiple of the range they are the cloud's own corners
-        // (C truncation included) shifted by the origin
-        int clo[3], chi[3];
-        for (int a = 0; a < 3; a++) {
-            if (o[a] % rr == 0) {
-                clo[a] = bmin[a] / rr * rr + o[a];
-                chi[a] = bmax[a] / rr * rr + o[a];
-            } else {
-                clo[a] = (max(bmin[a], 0) + o[a]) / rr * rr;
-                chi[a] = (bmax[a] + o[a]) / rr * rr;
+        // the box's node corners in absolute coordinates; for a batched cloud
+        // whose origin is a multiple of the range they are the cloud's own
+        // corners (C truncation included) shifted by the origin
+        int clo[3] = {0, 0, 0}, nn[3] = {0, 0, 0};
+        int cnt = 0;
+        if (valid) {
+            for (int a = 0; a < 3; a++) {
+                int chi;
+                if (o[a] % rr == 0) {
+                    clo[a] = bmin[a] / rr * rr + o[a];
+                    chi = bmax[a] / rr * rr + o[a];
+                } else {
+                    clo[a] = (max(bmin[a], 0) + o[a]) / rr * rr;
+                    chi = (bmax[a] + o[a]) / rr * rr;
+                }
+                nn[a] = chi >= clo[a] ? (chi - clo[a]) / rr + 1 : 0;
+            }
+            cnt = nn[0] * nn[1] * nn[2];
+        }
+        const int rounds = __reduce_max_sync(0xffffffffu, cnt);
+        for (int t = 0; t < rounds; t++) {
+            bool has = t < cnt;
+            int nd[3] = {0, 0, 0};
+            if (has) { // x outer, z inner, as the reference's loops
+                nd[0] = clo[0] + (t / (nn[1] * nn[2])) * rr;
+                nd[1] = clo[1] + (t / nn[2] % nn[1]) * rr;
+                nd[2] = clo[2] + (t % nn[2]) * rr;
+                for (int a = 0; a < 3; a++)
+                    has = has && !(nd[a] < root->mPos[a] || (int64_t)nd[a] >= root->mPos[a] + rr_root);
+            }
+            const uint64_t bkey = has ? pack_key(nd[0] / rr, nd[1] / rr, nd[2] / rr, g.b) : 0;
+            const uint64_t key = has ? (((uint64_t)lev << (3 * g.b)) | bkey) : ~0ull;
+            const unsigned peers = __match_any_sync(0xffffffffu, (unsigned long long)key);
+            if (!has || lane != __ffs(peers) - 1) continue;
+            // the leaf map holds exactly the leaves linked in the tree, so a
+            // level-0 lookup there finds what the walk from the root finds
+            const int64_t pid = (lev == 0 && use_map) ? (int64_t)hm_lookup(lk, lv, lmask, bkey) : tv_pos_parent(T, nd, lev);
+            if (pid == -1) {
+                const int r = hs_insert(hs, mask, key);
+                if (r > 0) atomicAdd(count, 1);
+                if (r < 0) atomicOr(status, kDevHashFull);
+            } else if (lev == 0 && pid >= 0 && pid < total) {
+                marker[pid] = 1;
             }
         }
-        int nd[3];
-        for (nd[0] = clo[0]; nd[0] <= chi[0]; nd[0] += rr)
-            for (nd[1] = clo[1]; nd[1] <= chi[1]; nd[1] += rr)
-                for (nd[2] = clo[2]; nd[2] <= chi[2]; nd[2] += rr) {
-                    bool out = false;
-                    for (int a = 0; a < 3; a++)
-                        out |= nd[a] < root->mPos[a] || (int64_t)nd[a] >= root->mPos[a] + rr_root;
-                    if (out) continue;
-                    int64_t pid = tv_pos_parent(T, nd, lev);
-                    if (pid == -1) {
-                        uint64_t key = ((uint64_t)lev << (3 * b)) | pack_key(nd[0] / rr, nd[1] / rr, nd[2] / rr, b);
-                        int r = hs_insert(hs, mask, key);
-                        if (r > 0) atomicAdd(count, 1);
-                        if (r < 0) atomicOr(status, kDevHashFull);
-                    } else if (lev == 0 && pid >= 0 && pid < total) {
-                        marker[pid] = 1;
-                    }
-                }
     }
 }
 
@@ -1648,8 +1676,10 @@ gvdb2_status incremental_activate(Volume *v, int n, float radius, const float or
         k_init_markers<<<grid_for(total, 256, 1ll << 31), 256, 0, s>>>(v->pool_ptr(0), total, accum ? 1 : 0, marker);
         if (n > 0)
             k_incre_mark<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(
-                v->pos, n, make_float3(orig[0], orig[1], orig[2]), radius, tree_view(v), b, v->hs_keys[0].as<uint64_t>(),
-                cap - 1, marker, total, dev_words(v)->count, &dev_words(v)->status);
+                v->pos, n, make_float3(orig[0], orig[1], orig[2]), radius, tree_view(v), g,
+                v->hs_keys[0].as<uint64_t>(), cap - 1, marker, total, dev_words(v)->count, &dev_words(v)->status,
+                v->leafmap_keys.as<uint64_t>(), v->leafmap_vals.as<int32_t>(), v->leafmap_mask,
+                v->leafmap_is_tree ? 1 : 0);
         GV_CUDA(v, cudaGetLastError());
         GV_TRY(read_words(v));
         nnew = host_words(v)->count[0];
@@ -1715,6 +1745,7 @@ gvdb2_status incremental_activate(Volume *v, int n, float radius, const float or
     GV_CUDA(v, v->leafmap_vals.ensure(sizeof(int32_t) * lcap, s));
     GV_CUDA(v, cudaMemsetAsync(v->leafmap_keys.p, 0xFF, sizeof(uint64_t) * lcap, s));
     v->leafmap_mask = lcap - 1;
+    v->leafmap_is_tree = true;
     GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count, 0, sizeof(int32_t) * 8 + sizeof(int32_t), s));
     k_leafmap_fill<<<grid_for(v->pool_cnt[0], 256, 1ll << 31), 256, 0, s>>>(
         v->pool_ptr(0), v->pool_cnt[0], g, v->leafmap_keys.as<uint64_t>(), v->leafmap_vals.as<int32_t>(),
@@ -1757,6 +1788,7 @@ gvdb2_status adopt_pools(Volume *v, int depth) {
     GV_CUDA(v, v->leafmap_vals.ensure(sizeof(int32_t) * lcap, s));
     GV_CUDA(v, cudaMemsetAsync(v->leafmap_keys.p, 0xFF, sizeof(uint64_t) * lcap, s));
     v->leafmap_mask = lcap - 1;
+    v->leafmap_is_tree = false;
     GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count, 0, sizeof(int32_t) * 8 + sizeof(int32_t), s));
     if (v->pool_cnt[0] > 0)
         k_leafmap_fill<<<grid_for(v->pool_cnt[0], 256, 1ll << 31), 256, 0, s>>>(
