@@ -116,11 +116,20 @@ __global__ void k_bin_keys(const int32_t *pbin, int64_t n, uint64_t *keys, int32
     vals[i] = (int32_t)i;
 }
 
-__global__ void k_bin_fill(const int32_t *pbin, const int32_t *prank, int64_t n, const uint32_t *off, int32_t *perm) {
+// Each binned point's entry of the bin order: perm[j] = i and, in the same
+// pass, bin_pos[j] = its translated position and cloud index (as
+// k_bin_pack_pos writes them; the positions are read in point order).
+__global__ void k_bin_fill(const int32_t *pbin, const int32_t *prank, int64_t n, const uint32_t *off, int32_t *perm,
+                           PointsView pos, float3 trans, float4 *bin_pos) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int32_t b = pbin[i];
-    if (b >= 0) perm[off[b] + prank[i]] = (int32_t)i;
+    if (b < 0) return;
+    const int64_t j = (int64_t)off[b] + prank[i];
+    perm[j] = (int32_t)i;
+    const float3 q = load_f3(pos, i);
+    const int32_t cloud = pos.cloud ? pos.cloud[i] : -1;
+    bin_pos[j] = make_float4(q.x + trans.x, q.y + trans.y, q.z + trans.z, __int_as_float(cloud));
 }
 
 // bin_pos[j] = the translated position of the point at bin-order entry j
@@ -372,14 +381,16 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
         uint64_t *keys = v->tmp_c.as<uint64_t>();
         k_bin_keys<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pbin.as<int32_t>(), n, keys, v->perm.as<int32_t>());
         GV_TRY(radix_sort_u64(v, keys, v->perm.as<int32_t>(), n, 0, 32));
-    } else if (n > 0) {
-        k_bin_fill<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pbin.as<int32_t>(), v->prank.as<int32_t>(), n,
-                                                               v->reg_off.as<uint32_t>(), v->perm.as<int32_t>());
-        GV_CUDA(v, cudaGetLastError());
     }
-    // the points' positions in bin order
+    // the points' positions in bin order: with the bin order itself from
+    // the ranks, else from the sorted order
     GV_CUDA(v, v->bin_pos.ensure(sizeof(float4) * (size_t)std::max(n, 1), s));
-    if (n > 0) {
+    if (n > 0 && !v->deterministic) {
+        k_bin_fill<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pbin.as<int32_t>(), v->prank.as<int32_t>(), n,
+                                                               v->reg_off.as<uint32_t>(), v->perm.as<int32_t>(), v->pos,
+                                                               t, v->bin_pos.as<float4>());
+        GV_CUDA(v, cudaGetLastError());
+    } else if (n > 0) {
         k_bin_pack_pos<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->perm.as<int32_t>(), v->reg_off.as<uint32_t>(), nreg,
                                                                   v->pos, t, v->bin_pos.as<float4>());
         GV_CUDA(v, cudaGetLastError());
