@@ -1023,8 +1023,13 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
                     acc[z][xp][c] = (c & 1) ? make_float2(a0.y, a1.y) : make_float2(a0.x, a1.x);
                 }
     }
-    // cells with a dense cell around get its partials from k_scatter_merge
-    if (any_part && lane == 0) S.merge_list[atomicAdd(S.merge_cnt, 1u)] = (int32_t)cell;
+    // cells with a dense cell around get its partials from k_scatter_merge;
+    // one without sources of its own (all zero here) is listed as ~cell and
+    // left for the merge to write
+    if (any_part) {
+        if (lane == 0) S.merge_list[atomicAdd(S.merge_cnt, 1u)] = total_src == 0 ? ~(int32_t)cell : (int32_t)cell;
+        if (total_src == 0) return;
+    }
     // each lane writes its 4 x 4 voxels of every channel once
     const int a = S.apron, tl = S.tile;
     const int64_t base = slot * S.tvox + (int64_t)(kCell * cx + 4 * q + a);
@@ -1044,7 +1049,8 @@ __global__ void __launch_bounds__(32 * kScWarps, GVDB2_SC_MIN_BLOCKS) k_scatter_
 // (those with a dense cell among their 27): a CTA per listed cell (CTAs
 // past the list's end return), a thread per interior voxel, which adds, in
 // the order of kMergeMap, the partials that cover the voxel to the sum the
-// owner-computes pass wrote.
+// owner-computes pass wrote -- or writes them, for a cell listed as ~cell
+// (no owner sources: its sum is 0, and 0 + x is x).
 template <int KERNEL, int NCH>
 __global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S) {
     using X = ExtTile<KERNEL>;
@@ -1052,7 +1058,10 @@ __global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S) {
     const uint32_t li = blockIdx.x;
     if (li >= *S.merge_cnt) return;
     {
-        const int64_t cell = S.merge_list[li];
+        const int32_t entry = S.merge_list[li];
+        const bool overwrite = entry < 0; // no owner sum to add to
+        const int64_t cell = overwrite ? ~entry : entry;
+        if (!in_range(S.lim, cell, S.ncell, 23)) return;
         int64_t slot;
         int cx, cy, cz;
         cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
@@ -1092,7 +1101,7 @@ __global__ void __launch_bounds__(512) k_scatter_merge(SplatArgs S) {
         const int64_t at = slot * S.tvox + ((int64_t)(kCell * cz + vz + a) * tl + (kCell * cy + vy + a)) * tl +
                            (kCell * cx + vx + a);
 #pragma unroll
-        for (int c = 0; c < NCH; c++) S.chan[c][at] += add[c];
+        for (int c = 0; c < NCH; c++) S.chan[c][at] = overwrite ? add[c] : S.chan[c][at] + add[c];
     }
 }
 
