@@ -544,9 +544,9 @@ def run_ours(a):
 # launch moves about this many bytes x bricks.
 TRAFFIC_PER_BRICK = {
     # k_pack_amounts, k_scatter_part, k_scatter_cells, k_scatter_merge
-    "scatter": ((33.6 + 0.9) + (66.8 + 12.7) + (20.7 + 18.9) + (99.4 + 1.3)) * 1e6 / 3240,
+    "scatter": ((33.6 + 1.0) + (66.8 + 14.0) + (8.9 + 7.4) + (88.4 + 4.6)) * 1e6 / 3240,
     # k_gather_tile, k_gather_light
-    "gather": ((70.5 + 3.1) + (12.4 + 0.0)) * 1e6 / 3240,
+    "gather": ((70.6 + 2.7) + (12.4 + 0.0)) * 1e6 / 3240,
 }
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 2,097,152-point block at the "
                   "16,777,216-point step's density, scaled by bricks")
