@@ -914,20 +914,26 @@ constexpr int64_t kMaxGridBits = 1ll << 28; // bitmap path up to 2^28 bricks (32
 
 // Node key sets through brick bitmaps; *used = false when the grid would be
 // too large or a brick fell outside it (then nothing was changed).
+// kmax: the box reaches kmax * radius above a point (2 for the full
+// rebuild's extra bricks, 1 for the incremental box); force_box: the box set
+// even for radius < 1 (the incremental box).
 gvdb2_status key_sets_bitmap(Volume *v, int n, float radius, const float orig[3], const KeyGeom &g, int64_t nB[],
-                             int64_t nE[], bool *used) {
+                             int64_t nE[], bool *used, float kmax = 2.0f, bool force_box = false) {
     *used = false;
     cudaStream_t s = v->stream;
     const int depth = v->depth;
-    const bool do_box = radius >= 1.0f;
+    const bool do_box = force_box || radius >= 1.0f;
     const float r = do_box ? radius : 0.0f;
     BitGrid G[kMaxLev];
     int64_t off[kMaxLev + 1];
     off[0] = 0;
     int lo0[3], hi0[3];
     for (int a = 0; a < 3; a++) {
-        const float lo_v = std::max(0.0f, std::floor(v->posmin[a] - r - 2.0f));
-        const float hi_v = v->posmax[a] + 2.0f * r + 2.0f;
+        // the box's reach below and above the points (a forced box of radius
+        // < 1 still reaches the voxel below and above)
+        const float below = force_box ? std::max(r, 1.0f) : r, above = force_box ? std::max(kmax * r, 1.0f) : 2.0f * r;
+        const float lo_v = std::max(0.0f, std::floor(v->posmin[a] - below - 2.0f));
+        const float hi_v = v->posmax[a] + above + 2.0f;
         if (!(hi_v < 2.0e9f)) return GVDB2_OK;
         lo0[a] = std::max(g.lo[a], (int)lo_v >> g.log2r0);
         hi0[a] = std::min(g.lo[a] + g.span - 1, (int)hi_v >> g.log2r0);
@@ -962,11 +968,11 @@ gvdb2_status key_sets_bitmap(Volume *v, int n, float radius, const float orig[3]
         // as many CTAs as fit on an SM (each keeps its own copy of the bitmaps,
         // flushed once), so that the points' loads overlap
         const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / std::max<size_t>(smem, 1)));
-        k<<<std::min(grid_for(n, 256), per_sm * kSmCount), 256, smem, s>>>(v->pos, n, t3, radius, 2.0f,
+        k<<<std::min(grid_for(n, 256), per_sm * kSmCount), 256, smem, s>>>(v->pos, n, t3, radius, kmax,
                                                                             do_box ? 1 : 0, g, G[0],
                                                                             &dev_words(v)->status);
     } else if (n > 0) {
-        k_mark_bits<false><<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t3, radius, 2.0f, do_box ? 1 : 0, g,
+        k_mark_bits<false><<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t3, radius, kmax, do_box ? 1 : 0, g,
                                                                         G[0], &dev_words(v)->status);
     }
     for (int l = 1; l < depth; l++) {
@@ -1516,6 +1522,29 @@ __global__ void k_incre_mark(PointsView pos, int64_t n, float3 orig, float radiu
     }
 }
 
+// The incremental marking from the activation box's unique nodes (the box
+// bitmaps' keys of one level and set): a node the tree has marks its leaf,
+// a node it lacks goes into the new-node set.
+__global__ void k_incre_keys(const uint64_t *bkeys, int64_t nk, int lev, TreeView T, KeyGeom g, uint64_t *hs,
+                             uint32_t mask, int32_t *marker, int64_t total, int32_t *count, int32_t *status,
+                             const uint64_t *lk, const int32_t *lv, uint32_t lmask, int use_map) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nk || T.cnt[T.depth] < 1) return;
+    const uint64_t bkey = bkeys[i];
+    int nd[3];
+    unpack_key(bkey, g.b, nd[0], nd[1], nd[2]);
+    const int rr = (int)T.range[lev];
+    for (int a = 0; a < 3; a++) nd[a] *= rr;
+    const int64_t pid = (lev == 0 && use_map) ? (int64_t)hm_lookup(lk, lv, lmask, bkey) : tv_pos_parent(T, nd, lev);
+    if (pid == -1) {
+        const int r = hs_insert(hs, mask, ((uint64_t)lev << (3 * g.b)) | bkey);
+        if (r > 0) atomicAdd(count, 1);
+        if (r < 0) atomicOr(status, kDevHashFull);
+    } else if (lev == 0 && pid >= 0 && pid < total) {
+        marker[pid] = 1;
+    }
+}
+
 __global__ void k_init_markers(const Node *leaves, int64_t total, int accum, int32_t *marker) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < total) marker[i] = accum ? (int32_t)leaves[i].mFlags : 0;
@@ -1666,7 +1695,13 @@ gvdb2_status incremental_activate(Volume *v, int n, float radius, const float or
     GV_CUDA(v, v->tmp_c.ensure(sizeof(int32_t) * (size_t)total, s));
     int32_t *marker = v->tmp_c.as<int32_t>();
 
-    // 1. marks and new keys, into a hash set sized from the pool (grown on overflow)
+    // 1. marks and new keys, into a hash set sized from the pool (grown on
+    // overflow).  The box's nodes come from brick bitmaps when the cloud's
+    // extent allows (each level's nodes once, looked up once), else from
+    // every point's box.
+    int64_t nB[kMaxLev] = {0}, nE[kMaxLev] = {0};
+    bool boxed = false;
+    if (n > 0) GV_TRY(key_sets_bitmap(v, n, radius, orig, g, nB, nE, &boxed, 1.0f, true));
     uint32_t cap = next_pow2((uint64_t)std::max<int64_t>(4 * total, 1 << 16));
     int64_t nnew = 0;
     for (int attempt = 0;; attempt++) {
@@ -1674,7 +1709,18 @@ gvdb2_status incremental_activate(Volume *v, int n, float radius, const float or
         GV_CUDA(v, cudaMemsetAsync(v->hs_keys[0].p, 0xFF, sizeof(uint64_t) * cap, s));
         GV_CUDA(v, cudaMemsetAsync(dev_words(v)->count, 0, sizeof(int32_t) * 8 + sizeof(int32_t), s));
         k_init_markers<<<grid_for(total, 256, 1ll << 31), 256, 0, s>>>(v->pool_ptr(0), total, accum ? 1 : 0, marker);
-        if (n > 0)
+        if (boxed) {
+            const TreeView T = tree_view(v);
+            for (int l = 0; l < depth; l++)
+                for (int set = 0; set < 2; set++) {
+                    const int64_t nk = set ? nE[l] : nB[l];
+                    if (nk > 0)
+                        k_incre_keys<<<grid_for(nk, 256, 1ll << 31), 256, 0, s>>>(
+                            v->lev_keys[l][set].as<uint64_t>(), nk, l, T, g, v->hs_keys[0].as<uint64_t>(), cap - 1,
+                            marker, total, dev_words(v)->count, &dev_words(v)->status, v->leafmap_keys.as<uint64_t>(),
+                            v->leafmap_vals.as<int32_t>(), v->leafmap_mask, v->leafmap_is_tree ? 1 : 0);
+                }
+        } else if (n > 0)
             k_incre_mark<<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(
                 v->pos, n, make_float3(orig[0], orig[1], orig[2]), radius, tree_view(v), g,
                 v->hs_keys[0].as<uint64_t>(), cap - 1, marker, total, dev_words(v)->count, &dev_words(v)->status,
