@@ -558,7 +558,7 @@ STAGE_KERNELS = {"scatter": "scatter stage: k_pack_amounts<4> + k_scatter_part<c
 # ----------------------------------------------------------------------------
 # the rest of the metric, each measured in the same run (N = 1)
 # ----------------------------------------------------------------------------
-EXTRA_LEGS = ("incremental", "config1_4m", "adjoint", "batched", "vs_ref_kernels")
+EXTRA_LEGS = ("incremental", "config1_4m", "adjoint", "batched", "vs_ref_kernels", "nanovdb_export")
 # legs left out of the main line, with the reason (none)
 HELD_LEGS = {}
 
@@ -578,6 +578,8 @@ def run_leg(name, warmup):
         return measure_batched(steps=3, warmup=1)
     if name == "vs_ref_kernels":
         return extra_ref_kernels()
+    if name == "nanovdb_export":
+        return extra_nanovdb(warmup)
     raise ValueError(name)
 
 
@@ -607,6 +609,8 @@ def run_extras(a):
         summary["batched_over_loop"] = out["batched"]["speedup_vs_loop"]
     if isinstance(out.get("vs_ref_kernels"), dict) and "speedup_device" in out["vs_ref_kernels"]:
         summary["vs_ref_kernels_speedup"] = out["vs_ref_kernels"]["speedup_device"]
+    if isinstance(out.get("nanovdb_export"), dict) and "float" in out["nanovdb_export"]:
+        summary["nanovdb_export_ms"] = out["nanovdb_export"]["float"]["ms"]
     out.update(summary)
     return out
 
@@ -626,6 +630,49 @@ def extra_incremental(pos, vel, warmup):
         del pipe
     res["incremental_over_full_speedup"] = res["full"]["ms_per_step"] / res["incremental"]["ms_per_step"]
     res["workload"] = "16,777,216-pt dam block, 10 timed advect steps (dt 0.1), stale leaves kept by the state machine"
+    return res
+
+
+def extra_nanovdb(warmup):
+    """ExportToNanoVDB of the 16M-point step's volume (after one step): a
+    float grid of channel 0 (mass) and a Vec3f grid of channels 1-3
+    (momentum), each call timed end to end on the host (the call returns
+    with the buffer complete: device passes, one read-back of the level-2
+    headers, the root finished on the host and written back).  Algorithmic
+    bytes: the live bricks' interiors read from the atlas plus the buffer
+    written."""
+    import ctypes
+    import torch
+    import gvdb2.workloads as wl
+    w = WORKLOADS["dam16m"]
+    pos, vel = wl.dam_block(sites=w["sites"], spacing=w["spacing"])
+    pipe = Pipeline(0, pos, vel, full_rebuild=True)
+    timed_steps(pipe, 1, 1)
+    v = pipe.v
+    inf = v.info()
+    peak, kind = peaks()
+    res = {"workload": w["desc"] + ", the volume after one step", "leaves": int(inf.pool_count[0]),
+           "level1": int(inf.pool_count[1]), "level2": int(inf.pool_count[2]), "timed_calls": 10}
+    for name, chans in (("float", [0]), ("vec3f", [1, 2, 3])):
+        nv = len(chans)
+        size = ctypes.c_size_t()
+        v._check(v._L.gvdb2_nanovdb_size(v._h, nv, ctypes.byref(size)), "nanovdb_size")
+        buf = torch.empty(int(size.value), dtype=torch.uint8, device=pipe.dev)
+        ch, bg = (ctypes.c_int * nv)(*chans), (ctypes.c_float * nv)(*([0.0] * nv))
+
+        def call():
+            v._check(v._L.gvdb2_export_nanovdb(v._h, nv, ch, bg, b"dam16m", 0, ctypes.c_void_p(buf.data_ptr()),
+                                               int(size.value)), "export_nanovdb")
+        for _ in range(max(3, warmup)):
+            call()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(10):
+            call()
+        ms = (time.perf_counter() - t0) * 1e3 / 10
+        alg = int(inf.atlas_slots) * int(inf.res[0]) ** 3 * 4 * nv + int(size.value)
+        res[name] = {"ms": ms, "buffer_bytes": int(size.value), "algorithmic_bytes": alg,
+                     "gbs": alg / ms / 1e6, "frac_of_hbm": alg / ms / 1e6 / peak, "peak": f"{peak:.1f} GB/s {kind}"}
     return res
 
 

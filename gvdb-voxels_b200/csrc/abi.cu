@@ -200,6 +200,17 @@ gvdb2_status gvdb2_load_vbx(gvdb2_volume *h, const char *path) {
     return gvdb2::load_vbx(VOL(h), path);
 }
 
+gvdb2_status gvdb2_nanovdb_size(gvdb2_volume *h, int value_type, size_t *bytes) {
+    CHECK_HANDLE(h);
+    return gvdb2::nanovdb_size(VOL(h), value_type, bytes);
+}
+
+gvdb2_status gvdb2_export_nanovdb(gvdb2_volume *h, int value_type, const int32_t *chans, const float *background,
+                                  const char *grid_name, int32_t grid_class, void *dst_device, size_t dst_bytes) {
+    CHECK_HANDLE(h);
+    return gvdb2::export_nanovdb(VOL(h), value_type, chans, background, grid_name, grid_class, dst_device, dst_bytes);
+}
+
 gvdb2_status gvdb2_set_channel_default(gvdb2_volume *h, int cx, int cy, int cz) {
     CHECK_HANDLE(h);
     if (cx < 1 || cy < 1 || cz < 1) return gvdb2::fail(VOL(h), GVDB2_ERR_ARG, "bad axis counts");

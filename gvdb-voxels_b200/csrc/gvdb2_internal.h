@@ -282,6 +282,10 @@ gvdb2_status adopt_pools(Volume *v, int depth);
 gvdb2_status activate_space(Volume *v, const float *xyz, int64_t n, uint64_t *out);
 gvdb2_status compact_pools(Volume *v);
 gvdb2_status save_vbx(Volume *v, const char *path);
+// ---- nanovdb.cu ----
+gvdb2_status nanovdb_size(Volume *v, int value_type, size_t *bytes);
+gvdb2_status export_nanovdb(Volume *v, int value_type, const int32_t *chans, const float *background,
+                            const char *grid_name, int32_t grid_class, void *dst_device, size_t dst_bytes);
 gvdb2_status load_vbx(Volume *v, const char *path);
 gvdb2_status update_neighbors(Volume *v);
 gvdb2_status clear_channel(Volume *v, int chan);

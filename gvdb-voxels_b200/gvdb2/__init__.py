@@ -13,8 +13,8 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import (KERNEL_CUBIC2, KERNEL_TENT1, OPT_DETERMINISTIC, T_FLOAT, GvdbError, Info, PointsView,
-                   declared_symbols)
+from ._lib import (KERNEL_CUBIC2, KERNEL_TENT1, NV_FLOAT, NV_VEC3F, OPT_DETERMINISTIC, T_FLOAT, GvdbError, Info,
+                   PointsView, declared_symbols)
 
 NODE_DTYPE = np.dtype([
     ("mLev", np.uint8), ("mFlags", np.uint8), ("mPriority", np.uint8), ("pad", np.uint8),
@@ -207,6 +207,26 @@ class VolumeGVDB:
     def LoadVBX(self, fname):
         """Replaces the volume with a VBX file's (V:507-685)."""
         self._check(self._L.gvdb2_load_vbx(self._h, os.fsencode(fname)), "LoadVBX")
+
+    def ExportToNanoVDB(self, chans, background=0.0, grid_name="", grid_class=0):
+        """The volume as one NanoVDB-form device buffer (ExportToNanoVDB,
+        gNanoVDB/gvdb_export_nanovdb.cpp:379-700): a uint8 torch tensor on
+        the volume's device, laid out as gvdb2_nv_* in include/gvdb2.h.  One
+        channel gives a float grid, three channels (x, y, z) a Vec3f grid."""
+        import torch
+        chans = [int(c) for c in chans]
+        nv = {1: NV_FLOAT, 3: NV_VEC3F}.get(len(chans))
+        if nv is None:
+            raise GvdbError(1, "ExportToNanoVDB", "one or three channels")
+        bg = [float(b) for b in np.broadcast_to(np.asarray(background, np.float32), (len(chans),))]
+        size = ctypes.c_size_t()
+        self._check(self._L.gvdb2_nanovdb_size(self._h, nv, ctypes.byref(size)), "ExportToNanoVDB")
+        out = torch.empty(max(int(size.value), 1), dtype=torch.uint8, device=f"cuda:{self.device}")
+        self._check(self._L.gvdb2_export_nanovdb(self._h, nv, (ctypes.c_int * len(chans))(*chans),
+                                                 (ctypes.c_float * len(bg))(*bg), os.fsencode(grid_name),
+                                                 int(grid_class), ctypes.c_void_p(out.data_ptr()), int(size.value)),
+                    "ExportToNanoVDB")
+        return out[:int(size.value)]
 
     def InsertPointsSubcell_FP16(self, subcell_size, num_pnts, radius, trans=(0, 0, 0)):
         """InsertPointsSubcell with 16-bit list entries (V:5094-5189); returns the list length."""

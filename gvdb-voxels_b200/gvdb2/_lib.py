@@ -18,6 +18,8 @@ T_FLOAT = 3
 KERNEL_TENT1 = 1
 KERNEL_CUBIC2 = 2
 OPT_DETERMINISTIC = 1
+NV_FLOAT = 1
+NV_VEC3F = 3
 
 
 class PointsView(ctypes.Structure):
@@ -76,6 +78,8 @@ _SIGS = {
     "gvdb2_get_transform": [_vp, _fp, _fp, _fp, _fp],
     "gvdb2_save_vbx": [_vp, ctypes.c_char_p],
     "gvdb2_load_vbx": [_vp, ctypes.c_char_p],
+    "gvdb2_nanovdb_size": [_vp, _i32, ctypes.POINTER(ctypes.c_size_t)],
+    "gvdb2_export_nanovdb": [_vp, _i32, _ip, _fp, ctypes.c_char_p, _i32, _vp, ctypes.c_size_t],
     "gvdb2_gather_level_set_fp16": [_vp, _i32, _i32, _f32, _fp, _ip, _i32, _i32],
     "gvdb2_scatter_density": [_vp, _i32, _f32, _f32, _fp, _i32, _i32],
     "gvdb2_gather_density": [_vp, _i32, _i32, _f32, _fp, _ip, _i32, _i32, _i32],

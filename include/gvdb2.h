@@ -117,6 +117,98 @@ GVDB2_API gvdb2_status gvdb2_save_vbx(gvdb2_volume *v, const char *path);
  * other than 5 levels return GVDB2_ERR_UNSUPPORTED. */
 GVDB2_API gvdb2_status gvdb2_load_vbx(gvdb2_volume *v, const char *path);
 
+/* ---- NanoVDB-form export (gNanoVDB/gvdb_export_nanovdb.h:65-66) ----
+ * ExportToNanoVDB (gvdb_export_nanovdb.cpp:379-700, cuda_export_nanovdb.cu:
+ * 76-432) written into one device buffer the caller owns, in NanoVDB's
+ * section order: grid header (grid, tree and root fields), root tiles,
+ * level-2 nodes, level-1 nodes, leaves.  Each GVDB node of levels 0-2 becomes
+ * the record of the same pool index; values come from the atlas channel(s):
+ * GVDB2_NV_FLOAT reads chans[0], GVDB2_NV_VEC3F reads chans[0..2] as x, y, z
+ * (the reference reads one T_FLOAT3 channel; channels here are floats).
+ * Records are this library's (below), not NanoVDB's own structs, whose byte
+ * layout depends on the NanoVDB version: a consumer with NanoVDB copies the
+ * fields across.  Field rules, as the reference sets them:
+ *   leaf: value mask all on; values in (x*T + y)*T + z order; min/max over
+ *     the brick; bbox_min = mPos, bbox_dif = T (the brick width); a leaf left
+ *     stale by an incremental rebuild has no atlas brick and is written as
+ *     zeros (the record the reference's exporter means to leave for nodes
+ *     no longer in the tree);
+ *   level-1/2 node: value mask off; child mask and table in (x*T + y)*T + z
+ *     order (GVDB's child lists are (z*T + y)*T + x), a child's pool index or
+ *     the background; offset = nodes of the level - index; min/max and box
+ *     over the children's;
+ *   root: one tile per level-2 node, keyed by its box corner >> (sum of the
+ *     three log2 dims), 21 bits per axis, z lowest, sorted by key (ties by
+ *     node index); box and min/max over those nodes (a float grid's maximum
+ *     starts at FLT_MIN, as the reference's numeric_limits<float>::min());
+ *     active voxels = leaves in the pool x T^3.
+ * Log2 dims of levels 0-2 must lie in [2, 7] and the volume needs at least
+ * three levels.  gvdb2_nanovdb_size gives the buffer size; the export checks
+ * it and returns GVDB2_ERR_CAPACITY when dst_bytes is smaller.  The device
+ * work runs on the volume's stream; the root is finished on the host from the
+ * level-2 nodes' headers (one read-back), as the reference does. */
+#define GVDB2_NV_MAGIC 0x31564e3242445647ull /* "GVDB2NV1" */
+#define GVDB2_NV_FLOAT 1                     /* GridType Float: one float per voxel */
+#define GVDB2_NV_VEC3F 3                     /* GridType Vec3f: three floats per voxel */
+#define GVDB2_NV_HEADER 64                   /* bytes of a node's or a leaf's header */
+
+typedef struct gvdb2_nv_grid {
+    uint64_t magic;           /* GVDB2_NV_MAGIC */
+    uint64_t total_bytes;     /* whole buffer */
+    uint32_t value_type;      /* GVDB2_NV_FLOAT or GVDB2_NV_VEC3F (floats per value) */
+    uint32_t grid_class;      /* as given (nanovdb::GridClass numbering) */
+    int32_t log2dim[3];       /* leaf, level-1, level-2 */
+    uint32_t pad0;
+    uint64_t record_bytes[3]; /* record size of a leaf, a level-1, a level-2 node */
+    uint64_t section[4];      /* byte offsets from the buffer's start: leaves, level-1, level-2, tiles */
+    uint64_t count[4];        /* leaves, level-1 nodes, level-2 nodes, 1 (the root) */
+    char name[256];           /* grid name, zero padded */
+    float index_to_world[16]; /* the volume's transform (SetTransform, V:5770-5798), column-major:
+                                 world = M (i, j, k, 1) */
+    double voxel_size[3];     /* |M e_a - M 0| per axis */
+    double world_bbox[6];     /* the root box's 8 corners through M: min xyz, max xyz */
+    uint64_t active_voxels;   /* root */
+    uint32_t tile_count;
+    uint32_t pad1;
+    int32_t bbox[6];          /* root box: min xyz, max xyz */
+    float background[3];
+    float vmin[3], vmax[3];   /* root min/max (floats past value_type are 0) */
+    uint32_t pad2[3];
+} gvdb2_nv_grid;
+
+typedef struct gvdb2_nv_tile {
+    uint64_t key;   /* (z >> s) | (y >> s) << 21 | (x >> s) << 42 of the node's box corner */
+    uint32_t child; /* level-2 node index */
+    uint32_t state; /* 0 */
+} gvdb2_nv_tile;
+
+/* Header of a level-1/2 node record; then child mask and value mask words
+ * (T^3/64 uint64 each: value mask first, as all off), then T^3 table entries
+ * of value_type floats (a child's index as a uint32 in the first word, the
+ * rest 0, or the background).  Records are padded to 32 bytes. */
+typedef struct gvdb2_nv_node {
+    int32_t bbox_min[3], bbox_max[3];
+    uint32_t offset; /* nodes of this level - this node's index */
+    uint32_t flags;  /* 0 */
+    float vmin[3], vmax[3];
+    uint32_t pad[2];
+} gvdb2_nv_node;
+
+/* Header of a leaf record; then the value mask (T^3/64 uint64), then T^3
+ * values of value_type floats.  Records are padded to 32 bytes. */
+typedef struct gvdb2_nv_leaf {
+    int32_t bbox_min[3];
+    uint8_t bbox_dif[3];
+    uint8_t flags; /* 0 */
+    float vmin[3], vmax[3];
+    uint32_t pad[6];
+} gvdb2_nv_leaf;
+
+GVDB2_API gvdb2_status gvdb2_nanovdb_size(gvdb2_volume *v, int value_type, size_t *bytes);
+GVDB2_API gvdb2_status gvdb2_export_nanovdb(gvdb2_volume *v, int value_type, const int32_t *chans,
+                                            const float *background, const char *grid_name, int32_t grid_class,
+                                            void *dst_device, size_t dst_bytes);
+
 /* ---- points (SetPoints VH:541 / V:4900-4908) ---- */
 /* Non-owning views, as the reference's DataPtr.  The kernel splats and
  * gathers bin the points by cell once and reuse the bins while the topology,

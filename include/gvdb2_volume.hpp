@@ -146,6 +146,19 @@ class VolumeGVDB {
         check(gvdb2_load_vbx(v_, fname.c_str()), "LoadVBX");
         return true;
     }
+    // ExportToNanoVDB (gNanoVDB/gvdb_export_nanovdb.h:65-66): the export in a
+    // device buffer the caller owns (at least NanoVDBSize(nv) bytes, 32-byte
+    // aligned); nv = GVDB2_NV_FLOAT with one channel, GVDB2_NV_VEC3F with three.
+    size_t NanoVDBSize(int nv) {
+        size_t n = 0;
+        check(gvdb2_nanovdb_size(v_, nv, &n), "ExportToNanoVDB");
+        return n;
+    }
+    void ExportToNanoVDB(int nv, const int32_t *chans, const float *background, const char *grid_name,
+                         int32_t grid_class, void *dst_device, size_t dst_bytes) {
+        check(gvdb2_export_nanovdb(v_, nv, chans, background, grid_name, grid_class, dst_device, dst_bytes),
+              "ExportToNanoVDB");
+    }
     void UpdateApron() { check(gvdb2_update_apron(v_, -1, 0.0f), "UpdateApron"); }
     void UpdateApron(unsigned char chan, float boundval = 0.0f) {
         check(gvdb2_update_apron(v_, chan, boundval), "UpdateApron");
