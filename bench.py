@@ -558,7 +558,7 @@ STAGE_KERNELS = {"scatter": "scatter stage: k_pack_amounts<4> + k_scatter_part<c
 # ----------------------------------------------------------------------------
 # the rest of the metric, each measured in the same run (N = 1)
 # ----------------------------------------------------------------------------
-EXTRA_LEGS = ("incremental", "config1_4m", "adjoint", "batched", "vs_ref_kernels", "nanovdb_export")
+EXTRA_LEGS = ("incremental", "config1_4m", "adjoint", "batched", "vs_ref_kernels", "nanovdb_export", "autotune")
 # legs left out of the main line, with the reason (none)
 HELD_LEGS = {}
 
@@ -580,6 +580,8 @@ def run_leg(name, warmup):
         return extra_ref_kernels()
     if name == "nanovdb_export":
         return extra_nanovdb(warmup)
+    if name == "autotune":
+        return extra_autotune()
     raise ValueError(name)
 
 
@@ -673,6 +675,58 @@ def extra_nanovdb(warmup):
         alg = int(inf.atlas_slots) * int(inf.res[0]) ** 3 * 4 * nv + int(size.value)
         res[name] = {"ms": ms, "buffer_bytes": int(size.value), "algorithmic_bytes": alg,
                      "gbs": alg / ms / 1e6, "frac_of_hbm": alg / ms / 1e6 / peak, "peak": f"{peak:.1f} GB/s {kind}"}
+    return res
+
+
+def extra_autotune():
+    """The autotuner on the step's scatter (4 channels) and gather (3
+    channels), at 16,777,216 points (1,024 a cell) and 4,194,304 points (256
+    a cell), after one step: each call timed (CUDA events, 10 calls after 2)
+    with the default setting, then tuned (gvdb2_autotune_scatter / _gather on
+    the same call, cache in a temporary file), then timed again."""
+    import tempfile
+    import torch
+    import gvdb2
+    import gvdb2.workloads as wl
+
+    def per_call(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 10
+
+    res = {}
+    with tempfile.TemporaryDirectory() as td:
+        for wname in ("dam16m", "dam"):
+            w = WORKLOADS[wname]
+            pos, vel = wl.dam_block(sites=w["sites"], spacing=w["spacing"])
+            pipe = Pipeline(0, pos, vel, full_rebuild=True)
+            timed_steps(pipe, 1, 1)
+            v, n, K = pipe.v, pipe.n, gvdb2.KERNEL_CUBIC2
+            v.SetTuneCache(os.path.join(td, "tune.txt"))
+
+            def scat():
+                v.ScatterKernel(K, n, [0, 1, 2, 3], weight=1.0, attrs=pipe.attrs)
+
+            def gath():
+                v.GatherKernel(K, n, [1, 2, 3], out=pipe.out)
+            r = {"default": list(v.GetTuning()), "scatter_ms_default": per_call(scat),
+                 "gather_ms_default": per_call(gath)}
+            t0 = time.perf_counter()
+            v.AutotuneScatter(K, n, [0, 1, 2, 3], weight=1.0, attrs=pipe.attrs)
+            v.AutotuneGather(K, n, [1, 2, 3], out=pipe.out)
+            r["tuning_s"] = time.perf_counter() - t0
+            r["tuned"] = list(v.GetTuning())
+            r["scatter_ms_tuned"] = per_call(scat)
+            r["gather_ms_tuned"] = per_call(gath)
+            res[wname] = r
+            del pipe
     return res
 
 

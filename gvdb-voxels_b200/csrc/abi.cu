@@ -141,6 +141,10 @@ gvdb2_status gvdb2_set_option(gvdb2_volume *h, int option, int value) {
         h->v.deterministic = value ? 1 : 0;
         return GVDB2_OK;
     }
+    if (option == GVDB2_OPT_AUTOTUNE) {
+        h->v.autotune = value != 0;
+        return GVDB2_OK;
+    }
     return gvdb2::fail(VOL(h), GVDB2_ERR_ARG, "unknown option");
 }
 
@@ -404,6 +408,7 @@ gvdb2_status gvdb2_scatter_kernel(gvdb2_volume *h, int kernel, int n, const floa
                                   float weight_const, const gvdb2_points_view *attrs, const int *chans, int nch) {
     CHECK_HANDLE(h);
     const float zero[3] = {0, 0, 0};
+    gvdb2::apply_cached_tuning(VOL(h), "scatter", kernel, nch, n);
     return gvdb2::scatter_kernel(VOL(h), kernel, n, trans ? trans : zero, weight, weight_const, attrs, chans, nch);
 }
 
@@ -411,7 +416,57 @@ gvdb2_status gvdb2_gather_kernel(gvdb2_volume *h, int kernel, int n, const float
                                  float *out, int64_t out_stride) {
     CHECK_HANDLE(h);
     const float zero[3] = {0, 0, 0};
+    gvdb2::apply_cached_tuning(VOL(h), "gather", kernel, nch, n);
     return gvdb2::gather_kernel(VOL(h), kernel, n, trans ? trans : zero, chans, nch, out, out_stride);
+}
+
+gvdb2_status gvdb2_set_tuning(gvdb2_volume *h, const gvdb2_tuning *t) {
+    CHECK_HANDLE(h);
+    return gvdb2::set_tuning(VOL(h), t);
+}
+
+gvdb2_status gvdb2_get_tuning(gvdb2_volume *h, gvdb2_tuning *t) {
+    CHECK_HANDLE(h);
+    if (!t) return gvdb2::fail(VOL(h), GVDB2_ERR_ARG, "null tuning");
+    *t = gvdb2::get_tuning(VOL(h));
+    return GVDB2_OK;
+}
+
+gvdb2_status gvdb2_set_tune_cache(gvdb2_volume *h, const char *path) {
+    CHECK_HANDLE(h);
+    h->v.tune_cache = path ? path : "";
+    return GVDB2_OK;
+}
+
+gvdb2_status gvdb2_autotune_scatter(gvdb2_volume *h, int kernel, int n, const float trans[3], gvdb2_points_view weight,
+                                    float weight_const, const gvdb2_points_view *attrs, const int *chans, int nch,
+                                    gvdb2_tuning *chosen) {
+    CHECK_HANDLE(h);
+    gvdb2::Volume *v = VOL(h);
+    const float zero[3] = {0, 0, 0};
+    const float *t = trans ? trans : zero;
+    return gvdb2::autotune(v, "scatter", kernel, nch, n, gvdb2::scatter_candidates(v), [&]() {
+        return gvdb2::scatter_kernel(v, kernel, n, t, weight, weight_const, attrs, chans, nch);
+    }, chosen);
+}
+
+gvdb2_status gvdb2_autotune_gather(gvdb2_volume *h, int kernel, int n, const float trans[3], const int *chans,
+                                   int nch, float *out, int64_t out_stride, gvdb2_tuning *chosen) {
+    CHECK_HANDLE(h);
+    gvdb2::Volume *v = VOL(h);
+    const float zero[3] = {0, 0, 0};
+    const float *t = trans ? trans : zero;
+    return gvdb2::autotune(v, "gather", kernel, nch, n, gvdb2::gather_candidates(v), [&]() {
+        return gvdb2::gather_kernel(v, kernel, n, t, chans, nch, out, out_stride);
+    }, chosen);
+}
+
+gvdb2_status gvdb2_tune_cache_get(const char *path, const char *key, gvdb2_tuning *t, float *ms) {
+    return gvdb2::cache_get(path, key, t, ms);
+}
+
+gvdb2_status gvdb2_tune_cache_put(const char *path, const char *key, const gvdb2_tuning *t, float ms) {
+    return gvdb2::cache_put(path, key, t, ms);
 }
 
 gvdb2_status gvdb2_scatter_kernel_backward(gvdb2_volume *h, int kernel, int n, const float trans[3],

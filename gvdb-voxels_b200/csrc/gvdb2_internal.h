@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -208,7 +209,17 @@ struct Volume {
         float trans[3] = {0, 0, 0};
         uint64_t topo = 0;
         bool det = false;
+        int32_t tune[3] = {0, 0, 0}; // dense, slice, light thresholds the cell lists were made with
     } bin_key;
+
+    // launch settings of the kernel splats (gvdb2_tuning): cells of at least
+    // `dense` points take the scatter's partial-sum path (0: none), `slice`
+    // points per CTA there; cells of at most `light` points are gathered a
+    // warp per cell.  Defaults 512, 4096, 32; the autotuner (tune.cu) picks
+    // others per workload class.
+    int32_t tune_dense = 512, tune_slice = 4096, tune_light = 32;
+    bool autotune = false;   // GVDB2_OPT_AUTOTUNE: apply cached settings per call
+    std::string tune_cache;  // on-disk cache path ("" = GVDB2_TUNE_CACHE, else none)
 
     // subcells (InsertPointsSubcell)
     DevBuf sc_map, sc_flag, sc_cnt, sc_off, sc_nid, sc_pos, sc_pnt;
@@ -282,6 +293,17 @@ gvdb2_status adopt_pools(Volume *v, int depth);
 gvdb2_status activate_space(Volume *v, const float *xyz, int64_t n, uint64_t *out);
 gvdb2_status compact_pools(Volume *v);
 gvdb2_status save_vbx(Volume *v, const char *path);
+// ---- tune.cu ----
+gvdb2_status set_tuning(Volume *v, const gvdb2_tuning *t);
+gvdb2_tuning get_tuning(const Volume *v);
+std::string tune_key(Volume *v, const char *op, int kernel, int nch, int64_t n);
+void apply_cached_tuning(Volume *v, const char *op, int kernel, int nch, int64_t n);
+gvdb2_status cache_get(const char *path, const char *key, gvdb2_tuning *t, float *ms);
+gvdb2_status cache_put(const char *path, const char *key, const gvdb2_tuning *t, float ms);
+gvdb2_status autotune(Volume *v, const char *op, int kernel, int nch, int64_t n, const std::vector<gvdb2_tuning> &cands,
+                      const std::function<gvdb2_status()> &call, gvdb2_tuning *chosen);
+std::vector<gvdb2_tuning> scatter_candidates(const Volume *v);
+std::vector<gvdb2_tuning> gather_candidates(const Volume *v);
 // ---- nanovdb.cu ----
 gvdb2_status nanovdb_size(Volume *v, int value_type, size_t *bytes);
 gvdb2_status export_nanovdb(Volume *v, int value_type, const int32_t *chans, const float *background,

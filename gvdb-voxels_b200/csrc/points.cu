@@ -149,28 +149,29 @@ __global__ void k_bin_pack_pos(const int32_t *perm, const uint32_t *reg_off, int
 // heavy from its back, light in `light`; see cell_at).
 constexpr int64_t kCellCountReadback = 1 << 16; // cells
 
-// Cells of at least kDenseCell points are the scatter's dense cells: each
-// gets a partial slot (part[c], -1 for the other cells), ceil(k /
-// kSlicePts) work items (cell, slice, slices, accumulator slot) and, when
-// that is more than one, an accumulator slot for its integer sums.
+// Cells of at least `dense_min` points (dense_min > 0) are the scatter's dense
+// cells: each gets a partial slot (part[c], -1 for the other cells),
+// ceil(k / slice) work items (cell, slice, slices, accumulator slot) and,
+// when that is more than one, an accumulator slot for its integer sums.
+// Cells of at most `light` (<= kLightCell) points are light.
 __global__ void k_cell_list(const uint32_t *off, int64_t ncell, int32_t *list, int32_t *light, int32_t *part,
-                            int4 *work, uint32_t *cnt) {
+                            int4 *work, uint32_t *cnt, uint32_t dense_min, uint32_t slice, uint32_t light_max) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t k = c < ncell ? off[c + 1] - off[c] : 0u;
-    const int cls = k == 0 ? -1 : (k > kHeavyCell ? kCntHuge : (k > kLightCell ? kCntHeavy : kCntLight));
+    const int cls = k == 0 ? -1 : (k > kHeavyCell ? kCntHuge : (k > light_max ? kCntHeavy : kCntLight));
     const unsigned act = __ballot_sync(0xffffffffu, cls >= 0);
     if (cls >= 0) {
         const uint32_t r = warp_agg_inc(cnt, (uint32_t)cls, act);
         if (cls == kCntLight) light[r] = (int32_t)c;
         else list[cls == kCntHuge ? (int64_t)r : ncell - 1 - r] = (int32_t)c;
     }
-    const bool dense = k >= kDenseCell;
+    const bool dense = dense_min > 0 && k >= dense_min;
     const unsigned dn = __ballot_sync(0xffffffffu, dense);
     int32_t slot = -1;
     if (dense) slot = (int32_t)warp_agg_inc(cnt, (uint32_t)kCntDense, dn);
     if (c < ncell) part[c] = slot;
     if (dense) {
-        const uint32_t ns = (k + kSlicePts - 1) / kSlicePts;
+        const uint32_t ns = (k + slice - 1) / slice;
         const uint32_t first = atomicAdd(cnt + kCntWork, ns);
         const int32_t acc = ns > 1 ? (int32_t)atomicAdd(cnt + kCntMulti, 1u) : -1;
         for (uint32_t i = 0; i < ns; i++) work[first + i] = make_int4((int32_t)c, (int32_t)i, (int32_t)ns, acc);
@@ -343,7 +344,8 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     if (k.valid && k.n == n && k.kernel == kernel && k.topo == v->topo_version && k.det == (v->deterministic != 0) &&
         k.pos.base == v->pos.base &&
         k.pos.stride == v->pos.stride && k.pos.offset == v->pos.offset && k.trans[0] == trans[0] &&
-        k.trans[1] == trans[1] && k.trans[2] == trans[2])
+        k.trans[1] == trans[1] && k.trans[2] == trans[2] && k.tune[0] == v->tune_dense && k.tune[1] == v->tune_slice &&
+        k.tune[2] == v->tune_light)
         return GVDB2_OK;
     if (!v->atlas_valid) return fail(v, GVDB2_ERR_STATE, "UpdateAtlas must follow the topology rebuild");
     if (n < 0 || (n > 0 && (!v->pos.base || n > v->pos.count))) return fail(v, GVDB2_ERR_ARG, "bad point count");
@@ -400,11 +402,12 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     GV_CUDA(v, v->cell_list.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
     GV_CUDA(v, v->cell_light.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
     GV_CUDA(v, v->cell_part.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
-    // bounds from the point count: at most n / kDenseCell dense cells, and
-    // each slice beyond a cell's first holds kSlicePts of its points
-    v->dense_cap = std::min<int64_t>(nbins, n / (int64_t)kDenseCell);
-    v->work_cap = v->dense_cap + n / (int64_t)kSlicePts;
-    v->multi_cap = std::min<int64_t>(v->dense_cap, n / (int64_t)(kSlicePts + 1));
+    // bounds from the point count: at most n / dense dense cells, and each
+    // slice beyond a cell's first holds `slice` of its points
+    const int64_t dmin = v->tune_dense, sl = v->tune_slice;
+    v->dense_cap = dmin > 0 ? std::min<int64_t>(nbins, n / dmin) : 0;
+    v->work_cap = dmin > 0 ? v->dense_cap + n / sl : 0;
+    v->multi_cap = std::min<int64_t>(v->dense_cap, n / (sl + 1));
     GV_CUDA(v, v->part_work.ensure(sizeof(int4) * (size_t)std::max<int64_t>(v->work_cap, 1), s));
     GV_CUDA(v, v->cell_cnt.ensure(sizeof(uint32_t) * kCntWords, s));
     GV_CUDA(v, cudaMemsetAsync(v->cell_cnt.p, 0, sizeof(uint32_t) * kCntWords, s));
@@ -414,7 +417,8 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
         const int g = grid_for(nbins, 256, 1ll << 31);
         k_cell_list<<<g, 256, 0, s>>>(v->bin_off.as<uint32_t>(), nbins, v->cell_list.as<int32_t>(),
                                       v->cell_light.as<int32_t>(), v->cell_part.as<int32_t>(),
-                                      v->part_work.as<int4>(), v->cell_cnt.as<uint32_t>());
+                                      v->part_work.as<int4>(), v->cell_cnt.as<uint32_t>(), (uint32_t)v->tune_dense,
+                                      (uint32_t)v->tune_slice, (uint32_t)v->tune_light);
         GV_CUDA(v, cudaGetLastError());
         v->cell_grid = v->heavy_grid = v->light_grid = nbins;
         if (nbins > kCellCountReadback) {
@@ -438,6 +442,9 @@ gvdb2_status bin_points(Volume *v, int kernel, int n, const float trans[3]) {
     k.topo = v->topo_version;
     k.pos = v->pos;
     for (int a = 0; a < 3; a++) k.trans[a] = trans[a];
+    k.tune[0] = v->tune_dense;
+    k.tune[1] = v->tune_slice;
+    k.tune[2] = v->tune_light;
     return GVDB2_OK;
 }
 

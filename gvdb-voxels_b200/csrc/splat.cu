@@ -218,6 +218,7 @@ struct SplatArgs {
     // partial sums, integer accumulators and arrival counters, and the
     // capacities of the slots
     int64_t dense_cap, multi_cap;
+    uint32_t slice; // points per dense-cell work item
     SplatLimits lim;
     const int32_t *cell_part;
     const int4 *part_work;
@@ -232,7 +233,8 @@ struct SplatArgs {
 
 // ---- dense cells: partial sums ------------------------------------------
 //
-// A cell of at least kDenseCell points (a dense cell) is splatted on its
+// A cell of at least the volume's dense threshold (the tuning's `dense`,
+// kDenseCell = 512 by default) of points, a dense cell, is splatted on its
 // own, each point once with its whole stencil, into an extended tile
 // [-H, 8+H)^3 (H = N/2: 12^3 for the cubic B-spline, 10^3 for the tent):
 // the cell's partial sums.  The owner-computes scatter below then leaves a
@@ -245,7 +247,8 @@ struct SplatArgs {
 // its neighbourhood alone (a batched cloud gets what a volume of its own
 // gets).
 //
-// k_scatter_part: one CTA per work item, a slice of up to kSlicePts points
+// k_scatter_part: one CTA per work item, a slice of up to S.slice points
+// (the tuning's `slice`, kSlicePts = 4096 by default)
 // of a dense cell, accumulates its points' stencils in shared memory with
 // atomics.  A cell of one slice writes its partial directly; the slices of
 // a larger cell add their tiles into the cell's global accumulator, and the
@@ -352,7 +355,7 @@ constexpr int kPartChunk = 128; // points staged per pass, one per thread of the
 // row stride of the staged x and y weights: a point's taps (one row each)
 // fall in different banks
 constexpr int kPartRow = kPartChunk + 1;
-static_assert(kSlicePts % kPartChunk == 0, "slices are whole chunks");
+static_assert(kSlicePts % kPartChunk == 0, "slices are whole chunks"); // tuned slices are multiples of kPartChunk too
 
 template <int KERNEL, int NCH>
 constexpr size_t part_smem_bytes() {
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(kPartThreads) k_scatter_part(SplatArgs S) {
     if (!in_range(S.lim, pslot, S.dense_cap, 7) || (nslice > 1 && !in_range(S.lim, item.w, S.multi_cap, 8))) return;
     const uint32_t beg = S.bin_off[cell], R = S.bin_off[cell + 1] - beg;
     if (!in_range(S.lim, (int64_t)beg + R - 1, S.lim.nentry, 9)) return;
-    const uint32_t s0 = (uint32_t)item.y * kSlicePts, s1 = min(R, s0 + kSlicePts);
+    const uint32_t s0 = (uint32_t)item.y * S.slice, s1 = min(R, s0 + S.slice);
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, S.m, S.m3, slot, cx, cy, cz);
@@ -1409,8 +1412,9 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
 }
 
 // The points of light cells: one warp per cell, one lane per point (a light
-// cell holds at most kLightCell = 32), taps read straight from the atlas; a
-// staged halo would cost 12^3 floats per channel for a few points.
+// cell holds at most the tuning's `light` <= kLightCell = 32 points), taps
+// read straight from the atlas; a staged halo would cost 12^3 floats per
+// channel for a few points.
 template <int KERNEL, int MODE, int NCH>
 __device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t block) {
     constexpr int H = Taps<KERNEL>::N / 2;
@@ -1561,6 +1565,7 @@ gvdb2_status scatter_group(Volume *v, const SplatArgs &S0) {
     S.part_done = v->part_done.as<uint32_t>();
     S.dense_cap = v->dense_cap;
     S.multi_cap = v->multi_cap;
+    S.slice = (uint32_t)v->tune_slice;
     // the list's count sits in its last 16 bytes
     S.merge_cnt = reinterpret_cast<uint32_t *>(v->merge_list.as<char>() + v->merge_list.bytes - 16);
     S.merge_list = v->merge_list.as<int32_t>();

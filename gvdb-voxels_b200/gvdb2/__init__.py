@@ -13,8 +13,8 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import (KERNEL_CUBIC2, KERNEL_TENT1, NV_FLOAT, NV_VEC3F, OPT_DETERMINISTIC, T_FLOAT, GvdbError, Info,
-                   PointsView, declared_symbols)
+from ._lib import (KERNEL_CUBIC2, KERNEL_TENT1, NV_FLOAT, NV_VEC3F, OPT_AUTOTUNE, OPT_DETERMINISTIC, T_FLOAT, GvdbError,
+                   Info, PointsView, Tuning, declared_symbols)
 
 NODE_DTYPE = np.dtype([
     ("mLev", np.uint8), ("mFlags", np.uint8), ("mPriority", np.uint8), ("pad", np.uint8),
@@ -84,6 +84,11 @@ class VolumeGVDB:
 
     def SetDeterministic(self, flag=True):
         self._check(self._L.gvdb2_set_option(self._h, OPT_DETERMINISTIC, 1 if flag else 0), "SetDeterministic")
+
+    def SetAutotune(self, flag=True):
+        """GVDB2_OPT_AUTOTUNE: kernel splats and gathers take their workload
+        class's setting from the tuning cache when it has one."""
+        self._check(self._L.gvdb2_set_option(self._h, OPT_AUTOTUNE, 1 if flag else 0), "SetAutotune")
 
     # -- configuration (V:2364-2453) -----------------------------------------
     def Initialize(self):
@@ -307,10 +312,48 @@ class VolumeGVDB:
                     "GatherKernel")
         return out
 
+    def SetTuning(self, dense=512, slice=4096, light=32):
+        """Launch settings of the kernel splats (gvdb2_tuning)."""
+        t = Tuning(int(dense), int(slice), int(light))
+        self._check(self._L.gvdb2_set_tuning(self._h, ctypes.byref(t)), "SetTuning")
+
+    def GetTuning(self):
+        t = Tuning()
+        self._check(self._L.gvdb2_get_tuning(self._h, ctypes.byref(t)), "GetTuning")
+        return (t.dense, t.slice, t.light)
+
+    def SetTuneCache(self, path):
+        self._check(self._L.gvdb2_set_tune_cache(self._h, os.fsencode(path) if path else None), "SetTuneCache")
+
+    def AutotuneScatter(self, kernel, num_pnts, chans, weight=1.0, attrs=None, trans=(0, 0, 0)):
+        """ScatterKernel that times the scatter's candidate settings on this
+        call, keeps the fastest and caches it; returns (dense, slice, light)."""
+        wv = view_of(weight) if hasattr(weight, "data_ptr") else PointsView(None, 0, 0, 0)
+        wc = 1.0 if hasattr(weight, "data_ptr") else float(weight)
+        av = self._attr_array(attrs, len(chans))
+        self._keep["scatter"] = (weight, attrs, av)
+        t = Tuning()
+        self._check(self._L.gvdb2_autotune_scatter(self._h, kernel, int(num_pnts), _f3(trans), wv, wc,
+                                                   ctypes.cast(av, ctypes.c_void_p), self._chans(chans), len(chans),
+                                                   ctypes.byref(t)), "AutotuneScatter")
+        return (t.dense, t.slice, t.light)
+
+    def AutotuneGather(self, kernel, num_pnts, chans, out=None, trans=(0, 0, 0)):
+        """GatherKernel that times the gather's candidate settings on this
+        call, keeps the fastest and caches it; returns (out, tuning)."""
+        import torch
+        if out is None:
+            out = torch.empty((int(num_pnts), len(chans)), dtype=torch.float32, device=f"cuda:{self.device}")
+        t = Tuning()
+        self._check(self._L.gvdb2_autotune_gather(self._h, kernel, int(num_pnts), _f3(trans), self._chans(chans),
+                                                  len(chans), ctypes.c_void_p(out.data_ptr()), out.stride(0),
+                                                  ctypes.byref(t)), "AutotuneGather")
+        return out, (t.dense, t.slice, t.light)
+
     def GatherKernelNoAlloc(self, kernel, num_pnts, chans, out, trans=(0, 0, 0)):
         """GatherKernel for callers that cannot allocate device memory once
         running: no device allocation at all (binning scratch is a fixed
-        12.25 MB array per GPU; at most 1,048,576 points and 32,768 active
+        12.25 MiB array per GPU; at most 1,048,576 points and 32,768 active
         8^3 cells per call: bricks of 8^3 voxels, or an eighth as many of 16^3).  `out` is a caller-owned (N, nch) float32 CUDA
         tensor.  Calls whose GPU work overlaps share the scratch and race."""
         self._check(self._L.gvdb2_gather_kernel_noalloc(self._h, kernel, int(num_pnts), _f3(trans), self._chans(chans),

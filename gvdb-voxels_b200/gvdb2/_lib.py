@@ -18,6 +18,7 @@ T_FLOAT = 3
 KERNEL_TENT1 = 1
 KERNEL_CUBIC2 = 2
 OPT_DETERMINISTIC = 1
+OPT_AUTOTUNE = 2
 NV_FLOAT = 1
 NV_VEC3F = 3
 
@@ -36,6 +37,10 @@ class Info(ctypes.Structure):
                 ("tile_res", ctypes.c_int32), ("splat_cells", ctypes.c_int64),
                 ("vol_min", ctypes.c_float * 3), ("vol_max", ctypes.c_float * 3), ("vox_res", ctypes.c_float * 3),
                 ("vox_res_max", ctypes.c_float * 3)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("dense", ctypes.c_int32), ("slice", ctypes.c_int32), ("light", ctypes.c_int32)]
 
 
 class GvdbError(RuntimeError):
@@ -92,6 +97,13 @@ _SIGS = {
     "gvdb2_gather_kernel_noalloc": [_vp, _i32, _i32, _fp, _ip, _i32, _vp, _i64],
     "gvdb2_scatter_kernel_backward": [_vp, _i32, _i32, _fp, PointsView, _f32, _vp, _i32, _ip, _vp, _vp, _vp],
     "gvdb2_gather_kernel_backward": [_vp, _i32, _i32, _fp, _ip, _i32, _vp, _ip, _vp],
+    "gvdb2_set_tuning": [_vp, ctypes.POINTER(Tuning)],
+    "gvdb2_get_tuning": [_vp, ctypes.POINTER(Tuning)],
+    "gvdb2_set_tune_cache": [_vp, ctypes.c_char_p],
+    "gvdb2_autotune_scatter": [_vp, _i32, _i32, _fp, PointsView, _f32, _vp, _ip, _i32, ctypes.POINTER(Tuning)],
+    "gvdb2_autotune_gather": [_vp, _i32, _i32, _fp, _ip, _i32, _vp, _i64, ctypes.POINTER(Tuning)],
+    "gvdb2_tune_cache_get": [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_float)],
+    "gvdb2_tune_cache_put": [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(Tuning), ctypes.c_float],
     "gvdb2_get_info": [_vp, ctypes.POINTER(Info)],
     "gvdb2_copy_nodes": [_vp, _i32, _vp, _i64],
     "gvdb2_copy_childlists": [_vp, _i32, _vp, _i64],

@@ -51,6 +51,7 @@ typedef int gvdb2_status;
 #define GVDB2_KERNEL_CUBIC2 2    /* cubic B-spline, radius 2 voxels */
 
 #define GVDB2_OPT_DETERMINISTIC 1 /* 1: stable binning, so kernel splats and gathers are bit-reproducible */
+#define GVDB2_OPT_AUTOTUNE 2      /* 1: kernel splats and gathers take their workload class's cached tuning */
 
 typedef struct gvdb2_volume gvdb2_volume;
 
@@ -182,10 +183,10 @@ typedef struct gvdb2_nv_tile {
     uint32_t state; /* 0 */
 } gvdb2_nv_tile;
 
-/* Header of a level-1/2 node record; then child mask and value mask words
- * (T^3/64 uint64 each: value mask first, as all off), then T^3 table entries
- * of value_type floats (a child's index as a uint32 in the first word, the
- * rest 0, or the background).  Records are padded to 32 bytes. */
+/* Header of a level-1/2 node record; then the value mask (T^3/64 uint64,
+ * all off), the child mask (T^3/64 uint64), and T^3 table entries of
+ * value_type floats (a child's index as a uint32 in the first word, the rest
+ * 0, or the background).  Records are padded to 32 bytes. */
 typedef struct gvdb2_nv_node {
     int32_t bbox_min[3], bbox_max[3];
     uint32_t offset; /* nodes of this level - this node's index */
@@ -327,6 +328,46 @@ GVDB2_API gvdb2_status gvdb2_scatter_kernel_backward(gvdb2_volume *v, int kernel
 GVDB2_API gvdb2_status gvdb2_gather_kernel_backward(gvdb2_volume *v, int kernel, int n, const float trans[3],
                                           const int *chans, int nch, const float *grad_out,
                                           const int *grad_chans, float *grad_pos);
+
+/* ---- autotuner (no reference counterpart) ----
+ * Launch settings of the kernel splats and gathers.  dense: cells of at
+ * least this many points take the scatter's partial-sum path (a CTA per
+ * slice staging the cell's extended tile in shared memory), the other cells
+ * the owner-computes warps; 0 sends every cell to the owner warps (0 or
+ * [128, 2^24]).  slice: points per CTA of a dense cell (a multiple of 128 in
+ * [128, 65536]).  light: cells of at most this many points are gathered a
+ * warp per cell, a lane per point, with taps read from the atlas; the others
+ * through a halo tile staged in shared memory (0..32).  Defaults 512, 4096,
+ * 32.  Results agree within float rounding under every setting (the summation
+ * order changes with the path a cell takes); deterministic mode stays
+ * bit-reproducible under any one setting. */
+typedef struct gvdb2_tuning {
+    int32_t dense, slice, light;
+} gvdb2_tuning;
+GVDB2_API gvdb2_status gvdb2_set_tuning(gvdb2_volume *v, const gvdb2_tuning *t);
+GVDB2_API gvdb2_status gvdb2_get_tuning(gvdb2_volume *v, gvdb2_tuning *t);
+/* The on-disk cache: path for this volume (NULL or "": $GVDB2_TUNE_CACHE,
+ * else none). */
+GVDB2_API gvdb2_status gvdb2_set_tune_cache(gvdb2_volume *v, const char *path);
+/* Same arguments and results as gvdb2_scatter_kernel / gvdb2_gather_kernel:
+ * times the candidates on this call (CUDA events on the volume's stream,
+ * median of three after an untimed run), keeps the fastest on the volume and
+ * writes it to the cache under the call's workload class (device and SM
+ * count, operation, kernel, channels, brick width, points per active 8^3
+ * cell to the nearest power of two); chosen may be NULL.  The scatter tunes
+ * dense and slice, the gather light. */
+GVDB2_API gvdb2_status gvdb2_autotune_scatter(gvdb2_volume *v, int kernel, int n, const float trans[3],
+                                              gvdb2_points_view weight, float weight_const,
+                                              const gvdb2_points_view *attrs, const int *chans, int nch,
+                                              gvdb2_tuning *chosen);
+GVDB2_API gvdb2_status gvdb2_autotune_gather(gvdb2_volume *v, int kernel, int n, const float trans[3],
+                                             const int *chans, int nch, float *out, int64_t out_stride,
+                                             gvdb2_tuning *chosen);
+/* Cache entries by key, for seeding or inspecting a cache file (host only):
+ * get returns GVDB2_ERR_STATE when the key is absent; put rewrites the file
+ * with the entry added or replaced.  ms may be NULL on get. */
+GVDB2_API gvdb2_status gvdb2_tune_cache_get(const char *path, const char *key, gvdb2_tuning *t, float *ms);
+GVDB2_API gvdb2_status gvdb2_tune_cache_put(const char *path, const char *key, const gvdb2_tuning *t, float ms);
 
 /* The same gather as gvdb2_gather_kernel, for callers that cannot allocate
  * device memory once running (an application that fixes its GPU memory

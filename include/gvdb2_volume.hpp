@@ -159,6 +159,15 @@ class VolumeGVDB {
         check(gvdb2_export_nanovdb(v_, nv, chans, background, grid_name, grid_class, dst_device, dst_bytes),
               "ExportToNanoVDB");
     }
+    // launch settings of the kernel splats and their autotuner (no reference counterpart)
+    void SetTuning(const gvdb2_tuning &t) { check(gvdb2_set_tuning(v_, &t), "SetTuning"); }
+    gvdb2_tuning GetTuning() {
+        gvdb2_tuning t{};
+        check(gvdb2_get_tuning(v_, &t), "GetTuning");
+        return t;
+    }
+    void SetTuneCache(const std::string &path) { check(gvdb2_set_tune_cache(v_, path.c_str()), "SetTuneCache"); }
+    void SetAutotune(bool on) { check(gvdb2_set_option(v_, GVDB2_OPT_AUTOTUNE, on ? 1 : 0), "SetAutotune"); }
     void UpdateApron() { check(gvdb2_update_apron(v_, -1, 0.0f), "UpdateApron"); }
     void UpdateApron(unsigned char chan, float boundval = 0.0f) {
         check(gvdb2_update_apron(v_, chan, boundval), "UpdateApron");
