@@ -563,8 +563,9 @@ EXTRA_LEGS = ("incremental", "config1_4m", "adjoint", "batched", "vs_ref_kernels
 HELD_LEGS = {}
 
 
-def run_leg(name, warmup):
-    """One extra leg in this process; returns its result dict."""
+def run_leg(name, warmup, workload="dam16m"):
+    """One extra leg in this process; returns its result dict (the export
+    leg runs on `workload` when it is a dam block, else on dam16m)."""
     if name == "incremental":
         import gvdb2.workloads as wl
         w = WORKLOADS["dam16m"]
@@ -579,7 +580,7 @@ def run_leg(name, warmup):
     if name == "vs_ref_kernels":
         return extra_ref_kernels()
     if name == "nanovdb_export":
-        return extra_nanovdb(warmup)
+        return extra_nanovdb(warmup, workload if workload in ("dam16m", "dam") else "dam16m")
     if name == "autotune":
         return extra_autotune()
     raise ValueError(name)
@@ -635,7 +636,7 @@ def extra_incremental(pos, vel, warmup):
     return res
 
 
-def extra_nanovdb(warmup):
+def extra_nanovdb(warmup, wname="dam16m"):
     """ExportToNanoVDB of the 16M-point step's volume (after one step): a
     float grid of channel 0 (mass) and a Vec3f grid of channels 1-3
     (momentum), each call timed end to end on the host (the call returns
@@ -646,7 +647,7 @@ def extra_nanovdb(warmup):
     import ctypes
     import torch
     import gvdb2.workloads as wl
-    w = WORKLOADS["dam16m"]
+    w = WORKLOADS[wname]
     pos, vel = wl.dam_block(sites=w["sites"], spacing=w["spacing"])
     pipe = Pipeline(0, pos, vel, full_rebuild=True)
     timed_steps(pipe, 1, 1)
@@ -663,7 +664,7 @@ def extra_nanovdb(warmup):
         ch, bg = (ctypes.c_int * nv)(*chans), (ctypes.c_float * nv)(*([0.0] * nv))
 
         def call():
-            v._check(v._L.gvdb2_export_nanovdb(v._h, nv, ch, bg, b"dam16m", 0, ctypes.c_void_p(buf.data_ptr()),
+            v._check(v._L.gvdb2_export_nanovdb(v._h, nv, ch, bg, wname.encode(), 0, ctypes.c_void_p(buf.data_ptr()),
                                                int(size.value)), "export_nanovdb")
         for _ in range(max(3, warmup)):
             call()
@@ -1195,7 +1196,7 @@ def main():
     if a.leg:
         import torch
         torch.cuda.set_device(0)
-        print(json.dumps(run_leg(a.leg, a.warmup)), flush=True)
+        print(json.dumps(run_leg(a.leg, a.warmup, a.workload)), flush=True)
         return 0
     if a.impl == "reference":
         if a.workload not in WORKLOADS:

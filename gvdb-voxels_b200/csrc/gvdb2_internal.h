@@ -72,6 +72,7 @@ enum DevStatusBits : int32_t {
     kDevHashFull = 1,
     kDevCapacity = 2,
     kDevBadIndex = 4,
+    kDevTimeout = 8, // a bounded wait (bulk copy completion) ran out
 };
 
 // Growable device buffer, stream-ordered (cudaMallocAsync / cudaFreeAsync

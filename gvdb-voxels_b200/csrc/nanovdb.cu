@@ -7,10 +7,11 @@
 // layouts are gvdb2_nv_grid / gvdb2_nv_tile / gvdb2_nv_node / gvdb2_nv_leaf
 // (include/gvdb2.h).
 //
-// B200 form: a CTA per leaf stages its brick through shared memory in slabs
-// of x, reading the atlas tile in its x-fastest rows and writing the record's
-// z-fastest values as one contiguous run per slab; min/max reduce in
-// registers, then by warp shuffles.  A CTA per interior node walks the child
+// B200 form: a CTA per leaf stages its atlas tile in shared memory -- whole,
+// by bulk copies (cp.async.bulk, mbarrier-completed) when the tiles fit, else
+// in slabs of x-planes read in the tile's x-fastest rows -- and writes the
+// record's z-fastest values as contiguous runs; min/max reduce in registers,
+// then by warp shuffles.  A CTA per interior node walks the child
 // table in NanoVDB order, builds the child mask with warp ballots and folds
 // the children's ranges.  Every byte of every record is written by the
 // kernels (no memset pass over the buffer).  The root is finished on the host
@@ -172,6 +173,99 @@ __global__ void __launch_bounds__(kNvThreads) k_nv_leaves(const Node *leaves, co
     }
 }
 
+// Bulk copies: one cp.async.bulk per channel moves a leaf's whole atlas tile
+// (a contiguous, 16-byte-aligned run of t^3 floats) into shared memory,
+// completing on an mbarrier.  The wait is bounded: past kNvWaitLimit polls
+// the CTA sets kDevTimeout in *status, waits once more (bounded) so that no
+// copy still lands in its shared memory, and returns without using the data.
+constexpr int kNvWaitLimit = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, int limit) {
+    for (int i = 0; i < limit; i++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(bar), "r"(phase)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// ProcessLeaf with the tile staged by bulk copies (bricks whose NV tiles fit
+// kNvSlabBytes): the same record as k_nv_leaves, read from shared memory.
+template <int NV>
+__global__ void __launch_bounds__(kNvThreads) k_nv_leaves_bulk(const Node *leaves, const int32_t *leaf_slot,
+                                                               int64_t nslots, NvChans ch, int ld, int apron,
+                                                               uint8_t *out, uint64_t rec, int32_t *status) {
+    extern __shared__ __align__(16) float tile[];
+    __shared__ __align__(8) uint64_t bar;
+    const int64_t leaf = blockIdx.x;
+    uint8_t *rp = out + (uint64_t)leaf * rec;
+    const int slot = leaf_slot[leaf];
+    if (slot < 0 || slot >= nslots) { // stale: no brick in the atlas
+        zero_record(rp, rec);
+        return;
+    }
+    const int T = 1 << ld, T2 = T * T, t = T + 2 * apron;
+    const int64_t t3 = (int64_t)T2 * T;
+    const uint32_t tbytes = (uint32_t)t * t * t * 4u; // a multiple of 32 (t is even)
+    const uint32_t b = smem_u32(&bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(tbytes * NV) : "memory");
+#pragma unroll
+        for (int c = 0; c < NV; c++) {
+            const float *src = ch.c[c] + (int64_t)slot * t * t * t;
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             smem_u32(tile + (size_t)c * t * t * t)),
+                         "l"(src), "r"(tbytes), "r"(b)
+                         : "memory");
+        }
+    }
+    if (!mbar_wait(b, 0, kNvWaitLimit)) {
+        if (threadIdx.x == 0) atomicOr(status, kDevTimeout);
+        mbar_wait(b, 0, kNvWaitLimit);
+        return;
+    }
+    uint64_t *mask = reinterpret_cast<uint64_t *>(rp + GVDB2_NV_HEADER);
+    float *vals = reinterpret_cast<float *>(rp + GVDB2_NV_HEADER + t3 / 8);
+    for (int64_t w = threadIdx.x; w < t3 / 64; w += blockDim.x) mask[w] = ~uint64_t(0); // all voxels active
+    float lo[NV], hi[NV];
+#pragma unroll
+    for (int c = 0; c < NV; c++) lo[c] = FLT_MAX, hi[c] = -FLT_MAX;
+    // values[(x*T + y)*T + z] from tile voxel (x, y, z) + apron, z-major
+    for (int j = threadIdx.x; j < (int)t3; j += blockDim.x) {
+        const int x = j >> (2 * ld), y = (j >> ld) & (T - 1), z = j & (T - 1);
+        const int s = ((z + apron) * t + (y + apron)) * t + (x + apron);
+#pragma unroll
+        for (int c = 0; c < NV; c++) {
+            const float val = tile[c * t * t * t + s];
+            vals[(int64_t)j * NV + c] = val;
+            lo[c] = fminf(lo[c], val);
+            hi[c] = fmaxf(hi[c], val);
+        }
+    }
+    const uint64_t used = GVDB2_NV_HEADER + t3 / 8 + t3 * 4 * NV;
+    for (uint64_t p = used + threadIdx.x * 4; p < rec; p += blockDim.x * 4) *reinterpret_cast<uint32_t *>(rp + p) = 0;
+    block_minmax<NV>(lo, hi);
+    if (threadIdx.x == 0) {
+        const Node &nd = leaves[leaf];
+        gvdb2_nv_leaf h;
+        memset(&h, 0, sizeof(h));
+        for (int a = 0; a < 3; a++) h.bbox_min[a] = nd.mPos[a], h.bbox_dif[a] = (uint8_t)T;
+        for (int c = 0; c < NV; c++) h.vmin[c] = lo[c], h.vmax[c] = hi[c];
+        *reinterpret_cast<gvdb2_nv_leaf *>(rp) = h;
+    }
+}
+
 // ProcessInternalNode (cuda_export_nanovdb.cu:241-328): one CTA per pool node
 // of a level.  Table slot j = (x*T + y)*T + z holds GVDB child-list entry
 // g = (z*T + y)*T + x; an entry's child index is (int)(entry >> 16), -1 for
@@ -272,7 +366,21 @@ template <int NV>
 gvdb2_status launch_nv(Volume *v, const NvLayout &L, const int32_t *chans, float3 bg, uint8_t *dst, int32_t *status) {
     cudaStream_t s = v->stream;
     const int T = 1 << L.ld[0];
-    if (L.cnt[0] > 0) {
+    const int tr = T + 2 * v->apron;
+    const size_t tile_all = (size_t)tr * tr * tr * 4 * NV;
+    bool aligned = true;
+    for (int c = 0; c < NV; c++) aligned &= reinterpret_cast<uintptr_t>(v->atlas[chans[c]].p) % 16 == 0;
+    if (L.cnt[0] > 0 && tile_all <= kNvSlabBytes && aligned) {
+        // whole tiles by bulk copy (t even: each tile a multiple of 16 bytes)
+        NvChans ch{};
+        for (int c = 0; c < NV; c++) ch.c[c] = v->atlas[chans[c]].as<float>();
+        GV_CUDA(v, cudaFuncSetAttribute(k_nv_leaves_bulk<NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tile_all));
+        k_nv_leaves_bulk<NV><<<(unsigned)L.cnt[0], kNvThreads, tile_all, s>>>(
+            v->pool_ptr(0), v->leaf_slot.as<int32_t>(), v->atlas_last, ch, L.ld[0], v->apron, dst + L.sec[0],
+            L.rec[0], status);
+        GV_CUDA(v, cudaGetLastError());
+    } else if (L.cnt[0] > 0) {
         NvChans ch{};
         for (int c = 0; c < NV; c++) ch.c[c] = v->atlas[chans[c]].as<float>();
         // largest power-of-two slab of x-planes whose staging fits kNvSlabBytes (at least one plane)
@@ -372,6 +480,7 @@ gvdb2_status export_nanovdb(Volume *v, int value_type, const int32_t *chans, con
     GV_CUDA(v, cudaMemcpyAsync(&st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
     GV_CUDA(v, cudaStreamSynchronize(s));
     if (st & kDevBadIndex) return fail(v, GVDB2_ERR_STATE, "a child list names a node past its level's pool");
+    if (st & kDevTimeout) return fail(v, GVDB2_ERR_STATE, "a leaf's bulk copy did not complete");
 
     std::vector<uint8_t> hb((size_t)L.sec[2], 0);
     gvdb2_nv_grid &g = *reinterpret_cast<gvdb2_nv_grid *>(hb.data());
