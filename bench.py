@@ -864,7 +864,8 @@ def batched_step(v, K, n, chans_fwd, grad_chan, go):
     v.RebuildTopology(n, RADIUS)
     v.UpdateAtlas()
     v.ScatterKernel(K, n, chans_fwd, weight=1.0)
-    v.UpdateApron(-1, 0.0)
+    for c in chans_fwd:  # the aprons of the scattered channels
+        v.UpdateApron(c, 0.0)
     out = v.GatherKernel(K, n, chans_fwd, out=go[0])
     v.GatherDensityBackward(K, n, chans_fwd, out, grad_chans=[grad_chan], grad_pos=go[1])
     v.ScatterDensityBackward(K, n, [grad_chan], weight=1.0, grad_pos=go[2], grad_weight=go[3], grad_attr=go[4])

@@ -161,6 +161,7 @@ struct Volume {
     // scratch for the rebuild
     DevBuf hs_keys[2];        // hash sets (base, box)
     DevBuf bits;              // brick bitmaps per level (base, box) of the bitmap rebuild
+    DevBuf bits_chunks;       // per-chunk set-bit counts of the large-grid compaction
     uint32_t hs_mask = 0;
     DevBuf lev_keys[kMaxLev][2]; // sorted unique keys per level: [0]=base [1]=extra (or new)
     int64_t lev_count[kMaxLev][2] = {{0}};

@@ -694,7 +694,7 @@ gvdb2_status incremental_activate(Volume *v, int n, float radius, const float or
 // ---- full rebuild over brick bitmaps --------------------------------------
 //
 // For a cloud whose bounding box (in level-0 bricks, widened by the
-// activation box) holds at most 2^31 bricks, the node sets of every level are
+// activation box) holds at most 2^30 bricks, the node sets of every level are
 // bitmaps over that box instead of hash sets.  Bit (x, y, z) sits at
 // ((x-ox)*dy + (y-oy))*dz + (z-oz), i.e. in the order of the packed keys, so
 // an ordered compaction of the set bits yields the sorted unique keys with
@@ -910,7 +910,159 @@ __global__ void __launch_bounds__(kCompactThreads) k_bits_compact(CompactSets S)
     if (threadIdx.x == 0) *C.count = (int32_t)running;
 }
 
-constexpr int64_t kMaxGridBits = 1ll << 28; // bitmap path up to 2^28 bricks (32 MB per bitmap)
+// ---- brick bitmaps of large grids (batched clouds, sparse extents) ---------
+//
+// Above kLargeGridBits bits at level 0 the per-parent scan of k_parent_bits
+// (every child bit read one by one) and the single-CTA compaction of
+// k_bits_compact would take milliseconds, so both run over words across
+// the whole GPU instead; the sets and their key order are the same.
+constexpr int64_t kLargeGridBits = 1ll << 22;
+constexpr int kChunkThreads = 256;
+constexpr int kChunkWordsPerThread = 16;
+constexpr int64_t kChunkWords = (int64_t)kChunkThreads * kChunkWordsPerThread;
+
+// Parent bits from the child level's words: a thread per child word; each
+// set bit ORs its parent's bit (read first: siblings mostly set it already).
+__global__ void k_parent_bits_words(BitGrid C, BitGrid P, int sh) {
+    const int64_t nbits = (int64_t)C.d[0] * C.d[1] * C.d[2];
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < C.words;
+         w += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            uint32_t x = s ? C.box[w] : C.base[w];
+            uint32_t *pbits = s ? P.box : P.base;
+            int64_t last = -1;
+            while (x) {
+                const int j = __ffs(x) - 1;
+                x &= x - 1;
+                const int64_t b = (w << 5) + j;
+                if (b >= nbits) break;
+                const int64_t t = b / C.d[2];
+                const int z = (int)(b - t * C.d[2]) + C.o[2];
+                const int y = (int)(t % C.d[1]) + C.o[1];
+                const int xx = (int)(t / C.d[1]) + C.o[0];
+                const int64_t p = bg_bit(P, xx >> sh, y >> sh, z >> sh);
+                if (p == last) continue;
+                last = p;
+                bg_set(pbits, p);
+            }
+        }
+    }
+}
+
+// The chunks of every set of a large-grid compaction, numbered across the
+// sets: set j owns chunks [first[j], first[j + 1]).
+struct ChunkedSets {
+    CompactSets S;
+    int64_t first[2 * kMaxLev + 1];
+    int nsets;
+    uint32_t *cnt; // per chunk: set bits, then (after k_chunk_scan) the chunk's first key index
+};
+
+__device__ __forceinline__ int chunk_set(const ChunkedSets &K, int64_t c) {
+    int j = 0;
+    while (j + 1 < K.nsets && K.first[j + 1] <= c) j++;
+    return j;
+}
+
+__device__ __forceinline__ uint32_t chunk_word(const CompactSet &C, int64_t wi) {
+    if (wi >= C.G.words) return 0;
+    uint32_t x = C.a[wi];
+    if (C.mask) x &= ~C.mask[wi];
+    return x;
+}
+
+// Exclusive scan of one value per thread over a CTA of kChunkThreads;
+// *total receives the CTA's sum.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *warp_sum, uint32_t *total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) warp_sum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t ws = lane < kChunkThreads / 32 ? warp_sum[lane] : 0;
+        uint32_t wsum = ws;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, wsum, o);
+            if (lane >= o) wsum += y;
+        }
+        if (lane < kChunkThreads / 32) warp_sum[lane] = wsum - ws;
+        if (lane == 31) *total = wsum;
+    }
+    __syncthreads();
+    return warp_sum[warp] + inc - v;
+}
+
+// Pass 1: set bits per chunk.
+__global__ void __launch_bounds__(kChunkThreads) k_chunk_count(ChunkedSets K) {
+    __shared__ uint32_t warp_sum[32];
+    __shared__ uint32_t total;
+    const int64_t c = blockIdx.x;
+    const int j = chunk_set(K, c);
+    const CompactSet &C = K.S.set[j];
+    const int64_t w0 = (c - K.first[j]) * kChunkWords + (int64_t)threadIdx.x * kChunkWordsPerThread;
+    uint32_t n = 0;
+#pragma unroll 4
+    for (int k = 0; k < kChunkWordsPerThread; k++) n += __popc(chunk_word(C, w0 + k));
+    block_excl_scan(n, warp_sum, &total);
+    if (threadIdx.x == 0) K.cnt[c] = total;
+}
+
+// Pass 2: a CTA per set turns its chunk counts into first key indices and
+// writes the set's key count.
+__global__ void __launch_bounds__(kChunkThreads) k_chunk_scan(ChunkedSets K) {
+    __shared__ uint32_t warp_sum[32];
+    __shared__ uint32_t total;
+    const int j = blockIdx.x;
+    uint32_t running = 0;
+    for (int64_t c0 = K.first[j]; c0 < K.first[j + 1]; c0 += kChunkThreads) {
+        const int64_t c = c0 + threadIdx.x;
+        const uint32_t v = c < K.first[j + 1] ? K.cnt[c] : 0;
+        const uint32_t ex = block_excl_scan(v, warp_sum, &total);
+        if (c < K.first[j + 1]) K.cnt[c] = running + ex;
+        running += total;
+        __syncthreads(); // warp_sum / total are rewritten next round
+    }
+    if (threadIdx.x == 0) *K.S.set[j].count = (int32_t)running;
+}
+
+// Pass 3: each thread writes the keys of its words, in bit order, from its
+// chunk's first key index plus its rank in the chunk.
+__global__ void __launch_bounds__(kChunkThreads) k_chunk_write(ChunkedSets K) {
+    __shared__ uint32_t warp_sum[32];
+    __shared__ uint32_t total;
+    const int64_t c = blockIdx.x;
+    const int j = chunk_set(K, c);
+    const CompactSet &C = K.S.set[j];
+    const BitGrid &G = C.G;
+    const int64_t nbits = (int64_t)G.d[0] * G.d[1] * G.d[2];
+    const int64_t w0 = (c - K.first[j]) * kChunkWords + (int64_t)threadIdx.x * kChunkWordsPerThread;
+    uint32_t n = 0;
+#pragma unroll 4
+    for (int k = 0; k < kChunkWordsPerThread; k++) n += __popc(chunk_word(C, w0 + k));
+    uint32_t pos = K.cnt[c] + block_excl_scan(n, warp_sum, &total);
+    if (!n) return;
+    for (int k = 0; k < kChunkWordsPerThread; k++) {
+        const int64_t wi = w0 + k;
+        uint32_t x = chunk_word(C, wi);
+        while (x) {
+            const int jb = __ffs(x) - 1;
+            x &= x - 1;
+            const int64_t b = (wi << 5) + jb;
+            if (b >= nbits) break;
+            const int64_t t = b / G.d[2];
+            const int z = (int)(b - t * G.d[2]);
+            const int y = (int)(t % G.d[1]), xx = (int)(t / G.d[1]);
+            C.out[pos++] = pack_key(xx + G.o[0], y + G.o[1], z + G.o[2], K.S.b);
+        }
+    }
+}
+
+constexpr int64_t kMaxGridBits = 1ll << 30; // bitmap path up to 2^30 bricks (128 MB per bitmap)
 
 // Node key sets through brick bitmaps; *used = false when the grid would be
 // too large or a brick fell outside it (then nothing was changed).
@@ -975,9 +1127,15 @@ gvdb2_status key_sets_bitmap(Volume *v, int n, float radius, const float orig[3]
         k_mark_bits<false><<<grid_for(n, 256, 1ll << 31), 256, 0, s>>>(v->pos, n, t3, radius, kmax, do_box ? 1 : 0, g,
                                                                         G[0], &dev_words(v)->status);
     }
+    const int64_t nbits0 = (int64_t)G[0].d[0] * G[0].d[1] * G[0].d[2];
+    const bool large = nbits0 > kLargeGridBits; // level 0 is the largest grid
     for (int l = 1; l < depth; l++) {
         const int64_t nbits = (int64_t)G[l].d[0] * G[l].d[1] * G[l].d[2];
-        k_parent_bits<<<grid_for(nbits, 256, 8 * kSmCount), 256, 0, s>>>(G[l - 1], G[l], v->logdim[l]);
+        if (large)
+            k_parent_bits_words<<<grid_for(G[l - 1].words, 256, 16 * kSmCount), 256, 0, s>>>(G[l - 1], G[l],
+                                                                                              v->logdim[l]);
+        else
+            k_parent_bits<<<grid_for(nbits, 256, 8 * kSmCount), 256, 0, s>>>(G[l - 1], G[l], v->logdim[l]);
     }
     // compaction of every (level, set) in one launch; for small grids the key
     // arrays are sized by the grid and a single pass both counts and writes
@@ -990,7 +1148,16 @@ gvdb2_status key_sets_bitmap(Volume *v, int n, float radius, const float orig[3]
         C.set[nsets++] = CompactSet{G[l].base, nullptr, G[l], nullptr, dev_words(v)->count + 2 * l};
         if (do_box) C.set[nsets++] = CompactSet{G[l].box, G[l].base, G[l], nullptr, dev_words(v)->count + 2 * l + 1};
     }
-    const bool one_pass = maxbits <= (1ll << 22);
+    const bool one_pass = maxbits <= kLargeGridBits;
+    ChunkedSets K;
+    if (!one_pass) {
+        // counts per chunk, then per set, over the whole GPU
+        K.nsets = nsets;
+        K.first[0] = 0;
+        for (int j = 0; j < nsets; j++) K.first[j + 1] = K.first[j] + (C.set[j].G.words + kChunkWords - 1) / kChunkWords;
+        GV_CUDA(v, v->bits_chunks.ensure(sizeof(uint32_t) * (size_t)std::max<int64_t>(K.first[nsets], 1), s));
+        K.cnt = v->bits_chunks.as<uint32_t>();
+    }
     if (one_pass) {
         int k = 0;
         for (int l = 0; l < depth; l++) {
@@ -1005,7 +1172,13 @@ gvdb2_status key_sets_bitmap(Volume *v, int n, float radius, const float orig[3]
             }
         }
     }
-    k_bits_compact<<<nsets, kCompactThreads, 0, s>>>(C);
+    if (one_pass) {
+        k_bits_compact<<<nsets, kCompactThreads, 0, s>>>(C);
+    } else {
+        K.S = C;
+        k_chunk_count<<<(unsigned)K.first[nsets], kChunkThreads, 0, s>>>(K);
+        k_chunk_scan<<<nsets, kChunkThreads, 0, s>>>(K);
+    }
     GV_CUDA(v, cudaGetLastError());
     GV_TRY(read_words(v));
     if (host_words(v)->status & kDevCapacity) return GVDB2_OK; // a brick outside the grid: hash path
@@ -1022,7 +1195,8 @@ gvdb2_status key_sets_bitmap(Volume *v, int n, float radius, const float orig[3]
             C.set[k++].out = v->lev_keys[l][0].as<uint64_t>();
             if (do_box) C.set[k++].out = v->lev_keys[l][1].as<uint64_t>();
         }
-        k_bits_compact<<<nsets, kCompactThreads, 0, s>>>(C);
+        K.S = C;
+        k_chunk_write<<<(unsigned)K.first[nsets], kChunkThreads, 0, s>>>(K);
         GV_CUDA(v, cudaGetLastError());
     }
     *used = true;

@@ -256,6 +256,26 @@ def test_sparse_extent_takes_hash_path(gvdb2_mod, oracle_mod):
     assert np.array_equal(v.atlas_map(), o.atlas_map())
 
 
+def test_large_extent_bitmaps_bit_exact(gvdb2_mod, oracle_mod):
+    """Two clusters 4,000 voxels apart: their level-0 brick grid (about
+    500^3 bricks) is within the bitmap limit but past the size where the
+    parent levels and the compaction run over words across the GPU; the
+    node pools, child lists and atlas map still match bit for bit, for a
+    full rebuild with extra bricks and for one without (radius 0.5)."""
+    a = shell_points(20_000, seed=41, r_in=20, r_out=24, center=(200.0, 260.0, 230.0))
+    b = shell_points(20_000, seed=42, r_in=20, r_out=24, center=(4_200.0, 3_900.0, 4_100.0))
+    pts = np.concatenate([a, b]).astype(np.float32)
+    for radius in (2.0, 0.5):
+        o = make_oracle(oracle_mod)
+        assert o.rebuild_topology(pts, radius) == 0
+        o.update_atlas()
+        v = gpu_volume(gvdb2_mod, pts)
+        v.RebuildTopology(len(pts), radius)
+        v.UpdateAtlas()
+        compare_topology(v, o)
+        assert np.array_equal(v.atlas_map(), o.atlas_map())
+
+
 def test_compact_pools_bit_exact(gvdb2_mod, oracle_mod):
     """CompactPools after incremental rebuilds left delinked nodes: pools,
     child lists and atlas map match the oracle's compaction bit for bit, and
