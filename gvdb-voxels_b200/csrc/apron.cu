@@ -28,27 +28,38 @@ struct ApronChans {
 // One CTA per slot; every channel of the call in one pass.  `list` holds,
 // in tile order, every apron voxel of a tile: its tile offset and the
 // neighbour k (0..26) that owns it with the offset of the owner's interior
-// voxel, so the kernel does no index arithmetic.  For each voxel all loads
-// (up to 4 channels at a time) are issued before the stores.
+// voxel, so the kernel does no index arithmetic.  A thread takes two list
+// entries at a time (488 apron voxels of an 8^3 brick: one round of 256
+// threads), and all their loads (up to 4 channels at a time) are issued
+// before the stores: the kernel is bound by the latency of these scattered
+// reads.
 __global__ void __launch_bounds__(256) k_apron(ApronChans C, const int32_t *nbr27, const int2 *list, int nlist,
                                                int64_t tvox, float boundval) {
     const int64_t slot = blockIdx.x;
     __shared__ int32_t nbs[27];
     if (threadIdx.x < 27) nbs[threadIdx.x] = nbr27[slot * 27 + threadIdx.x];
     __syncthreads();
-    for (int i = threadIdx.x; i < nlist; i += blockDim.x) {
-        const int2 e = list[i];
-        const int32_t nb = nbs[e.y >> 24];
-        const int64_t src = (int64_t)nb * tvox + (e.y & 0xFFFFFF);
-        const int64_t dst = slot * tvox + e.x;
+    for (int i = threadIdx.x; i < nlist; i += 2 * blockDim.x) {
+        const int i1 = i + blockDim.x;
+        const bool two = i1 < nlist;
+        const int2 e0 = list[i], e1 = list[two ? i1 : i];
+        const int32_t nb0 = nbs[e0.y >> 24], nb1 = nbs[e1.y >> 24];
+        const int64_t src0 = (int64_t)nb0 * tvox + (e0.y & 0xFFFFFF), src1 = (int64_t)nb1 * tvox + (e1.y & 0xFFFFFF);
+        const int64_t dst0 = slot * tvox + e0.x, dst1 = slot * tvox + e1.x;
         for (int c0 = 0; c0 < C.nch; c0 += 4) {
-            float val[4];
+            float val0[4], val1[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const bool in = c0 + j < C.nch;
+                val0[j] = (in && nb0 >= 0) ? __ldcg(C.chan[c0 + j] + src0) : boundval;
+                val1[j] = (in && two && nb1 >= 0) ? __ldcg(C.chan[c0 + j] + src1) : boundval;
+            }
 #pragma unroll
             for (int j = 0; j < 4; j++)
-                val[j] = (c0 + j < C.nch && nb >= 0) ? __ldcg(C.chan[c0 + j] + src) : boundval;
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (c0 + j < C.nch) C.chan[c0 + j][dst] = val[j];
+                if (c0 + j < C.nch) {
+                    C.chan[c0 + j][dst0] = val0[j];
+                    if (two) C.chan[c0 + j][dst1] = val1[j];
+                }
         }
     }
 }

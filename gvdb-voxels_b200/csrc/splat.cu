@@ -1411,20 +1411,18 @@ __device__ __forceinline__ void gather_tile_cell(const GatherArgs &G, int64_t bl
     }
 }
 
-// The points of light cells: one warp per cell, one lane per point (a light
-// cell holds at most the tuning's `light` <= kLightCell = 32 points), taps
-// read straight from the atlas; a staged halo would cost 12^3 floats per
-// channel for a few points.
+// The points of light cells: kLightPack light cells per warp (a light cell
+// holds at most the tuning's `light` <= kLightCell = 32 points), one lane
+// per point, the group's points dealt to the lanes in rounds of 32; taps
+// read straight from the atlas (a staged halo would cost 12^3 floats per
+// channel for a few points).  Each point is served by one lane with the
+// same taps in the same order whichever warp holds it, so the packing
+// changes no result.
+constexpr int kLightPack = 4;
+
 template <int KERNEL, int MODE, int NCH>
-__device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t block) {
+__device__ __forceinline__ void gather_light_point(const GatherArgs &G, int64_t cell, int64_t entry) {
     constexpr int H = Taps<KERNEL>::N / 2;
-    const int64_t w = (block * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= (int64_t)G.cell_cnt[2]) return;
-    const int64_t cell = G.cell_light[w];
-    if (!in_range(G.lim, cell, G.ncell, 17)) return;
-    const uint32_t beg = G.bin_off[cell], cnt = G.bin_off[cell + 1] - beg;
-    if ((uint32_t)lane >= cnt || !in_range(G.lim, (int64_t)beg + lane, G.lim.nentry, 18)) return;
     int64_t slot;
     int cx, cy, cz;
     cell_coords(cell, G.m, G.m3, slot, cx, cy, cz);
@@ -1445,12 +1443,56 @@ __device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t 
 #pragma unroll
         for (int c = 0; c < NCH; c++) g[c] = ns >= 0 ? __ldg(G.chan[c] + off) : 0.0f;
     };
-    gather_point<KERNEL, MODE, NCH>(G, G.perm[beg + lane], (int64_t)beg + lane, nd.mPos[0] + fx0, nd.mPos[1] + fy0, nd.mPos[2] + fz0,
+    gather_point<KERNEL, MODE, NCH>(G, G.perm[entry], entry, nd.mPos[0] + fx0, nd.mPos[1] + fy0, nd.mPos[2] + fz0,
                                     fetch);
 }
 
+template <int KERNEL, int MODE, int NCH>
+__device__ __forceinline__ void gather_light_cells(const GatherArgs &G, int64_t block) {
+    const int64_t w = (block * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t nlight = (int64_t)G.cell_cnt[2];
+    const int64_t i0 = w * kLightPack;
+    if (i0 >= nlight) return; // the same for the whole warp
+    // lane j < kLightPack reads light cell i0 + j's bin range
+    int64_t cell = -1;
+    uint32_t beg = 0, cnt = 0;
+    if (lane < kLightPack && i0 + lane < nlight) {
+        cell = G.cell_light[i0 + lane];
+        if (in_range(G.lim, cell, G.ncell, 17)) {
+            beg = G.bin_off[cell];
+            cnt = G.bin_off[cell + 1] - beg;
+        } else {
+            cell = -1;
+        }
+    }
+    uint32_t inc = cnt; // inclusive prefix of the group's counts
+#pragma unroll
+    for (int o = 1; o < kLightPack; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, inc, kLightPack - 1);
+    // rounds of 32 points, the same number for the whole warp (the shuffles
+    // below take every lane)
+    for (uint32_t r = 0; r < total; r += 32) {
+        const uint32_t t = r + lane;
+        int j = 0; // the group's cell holding index t
+#pragma unroll
+        for (int k = 0; k < kLightPack - 1; k++) j += t >= __shfl_sync(0xffffffffu, inc, k) ? 1 : 0;
+        j = min(j, kLightPack - 1);
+        const int64_t c = __shfl_sync(0xffffffffu, cell, j);
+        const uint32_t b = __shfl_sync(0xffffffffu, beg, j);
+        const uint32_t first = __shfl_sync(0xffffffffu, inc - cnt, j);
+        if (t >= total || c < 0) continue;
+        const int64_t entry = (int64_t)b + (t - first);
+        if (!in_range(G.lim, entry, G.lim.nentry, 18)) continue;
+        gather_light_point<KERNEL, MODE, NCH>(G, c, entry);
+    }
+}
+
 // Two launches: a halo tile per huge or heavy cell (every cell, in cell
-// order, when no cell list is given), then the light cells, a warp each.
+// order, when no cell list is given), then the light cells, kLightPack a warp.
 // One fused launch measured slower: the light path's registers (66) halved
 // the tiles' occupancy.
 template <int KERNEL, int MODE, int NCH>
@@ -1633,7 +1675,8 @@ gvdb2_status launch_gather(Volume *v, const GatherArgs &G) {
     const int64_t heavy = G.cell_list ? v->heavy_grid : G.ncell;
     if (heavy > 0) k<<<(unsigned)heavy, kGatherThreads, smem, v->stream>>>(G);
     if (G.cell_list && v->light_grid > 0)
-        k_gather_light<KERNEL, MODE, NCH><<<(unsigned)((v->light_grid + 7) / 8), 256, 0, v->stream>>>(G);
+        k_gather_light<KERNEL, MODE, NCH><<<(unsigned)((v->light_grid + 8 * kLightPack - 1) / (8 * kLightPack)), 256, 0,
+                                            v->stream>>>(G);
     GV_CUDA(v, cudaGetLastError());
     return GVDB2_OK;
 }
