@@ -64,6 +64,8 @@ def parse():
                          "differentiable splat, adjoint vs forward; sparse67m: the large sparse scene "
                          "(67,108,864-point Gaussian mixture, 32^3 bricks, forward + adjoint)")
     ap.add_argument("--points", type=int, default=0, help="sparse67m: fewer points (smaller cases for profiling)")
+    ap.add_argument("--clouds", type=int, default=0, help="batched: the first K clouds only (smaller cases for "
+                                                             "profiling)")
     return ap.parse_args()
 
 
@@ -857,31 +859,45 @@ def extra_ref_kernels(steps=3, warmup=1):
 BATCH_SPACE_LOG2 = 10
 
 
-def batched_step(v, K, n, chans_fwd, grad_chan, go):
+BATCH_STAGES = ("rebuild", "atlas", "scatter", "apron", "gather", "gather_adjoint", "scatter_adjoint")
+
+
+def batched_step(v, K, n, chans_fwd, grad_chan, go, mark=None):
     """Forward (rebuild, splat, apron, gather) and adjoint (gather adjoint into
-    the gradient channel, then the splat adjoint) over the volume's points."""
+    the gradient channel, then the splat adjoint) over the volume's points.
+    `mark`, if given, is called after each of BATCH_STAGES (event records)."""
+    mark = mark or (lambda: None)
     v.RequestFullRebuild(True)
     v.RebuildTopology(n, RADIUS)
+    mark()
     v.UpdateAtlas()
+    mark()
     v.ScatterKernel(K, n, chans_fwd, weight=1.0)
+    mark()
     for c in chans_fwd:  # the aprons of the scattered channels
         v.UpdateApron(c, 0.0)
+    mark()
     out = v.GatherKernel(K, n, chans_fwd, out=go[0])
+    mark()
     v.GatherDensityBackward(K, n, chans_fwd, out, grad_chans=[grad_chan], grad_pos=go[1])
+    mark()
     v.ScatterDensityBackward(K, n, [grad_chan], weight=1.0, grad_pos=go[2], grad_weight=go[3], grad_attr=go[4])
+    mark()
 
 
-def measure_batched(steps, warmup, env=None):
+def measure_batched(steps, warmup, env=None, nclouds=0):
     """The 64 clouds in one batched pass against a per-cloud loop.  Under
     torchrun the clouds are spread over the ranks (LPT by size, no data-path
     collective); each rank batches its own share and the time is the max
-    over the ranks."""
+    over the ranks.  nclouds > 0 keeps the first nclouds clouds only."""
     import torch
     import gvdb2
     import gvdb2.workloads as wl
     from gvdb2 import shard
     env = env or shard.RankEnv()
     all_clouds, _ = wl.batched_clouds()
+    if nclouds > 0:
+        all_clouds = all_clouds[:nclouds]
     mine = shard.lpt_partition([len(c) for c in all_clouds], env.world)[env.rank]
     clouds = [all_clouds[i] for i in mine]
     dev = [torch.from_numpy(c).cuda() for c in clouds]
@@ -938,6 +954,20 @@ def measure_batched(steps, warmup, env=None):
     ms_b = timed(step_batched, steps)
     ms_l = timed(step_loop, max(1, steps))
     clk = clocks.stop()
+    # one more batched pass with an event after each stage (on the volume's
+    # stream, which is torch's current one here)
+    ev = [torch.cuda.Event(enable_timing=True)]
+    ev[0].record()
+
+    def mark():
+        ev.append(torch.cuda.Event(enable_timing=True))
+        ev[-1].record()
+    vb.BatchPoints(dev, BATCH_SPACE_LOG2)
+    mark()
+    batched_step(vb, K, total, [0], 1, gob, mark)
+    torch.cuda.synchronize()
+    stages = {"pack": ev[0].elapsed_time(ev[1])}
+    stages.update({name: ev[i + 1].elapsed_time(ev[i + 2]) for i, name in enumerate(BATCH_STAGES)})
     # identical results, cloud by cloud, with stable binning on both sides
     # (each cell then adds its points in the same order)
     vb.SetDeterministic(True)
@@ -948,11 +978,13 @@ def measure_batched(steps, warmup, env=None):
     same = all(bool(torch.equal(gob[0][first[c]:first[c + 1]], gol[c][0])) and
                bool(torch.equal(gob[2][first[c]:first[c + 1]], gol[c][2])) for c in range(len(clouds)))
     same = shard.max_over_ranks(0.0 if same else 1.0, device=f"cuda:{env.local}") == 0.0
+    bricks = int(vb.info().used_leaves)
     del vb, vl
     return {"workload": f"batched: {len(all_clouds)} Gaussian clouds, {job_total} points, sizes log-uniform in "
                         "[1e4, 2e6], each in its own 1024^3 space; cubic B-spline r=2, density; forward + adjoint",
             "value": job_total / (ms_b / 1e3), "unit": "points/s", "ms_per_step": ms_b,
             "per_cloud_loop": {"value": job_total / (ms_l / 1e3), "ms_per_step": ms_l},
+            "batched_stage_ms": stages, "bricks": bricks,
             "speedup_vs_loop": ms_l / ms_b, "identical_to_loop": same, "n_gpus": env.world,
             "scaling": "strong", "parallelism": f"clouds over {env.world} ranks (LPT by size)", "steps": steps,
             "clocks": clk}
@@ -967,7 +999,7 @@ def run_batched(a):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    res = measure_batched(a.steps, a.warmup, env)
+    res = measure_batched(a.steps, a.warmup, env, a.clouds)
     if env.rank == 0:
         line = {"metric": METRIC}
         line.update(res)
