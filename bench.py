@@ -134,12 +134,17 @@ def workload_points(a):
     return pos, vel, desc
 
 
+L2_BYTES = 126 * 1000 * 1000  # B200 L2
+
+
 def static_config(a, n, ws):
     """The workload as both arms name it (no measured quantities)."""
     desc = WORKLOADS[a.workload]["desc"] if not a.sites else f"{a.workload} sites {a.sites}"
     return {"workload": desc, "points_per_gpu": int(n),
             "rebuild": "incremental state machine" if a.incremental else "full rebuild every step",
-            "l2": "inputs larger than L2 (positions + velocities alone exceed 126 MB)",
+            "l2": (f"inputs larger than L2 (positions, velocities and gathered velocities: {36 * n / 1e6:.0f} MB "
+                   "per step, atlas not counted)" if 36 * n > L2_BYTES else
+                   "inputs smaller than L2 (a reduced case for profiling; not a benchmark line)"),
             "parallelism": f"replicas x{ws}"}
 
 

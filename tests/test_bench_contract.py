@@ -37,6 +37,7 @@ def test_reference_arm_line():
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
     assert d["config"]["points_per_gpu"] == 32 * 16 * 32
+    assert d["config"]["l2"].startswith("inputs smaller than L2")  # 384 KB of positions and velocities
 
 
 def test_reference_arm_other_ranks_silent():
